@@ -1,0 +1,372 @@
+"""Benchmark: query points/sec of the point-by-polygon join on B200.
+
+Default workload (one JSON line on rank 0):
+  zipf_join -- 50M FP64 points x 1M footprint polygons, cluster centres
+  Zipf(s=1.1)-weighted over 1024 sites in [0,1000]^2 (the learned-index
+  scale-up case), predicate 'within'.  A step = one join of all points
+  against the resident polygon index (built once before timing, as an
+  ``sindex`` is reused across queries).  Inputs (800 MB of points) exceed the
+  126 MB L2, so no explicit flush is needed between steps.
+
+Arms:
+  --impl ours (default)  the CUDA path through the C-ABI (libvsjoin.so)
+  --impl reference       the reference CPU path of this join, timed on the
+                         host cores: the reference needs Shapely/GEOS, which
+                         cannot be installed here, so the exact CPU oracle
+                         (oracle/, C + OpenMP, kind "port") stands in for it.
+
+Multi-GPU (torchrun, one rank per GPU): the join shards by query points; each
+rank joins its own 50M-point batch against its replica of the index (weak
+scaling, no collective on the data path).  Time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(name: str, rank: int = 0, scale: float = 1.0):
+    from vibespatial_b200.testing import synthetic as syn
+
+    if name == "zipf":
+        return syn.zipf_join(seed=3 + 1000 * rank, n_points=int(50_000_000 * scale), n_polys=int(1_000_000 * scale))
+    if name == "utm":
+        return syn.utm_join(seed=1 + 1000 * rank, n_points=int(10_000_000 * scale), n_polys=int(100_000 * scale))
+    if name == "star":
+        return syn.star_join(seed=0 + 1000 * rank, n_points=int(100_000 * scale), n_polys=int(1_000 * scale))
+    if name == "degenerate":
+        return syn.degenerate_join(seed=5 + 1000 * rank, n_points=int(20_000_000 * scale),
+                                   n_polys=int(200_000 * scale))
+    raise ValueError(name)
+
+
+WORKLOAD_DESC = {
+    "zipf": "zipf_join: 50M FP64 points x 1M footprints, Zipf(s=1.1) clusters over 1024 sites in [0,1000]^2",
+    "utm": "utm_join: 10M FP64 points (64-component GMM) x 100k footprints, UTM-like frame",
+    "star": "star_join: 100k points x 1k star polygons in [0,1000]^2",
+    "degenerate": "degenerate_join: 20M points x 200k polygons with holes/multiparts, on-edge and 1-ulp points",
+}
+
+
+def algorithmic_bytes(w, n_pairs: int) -> int:
+    """Bytes the join must move at least once: points, polygon SoA, pair output."""
+    p = w.polys
+    return int(16 * w.n_points + 16 * p.n_coords + 4 * (len(p.ring_off) + len(p.part_off) + len(p.geom_off))
+               + 8 * n_pairs)
+
+
+def cpu_sample_rate(w, predicate: str, threads: int, target_s: float = 10.0):
+    """Oracle (all host threads) on a bounded prefix of the same points; points/sec."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+    n = min(w.n_points, 200_000)
+    t0 = time.perf_counter()
+    O.join(w.px[:n], w.py[:n], None, P, predicate, threads)
+    dt = time.perf_counter() - t0
+    # grow the sample towards ~target_s of work (bounded by the workload)
+    n2 = int(min(w.n_points, max(n, n * target_s / max(dt, 1e-3) * 0.5)))
+    t0 = time.perf_counter()
+    O.join(w.px[:n2], w.py[:n2], None, P, predicate, threads)
+    dt2 = time.perf_counter() - t0
+    return n2 / dt2, n2, dt2
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    w = make_workload(args.workload, 0, args.scale)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+    n = min(w.n_points, args.ref_sample)
+    for _ in range(args.warmup):
+        O.join(w.px[:n], w.py[:n], None, P, args.predicate, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.join(w.px[:n], w.py[:n], None, P, args.predicate, threads)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = n * len(times) / tot
+    line = {
+        "impl": "reference", "metric": "query points/sec", "value": value, "unit": "points/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "predicate": args.predicate,
+                   "sample_points": n, "n_polygons": len(w.polys)},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
+                         "sample": f"first {n} of {w.n_points} points vs all {len(w.polys)} polygons, "
+                                   "exact CPU oracle (C + OpenMP): Shapely/GEOS is not installable here"},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from vibespatial_b200 import _abi
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    w = make_workload(args.workload, rank, args.scale)
+    N = w.n_points
+    ctx = _abi.Context(dev)
+    stream = ctx.torch_stream
+    pol = w.polys
+    d_poly = {k: torch.from_numpy(np.ascontiguousarray(getattr(pol, k))).to(dev)
+              for k in ("x", "y", "ring_off", "part_off", "geom_off")}
+    P = _abi.make_polygons(d_poly["x"], d_poly["y"], d_poly["ring_off"], d_poly["part_off"], d_poly["geom_off"])
+    method = _abi.METHOD_LEARNED if args.method == "learned" else _abi.METHOD_RTREE
+    pred = {"within": _abi.PRED_WITHIN, "intersects": _abi.PRED_INTERSECTS}[args.predicate]
+    t0 = time.perf_counter()
+    index = _abi.DeviceIndex(ctx, P, learned=(method == _abi.METHOD_LEARNED))
+    build_wall = time.perf_counter() - t0
+    info = index.info()
+    del d_poly
+    dx = torch.from_numpy(w.px).to(dev)
+    dy = torch.from_numpy(w.py).to(dev)
+    pts = _abi.make_points(dx, dy)
+    # size the pair buffers once (exact count from a first join)
+    cap = max(1024, N)
+    left = torch.empty(cap, dtype=torch.int32, device=dev)
+    right = torch.empty(cap, dtype=torch.int32, device=dev)
+    try:
+        n_pairs, stats = index.join_into(pts, pred, method, left, right)
+    except _abi.CapacityError as e:
+        cap = e.required
+        left = torch.empty(cap, dtype=torch.int32, device=dev)
+        right = torch.empty(cap, dtype=torch.int32, device=dev)
+        n_pairs, stats = index.join_into(pts, pred, method, left, right)
+    # plain R-tree on the same GPU, for the learned-vs-plain ratio
+    plain = None
+    if method == _abi.METHOD_LEARNED:
+        n_plain, st_plain = index.join_into(pts, pred, _abi.METHOD_RTREE, left, right)
+        assert n_plain == n_pairs, (n_plain, n_pairs)
+
+    for _ in range(args.warmup):
+        index.join_into(pts, pred, method, left, right)
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms = []
+    with ClockSampler(dev) as clk:
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            n_k, st = index.join_into(pts, pred, method, left, right)
+            ev[k][1].record(stream)
+            kernel_ms.append(st["kernel_ms"])
+            assert n_k == n_pairs
+        torch.cuda.synchronize()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        # plain method timing (same GPU, same buffers) after the timed region
+        if method == _abi.METHOD_LEARNED:
+            pm = []
+            for _ in range(max(3, args.steps // 2)):
+                _, stp = index.join_into(pts, pred, _abi.METHOD_RTREE, left, right)
+                pm.append(stp["kernel_ms"])
+            plain = float(np.median(pm))
+        # e2e through the C-ABI with host buffers: H2D points, join, D2H pairs
+        hx = torch.from_numpy(w.px).pin_memory()
+        hy = torch.from_numpy(w.py).pin_memory()
+        hl = torch.empty(cap, dtype=torch.int32).pin_memory()
+        hr = torch.empty(cap, dtype=torch.int32).pin_memory()
+        ex = torch.empty_like(dx)
+        ey = torch.empty_like(dy)
+        epts = _abi.make_points(ex, ey)
+        e2e_ms = []
+        for k in range(max(3, args.steps)):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                a.record(stream)
+                ex.copy_(hx, non_blocking=True)
+                ey.copy_(hy, non_blocking=True)
+                n_e, _ = index.join_into(epts, pred, method, left, right)
+                hl[:n_e].copy_(left[:n_e], non_blocking=True)
+                hr[:n_e].copy_(right[:n_e], non_blocking=True)
+                b.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms.append(a.elapsed_time(b))
+    total_ms = float(sum(step_ms))
+    if dist:
+        t = torch.tensor([total_ms, float(np.median(e2e_ms))], device=dev, dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        total_ms, e2e_med = float(t[0]), float(t[1])
+    else:
+        e2e_med = float(np.median(e2e_ms))
+    value = world * N * args.steps / (total_ms / 1e3)
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    kmed = float(np.median(kernel_ms))
+    B = algorithmic_bytes(w, n_pairs)
+    achieved = B / (kmed / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / f"traffic_{args.workload}_{args.method}.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("traffic_bytes_per_launch")
+        except Exception:
+            traffic = None
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        threads = os.cpu_count() or 1
+        rate, n_s, dt = cpu_sample_rate(w, args.predicate, threads, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "points/s", "cores": threads, "kind": "port",
+               "sample": f"first {n_s} of {N} points vs all {len(w.polys)} polygons ({dt:.1f} s), exact CPU "
+                         "oracle (C + OpenMP); Shapely/GEOS is not installable here"}
+    line = {
+        "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "predicate": args.predicate, "method": args.method,
+                   "n_points_per_gpu": N, "n_polygons": len(w.polys), "n_pairs": n_pairs,
+                   "parallelism": f"points sharded over {world} GPU(s), index replicated",
+                   "l2": "inputs (800 MB of points) larger than L2; no flush",
+                   "index_build_ms": info["build_ms"], "index_build_wall_s": build_wall,
+                   "index_device_bytes": info["device_bytes"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel_ms": kmed,
+                     "algorithmic_bytes_per_launch": B},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
+                "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int(8 * n_pairs)},
+        "gpu_launches": args.steps * 1,
+        "join_stats": stats,
+    }
+    if plain is not None:
+        line["plain_rtree_ms"] = plain
+        line["learned_vs_plain"] = plain / kmed
+    line["clocks"] = clk.summary()
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOAD_DESC), default="zipf")
+    ap.add_argument("--predicate", choices=["within", "intersects"], default="within")
+    ap.add_argument("--method", choices=["learned", "rtree"], default="rtree")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--ref-sample", type=int, default=4_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                 device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

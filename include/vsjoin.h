@@ -1,0 +1,186 @@
+/*
+ * vsjoin: B200-native point-by-polygon spatial join, C-ABI.
+ *
+ * Every pointer argument named d_* is a DEVICE pointer on the context's
+ * device; h_* are host pointers.  Polygonal inputs use the GeoArrow-style
+ * MultiPolygon SoA that the reference's OwnedGeometryArray uses for its
+ * polygon/multipolygon families (src/vibespatial/geometry/buffers.py:140-249):
+ * geom_off (row -> part), part_off (part -> ring), ring_off (ring -> coord),
+ * x[] and y[] coordinates.  A Polygon row is a MultiPolygon row with one part.
+ *
+ * Status codes: every entry point returns VS_OK or one of the VS_E_* codes
+ * and leaves a message in vs_last_error() (thread-local).  This mirrors the
+ * reference's error classes: ValueError for bad arguments (VS_E_ARG),
+ * CandidateRelationCapacityError for an undersized pair buffer
+ * (VS_E_CAPACITY, src/vibespatial/spatial/query_types.py:41-93) and
+ * RuntimeError for driver failures (VS_E_CUDA,
+ * src/vibespatial/cuda/_runtime.py:95-108).
+ */
+#ifndef VSJOIN_H
+#define VSJOIN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VSJOIN_ABI_VERSION 1
+
+enum vs_status {
+    VS_OK = 0,
+    VS_E_ARG = 1,      /* invalid argument */
+    VS_E_OOM = 2,      /* device allocation failed */
+    VS_E_CAPACITY = 3, /* pair buffer too small; *n_pairs holds the required size */
+    VS_E_CUDA = 4,     /* CUDA runtime error */
+    VS_E_TIMEOUT = 5,  /* a bounded device wait gave up */
+    VS_E_STATE = 6     /* inconsistent handle / device-side consistency check failed */
+};
+
+/* Predicates, stated with the POINT as the query (left) side and the polygon
+ * as the tree (right) side.  Location -> predicate mapping follows
+ * src/vibespatial/predicates/point_relations.py:100-130 (point_on_left):
+ *   WITHIN      interior                 (sjoin predicate='within')
+ *   INTERSECTS  interior or boundary     (predicate='intersects')
+ *   COVERED_BY  interior or boundary
+ *   TOUCHES     boundary
+ *   BBOX        bounding-box candidates only (predicate=None)
+ * Polygon-on-the-left predicates (contains, covers, contains_properly) are the
+ * mirror images: the host swaps sides (src/vibespatial/api/tools/sjoin.py:1049-1082). */
+enum vs_predicate {
+    VS_PRED_BBOX = 0,
+    VS_PRED_INTERSECTS = 1,
+    VS_PRED_WITHIN = 2,
+    VS_PRED_COVERED_BY = 3,
+    VS_PRED_TOUCHES = 4
+};
+
+/* Query methods. */
+enum vs_method {
+    VS_METHOD_RTREE = 0,   /* plain: packed Hilbert R-tree traversal, FP64 filter, exact refine */
+    VS_METHOD_LEARNED = 1, /* learned cell index + FP32 tile-relative filter, exact fallback */
+    VS_METHOD_BRUTE = 2    /* every point against every polygon box (small joins, testing) */
+};
+
+/* Join flags. */
+#define VS_JOIN_SORT 1u /* return pairs sorted by (left, right) */
+
+typedef struct vs_context vs_context;
+typedef struct vs_index vs_index;
+
+typedef struct vs_polygons {
+    const double* d_x;
+    const double* d_y;
+    const int32_t* d_ring_off; /* n_rings + 1 */
+    const int32_t* d_part_off; /* n_parts + 1 */
+    const int32_t* d_geom_off; /* n_geoms + 1 */
+    const uint8_t* d_valid;    /* n_geoms, nullable: 0 = null row (never matches) */
+    int64_t n_coords;
+    int32_t n_rings;
+    int32_t n_parts;
+    int32_t n_geoms;
+} vs_polygons;
+
+typedef struct vs_points {
+    const double* d_x;
+    const double* d_y;
+    const uint8_t* d_valid; /* nullable: 0 = null row; NaN coordinates = empty point */
+    int64_t n;
+} vs_points;
+
+typedef struct vs_index_options {
+    int32_t method_mask; /* bit 0: R-tree (always built), bit 1: learned cell index */
+    int32_t cell_level;  /* learned index grid level (0 = choose automatically) */
+    int32_t rmi_leaves;  /* learned index leaf models (0 = 4096) */
+    int32_t rmi_train_steps; /* 0 = default */
+} vs_index_options;
+
+typedef struct vs_join_stats {
+    int64_t candidates;       /* point/polygon pairs that passed the box filter */
+    int64_t exact_fallbacks;  /* orientation signs that needed the exact expansion stage */
+    int64_t fp32_edges;       /* edges decided by the FP32 tile-relative filter */
+    int64_t fp64_edges;       /* edges re-decided in FP64 because the FP32 bound was inconclusive */
+    int64_t rmi_fallbacks;    /* learned-index lookups that left their error window (must be 0) */
+    float kernel_ms;          /* device time of the join kernels */
+    float sort_ms;            /* device time of the optional pair sort */
+} vs_join_stats;
+
+typedef struct vs_index_info {
+    int32_t n_geoms;
+    int32_t fanout;
+    int32_t levels;
+    int32_t cell_level;
+    int64_t n_cells;          /* non-empty learned-index cells */
+    int64_t n_cell_entries;   /* (cell, polygon) entries */
+    int64_t device_bytes;     /* bytes owned by the index */
+    float build_ms;
+    float rmi_train_ms;
+    float rmi_mean_window;    /* mean learned-index search window (entries) */
+    int32_t rmi_max_window;
+} vs_index_info;
+
+/* ---------------------------------------------------------------------- */
+
+/* ABI version (VSJOIN_ABI_VERSION). */
+int vs_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* vs_last_error(void);
+
+/* A context = one device + one stream + a scratch arena.  `stream` is a
+ * cudaStream_t (NULL: the context creates its own).  Not thread-safe: callers
+ * serialise use of one context.  Replaces the reference's per-process runtime
+ * (src/vibespatial/cuda/_runtime.py:1821-1852, launches on CuPy's stream). */
+int vs_context_create(int device, void* stream, vs_context** out);
+int vs_context_destroy(vs_context* ctx);
+int vs_context_synchronize(vs_context* ctx);
+
+/* Build the spatial index of a polygon/multipolygon array (the tree side).
+ * Replaces build_flat_spatial_index (src/vibespatial/spatial/indexing.py:1357)
+ * and its Morton-key + CCCL sort_pairs steps (:1265-1322).  The index copies
+ * what it needs; the input buffers may be freed after the call returns. */
+int vs_index_build(vs_context* ctx, const vs_polygons* polys, const vs_index_options* opts,
+                   vs_index** out);
+int vs_index_info_get(const vs_index* index, vs_index_info* info);
+int vs_index_free(vs_index* index);
+
+/* Join points (query side) against the index (tree side).  Replaces
+ * query_spatial_index (src/vibespatial/spatial/query.py:247) for point
+ * queries: candidate generation (spatial_index_device_query,
+ * src/vibespatial/spatial/spatial_index_device.py:228) + exact refine
+ * (_filter_predicate_pairs_owned, src/vibespatial/spatial/query_utils.py:578).
+ * Writes (left = point row, right = polygon row) int32 pairs to d_left /
+ * d_right (capacity entries each).  If more pairs exist than `capacity`,
+ * returns VS_E_CAPACITY with *n_pairs = the required size and the buffers
+ * partially written.  Blocks until the pairs are resident. */
+int vs_join(vs_context* ctx, const vs_index* index, const vs_points* pts, int32_t predicate,
+            int32_t method, uint32_t flags, int32_t* d_left, int32_t* d_right, int64_t capacity,
+            int64_t* n_pairs, vs_join_stats* stats);
+
+/* Element-wise location of point row i in polygon row i (aligned arrays):
+ * d_out[i] = 0 outside / 1 boundary / 2 interior / 255 null-or-empty.
+ * Replaces the point-region fast path of GeometryArray.within/contains
+ * (src/vibespatial/predicates/binary.py:1469-1692). */
+int vs_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys,
+                      uint8_t* d_out);
+
+/* Sort int32 pairs in place by (left, right) with the in-house radix sort.
+ * Mirrors the lexsort the reference applies to host-path pairs
+ * (src/vibespatial/api/tools/sjoin.py:1079-1082). */
+int vs_sort_pairs(vs_context* ctx, int32_t* d_left, int32_t* d_right, int64_t n);
+
+/* Sort (u64 key, u32 value) pairs in place by key (in-house LSD radix sort;
+ * replaces CCCL sort_pairs, src/vibespatial/cuda/cccl_primitives.py:1054). */
+int vs_radix_sort_pairs(vs_context* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n,
+                        int32_t key_bits);
+
+/* 64-bit Hilbert keys of (x, y) on the 2^32 grid spanning the given frame
+ * (replaces morton_keys_from_bounds, src/vibespatial/spatial/indexing_kernels.py:20-49). */
+int vs_hilbert_keys(vs_context* ctx, const double* d_x, const double* d_y, int64_t n,
+                    double minx, double miny, double maxx, double maxy, uint64_t* d_keys);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VSJOIN_H */

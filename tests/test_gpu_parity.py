@@ -1,0 +1,195 @@
+"""CUDA join parity against the exact CPU oracle (bit-exact pair sets).
+
+Every test calls through the C-ABI (libvsjoin.so via ctypes) and compares
+with oracle/ on the same seeded inputs.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import _shapes as S
+from _helpers import PRED_CODES, assert_same_pairs, gpu_join, oracle_polys, to_dev, upload_points, upload_polys
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+METHODS = {"rtree": 0, "brute": 2}
+
+
+def _check(vsabi, ctx, oracle, w, predicate, method=0, pvalid=None):
+    P = oracle_polys(oracle, w.polys)
+    el, er = oracle.join(w.px, w.py, pvalid, P, predicate)
+    gl, gr, stats = gpu_join(vsabi, ctx, w.px, w.py, w.polys, predicate, method, pvalid)
+    assert_same_pairs(gl, gr, el, er)
+    return stats
+
+
+@pytest.mark.parametrize("predicate", ["within", "intersects", "covered_by", "touches", None])
+@pytest.mark.parametrize("method", ["rtree", "brute"])
+def test_star_join_all_predicates(vsabi, ctx, oracle, predicate, method):
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.star_join(seed=0)  # 100k points x 1k star polygons
+    _check(vsabi, ctx, oracle, w, predicate, METHODS[method])
+
+
+@pytest.mark.parametrize("predicate", ["within", "intersects"])
+def test_utm_join_reduced(vsabi, ctx, oracle, predicate):
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.utm_join(seed=1, n_points=1_000_000, n_polys=100_000)
+    _check(vsabi, ctx, oracle, w, predicate)
+
+
+def test_zipf_join_reduced(vsabi, ctx, oracle):
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.zipf_join(seed=3, n_points=2_000_000, n_polys=100_000)
+    _check(vsabi, ctx, oracle, w, "within")
+
+
+@pytest.mark.parametrize("predicate", ["within", "intersects", "touches"])
+def test_degenerate_join_reduced(vsabi, ctx, oracle, predicate):
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.degenerate_join(seed=5, n_points=400_000, n_polys=4_000)
+    stats = _check(vsabi, ctx, oracle, w, predicate)
+    if predicate != "within":
+        assert stats["exact_fallbacks"] > 0  # on-edge points must reach the exact stage
+
+
+@pytest.mark.parametrize("name", sorted(S.KNOWN_COVERS))
+def test_known_cases_aligned(vsabi, ctx, oracle, name):
+    polys, pts, expected = S.KNOWN_COVERS[name]
+    P = S.soa(polys)
+    px, py, pv = S.points(pts)
+    exp = oracle.locate_aligned(px, py, pv, oracle.Polygons(P.x, P.y, P.ring_off, P.part_off, P.geom_off, P.valid))
+    dpts, k1 = upload_points(vsabi, px, py, pv)
+    dpol, k2 = upload_polys(vsabi, P)
+    import torch
+
+    out = torch.empty(len(px), dtype=torch.uint8, device="cuda")
+    vsabi.locate_aligned(ctx, dpts, dpol, out)
+    np.testing.assert_array_equal(out.cpu().numpy(), exp)
+
+
+def test_known_cases_join(vsabi, ctx, oracle):
+    tree, pts, (el, er) = S.SPATIAL_QUERY_CASE
+    P = S.soa(tree)
+    px, py, _ = S.points(pts)
+    gl, gr, _ = gpu_join(vsabi, ctx, px, py, P, "intersects")
+    assert gl.tolist() == el and gr.tolist() == er
+
+
+def test_nybb_and_natural_earth(vsabi, ctx, oracle):
+    from test_oracle_golden import nybb_points
+
+    exp = json.loads((GOLDEN / "expected.json").read_text())
+    d = dict(np.load(GOLDEN / "nybb.npz"))
+    P, px, py = nybb_points(d, oracle)
+    poly = S.SoA(d["x"], d["y"], d["ring_off"], d["part_off"], d["geom_off"], np.ones(len(d["geom_off"]) - 1))
+    gl, gr, _ = gpu_join(vsabi, ctx, px, py, poly, "intersects")
+    assert len(gl) == exp["nybb_inner_intersects_shape"]["value"][0]
+    el, er = oracle.join(px, py, None, P, "intersects")
+    assert_same_pairs(gl, gr, el, er)
+    w = dict(np.load(GOLDEN / "naturalearth_lowres.npz"))
+    c = dict(np.load(GOLDEN / "naturalearth_cities.npz"))
+    wp = S.SoA(w["x"], w["y"], w["ring_off"], w["part_off"], w["geom_off"], np.ones(len(w["geom_off"]) - 1))
+    gl, gr, _ = gpu_join(vsabi, ctx, c["x"], c["y"], wp, "intersects")
+    assert len(gl) == exp["cities_countries_inner_intersects_shape"]["value"][0]
+
+
+def test_edge_cases(vsabi, ctx, oracle):
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.star_join(seed=4, n_points=5000, n_polys=50)
+    # empty point set
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px[:0], w.py[:0], w.polys, "within")
+    assert len(gl) == 0
+    # empty polygon set
+    empty = S.soa([])
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, empty, "within")
+    assert len(gl) == 0
+    # one polygon (the root is the only item)
+    one = S.soa([S.box(100, 100, 900, 900)])
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, one, "intersects")
+    el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, one), "intersects")
+    assert_same_pairs(gl, gr, el, er)
+    # null / NaN points and null / empty polygons never match
+    px, py = w.px.copy(), w.py.copy()
+    pv = np.ones(len(px), np.uint8)
+    pv[::7] = 0
+    px[::11] = np.nan
+    gl, gr, _ = gpu_join(vsabi, ctx, px, py, w.polys, "intersects", pvalid=pv)
+    el, er = oracle.join(px, py, pv, oracle_polys(oracle, w.polys), "intersects")
+    assert_same_pairs(gl, gr, el, er)
+    mixed = S.soa([None, [], S.box(0, 0, 500, 500), None, S.box(400, 400, 1000, 1000)])
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, mixed, "within")
+    el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, mixed), "within")
+    assert_same_pairs(gl, gr, el, er)
+    assert set(np.unique(gr)) <= {2, 4}
+
+
+def test_capacity_error_reports_required_size(vsabi, ctx, oracle):
+    import torch
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.star_join(seed=0)
+    el, _ = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), "within")
+    dpts, k1 = upload_points(vsabi, w.px, w.py)
+    dpol, k2 = upload_polys(vsabi, w.polys)
+    index = vsabi.DeviceIndex(ctx, dpol)
+    small = torch.empty(100, dtype=torch.int32, device="cuda")
+    small2 = torch.empty(100, dtype=torch.int32, device="cuda")
+    with pytest.raises(vsabi.CapacityError) as ei:
+        index.join_into(dpts, PRED_CODES["within"], 0, small, small2)
+    assert ei.value.required == len(el)
+    # bad arguments are rejected before any launch
+    with pytest.raises(ValueError):
+        index.join_into(dpts, 99, 0, small, small2)
+
+
+def test_radix_sort_and_hilbert_keys(vsabi, ctx):
+    import torch
+
+    rng = np.random.default_rng(9)
+    for n, bits in [(1, 64), (4095, 64), (4097, 24), (300_000, 64), (1_000_003, 40)]:
+        keys = rng.integers(0, 2**63, n, dtype=np.int64).view(np.uint64) >> np.uint64(64 - bits)
+        keys[::3] = keys[0]  # duplicates: stability check
+        vals = np.arange(n, dtype=np.uint32)
+        dk = torch.from_numpy(keys.view(np.int64)).cuda()
+        dv = torch.from_numpy(vals.view(np.int32)).cuda()
+        vsabi.radix_sort_pairs(ctx, dk, dv, bits)
+        order = np.argsort(keys, kind="stable")
+        np.testing.assert_array_equal(dk.cpu().numpy().view(np.uint64), keys[order])
+        np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[order])
+    x = rng.uniform(0, 10, 1000)
+    y = rng.uniform(0, 10, 1000)
+    out = torch.empty(1000, dtype=torch.int64, device="cuda")
+    vsabi.hilbert_keys(ctx, to_dev(x), to_dev(y), (0, 0, 10, 10), out)
+    got = out.cpu().numpy().view(np.uint64)
+    sc = 4294967295.0 / 10
+    exp = [vsabi.hilbert_key_host(min(int(a * sc), 0xFFFFFFFF), min(int(b * sc), 0xFFFFFFFF)) for a, b in zip(x, y)]
+    np.testing.assert_array_equal(got, np.array(exp, dtype=np.uint64))
+
+
+def test_pair_sort(vsabi, ctx):
+    import torch
+
+    rng = np.random.default_rng(1)
+    l = rng.integers(0, 1 << 30, 200_000).astype(np.int32)
+    r = rng.integers(0, 1 << 30, 200_000).astype(np.int32)
+    dl, dr = torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()
+    vsabi.sort_pairs(ctx, dl, dr)
+    o = np.lexsort((r, l))
+    np.testing.assert_array_equal(dl.cpu().numpy(), l[o])
+    np.testing.assert_array_equal(dr.cpu().numpy(), r[o])
+
+
+def test_full_size_utm_join(vsabi, ctx, oracle):
+    """BASELINE configs[1] at full size (10M x 100k), within: whole pair set equal."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.utm_join(seed=1)
+    _check(vsabi, ctx, oracle, w, "within")

@@ -1,0 +1,305 @@
+"""ctypes binding of ``libvsjoin.so`` (the C-ABI declared in ``include/vsjoin.h``).
+
+Device buffers are torch CUDA tensors: torch provides device memory and the
+stream, the library does the work.  There is no CPU fallback: if the library
+or a GPU is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "_lib" / "libvsjoin.so"
+
+VS_OK, VS_E_ARG, VS_E_OOM, VS_E_CAPACITY, VS_E_CUDA, VS_E_TIMEOUT, VS_E_STATE = range(7)
+PRED_BBOX, PRED_INTERSECTS, PRED_WITHIN, PRED_COVERED_BY, PRED_TOUCHES = range(5)
+METHOD_RTREE, METHOD_LEARNED, METHOD_BRUTE = range(3)
+JOIN_SORT = 1
+
+# Every function the header declares; tests check the library exports them.
+EXPORTED = (
+    "vs_version", "vs_last_error", "vs_context_create", "vs_context_destroy",
+    "vs_context_synchronize", "vs_index_build", "vs_index_info_get", "vs_index_free",
+    "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
+)
+
+
+class VsError(RuntimeError):
+    """A C-ABI call returned a status other than VS_OK."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[vsjoin status {status}] {message}")
+        self.status = status
+
+
+class CapacityError(VsError, MemoryError):
+    """Pair buffer too small (mirrors the reference's CandidateRelationCapacityError)."""
+
+    def __init__(self, status, message, required):
+        super().__init__(status, message)
+        self.required = required
+
+
+class Polygons(ctypes.Structure):
+    _fields_ = [
+        ("d_x", ctypes.c_void_p), ("d_y", ctypes.c_void_p),
+        ("d_ring_off", ctypes.c_void_p), ("d_part_off", ctypes.c_void_p),
+        ("d_geom_off", ctypes.c_void_p), ("d_valid", ctypes.c_void_p),
+        ("n_coords", ctypes.c_int64), ("n_rings", ctypes.c_int32),
+        ("n_parts", ctypes.c_int32), ("n_geoms", ctypes.c_int32),
+    ]
+
+
+class Points(ctypes.Structure):
+    _fields_ = [("d_x", ctypes.c_void_p), ("d_y", ctypes.c_void_p),
+                ("d_valid", ctypes.c_void_p), ("n", ctypes.c_int64)]
+
+
+class IndexOptions(ctypes.Structure):
+    _fields_ = [("method_mask", ctypes.c_int32), ("cell_level", ctypes.c_int32),
+                ("rmi_leaves", ctypes.c_int32), ("rmi_train_steps", ctypes.c_int32)]
+
+
+class JoinStats(ctypes.Structure):
+    _fields_ = [
+        ("candidates", ctypes.c_int64), ("exact_fallbacks", ctypes.c_int64),
+        ("fp32_edges", ctypes.c_int64), ("fp64_edges", ctypes.c_int64),
+        ("rmi_fallbacks", ctypes.c_int64), ("kernel_ms", ctypes.c_float),
+        ("sort_ms", ctypes.c_float),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class IndexInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_geoms", ctypes.c_int32), ("fanout", ctypes.c_int32), ("levels", ctypes.c_int32),
+        ("cell_level", ctypes.c_int32), ("n_cells", ctypes.c_int64),
+        ("n_cell_entries", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+        ("build_ms", ctypes.c_float), ("rmi_train_ms", ctypes.c_float),
+        ("rmi_mean_window", ctypes.c_float), ("rmi_max_window", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: Path | str | None = None):
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is not None and path is None:
+            return _lib
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise RuntimeError(
+                f"{p} is missing: build it with `python -m vibespatial_b200._build` "
+                "(the join has no CPU fallback)"
+            )
+        L = ctypes.CDLL(str(p))
+        vp, i32, i64, u32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32
+        sig = {
+            "vs_version": (ctypes.c_int, []),
+            "vs_last_error": (ctypes.c_char_p, []),
+            "vs_context_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(vp)]),
+            "vs_context_destroy": (ctypes.c_int, [vp]),
+            "vs_context_synchronize": (ctypes.c_int, [vp]),
+            "vs_index_build": (ctypes.c_int, [vp, ctypes.POINTER(Polygons), ctypes.POINTER(IndexOptions), ctypes.POINTER(vp)]),
+            "vs_index_info_get": (ctypes.c_int, [vp, ctypes.POINTER(IndexInfo)]),
+            "vs_index_free": (ctypes.c_int, [vp]),
+            "vs_join": (ctypes.c_int, [vp, vp, ctypes.POINTER(Points), i32, i32, u32, vp, vp, i64,
+                                       ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
+            "vs_locate_aligned": (ctypes.c_int, [vp, ctypes.POINTER(Points), ctypes.POINTER(Polygons), vp]),
+            "vs_sort_pairs": (ctypes.c_int, [vp, vp, vp, i64]),
+            "vs_radix_sort_pairs": (ctypes.c_int, [vp, vp, vp, i64, i32]),
+            "vs_hilbert_keys": (ctypes.c_int, [vp, vp, vp, i64, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        if path is None:
+            _lib = L
+        return L
+
+
+def last_error() -> str:
+    msg = load().vs_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int, required: int | None = None) -> None:
+    if status == VS_OK:
+        return
+    msg = last_error()
+    if status == VS_E_CAPACITY:
+        raise CapacityError(status, msg, required)
+    if status == VS_E_ARG:
+        raise ValueError(f"[vsjoin] {msg}")
+    if status == VS_E_OOM:
+        raise MemoryError(f"[vsjoin] {msg}")
+    raise VsError(status, msg)
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else int(t.data_ptr())
+
+
+class Context:
+    """One device + one stream (torch's current stream by default)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("vsjoin needs a CUDA device; none is visible")
+        self.device = int(device)
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        self.torch_stream = stream
+        h = ctypes.c_void_p()
+        check(load().vs_context_create(self.device, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)))
+        self.handle = h
+
+    def synchronize(self):
+        check(load().vs_context_synchronize(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().vs_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    ctx = _default_ctx.get(device)
+    if ctx is None:
+        ctx = _default_ctx[device] = Context(device)
+    return ctx
+
+
+def make_points(x, y, valid=None) -> Points:
+    return Points(_ptr(x), _ptr(y), _ptr(valid), int(x.numel()))
+
+
+def make_polygons(x, y, ring_off, part_off, geom_off, valid=None) -> Polygons:
+    return Polygons(_ptr(x), _ptr(y), _ptr(ring_off), _ptr(part_off), _ptr(geom_off), _ptr(valid),
+                    int(x.numel()), int(ring_off.numel()) - 1, int(part_off.numel()) - 1,
+                    int(geom_off.numel()) - 1)
+
+
+class DeviceIndex:
+    """Owned handle of a built index (vs_index*)."""
+
+    def __init__(self, ctx: Context, polys: Polygons, *, learned: bool = False, cell_level: int = 0,
+                 rmi_leaves: int = 0, rmi_train_steps: int = 0):
+        self.ctx = ctx
+        opts = IndexOptions(1 | (2 if learned else 0), int(cell_level), int(rmi_leaves), int(rmi_train_steps))
+        h = ctypes.c_void_p()
+        check(load().vs_index_build(ctx.handle, ctypes.byref(polys), ctypes.byref(opts), ctypes.byref(h)))
+        self.handle = h
+        self.learned = learned
+
+    def info(self) -> dict:
+        inf = IndexInfo()
+        check(load().vs_index_info_get(self.handle, ctypes.byref(inf)))
+        return inf.as_dict()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().vs_index_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def join_into(self, pts: Points, predicate: int, method: int, left, right, *, sort: bool = False):
+        """One vs_join call into caller buffers; returns (n_pairs, stats dict).
+
+        Raises CapacityError (with .required) if the buffers are too small.
+        """
+        n = ctypes.c_int64(0)
+        st = JoinStats()
+        cap = 0 if left is None else int(left.numel())
+        status = load().vs_join(self.ctx.handle, self.handle, ctypes.byref(pts), int(predicate), int(method),
+                                JOIN_SORT if sort else 0, _ptr(left), _ptr(right), cap, ctypes.byref(n),
+                                ctypes.byref(st))
+        check(status, required=int(n.value))
+        return int(n.value), st.as_dict()
+
+    def join(self, pts: Points, predicate: int, method: int = METHOD_RTREE, *, sort: bool = True,
+             capacity: int | None = None):
+        """Join into freshly allocated int32 device tensors, growing them once if needed."""
+        import torch
+
+        dev = torch.device("cuda", self.ctx.device)
+        cap = int(capacity) if capacity is not None else max(1024, int(pts.n))
+        for _ in range(2):
+            left = torch.empty(cap, dtype=torch.int32, device=dev)
+            right = torch.empty(cap, dtype=torch.int32, device=dev)
+            try:
+                n, stats = self.join_into(pts, predicate, method, left, right, sort=sort)
+                return left[:n], right[:n], stats
+            except CapacityError as e:
+                cap = max(e.required, 1)
+        raise RuntimeError("pair buffer sizing did not converge")
+
+
+def locate_aligned(ctx: Context, pts: Points, polys: Polygons, out) -> None:
+    check(load().vs_locate_aligned(ctx.handle, ctypes.byref(pts), ctypes.byref(polys), _ptr(out)))
+
+
+def sort_pairs(ctx: Context, left, right) -> None:
+    check(load().vs_sort_pairs(ctx.handle, _ptr(left), _ptr(right), int(left.numel())))
+
+
+def radix_sort_pairs(ctx: Context, keys, vals, key_bits: int = 64) -> None:
+    check(load().vs_radix_sort_pairs(ctx.handle, _ptr(keys), _ptr(vals), int(keys.numel()), int(key_bits)))
+
+
+def hilbert_keys(ctx: Context, x, y, frame, out) -> None:
+    minx, miny, maxx, maxy = (float(v) for v in frame)
+    check(load().vs_hilbert_keys(ctx.handle, _ptr(x), _ptr(y), int(x.numel()), minx, miny, maxx, maxy, _ptr(out)))
+
+
+def hilbert_key_host(x: int, y: int, levels: int = 32) -> int:
+    """Host restatement of the device Hilbert key (used by tests)."""
+    d = 0
+    mask = 0xFFFFFFFF
+    for lv in range(31, 31 - levels, -1):
+        rx = (x >> lv) & 1
+        ry = (y >> lv) & 1
+        d = (d << 2) | ((3 * rx) ^ ry)
+        if ry == 0:
+            if rx == 1:
+                x = ~x & mask
+                y = ~y & mask
+            x, y = y, x
+    return d
+
+
+def _np_to_torch(a: np.ndarray, device):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device)

@@ -1,0 +1,367 @@
+// extern "C" entry points of libvsjoin.so (declared in include/vsjoin.h).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <new>
+
+#include "index.cuh"
+#include "join.cuh"
+#include "primitives.cuh"
+
+namespace vs {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+namespace {
+
+int use_device(int device) {
+    int cur = -1;
+    VS_CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != device) VS_CUDA_TRY(cudaSetDevice(device));
+    return VS_OK;
+}
+
+int check_polygons(const vs_polygons* p) {
+    if (!p) {
+        set_error("polygons is NULL");
+        return VS_E_ARG;
+    }
+    if (p->n_geoms < 0 || p->n_parts < 0 || p->n_rings < 0 || p->n_coords < 0) {
+        set_error("negative polygon sizes");
+        return VS_E_ARG;
+    }
+    if (p->n_coords > 0x7fffffffLL) {
+        set_error("more than 2^31-1 polygon coordinates (int32 offsets)");
+        return VS_E_ARG;
+    }
+    if (!p->d_geom_off || !p->d_part_off || !p->d_ring_off) {
+        set_error("polygon offset buffers must not be NULL");
+        return VS_E_ARG;
+    }
+    if (p->n_coords > 0 && (!p->d_x || !p->d_y)) {
+        set_error("polygon coordinate buffers must not be NULL");
+        return VS_E_ARG;
+    }
+    return VS_OK;
+}
+
+int check_points(const vs_points* p) {
+    if (!p) {
+        set_error("points is NULL");
+        return VS_E_ARG;
+    }
+    if (p->n < 0 || p->n > 0x7fffffffLL) {
+        set_error("point count %lld outside [0, 2^31-1]", (long long)p->n);
+        return VS_E_ARG;
+    }
+    if (p->n > 0 && (!p->d_x || !p->d_y)) {
+        set_error("point coordinate buffers must not be NULL");
+        return VS_E_ARG;
+    }
+    return VS_OK;
+}
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~EventPair() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    float ms() {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        return t;
+    }
+};
+
+}  // namespace
+}  // namespace vs
+
+using namespace vs;
+
+extern "C" {
+
+int vs_version(void) { return VSJOIN_ABI_VERSION; }
+
+const char* vs_last_error(void) { return g_err; }
+
+int vs_context_create(int device, void* stream, vs_context** out) {
+    if (!out) {
+        set_error("out is NULL");
+        return VS_E_ARG;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    VS_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) {
+        set_error("device %d out of range (%d devices)", device, ndev);
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(device));
+    vs_context* ctx = new (std::nothrow) vs_context{};
+    if (!ctx) {
+        set_error("host allocation failed");
+        return VS_E_OOM;
+    }
+    ctx->device = device;
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+        ctx->owns_stream = false;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete ctx;
+            set_error("cudaStreamCreate failed: %s", cudaGetErrorString(e));
+            return VS_E_CUDA;
+        }
+        ctx->owns_stream = true;
+    }
+    // Keep freed stream-ordered scratch in the pool between calls.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    if (cudaMallocHost((void**)&ctx->h_counter, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc((void**)&ctx->d_counters, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+        set_error("context buffer allocation failed");
+        if (ctx->h_counter) cudaFreeHost(ctx->h_counter);
+        if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return VS_E_OOM;
+    }
+    *out = ctx;
+    return VS_OK;
+}
+
+int vs_context_destroy(vs_context* ctx) {
+    if (!ctx) return VS_OK;
+    use_device(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_counters);
+    cudaFreeHost(ctx->h_counter);
+    if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return VS_OK;
+}
+
+int vs_context_synchronize(vs_context* ctx) {
+    if (!ctx) {
+        set_error("ctx is NULL");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    VS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return VS_OK;
+}
+
+int vs_index_build(vs_context* ctx, const vs_polygons* polys, const vs_index_options* opts, vs_index** out) {
+    if (!ctx || !out) {
+        set_error("ctx/out is NULL");
+        return VS_E_ARG;
+    }
+    *out = nullptr;
+    VS_TRY(check_polygons(polys));
+    VS_TRY(use_device(ctx->device));
+    vs_index* idx = new (std::nothrow) vs_index{};
+    if (!idx) {
+        set_error("host allocation failed");
+        return VS_E_OOM;
+    }
+    idx->device = ctx->device;
+    EventPair ev;
+    cudaEventRecord(ev.a, ctx->stream);
+    int st = build_rtree(ctx, polys, idx);
+    if (st == VS_OK && opts && (opts->method_mask & 2)) st = build_learned_index(ctx, idx, opts);
+    if (st != VS_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        free_index_memory(idx);
+        delete idx;
+        return st;
+    }
+    cudaEventRecord(ev.b, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        set_error("index build failed: %s", cudaGetErrorString(e));
+        free_index_memory(idx);
+        delete idx;
+        return VS_E_CUDA;
+    }
+    idx->build_ms = ev.ms();
+    *out = idx;
+    return VS_OK;
+}
+
+int vs_index_info_get(const vs_index* idx, vs_index_info* info) {
+    if (!idx || !info) {
+        set_error("index/info is NULL");
+        return VS_E_ARG;
+    }
+    memset(info, 0, sizeof(*info));
+    info->n_geoms = idx->n_geoms;
+    info->fanout = kFanout;
+    info->levels = idx->levels;
+    info->cell_level = idx->has_learned ? idx->learned.level : 0;
+    info->n_cells = idx->has_learned ? idx->learned.n_cells : 0;
+    info->n_cell_entries = idx->has_learned ? idx->learned.n_entries : 0;
+    info->device_bytes = idx->device_bytes;
+    info->build_ms = idx->build_ms;
+    info->rmi_train_ms = idx->learned.rmi_train_ms;
+    info->rmi_mean_window = idx->learned.mean_window;
+    info->rmi_max_window = idx->learned.max_window;
+    return VS_OK;
+}
+
+int vs_index_free(vs_index* idx) {
+    if (!idx) return VS_OK;
+    use_device(idx->device);
+    cudaDeviceSynchronize();
+    free_index_memory(idx);
+    delete idx;
+    return VS_OK;
+}
+
+int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t predicate, int32_t method,
+            uint32_t flags, int32_t* d_left, int32_t* d_right, int64_t capacity, int64_t* n_pairs,
+            vs_join_stats* stats) {
+    if (!ctx || !idx || !n_pairs) {
+        set_error("ctx/index/n_pairs is NULL");
+        return VS_E_ARG;
+    }
+    *n_pairs = 0;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    VS_TRY(check_points(pts));
+    if (capacity < 0 || (capacity > 0 && (!d_left || !d_right))) {
+        set_error("invalid pair buffers (capacity %lld)", (long long)capacity);
+        return VS_E_ARG;
+    }
+    if (idx->device != ctx->device) {
+        set_error("index lives on device %d, context on device %d", idx->device, ctx->device);
+        return VS_E_ARG;
+    }
+    int mask = 0;
+    VS_TRY(accept_mask_for(predicate, &mask));
+    if (method != VS_METHOD_RTREE && method != VS_METHOD_LEARNED && method != VS_METHOD_BRUTE) {
+        set_error("unknown method %d", method);
+        return VS_E_ARG;
+    }
+    if (method == VS_METHOD_LEARNED && !idx->has_learned) {
+        set_error("index was built without the learned cell index (method_mask bit 1)");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    if (pts->n == 0 || idx->n_geoms == 0 || !(idx->h_frame[0] <= idx->h_frame[2])) return VS_OK;
+    cudaStream_t s = ctx->stream;
+    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, 8 * sizeof(unsigned long long), s));
+    EventPair ev;
+    cudaEventRecord(ev.a, s);
+    if (method == VS_METHOD_LEARNED)
+        VS_TRY(launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity));
+    else
+        VS_TRY(launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, d_left, d_right, capacity));
+    cudaEventRecord(ev.b, s);
+    VS_CUDA_TRY(cudaMemcpyAsync(ctx->h_counter, ctx->d_counters, 8 * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    const unsigned long long* c = ctx->h_counter;
+    const int64_t n = (int64_t)c[0];
+    *n_pairs = n;
+    if (stats) {
+        stats->exact_fallbacks = (int64_t)c[1];
+        stats->fp32_edges = (int64_t)c[2];
+        stats->fp64_edges = (int64_t)c[3];
+        stats->candidates = (int64_t)c[5];
+        stats->rmi_fallbacks = (int64_t)c[6];
+        stats->kernel_ms = ev.ms();
+    }
+    if (c[4] != 0) {
+        set_error("device-side consistency check failed (flags 0x%llx)", (unsigned long long)c[4]);
+        return VS_E_STATE;
+    }
+    if (n > capacity) {
+        set_error("pair buffer holds %lld pairs, %lld required", (long long)capacity, (long long)n);
+        return VS_E_CAPACITY;
+    }
+    if (flags & VS_JOIN_SORT) {
+        EventPair es;
+        cudaEventRecord(es.a, s);
+        VS_TRY(sort_pairs(ctx, d_left, d_right, n, (uint64_t)pts->n, (uint64_t)idx->n_geoms));
+        cudaEventRecord(es.b, s);
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (stats) stats->sort_ms = es.ms();
+    }
+    return VS_OK;
+}
+
+int vs_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, uint8_t* d_out) {
+    if (!ctx) {
+        set_error("ctx is NULL");
+        return VS_E_ARG;
+    }
+    VS_TRY(check_points(pts));
+    VS_TRY(check_polygons(polys));
+    if ((int64_t)polys->n_geoms != pts->n) {
+        set_error("aligned arrays differ in length (%lld points, %d polygons)", (long long)pts->n, polys->n_geoms);
+        return VS_E_ARG;
+    }
+    if (pts->n > 0 && !d_out) {
+        set_error("d_out is NULL");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    VS_TRY(launch_locate_aligned(ctx, pts, polys, d_out));
+    VS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return VS_OK;
+}
+
+int vs_sort_pairs(vs_context* ctx, int32_t* d_left, int32_t* d_right, int64_t n) {
+    if (!ctx || n < 0 || (n > 0 && (!d_left || !d_right))) {
+        set_error("invalid arguments to vs_sort_pairs");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    VS_TRY(sort_pairs(ctx, d_left, d_right, n, 0xffffffffull, 0xffffffffull));
+    VS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return VS_OK;
+}
+
+int vs_radix_sort_pairs(vs_context* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits) {
+    if (!ctx || n < 0 || (n > 0 && (!d_keys || !d_vals))) {
+        set_error("invalid arguments to vs_radix_sort_pairs");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    VS_TRY(radix_sort_u64_u32(d_keys, d_vals, n, key_bits, ctx->stream));
+    VS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return VS_OK;
+}
+
+int vs_hilbert_keys(vs_context* ctx, const double* d_x, const double* d_y, int64_t n, double minx, double miny,
+                    double maxx, double maxy, uint64_t* d_keys) {
+    if (!ctx || n < 0 || (n > 0 && (!d_x || !d_y || !d_keys))) {
+        set_error("invalid arguments to vs_hilbert_keys");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    if (n == 0) return VS_OK;
+    VS_TRY(hilbert_point_keys(d_x, d_y, n, minx, miny, maxx, maxy, d_keys, ctx->stream));
+    VS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return VS_OK;
+}
+
+}  // extern "C"

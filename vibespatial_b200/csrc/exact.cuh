@@ -1,0 +1,212 @@
+// Exact point-in-polygon location on the device.
+//
+// Location codes follow the reference: 0 outside, 1 boundary, 2 interior
+// (src/vibespatial/predicates/point_relations_kernels.py:37-96).  The ring
+// walk keeps the reference's crossing rule, the half-open (ay > py) != (by > py)
+// test plus the closed-bbox boundary check
+// (src/vibespatial/cuda/device_functions/point_in_ring.py:148-188), but the
+// orientation sign is decided exactly: a Shewchuk stage-A filter on rounded
+// differences, then an exact expansion sum over the split differences
+// (Shewchuk 1997, sections 2.4-2.6).  The reference's vs_orient2d
+// (src/vibespatial/cuda/device_functions/orient2d.py:37-85) rounds ax-cx before
+// its error-free stage; this one does not.
+//
+// Every floating-point step that the exactness argument depends on uses the
+// explicit round-to-nearest intrinsics so that nvcc cannot contract it into
+// an FMA.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vs {
+
+enum : int { LOC_OUTSIDE = 0, LOC_BOUNDARY = 1, LOC_INTERIOR = 2 };
+
+__device__ __forceinline__ void two_sum(double a, double b, double& x, double& y) {
+    x = __dadd_rn(a, b);
+    const double bv = __dsub_rn(x, a);
+    const double av = __dsub_rn(x, bv);
+    const double br = __dsub_rn(b, bv);
+    const double ar = __dsub_rn(a, av);
+    y = __dadd_rn(ar, br);
+}
+
+__device__ __forceinline__ void two_diff(double a, double b, double& x, double& y) {
+    x = __dsub_rn(a, b);
+    const double bv = __dsub_rn(a, x);
+    const double av = __dadd_rn(x, bv);
+    const double br = __dsub_rn(bv, b);
+    const double ar = __dsub_rn(a, av);
+    y = __dadd_rn(ar, br);
+}
+
+__device__ __forceinline__ void two_product(double a, double b, double& x, double& y) {
+    x = __dmul_rn(a, b);
+    y = __fma_rn(a, b, -x);
+}
+
+// h := e + b with zero elimination; e is nonoverlapping, increasing magnitude.
+__device__ __forceinline__ int grow_expansion(int elen, const double* e, double b, double* h) {
+    double q = b, hh;
+    int n = 0;
+    for (int i = 0; i < elen; ++i) {
+        two_sum(q, e[i], q, hh);
+        if (hh != 0.0) h[n++] = hh;
+    }
+    if (q != 0.0 || n == 0) h[n++] = q;
+    return n;
+}
+
+// Exact sign of (ax-cx)(by-cy) - (ay-cy)(bx-cx): sixteen exact partial
+// products summed as a nonoverlapping expansion; the sign is the sign of the
+// largest component.  Kept out of line: it runs only when the filter fails.
+__device__ __noinline__ int orient2d_exact(double ax, double ay, double bx, double by,
+                                           double cx, double cy) {
+    double acx, acxt, bcx, bcxt, acy, acyt, bcy, bcyt;
+    two_diff(ax, cx, acx, acxt);
+    two_diff(bx, cx, bcx, bcxt);
+    two_diff(ay, cy, acy, acyt);
+    two_diff(by, cy, bcy, bcyt);
+    const double la[4] = {acx, acx, acxt, acxt};
+    const double lb[4] = {bcy, bcyt, bcy, bcyt};
+    const double ra[4] = {acy, acy, acyt, acyt};
+    const double rb[4] = {bcx, bcxt, bcx, bcxt};
+    double e[34], f[34];
+    double* cur = e;
+    double* nxt = f;
+    int n = 0;
+#pragma unroll 1
+    for (int k = 0; k < 4; ++k) {
+        double p, q, t[4];
+        two_product(la[k], lb[k], p, q);
+        t[0] = q;
+        t[1] = p;
+        two_product(ra[k], rb[k], p, q);
+        t[2] = -q;
+        t[3] = -p;
+#pragma unroll 1
+        for (int m = 0; m < 4; ++m) {
+            n = grow_expansion(n, cur, t[m], nxt);
+            double* s = cur;
+            cur = nxt;
+            nxt = s;
+        }
+    }
+    const double top = cur[n - 1];
+    return (top > 0.0) - (top < 0.0);
+}
+
+// Shewchuk's stage-A bound (3 + 16 eps) eps with eps = 2^-53.
+constexpr double kCcwErrBoundA = 3.3306690738754716e-16;
+
+// Exact orientation sign; counts calls that needed the exact stage.
+__device__ __forceinline__ int orient2d(double ax, double ay, double bx, double by,
+                                        double cx, double cy, unsigned& n_exact) {
+    const double acx = __dsub_rn(ax, cx), bcx = __dsub_rn(bx, cx);
+    const double acy = __dsub_rn(ay, cy), bcy = __dsub_rn(by, cy);
+    const double l = __dmul_rn(acx, bcy), r = __dmul_rn(acy, bcx);
+    const double det = __dsub_rn(l, r);
+    const double bound = __dmul_rn(kCcwErrBoundA, __dadd_rn(fabs(l), fabs(r)));
+    if (det > bound) return 1;
+    if (-det > bound) return -1;
+    ++n_exact;
+    return orient2d_exact(ax, ay, bx, by, cx, cy);
+}
+
+// Ring walk over interleaved vertices xy[start, end); the edge (end-1 -> start)
+// closes the ring exactly as in the reference's (i, j = i - 1) loop.
+__device__ __forceinline__ int ring_location(double px, double py, const double2* __restrict__ xy,
+                                             int start, int end, unsigned& n_exact) {
+    if (end - start < 2) return LOC_OUTSIDE;
+    bool inside = false;
+    double2 a = xy[end - 1];
+    for (int i = start; i < end; ++i) {
+        const double2 b = xy[i];
+        const double ax = a.x, ay = a.y, bx = b.x, by = b.y;
+        a = b;
+        const bool crosses = (ay > py) != (by > py);
+        const double minx = fmin(ax, bx), maxx = fmax(ax, bx);
+        const bool on_bbox = py >= fmin(ay, by) && py <= fmax(ay, by) && px >= minx && px <= maxx;
+        if (!crosses && !on_bbox) continue;
+        if (crosses && px < minx) {
+            inside = !inside;
+            continue;
+        }
+        if (crosses && px > maxx) continue;
+        const int o = orient2d(ax, ay, bx, by, px, py, n_exact);
+        if (on_bbox && o == 0) return LOC_BOUNDARY;
+        if (crosses && ((o > 0) == (by > ay))) inside = !inside;
+    }
+    return inside ? LOC_INTERIOR : LOC_OUTSIDE;
+}
+
+// Same walk over separate x[] / y[] arrays (caller-layout inputs).
+__device__ __forceinline__ int ring_location_soa(double px, double py, const double* __restrict__ x,
+                                                 const double* __restrict__ y, int start, int end,
+                                                 unsigned& n_exact) {
+    if (end - start < 2) return LOC_OUTSIDE;
+    bool inside = false;
+    double ax = x[end - 1], ay = y[end - 1];
+    for (int i = start; i < end; ++i) {
+        const double bx = x[i], by = y[i];
+        const double cax = ax, cay = ay;
+        ax = bx;
+        ay = by;
+        const bool crosses = (cay > py) != (by > py);
+        const double minx = fmin(cax, bx), maxx = fmax(cax, bx);
+        const bool on_bbox = py >= fmin(cay, by) && py <= fmax(cay, by) && px >= minx && px <= maxx;
+        if (!crosses && !on_bbox) continue;
+        if (crosses && px < minx) {
+            inside = !inside;
+            continue;
+        }
+        if (crosses && px > maxx) continue;
+        const int o = orient2d(cax, cay, bx, by, px, py, n_exact);
+        if (on_bbox && o == 0) return LOC_BOUNDARY;
+        if (crosses && ((o > 0) == (by > cay))) inside = !inside;
+    }
+    return inside ? LOC_INTERIOR : LOC_OUTSIDE;
+}
+
+// Location of a point in polygonal geometry g (a Polygon is a one-part
+// MultiPolygon): geom_off -> parts, part_off -> rings, ring_off -> vertices.
+__device__ __forceinline__ int geometry_location(double px, double py, const double2* __restrict__ xy,
+                                                 const int32_t* __restrict__ ring_off,
+                                                 const int32_t* __restrict__ part_off,
+                                                 const int32_t* __restrict__ geom_off, int g,
+                                                 unsigned& n_exact) {
+    const int p0 = geom_off[g], p1 = geom_off[g + 1];
+    for (int part = p0; part < p1; ++part) {
+        bool inside = false;
+        const int r0 = part_off[part], r1 = part_off[part + 1];
+        for (int ring = r0; ring < r1; ++ring) {
+            const int k = ring_location(px, py, xy, ring_off[ring], ring_off[ring + 1], n_exact);
+            if (k == LOC_BOUNDARY) return LOC_BOUNDARY;
+            if (k == LOC_INTERIOR) inside = !inside;
+        }
+        if (inside) return LOC_INTERIOR;
+    }
+    return LOC_OUTSIDE;
+}
+
+__device__ __forceinline__ int geometry_location_soa(double px, double py, const double* __restrict__ x,
+                                                     const double* __restrict__ y,
+                                                     const int32_t* __restrict__ ring_off,
+                                                     const int32_t* __restrict__ part_off,
+                                                     const int32_t* __restrict__ geom_off, int g,
+                                                     unsigned& n_exact) {
+    const int p0 = geom_off[g], p1 = geom_off[g + 1];
+    for (int part = p0; part < p1; ++part) {
+        bool inside = false;
+        const int r0 = part_off[part], r1 = part_off[part + 1];
+        for (int ring = r0; ring < r1; ++ring) {
+            const int k = ring_location_soa(px, py, x, y, ring_off[ring], ring_off[ring + 1], n_exact);
+            if (k == LOC_BOUNDARY) return LOC_BOUNDARY;
+            if (k == LOC_INTERIOR) inside = !inside;
+        }
+        if (inside) return LOC_INTERIOR;
+    }
+    return LOC_OUTSIDE;
+}
+
+}  // namespace vs

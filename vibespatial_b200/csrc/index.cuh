@@ -1,0 +1,81 @@
+// Device-resident spatial index of the polygon (tree) side.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "vs_common.cuh"
+
+namespace vs {
+
+constexpr int kFanout = 16;      // children per R-tree node
+constexpr int kMaxLevels = 16;   // 16^15 > 2^31 items
+
+// Learned cell index (the headline query path): the frame is cut into a
+// 2^L x 2^L grid, every polygon box is registered in the cells it overlaps,
+// and the non-empty cells are stored as a sorted array of Hilbert cell keys
+// with a CSR list of polygon slots.  A two-stage RMI (FP32 MLP root 1->32->32->1
+// + linear leaves) predicts a key's position in that array, and a per-leaf
+// error window bounds the search, so every lookup is exact.
+constexpr int kRmiHidden = 32;
+
+struct RmiModel {
+    // root MLP weights (FP32): h1 = relu(w1 * x + b1); h2 = relu(W2 h1 + b2); y = w3 . h2 + b3
+    float w1[kRmiHidden], b1[kRmiHidden];
+    float w2[kRmiHidden * kRmiHidden], b2[kRmiHidden];
+    float w3[kRmiHidden], b3;
+    // input normalisation: x = (key - key_lo) * key_scale   (double)
+    double key_lo, key_scale;
+    int32_t n_leaves;
+    int32_t n_keys;
+};
+
+struct LearnedIndex {
+    int32_t level = 0;            // grid level L (cells of span / 2^L)
+    int64_t n_cells = 0;          // non-empty cells
+    int64_t n_entries = 0;        // (cell, polygon) registrations
+    uint64_t* cell_keys = nullptr;   // [n_cells] sorted Hilbert keys of level L
+    uint32_t* cell_start = nullptr;  // [n_cells + 1] CSR offsets into entries
+    uint32_t* entries = nullptr;     // [n_entries] polygon slots (sorted order)
+    // RMI: root weights (device copy of RmiModel) + per-leaf linear model and window
+    RmiModel* model = nullptr;       // device
+    float2* leaf_ab = nullptr;       // [n_leaves] pos = a + b * x_local
+    int2* leaf_err = nullptr;        // [n_leaves] (lo, hi) error window, inclusive
+    double* leaf_x0 = nullptr;       // [n_leaves] leaf-local origin of x
+    // FP32 tile-relative copies used by the split-precision filter
+    float4* box32 = nullptr;         // [n_geoms] slot boxes relative to the slot origin, rounded outward
+    double2* origin = nullptr;       // [n_geoms] slot origin (box centre, FP64)
+    float2* xy32 = nullptr;          // [n_coords] vertices relative to their slot origin (nearest)
+    float* err32 = nullptr;          // [n_geoms] max |vertex rounding error| per slot
+    float rmi_train_ms = 0.f;
+    float mean_window = 0.f;
+    int32_t max_window = 0;
+};
+
+}  // namespace vs
+
+struct vs_index {
+    int device = 0;
+    int32_t n_geoms = 0, n_parts = 0, n_rings = 0;
+    int64_t n_coords = 0;
+    int32_t levels = 0;
+    int64_t level_off[vs::kMaxLevels] = {};
+    int64_t level_size[vs::kMaxLevels] = {};
+    vs_box* nodes = nullptr;      // all levels, level 0 = polygon boxes in Hilbert order
+    int32_t* item_geom = nullptr; // slot -> original polygon row
+    // polygon data re-laid out in slot (Hilbert) order, vertices interleaved
+    int32_t* geom_off = nullptr;
+    int32_t* part_off = nullptr;
+    int32_t* ring_off = nullptr;
+    double2* xy = nullptr;
+    double* frame = nullptr;      // device [4]: minx, miny, maxx, maxy of valid boxes
+    double h_frame[4] = {0, 0, 0, 0};
+    bool has_learned = false;
+    vs::LearnedIndex learned;
+    int64_t device_bytes = 0;
+    float build_ms = 0.f;
+};
+
+namespace vs {
+int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* opts);
+void free_learned_index(vs_index* idx);
+}  // namespace vs

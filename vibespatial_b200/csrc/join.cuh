@@ -1,0 +1,21 @@
+// Host-side launchers shared by the C-ABI translation unit.
+#pragma once
+#include <stdint.h>
+
+#include "index.cuh"
+#include "vs_common.cuh"
+
+namespace vs {
+int accept_mask_for(int predicate, int* mask);
+int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
+                      int32_t* d_left, int32_t* d_right, int64_t capacity);
+int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
+                        int32_t* d_left, int32_t* d_right, int64_t capacity);
+int launch_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, uint8_t* d_out);
+int sort_pairs(vs_context* ctx, int32_t* d_left, int32_t* d_right, int64_t n, uint64_t max_left,
+               uint64_t max_right);
+int build_rtree(vs_context* ctx, const vs_polygons* P, vs_index* idx);
+void free_index_memory(vs_index* idx);
+int hilbert_point_keys(const double* x, const double* y, int64_t n, double minx, double miny, double maxx,
+                       double maxy, uint64_t* keys, cudaStream_t s);
+}  // namespace vs

@@ -1,0 +1,250 @@
+// Exclusive scan (reduce -> scan of block sums -> downsweep) and a stable
+// LSD radix sort of (u64 key, u32 value) pairs, 8 bits per pass.
+//
+// Radix sort per pass: (1) per-tile digit histograms with shared atomics,
+// written digit-major so that one exclusive scan over [digit][tile] gives
+// every (digit, tile) its global output offset; (2) a scatter that ranks each
+// key stably inside its tile with __match_any_sync (peers with the same digit
+// in a warp) plus per-warp digit counts scanned in shared memory.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "primitives.cuh"
+
+namespace vs {
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <class T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread.
+template <class T>
+__device__ __forceinline__ void block_exclusive_scan(T v, T& excl) {
+    __shared__ T warp_tot[kScanThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = warp_inclusive_scan(v);
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < kScanThreads / 32 ? warp_tot[lane] : T(0);
+        T wi = warp_inclusive_scan(w);
+        if (lane < kScanThreads / 32) warp_tot[lane] = wi - w;
+    }
+    __syncthreads();
+    excl = warp_tot[warp] + inc - v;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const T* __restrict__ in, int64_t n,
+                                                                   T* __restrict__ sums) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + (int64_t)k * kScanThreads + threadIdx.x;
+        if (i < n) acc += in[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ T ws[kScanThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T t = 0;
+        for (int w = 0; w < kScanThreads / 32; ++w) t += ws[w];
+        sums[blockIdx.x] = t;
+    }
+}
+
+// Each thread owns kScanItems consecutive items.
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) scan_downsweep_kernel(const T* in, T* out, int64_t n,
+                                                                      const T* __restrict__ offsets,
+                                                                      T* __restrict__ d_total) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    T v[kScanItems];
+    T local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + k;
+        v[k] = i < n ? in[i] : T(0);
+        local += v[k];
+    }
+    T excl;
+    block_exclusive_scan<T>(local, excl);
+    T run = excl + (offsets ? offsets[blockIdx.x] : T(0));
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+        if (d_total && i == n - 1) *d_total = run;
+    }
+}
+
+template <class T>
+int exclusive_scan_impl(const T* in, T* out, int64_t n, T* d_total, cudaStream_t s) {
+    if (n <= 0) {
+        if (d_total) VS_CUDA_TRY(cudaMemsetAsync(d_total, 0, sizeof(T), s));
+        return VS_OK;
+    }
+    const int64_t nb = (n + kScanTile - 1) / kScanTile;
+    if (nb > 0x7fffffff) {
+        set_error("scan too large (%lld items)", (long long)n);
+        return VS_E_ARG;
+    }
+    if (nb == 1) {
+        scan_downsweep_kernel<T><<<1, kScanThreads, 0, s>>>(in, out, n, nullptr, d_total);
+        VS_CUDA_TRY(cudaGetLastError());
+        return VS_OK;
+    }
+    Scratch<T> sums;
+    VS_TRY(sums.alloc((size_t)nb, s));
+    scan_reduce_kernel<T><<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, sums.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(exclusive_scan_impl<T>(sums.p, sums.p, nb, (T*)nullptr, s));
+    scan_downsweep_kernel<T><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, sums.p, d_total);
+    VS_CUDA_TRY(cudaGetLastError());
+    return VS_OK;
+}
+
+// ------------------------------------------------------------------------
+// Radix sort
+// ------------------------------------------------------------------------
+constexpr int kRsThreads = 256;
+constexpr int kRsWarps = kRsThreads / 32;
+constexpr int kRsRounds = 16;
+constexpr int kRsTile = kRsThreads * kRsRounds;  // 4096 keys per tile
+constexpr int kRadix = 256;
+
+__global__ void __launch_bounds__(kRsThreads) rs_histogram_kernel(const uint64_t* __restrict__ keys, int64_t n,
+                                                                  int shift, uint32_t* __restrict__ hist,
+                                                                  int ntiles) {
+    __shared__ uint32_t h[kRadix];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kRsTile;
+#pragma unroll 4
+    for (int r = 0; r < kRsRounds; ++r) {
+        const int64_t i = base + (int64_t)r * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(unsigned)(keys[i] >> shift) & 0xffu], 1u);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t* __restrict__ kin,
+                                                                const uint32_t* __restrict__ vin,
+                                                                uint64_t* __restrict__ kout,
+                                                                uint32_t* __restrict__ vout, int64_t n,
+                                                                int shift,
+                                                                const uint32_t* __restrict__ offsets,
+                                                                int ntiles) {
+    __shared__ uint32_t base[kRadix];
+    __shared__ uint32_t wcnt[kRsWarps][kRadix];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    base[tid] = offsets[(int64_t)tid * ntiles + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < kRsWarps; ++w) wcnt[w][tid] = 0;
+    __syncthreads();
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int64_t tile0 = (int64_t)blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsRounds; ++r) {
+        const int64_t i = tile0 + (int64_t)r * kRsThreads + tid;
+        const bool valid = i < n;
+        uint64_t key = 0;
+        uint32_t val = 0;
+        unsigned d = kRadix;  // sentinel digit for out-of-range lanes
+        if (valid) {
+            key = kin[i];
+            val = vin[i];
+            d = (unsigned)(key >> shift) & 0xffu;
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned rank = __popc(peers & lt_mask);
+        if (valid && (__ffs(peers) - 1) == lane) wcnt[warp][d] = __popc(peers);
+        __syncthreads();
+        uint32_t acc = 0;
+        {
+#pragma unroll
+            for (int w = 0; w < kRsWarps; ++w) {
+                const uint32_t c = wcnt[w][tid];
+                wcnt[w][tid] = acc;
+                acc += c;
+            }
+        }
+        __syncthreads();
+        if (valid) {
+            const uint32_t pos = base[d] + wcnt[warp][d] + rank;
+            kout[pos] = key;
+            vout[pos] = val;
+        }
+        __syncthreads();
+        base[tid] += acc;
+#pragma unroll
+        for (int w = 0; w < kRsWarps; ++w) wcnt[w][tid] = 0;
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* d_total, cudaStream_t s) {
+    return exclusive_scan_impl<uint32_t>(in, out, n, d_total, s);
+}
+int exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, uint64_t* d_total, cudaStream_t s) {
+    return exclusive_scan_impl<uint64_t>(in, out, n, d_total, s);
+}
+
+int radix_sort_u64_u32(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s) {
+    if (n <= 1) return VS_OK;
+    if (n > 0xffffffffLL) {
+        set_error("radix sort supports at most 2^32-1 items (got %lld)", (long long)n);
+        return VS_E_ARG;
+    }
+    if (key_bits <= 0 || key_bits > 64) key_bits = 64;
+    const int passes = (key_bits + 7) / 8;
+    const int ntiles = (int)((n + kRsTile - 1) / kRsTile);
+    Scratch<uint64_t> kalt;
+    Scratch<uint32_t> valt, hist;
+    VS_TRY(kalt.alloc((size_t)n, s));
+    VS_TRY(valt.alloc((size_t)n, s));
+    VS_TRY(hist.alloc((size_t)kRadix * ntiles, s));
+    uint64_t* ka = keys;
+    uint32_t* va = vals;
+    uint64_t* kb = kalt.p;
+    uint32_t* vb = valt.p;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        rs_histogram_kernel<<<ntiles, kRsThreads, 0, s>>>(ka, n, shift, hist.p, ntiles);
+        VS_CUDA_TRY(cudaGetLastError());
+        VS_TRY(exclusive_scan_u32(hist.p, hist.p, (int64_t)kRadix * ntiles, nullptr, s));
+        rs_scatter_kernel<<<ntiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist.p, ntiles);
+        VS_CUDA_TRY(cudaGetLastError());
+        uint64_t* tk = ka;
+        ka = kb;
+        kb = tk;
+        uint32_t* tv = va;
+        va = vb;
+        vb = tv;
+    }
+    if (ka != keys) {
+        VS_CUDA_TRY(cudaMemcpyAsync(keys, ka, (size_t)n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        VS_CUDA_TRY(cudaMemcpyAsync(vals, va, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    }
+    return VS_OK;
+}
+
+}  // namespace vs

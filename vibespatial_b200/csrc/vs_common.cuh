@@ -1,0 +1,85 @@
+// Shared definitions for the vsjoin CUDA library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/vsjoin.h"
+
+namespace vs {
+
+// Thread-local last-error message, exported through vs_last_error().
+void set_error(const char* fmt, ...);
+
+#define VS_CUDA_TRY(expr)                                                        \
+    do {                                                                         \
+        cudaError_t _e = (expr);                                                 \
+        if (_e != cudaSuccess) {                                                 \
+            ::vs::set_error("%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), \
+                            __FILE__, __LINE__);                                 \
+            return VS_E_CUDA;                                                    \
+        }                                                                        \
+    } while (0)
+
+#define VS_TRY(expr)                 \
+    do {                             \
+        int _s = (expr);             \
+        if (_s != VS_OK) return _s;  \
+    } while (0)
+
+constexpr int kNumSMs = 148;  // B200: 2 dies x 74 SMs
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Grid size for a grid-stride kernel: a multiple of the SM count, at most
+// enough blocks to cover n items once.
+inline int grid_for(int64_t n, int block, int per_sm = 8) {
+    int64_t need = (n + block - 1) / block;
+    int64_t cap = (int64_t)kNumSMs * per_sm;
+    if (need < 1) need = 1;
+    return (int)(need < cap ? need : cap);
+}
+
+// Order-preserving map from double to int64 so atomicMin/atomicMax on
+// long long order doubles correctly (NaN excluded by the callers).
+__device__ __forceinline__ long long dbl_to_ordered(double v) {
+    long long i = __double_as_longlong(v);
+    return i >= 0 ? i : (i ^ 0x7fffffffffffffffLL);
+}
+__device__ __forceinline__ double ordered_to_dbl(long long i) {
+    return __longlong_as_double(i >= 0 ? i : (i ^ 0x7fffffffffffffffLL));
+}
+inline long long host_dbl_to_ordered(double v) {
+    long long i;
+    static_assert(sizeof(i) == sizeof(v), "");
+    __builtin_memcpy(&i, &v, sizeof(i));
+    return i >= 0 ? i : (i ^ 0x7fffffffffffffffLL);
+}
+
+// Growable device scratch owned by a context; every allocation is stream
+// ordered on the context stream.
+struct Arena {
+    void* base = nullptr;
+    size_t cap = 0;
+    size_t used = 0;
+};
+
+}  // namespace vs
+
+// Axis-aligned box; an inverted box (min > max) contains nothing.
+struct __align__(32) vs_box {
+    double minx, miny, maxx, maxy;
+};
+
+// Opaque handles of the C-ABI.
+struct vs_context {
+    int device;
+    cudaStream_t stream;
+    bool owns_stream;
+    vs::Arena arena;
+    // Pinned host word used to read back pair counts.
+    unsigned long long* h_counter;
+    // Device counters: [0] pair count, [1] exact-fallback count,
+    // [2] fp32-filter decided edges, [3] edges sent past the fp32 filter,
+    // [4] error flags, [5] candidate (bbox) count, [6..7] spare.
+    unsigned long long* d_counters;
+};
