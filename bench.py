@@ -132,6 +132,12 @@ def algorithmic_bytes(w, n_pairs: int) -> int:
                + 8 * n_pairs)
 
 
+def launches_per_join(method: int) -> int:
+    """Kernels of ours one vs_join launches: point keys, 4 radix passes x
+    (histogram + 2 scan kernels + scatter), the join kernel."""
+    return 1 + 4 * 4 + 1
+
+
 def cpu_sample_rate(w, predicate: str, threads: int, target_s: float = 10.0):
     """Oracle (all host threads) on a bounded prefix of the same points; points/sec."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -239,6 +245,8 @@ def run_ours(args, rank, world, local_rank):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     kernel_ms = []
     with ClockSampler(dev) as clk:
+        if args.profile:
+            torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
         for k in range(args.steps):
             ev[k][0].record(stream)
             n_k, st = index.join_into(pts, pred, method, left, right)
@@ -246,6 +254,8 @@ def run_ours(args, rank, world, local_rank):
             kernel_ms.append(st["kernel_ms"])
             assert n_k == n_pairs
         torch.cuda.synchronize()
+        if args.profile:
+            torch.cuda.profiler.stop()
         step_ms = [a.elapsed_time(b) for a, b in ev]
         # plain method timing (same GPU, same buffers) after the timed region
         if method == _abi.METHOD_LEARNED:
@@ -319,8 +329,9 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
                 "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int(8 * n_pairs)},
-        "gpu_launches": args.steps * 1,
+        "gpu_launches": args.steps * launches_per_join(method),
         "join_stats": stats,
+        "index_info": info,
     }
     if plain is not None:
         line["plain_rtree_ms"] = plain
@@ -337,11 +348,13 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOAD_DESC), default="zipf")
     ap.add_argument("--predicate", choices=["within", "intersects"], default="within")
-    ap.add_argument("--method", choices=["learned", "rtree"], default="rtree")
+    ap.add_argument("--method", choices=["learned", "rtree"], default="learned")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-sample", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -58,7 +58,8 @@ enum vs_predicate {
 /* Query methods. */
 enum vs_method {
     VS_METHOD_RTREE = 0,   /* plain: packed Hilbert R-tree traversal, FP64 filter, exact refine */
-    VS_METHOD_LEARNED = 1, /* learned cell index + FP32 tile-relative filter, exact fallback */
+    VS_METHOD_LEARNED = 1, /* learned cell index + FP32 tile-relative filter, exact fallback;
+                              an index built without it answers with the R-tree */
     VS_METHOD_BRUTE = 2    /* every point against every polygon box (small joins, testing) */
 };
 
@@ -100,7 +101,7 @@ typedef struct vs_join_stats {
     int64_t exact_fallbacks;  /* orientation signs that needed the exact expansion stage */
     int64_t fp32_edges;       /* edges decided by the FP32 tile-relative filter */
     int64_t fp64_edges;       /* edges re-decided in FP64 because the FP32 bound was inconclusive */
-    int64_t rmi_fallbacks;    /* learned-index lookups that left their error window (must be 0) */
+    int64_t rmi_fallbacks;    /* learned-index lookups whose error window exceeded 256 cells (binary search) */
     float kernel_ms;          /* device time of the join kernels */
     float sort_ms;            /* device time of the optional pair sort */
 } vs_join_stats;

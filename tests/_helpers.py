@@ -30,11 +30,11 @@ def upload_points(abi, px, py, pvalid=None):
     return abi.make_points(bufs["x"], bufs["y"], bufs["valid"]), bufs
 
 
-def gpu_join(abi, ctx, px, py, polys, predicate="within", method=0, pvalid=None, learned=False, index=None):
+def gpu_join(abi, ctx, px, py, polys, predicate="within", method=0, pvalid=None, learned=None, index=None):
     pts, keep1 = upload_points(abi, px, py, pvalid)
     if index is None:
         P, keep2 = upload_polys(abi, polys)
-        index = abi.DeviceIndex(ctx, P, learned=learned)
+        index = abi.DeviceIndex(ctx, P, learned=(method == 1) if learned is None else learned)
     left, right, stats = index.join(pts, PRED_CODES[predicate], method, sort=True)
     return left.cpu().numpy(), right.cpu().numpy(), stats
 

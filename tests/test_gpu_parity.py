@@ -14,7 +14,7 @@ from _helpers import PRED_CODES, assert_same_pairs, gpu_join, oracle_polys, to_d
 
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
-METHODS = {"rtree": 0, "brute": 2}
+METHODS = {"rtree": 0, "learned": 1, "brute": 2}
 
 
 def _check(vsabi, ctx, oracle, w, predicate, method=0, pvalid=None):
@@ -26,7 +26,7 @@ def _check(vsabi, ctx, oracle, w, predicate, method=0, pvalid=None):
 
 
 @pytest.mark.parametrize("predicate", ["within", "intersects", "covered_by", "touches", None])
-@pytest.mark.parametrize("method", ["rtree", "brute"])
+@pytest.mark.parametrize("method", ["rtree", "learned", "brute"])
 def test_star_join_all_predicates(vsabi, ctx, oracle, predicate, method):
     from vibespatial_b200.testing import synthetic as syn
 
@@ -34,29 +34,57 @@ def test_star_join_all_predicates(vsabi, ctx, oracle, predicate, method):
     _check(vsabi, ctx, oracle, w, predicate, METHODS[method])
 
 
+@pytest.mark.parametrize("method", ["rtree", "learned"])
 @pytest.mark.parametrize("predicate", ["within", "intersects"])
-def test_utm_join_reduced(vsabi, ctx, oracle, predicate):
+def test_utm_join_reduced(vsabi, ctx, oracle, predicate, method):
     from vibespatial_b200.testing import synthetic as syn
 
     w = syn.utm_join(seed=1, n_points=1_000_000, n_polys=100_000)
-    _check(vsabi, ctx, oracle, w, predicate)
+    stats = _check(vsabi, ctx, oracle, w, predicate, METHODS[method])
+    if method == "learned":
+        assert stats["fp32_edges"] > 0
 
 
-def test_zipf_join_reduced(vsabi, ctx, oracle):
+@pytest.mark.parametrize("method", ["rtree", "learned"])
+def test_zipf_join_reduced(vsabi, ctx, oracle, method):
     from vibespatial_b200.testing import synthetic as syn
 
     w = syn.zipf_join(seed=3, n_points=2_000_000, n_polys=100_000)
-    _check(vsabi, ctx, oracle, w, "within")
+    _check(vsabi, ctx, oracle, w, "within", METHODS[method])
 
 
+@pytest.mark.parametrize("method", ["rtree", "learned"])
 @pytest.mark.parametrize("predicate", ["within", "intersects", "touches"])
-def test_degenerate_join_reduced(vsabi, ctx, oracle, predicate):
+def test_degenerate_join_reduced(vsabi, ctx, oracle, predicate, method):
     from vibespatial_b200.testing import synthetic as syn
 
     w = syn.degenerate_join(seed=5, n_points=400_000, n_polys=4_000)
-    stats = _check(vsabi, ctx, oracle, w, predicate)
+    stats = _check(vsabi, ctx, oracle, w, predicate, METHODS[method])
     if predicate != "within":
         assert stats["exact_fallbacks"] > 0  # on-edge points must reach the exact stage
+    if method == "learned":
+        assert stats["fp64_edges"] > 0  # near-boundary edges leave the FP32 filter
+
+
+def test_learned_index_is_judged_by_rtree(vsabi, ctx):
+    """Learned lookups and plain traversal give the same pair set (the R-tree is the judge)."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.zipf_join(seed=13, n_points=3_000_000, n_polys=200_000)
+    P, keep = upload_polys(vsabi, w.polys)
+    index = vsabi.DeviceIndex(ctx, P, learned=True)
+    info = index.info()
+    assert info["n_cells"] > 0 and info["rmi_max_window"] >= 1
+    for pred in ("within", "intersects", None):
+        al, ar, _ = gpu_join(vsabi, ctx, w.px, w.py, None, pred, 0, index=index)
+        bl, br, st = gpu_join(vsabi, ctx, w.px, w.py, None, pred, 1, index=index)
+        assert_same_pairs(bl, br, al, ar)
+    # explicit grid levels, including very coarse and very fine ones
+    for level in (3, 9, 15):
+        idx2 = vsabi.DeviceIndex(ctx, P, learned=True, cell_level=level, rmi_leaves=512, rmi_train_steps=50)
+        bl, br, _ = gpu_join(vsabi, ctx, w.px[:500_000], w.py[:500_000], None, "within", 1, index=idx2)
+        al, ar, _ = gpu_join(vsabi, ctx, w.px[:500_000], w.py[:500_000], None, "within", 0, index=idx2)
+        assert_same_pairs(bl, br, al, ar)
 
 
 @pytest.mark.parametrize("name", sorted(S.KNOWN_COVERS))
@@ -82,38 +110,40 @@ def test_known_cases_join(vsabi, ctx, oracle):
     assert gl.tolist() == el and gr.tolist() == er
 
 
-def test_nybb_and_natural_earth(vsabi, ctx, oracle):
+@pytest.mark.parametrize("method", [0, 1])
+def test_nybb_and_natural_earth(vsabi, ctx, oracle, method):
     from test_oracle_golden import nybb_points
 
     exp = json.loads((GOLDEN / "expected.json").read_text())
     d = dict(np.load(GOLDEN / "nybb.npz"))
     P, px, py = nybb_points(d, oracle)
     poly = S.SoA(d["x"], d["y"], d["ring_off"], d["part_off"], d["geom_off"], np.ones(len(d["geom_off"]) - 1))
-    gl, gr, _ = gpu_join(vsabi, ctx, px, py, poly, "intersects")
+    gl, gr, _ = gpu_join(vsabi, ctx, px, py, poly, "intersects", method)
     assert len(gl) == exp["nybb_inner_intersects_shape"]["value"][0]
     el, er = oracle.join(px, py, None, P, "intersects")
     assert_same_pairs(gl, gr, el, er)
     w = dict(np.load(GOLDEN / "naturalearth_lowres.npz"))
     c = dict(np.load(GOLDEN / "naturalearth_cities.npz"))
     wp = S.SoA(w["x"], w["y"], w["ring_off"], w["part_off"], w["geom_off"], np.ones(len(w["geom_off"]) - 1))
-    gl, gr, _ = gpu_join(vsabi, ctx, c["x"], c["y"], wp, "intersects")
+    gl, gr, _ = gpu_join(vsabi, ctx, c["x"], c["y"], wp, "intersects", method)
     assert len(gl) == exp["cities_countries_inner_intersects_shape"]["value"][0]
 
 
-def test_edge_cases(vsabi, ctx, oracle):
+@pytest.mark.parametrize("method", [0, 1])
+def test_edge_cases(vsabi, ctx, oracle, method):
     from vibespatial_b200.testing import synthetic as syn
 
     w = syn.star_join(seed=4, n_points=5000, n_polys=50)
     # empty point set
-    gl, gr, _ = gpu_join(vsabi, ctx, w.px[:0], w.py[:0], w.polys, "within")
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px[:0], w.py[:0], w.polys, "within", method)
     assert len(gl) == 0
     # empty polygon set
     empty = S.soa([])
-    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, empty, "within")
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, empty, "within", method)
     assert len(gl) == 0
     # one polygon (the root is the only item)
     one = S.soa([S.box(100, 100, 900, 900)])
-    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, one, "intersects")
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, one, "intersects", method)
     el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, one), "intersects")
     assert_same_pairs(gl, gr, el, er)
     # null / NaN points and null / empty polygons never match
@@ -121,11 +151,11 @@ def test_edge_cases(vsabi, ctx, oracle):
     pv = np.ones(len(px), np.uint8)
     pv[::7] = 0
     px[::11] = np.nan
-    gl, gr, _ = gpu_join(vsabi, ctx, px, py, w.polys, "intersects", pvalid=pv)
+    gl, gr, _ = gpu_join(vsabi, ctx, px, py, w.polys, "intersects", method, pvalid=pv)
     el, er = oracle.join(px, py, pv, oracle_polys(oracle, w.polys), "intersects")
     assert_same_pairs(gl, gr, el, er)
     mixed = S.soa([None, [], S.box(0, 0, 500, 500), None, S.box(400, 400, 1000, 1000)])
-    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, mixed, "within")
+    gl, gr, _ = gpu_join(vsabi, ctx, w.px, w.py, mixed, "within", method)
     el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, mixed), "within")
     assert_same_pairs(gl, gr, el, er)
     assert set(np.unique(gr)) <= {2, 4}
@@ -187,9 +217,18 @@ def test_pair_sort(vsabi, ctx):
     np.testing.assert_array_equal(dr.cpu().numpy(), r[o])
 
 
-def test_full_size_utm_join(vsabi, ctx, oracle):
-    """BASELINE configs[1] at full size (10M x 100k), within: whole pair set equal."""
+@pytest.mark.parametrize("method", ["rtree", "learned"])
+def test_full_size_utm_join(vsabi, ctx, oracle, method):
+    """The UTM-frame workload at full size (10M x 100k), within: whole pair set equal."""
     from vibespatial_b200.testing import synthetic as syn
 
     w = syn.utm_join(seed=1)
-    _check(vsabi, ctx, oracle, w, "within")
+    _check(vsabi, ctx, oracle, w, "within", METHODS[method])
+
+
+def test_full_size_zipf_join(vsabi, ctx, oracle):
+    """The skewed learned-index workload at full size (50M x 1M): learned pairs == oracle pairs."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.zipf_join(seed=3)
+    _check(vsabi, ctx, oracle, w, "within", METHODS["learned"])

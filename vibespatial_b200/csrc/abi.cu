@@ -259,10 +259,9 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
         set_error("unknown method %d", method);
         return VS_E_ARG;
     }
-    if (method == VS_METHOD_LEARNED && !idx->has_learned) {
-        set_error("index was built without the learned cell index (method_mask bit 1)");
-        return VS_E_ARG;
-    }
+    // The plain R-tree is the learned index's fallback: an index built without
+    // the learned cell index (or with nothing to index) answers with the R-tree.
+    if (method == VS_METHOD_LEARNED && !idx->has_learned) method = VS_METHOD_RTREE;
     VS_TRY(use_device(ctx->device));
     if (pts->n == 0 || idx->n_geoms == 0 || !(idx->h_frame[0] <= idx->h_frame[2])) return VS_OK;
     cudaStream_t s = ctx->stream;

@@ -60,7 +60,7 @@ __device__ __forceinline__ int grow_expansion(int elen, const double* e, double 
 // Exact sign of (ax-cx)(by-cy) - (ay-cy)(bx-cx): sixteen exact partial
 // products summed as a nonoverlapping expansion; the sign is the sign of the
 // largest component.  Kept out of line: it runs only when the filter fails.
-__device__ __noinline__ int orient2d_exact(double ax, double ay, double bx, double by,
+static __device__ __noinline__ int orient2d_exact(double ax, double ay, double bx, double by,
                                            double cx, double cy) {
     double acx, acxt, bcx, bcxt, acy, acyt, bcy, bcyt;
     two_diff(ax, cx, acx, acxt);
@@ -113,6 +113,27 @@ __device__ __forceinline__ int orient2d(double ax, double ay, double bx, double 
     return orient2d_exact(ax, ay, bx, by, cx, cy);
 }
 
+// One edge (a -> b) of the crossing-number walk, decided exactly.  Returns
+// true if the point lies on the edge (boundary); otherwise toggles `inside`
+// when the +x ray from the point crosses the edge.  Same decision sequence as
+// the reference's vs_ring_point_classify loop body.
+__device__ __forceinline__ bool edge_step_exact(double ax, double ay, double bx, double by, double px, double py,
+                                                bool& inside, unsigned& n_exact) {
+    const bool crosses = (ay > py) != (by > py);
+    const double minx = fmin(ax, bx), maxx = fmax(ax, bx);
+    const bool on_bbox = py >= fmin(ay, by) && py <= fmax(ay, by) && px >= minx && px <= maxx;
+    if (!crosses && !on_bbox) return false;
+    if (crosses && px < minx) {
+        inside = !inside;
+        return false;
+    }
+    if (crosses && px > maxx) return false;
+    const int o = orient2d(ax, ay, bx, by, px, py, n_exact);
+    if (on_bbox && o == 0) return true;
+    if (crosses && ((o > 0) == (by > ay))) inside = !inside;
+    return false;
+}
+
 // Ring walk over interleaved vertices xy[start, end); the edge (end-1 -> start)
 // closes the ring exactly as in the reference's (i, j = i - 1) loop.
 __device__ __forceinline__ int ring_location(double px, double py, const double2* __restrict__ xy,
@@ -122,20 +143,8 @@ __device__ __forceinline__ int ring_location(double px, double py, const double2
     double2 a = xy[end - 1];
     for (int i = start; i < end; ++i) {
         const double2 b = xy[i];
-        const double ax = a.x, ay = a.y, bx = b.x, by = b.y;
+        if (edge_step_exact(a.x, a.y, b.x, b.y, px, py, inside, n_exact)) return LOC_BOUNDARY;
         a = b;
-        const bool crosses = (ay > py) != (by > py);
-        const double minx = fmin(ax, bx), maxx = fmax(ax, bx);
-        const bool on_bbox = py >= fmin(ay, by) && py <= fmax(ay, by) && px >= minx && px <= maxx;
-        if (!crosses && !on_bbox) continue;
-        if (crosses && px < minx) {
-            inside = !inside;
-            continue;
-        }
-        if (crosses && px > maxx) continue;
-        const int o = orient2d(ax, ay, bx, by, px, py, n_exact);
-        if (on_bbox && o == 0) return LOC_BOUNDARY;
-        if (crosses && ((o > 0) == (by > ay))) inside = !inside;
     }
     return inside ? LOC_INTERIOR : LOC_OUTSIDE;
 }
@@ -149,21 +158,9 @@ __device__ __forceinline__ int ring_location_soa(double px, double py, const dou
     double ax = x[end - 1], ay = y[end - 1];
     for (int i = start; i < end; ++i) {
         const double bx = x[i], by = y[i];
-        const double cax = ax, cay = ay;
+        if (edge_step_exact(ax, ay, bx, by, px, py, inside, n_exact)) return LOC_BOUNDARY;
         ax = bx;
         ay = by;
-        const bool crosses = (cay > py) != (by > py);
-        const double minx = fmin(cax, bx), maxx = fmax(cax, bx);
-        const bool on_bbox = py >= fmin(cay, by) && py <= fmax(cay, by) && px >= minx && px <= maxx;
-        if (!crosses && !on_bbox) continue;
-        if (crosses && px < minx) {
-            inside = !inside;
-            continue;
-        }
-        if (crosses && px > maxx) continue;
-        const int o = orient2d(cax, cay, bx, by, px, py, n_exact);
-        if (on_bbox && o == 0) return LOC_BOUNDARY;
-        if (crosses && ((o > 0) == (by > cay))) inside = !inside;
     }
     return inside ? LOC_INTERIOR : LOC_OUTSIDE;
 }

@@ -30,23 +30,26 @@ struct RmiModel {
 };
 
 struct LearnedIndex {
-    int32_t level = 0;            // grid level L (cells of span / 2^L)
-    int64_t n_cells = 0;          // non-empty cells
-    int64_t n_entries = 0;        // (cell, polygon) registrations
-    uint64_t* cell_keys = nullptr;   // [n_cells] sorted Hilbert keys of level L
+    int32_t level = 0;               // grid level L (cells of frame / 2^L per axis)
+    int32_t occ_level = 0;           // occupancy bitmap level (<= L)
+    int64_t n_cells = 0;             // non-empty cells
+    int64_t n_entries = 0;           // (cell, polygon) registrations
+    uint32_t* cell_keys = nullptr;   // [n_cells] sorted level-L Hilbert keys
     uint32_t* cell_start = nullptr;  // [n_cells + 1] CSR offsets into entries
-    uint32_t* entries = nullptr;     // [n_entries] polygon slots (sorted order)
-    // RMI: root weights (device copy of RmiModel) + per-leaf linear model and window
+    uint32_t* entries = nullptr;     // [n_entries] polygon slots (Hilbert order)
+    uint32_t* occ = nullptr;         // occupancy bitmap of level occ_level
+    // RMI: root MLP + per-leaf linear model and error window
     RmiModel* model = nullptr;       // device
-    float2* leaf_ab = nullptr;       // [n_leaves] pos = a + b * x_local
-    int2* leaf_err = nullptr;        // [n_leaves] (lo, hi) error window, inclusive
-    double* leaf_x0 = nullptr;       // [n_leaves] leaf-local origin of x
+    double2* leaf_ab = nullptr;      // [n_leaves] position = a + b * (key - key_lo)
+    int2* leaf_err = nullptr;        // [n_leaves] inclusive error window (lo, hi)
+    int32_t n_leaves = 0;
     // FP32 tile-relative copies used by the split-precision filter
-    float4* box32 = nullptr;         // [n_geoms] slot boxes relative to the slot origin, rounded outward
     double2* origin = nullptr;       // [n_geoms] slot origin (box centre, FP64)
+    float4* box32 = nullptr;         // [n_geoms] slot box relative to the origin, rounded outward
+    float* err32 = nullptr;          // [n_geoms] bound on |vertex rounding error| of the slot
     float2* xy32 = nullptr;          // [n_coords] vertices relative to their slot origin (nearest)
-    float* err32 = nullptr;          // [n_geoms] max |vertex rounding error| per slot
     float rmi_train_ms = 0.f;
+    float rmi_final_loss = 0.f;
     float mean_window = 0.f;
     int32_t max_window = 0;
 };

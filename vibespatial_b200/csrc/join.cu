@@ -7,17 +7,24 @@
 //       the total -> scatter pass
 //   spatial/query_utils.py:578-868             refine: one thread per
 //       candidate pair, then boolean-mask compaction d_left[keep]
-// Here one kernel does both: each thread descends the R-tree for one point
-// (upper levels staged in shared memory), refines every leaf hit immediately
-// with the exact location, and appends accepted pairs to a shared-memory
-// buffer that is flushed to HBM with one global atomic per block iteration.
-// There is no candidate array, no count pass and no host fence inside the
-// join; the only read-back is the final pair count.
+//
+// Query points are first keyed (level-16 Hilbert key in the polygon frame;
+// points outside the frame, null or NaN get the sentinel key and are never
+// visited) and radix-sorted, so the 32 lanes of a warp hold spatially
+// coherent points.  Each warp then walks the R-tree once for its packet of
+// points: lanes 0-15 load the 16 children of the current node (coalesced,
+// upper levels from shared memory), test them against the packet's bounding
+// box and push the hits on a warp-shared stack in shared memory.  At the leaf
+// level every lane tests its own point against the hit item boxes and refines
+// each hit immediately with the exact location; accepted pairs go through the
+// block-buffered sink.  No candidate array, no count pass, no host fence.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
+#include "emit.cuh"
 #include "exact.cuh"
+#include "hilbert.cuh"
 #include "index.cuh"
 #include "join.cuh"
 #include "primitives.cuh"
@@ -26,15 +33,17 @@ namespace vs {
 namespace {
 
 constexpr int kJoinThreads = 256;
-constexpr int kOutBuf = 1024;     // pairs buffered per block iteration
-constexpr int kStack = 112;       // (fanout-1) * (max levels-2) + 1 < 112
-constexpr int kMaxStagedBoxes = 1365;  // 1 + 16 + 256 + 1092: ~43 KB of FP64 boxes
+constexpr int kWarps = kJoinThreads / 32;
+constexpr int kStack = 112;            // > (fanout-1) * (max levels-2) + 1
+constexpr int kMaxStagedBoxes = 1365;  // 1 + 16 + 256 + 1092 FP64 boxes (~43 KB)
 
 struct RtreeArgs {
     const double* px;
     const double* py;
     const uint8_t* pvalid;
     int64_t n;
+    const uint32_t* order;     // sorted position -> point row
+    const uint32_t* n_sorted;  // points with a valid key (a prefix of order)
     const vs_box* nodes;
     int64_t level_off[kMaxLevels];
     int64_t level_size[kMaxLevels];
@@ -47,9 +56,7 @@ struct RtreeArgs {
     const int32_t* ring_off;
     const double2* xy;
     int accept_mask;  // bit k: location k accepted; 0 = box candidates only
-    int32_t* out_left;
-    int32_t* out_right;
-    unsigned long long capacity;
+    PairSink sink;
     unsigned long long* counters;
 };
 
@@ -57,131 +64,141 @@ __device__ __forceinline__ bool box_has(const vs_box& b, double x, double y) {
     return x >= b.minx && x <= b.maxx && y >= b.miny && y <= b.maxy;
 }
 
-struct BlockOut {
-    int2* buf;
-    unsigned* cnt;
-};
+__device__ __forceinline__ bool box_overlaps(const vs_box& b, double x0, double y0, double x1, double y1) {
+    return b.minx <= x1 && b.maxx >= x0 && b.miny <= y1 && b.maxy >= y0;
+}
 
-__device__ __forceinline__ void emit(const BlockOut& o, int32_t l, int32_t r, unsigned long long capacity,
-                                     int32_t* out_left, int32_t* out_right, unsigned long long* counters) {
-    const unsigned pos = atomicAdd(o.cnt, 1u);
-    if (pos < (unsigned)kOutBuf) {
-        o.buf[pos] = make_int2(l, r);
-    } else {
-        const unsigned long long gp = atomicAdd(&counters[0], 1ull);
-        if (gp < capacity) {
-            out_left[gp] = l;
-            out_right[gp] = r;
+__global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ frame, uint32_t* __restrict__ keys,
+                                      uint32_t* __restrict__ idx, uint32_t* __restrict__ n_valid) {
+    const double f0 = frame[0], f1 = frame[1], f2 = frame[2], f3 = frame[3];
+    const double sx = f2 > f0 ? 4294967295.0 / (f2 - f0) : 0.0;
+    const double sy = f3 > f1 ? 4294967295.0 / (f3 - f1) : 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = p.d_x[i], y = p.d_y[i];
+        const bool ok = (p.d_valid == nullptr || p.d_valid[i]) && x >= f0 && x <= f2 && y >= f1 && y <= f3;
+        uint32_t k = 0xffffffffu;
+        if (ok) {
+            k = (uint32_t)hilbert_key(quantize(x, f0, sx), quantize(y, f1, sy), 16);
+            if (k == 0xffffffffu) k = 0xfffffffeu;  // keep the sentinel unique
         }
+        keys[i] = k;
+        idx[i] = (uint32_t)i;
+        const unsigned m = __ballot_sync(__activemask(), ok);
+        if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && m) atomicAdd(n_valid, (uint32_t)__popc(m));
     }
 }
 
-// Flush the block buffer; every thread of the block must call it.
-__device__ __forceinline__ void flush(const BlockOut& o, unsigned long long* s_base, unsigned* s_n,
-                                      unsigned long long capacity, int32_t* out_left, int32_t* out_right,
-                                      unsigned long long* counters) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned c = *o.cnt < (unsigned)kOutBuf ? *o.cnt : (unsigned)kOutBuf;
-        *s_n = c;
-        *s_base = c ? atomicAdd(&counters[0], (unsigned long long)c) : 0ull;
-        *o.cnt = 0;
-    }
-    __syncthreads();
-    const unsigned c = *s_n;
-    const unsigned long long b = *s_base;
-    for (unsigned k = threadIdx.x; k < c; k += blockDim.x) {
-        const unsigned long long gp = b + k;
-        if (gp < capacity) {
-            const int2 v = o.buf[k];
-            out_left[gp] = v.x;
-            out_right[gp] = v.y;
-        }
-    }
-    __syncthreads();
-}
-
-__device__ __forceinline__ void add_stats(unsigned long long* counters, unsigned long long cand, unsigned nexact) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        cand += __shfl_xor_sync(0xffffffffu, cand, o);
-        nexact += __shfl_xor_sync(0xffffffffu, nexact, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (cand) atomicAdd(&counters[5], cand);
-        if (nexact) atomicAdd(&counters[1], (unsigned long long)nexact);
-    }
-}
-
-__global__ void __launch_bounds__(kJoinThreads) join_rtree_kernel(const RtreeArgs a) {
+__global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const RtreeArgs a) {
     extern __shared__ vs_box s_nodes[];
     __shared__ int2 s_buf[kOutBuf];
     __shared__ unsigned s_cnt, s_n;
     __shared__ unsigned long long s_base;
+    __shared__ int s_stack[kWarps][kStack];
+    __shared__ vs_box s_items[kWarps][kFanout];
     const int64_t stage_base = a.level_off[a.stage_level];
     for (int k = threadIdx.x; k < a.staged; k += blockDim.x) s_nodes[k] = a.nodes[stage_base + k];
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
     const BlockOut out{s_buf, &s_cnt};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     const int top = a.levels - 1;
+    const int64_t n = (int64_t)*a.n_sorted;
     unsigned long long n_cand = 0;
     unsigned n_exact = 0;
-    int stack[kStack];
 
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < a.n; base += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
-        if (i < a.n && (a.pvalid == nullptr || a.pvalid[i])) {
-            const double x = a.px[i], y = a.py[i];
+        const bool active = i < n;
+        double x = 0.0, y = 0.0;
+        int32_t row = -1;
+        if (active) {
+            row = (int32_t)a.order[i];
+            x = a.px[row];
+            y = a.py[row];
+        }
+        double x0 = active ? x : INFINITY, x1 = active ? x : -INFINITY;
+        double y0 = active ? y : INFINITY, y1 = active ? y : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            x0 = fmin(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+            x1 = fmax(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+            y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+            y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+        }
+        if (__ballot_sync(0xffffffffu, active)) {
             int sp = 0;
             const vs_box root = s_nodes[a.level_off[top] - stage_base];
-            if (box_has(root, x, y)) {
+            if (box_overlaps(root, x0, y0, x1, y1)) {
                 if (top == 0) {
-                    // single polygon: the root is the item
-                    ++n_cand;
-                    const int loc = a.accept_mask ? geometry_location(x, y, a.xy, a.ring_off, a.part_off,
-                                                                      a.geom_off, 0, n_exact)
-                                                  : 0;
-                    if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                        emit(out, (int32_t)i, a.item_geom[0], a.capacity, a.out_left, a.out_right, a.counters);
+                    // a single polygon: the root is the item
+                    if (active && box_has(root, x, y)) {
+                        ++n_cand;
+                        const int loc = a.accept_mask ? geometry_location(x, y, a.xy, a.ring_off, a.part_off,
+                                                                          a.geom_off, 0, n_exact) : 0;
+                        if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) emit(out, a.sink, row, a.item_geom[0]);
+                    }
                 } else {
-                    stack[sp++] = top;  // node 0 of the top level
+                    if (lane == 0) s_stack[warp][0] = top;  // node 0 of the top level
+                    sp = 1;
                 }
             }
+            __syncwarp();
             while (sp > 0) {
-                const int e = stack[--sp];
-                const int lvl = e & 15;
-                const int64_t node = (int64_t)(e >> 4);
-                const int cl = lvl - 1;
-                const int64_t c0 = node * kFanout;
-                const int64_t cend = c0 + kFanout < a.level_size[cl] ? c0 + kFanout : a.level_size[cl];
-                const vs_box* cb = cl >= a.stage_level ? s_nodes + (a.level_off[cl] - stage_base)
-                                                       : a.nodes + a.level_off[cl];
-                for (int64_t c = c0; c < cend; ++c) {
-                    const vs_box b = cb[c];
-                    if (!box_has(b, x, y)) continue;
-                    if (cl == 0) {
-                        ++n_cand;
-                        const int slot = (int)c;
-                        int loc = 0;
-                        if (a.accept_mask)
-                            loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, n_exact);
-                        if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                            emit(out, (int32_t)i, a.item_geom[slot], a.capacity, a.out_left, a.out_right,
-                                 a.counters);
-                    } else if (sp < kStack) {
-                        stack[sp++] = (int)(c << 4) | cl;
-                    } else {
-                        atomicOr(&a.counters[4], 1ull);  // stack overflow: result incomplete
+                --sp;
+                const int e = s_stack[warp][sp];
+                __syncwarp();
+                const int cl = (e & 15) - 1;
+                const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
+                const bool in_range = lane < kFanout && c < a.level_size[cl];
+                vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
+                if (in_range)
+                    b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
+                const bool hit = in_range && box_overlaps(b, x0, y0, x1, y1);
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (cl > 0) {
+                    if (hit) {
+                        const int pos = sp + __popc(m & lt);
+                        if (pos < kStack) s_stack[warp][pos] = (int)(c << 4) | cl;
                     }
+                    int add = __popc(m);
+                    if (sp + add > kStack) {
+                        if (lane == 0) atomicOr(&a.counters[4], 1ull);  // cannot happen for < 2^31 items
+                        add = kStack - sp;
+                    }
+                    sp += add;
+                    __syncwarp();
+                } else {
+                    if (lane < kFanout) s_items[warp][lane] = b;
+                    __syncwarp();
+                    unsigned mm = m;
+                    const int64_t slot0 = (int64_t)(e >> 4) * kFanout;
+                    while (mm) {
+                        const int j = __ffs(mm) - 1;
+                        mm &= mm - 1;
+                        const vs_box ib = s_items[warp][j];
+                        if (active && box_has(ib, x, y)) {
+                            ++n_cand;
+                            const int slot = (int)(slot0 + j);
+                            int loc = 0;
+                            if (a.accept_mask)
+                                loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, n_exact);
+                            if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
+                                emit(out, a.sink, row, a.item_geom[slot]);
+                        }
+                    }
+                    __syncwarp();
                 }
             }
         }
-        flush(out, &s_base, &s_n, a.capacity, a.out_left, a.out_right, a.counters);
+        flush(out, a.sink, &s_base, &s_n);
     }
-    add_stats(a.counters, n_cand, n_exact);
+    add_counter(a.counters, 5, n_cand);
+    add_counter(a.counters, 1, n_exact);
 }
 
-// Every point against every polygon box (small joins and cross-checks).
+// Every point against every polygon box, one thread per point in input order
+// (small joins and cross-checks).
 __global__ void __launch_bounds__(kJoinThreads) join_brute_kernel(const RtreeArgs a) {
     __shared__ int2 s_buf[kOutBuf];
     __shared__ unsigned s_cnt, s_n;
@@ -202,13 +219,13 @@ __global__ void __launch_bounds__(kJoinThreads) join_brute_kernel(const RtreeArg
                 int loc = 0;
                 if (a.accept_mask)
                     loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, (int)c, n_exact);
-                if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                    emit(out, (int32_t)i, a.item_geom[c], a.capacity, a.out_left, a.out_right, a.counters);
+                if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) emit(out, a.sink, (int32_t)i, a.item_geom[c]);
             }
         }
-        flush(out, &s_base, &s_n, a.capacity, a.out_left, a.out_right, a.counters);
+        flush(out, a.sink, &s_base, &s_n);
     }
-    add_stats(a.counters, n_cand, n_exact);
+    add_counter(a.counters, 5, n_cand);
+    add_counter(a.counters, 1, n_exact);
 }
 
 __global__ void locate_aligned_kernel(vs_points pts, vs_polygons polys, uint8_t* __restrict__ out,
@@ -264,6 +281,19 @@ int accept_mask_for(int predicate, int* mask) {
     }
 }
 
+int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q) {
+    cudaStream_t s = ctx->stream;
+    const int64_t n = pts->n;
+    VS_TRY(q.keys.alloc((size_t)n, s));
+    VS_TRY(q.order.alloc((size_t)n, s));
+    VS_TRY(q.n_valid.alloc(1, s));
+    VS_CUDA_TRY(cudaMemsetAsync(q.n_valid.p, 0, sizeof(uint32_t), s));
+    point_sort_key_kernel<<<grid_for(n, 256, 16), 256, 0, s>>>(*pts, idx->frame, q.keys.p, q.order.p, q.n_valid.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(radix_sort_u32_u32(q.keys.p, q.order.p, n, 32, s));
+    return VS_OK;
+}
+
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
                       int32_t* d_left, int32_t* d_right, int64_t capacity) {
     RtreeArgs a{};
@@ -292,17 +322,20 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.ring_off = idx->ring_off;
     a.xy = idx->xy;
     a.accept_mask = accept_mask;
-    a.out_left = d_left;
-    a.out_right = d_right;
-    a.capacity = (unsigned long long)(capacity > 0 ? capacity : 0);
+    a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.counters = ctx->d_counters;
-    const int grid = grid_for(pts->n, kJoinThreads, 8);
     if (brute) {
-        join_brute_kernel<<<grid, kJoinThreads, 0, ctx->stream>>>(a);
-    } else {
-        const size_t smem = (size_t)a.staged * sizeof(vs_box);
-        join_rtree_kernel<<<grid, kJoinThreads, smem, ctx->stream>>>(a);
+        join_brute_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, 0, ctx->stream>>>(a);
+        VS_CUDA_TRY(cudaGetLastError());
+        return VS_OK;
     }
+    QueryOrder q;
+    VS_TRY(prepare_queries(ctx, idx, pts, q));
+    a.order = q.order.p;
+    a.n_sorted = q.n_valid.p;
+    const size_t smem = (size_t)a.staged * sizeof(vs_box);
+    VS_CUDA_TRY(cudaFuncSetAttribute(join_rtree_packet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    join_rtree_packet_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, smem, ctx->stream>>>(a);
     VS_CUDA_TRY(cudaGetLastError());
     return VS_OK;
 }

@@ -3,9 +3,16 @@
 #include <stdint.h>
 
 #include "index.cuh"
+#include "primitives.cuh"
 #include "vs_common.cuh"
 
 namespace vs {
+// Query points keyed by their level-16 Hilbert key in the polygon frame and
+// radix-sorted; order[0, *n_valid) are the points that can match.
+struct QueryOrder {
+    Scratch<uint32_t> keys, order, n_valid;
+};
+int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q);
 int accept_mask_for(int predicate, int* mask);
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
                       int32_t* d_left, int32_t* d_right, int64_t capacity);

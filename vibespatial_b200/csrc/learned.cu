@@ -1,15 +1,861 @@
-// Learned cell index (placeholder until the RMI path lands).
+// Learned cell index: build, RMI training, and the learned + split-precision join.
+//
+// Build (after the packed R-tree, reusing its Hilbert slot order and frame):
+//   1. every polygon box is registered in the level-L grid cells it overlaps
+//      (cell key = level-L Hilbert key, the top 2L bits of a point's key)
+//   2. (cell key, slot) pairs are radix-sorted; unique keys + CSR offsets
+//      give the sorted build-side array the RMI indexes
+//   3. an occupancy bitmap at a coarser level lets empty regions skip lookups
+//   4. the RMI (FP32 MLP 1->32->32->1 root + linear leaves) is trained on the
+//      sorted cell keys with hand-written forward/backward and Adam kernels;
+//      every key is then routed through the same inference functions to fit
+//      the leaves and to measure each leaf's inclusive error window
+//   5. FP32 copies of every polygon relative to its own origin (box centre),
+//      with a per-polygon bound on the rounding error, for the split filter
+//
+// Query (points already keyed and sorted, see prepare_queries): for each
+// distinct cell among a warp's 32 points the warp evaluates the root MLP
+// cooperatively (lane = hidden unit), predicts the position with the leaf
+// model and searches the error window; each lane then scans its cell's
+// polygon list, filters boxes in FP32 (rounded outward), and refines with the
+// FP32 crossing test, re-deciding in FP64 (and exactly, if needed) only the
+// edges whose FP32 decision is within its rounding-error bound.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "emit.cuh"
+#include "exact.cuh"
+#include "hilbert.cuh"
 #include "index.cuh"
 #include "join.cuh"
+#include "primitives.cuh"
+#include "rmi.cuh"
 
 namespace vs {
-int build_learned_index(vs_context*, vs_index*, const vs_index_options*) {
-    set_error("learned cell index not available in this build");
-    return VS_E_ARG;
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRmiP = kRmiHidden + kRmiHidden + kRmiHidden * kRmiHidden + kRmiHidden + kRmiHidden + 1;  // 1153
+constexpr int kOffW1 = 0, kOffB1 = 32, kOffW2 = 64, kOffB2 = 64 + 1024, kOffW3 = 64 + 1024 + 32,
+              kOffB3 = 64 + 1024 + 64;
+constexpr int kTrainBlocks = 64;
+
+__device__ __forceinline__ void frame_q(const double* fr, double& lox, double& loy, double& sx, double& sy) {
+    lox = fr[0];
+    loy = fr[1];
+    sx = fr[2] > fr[0] ? 4294967295.0 / (fr[2] - fr[0]) : 0.0;
+    sy = fr[3] > fr[1] ? 4294967295.0 / (fr[3] - fr[1]) : 0.0;
 }
-void free_learned_index(vs_index*) {}
-int launch_learned_join(vs_context*, const vs_index*, const vs_points*, int, int32_t*, int32_t*, int64_t) {
-    set_error("learned cell index not available in this build");
-    return VS_E_ARG;
+
+// ---------------------------------------------------------------- build ---
+__global__ void box_side_kernel(const vs_box* __restrict__ box, int64_t M, double* __restrict__ acc) {
+    double s = 0.0, c = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+        const vs_box b = box[i];
+        if (b.minx <= b.maxx) {
+            s += fmax(b.maxx - b.minx, b.maxy - b.miny);
+            c += 1.0;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if ((threadIdx.x & 31) == 0 && c > 0) {
+        atomicAdd(&acc[0], s);
+        atomicAdd(&acc[1], c);
+    }
 }
+
+__device__ __forceinline__ bool cell_range(const vs_box& b, const double* fr, int L, uint32_t& cx0, uint32_t& cx1,
+                                           uint32_t& cy0, uint32_t& cy1) {
+    if (!(b.minx <= b.maxx)) return false;
+    double lox, loy, sx, sy;
+    frame_q(fr, lox, loy, sx, sy);
+    const int sh = 32 - L;
+    cx0 = quantize(b.minx, lox, sx) >> sh;
+    cx1 = quantize(b.maxx, lox, sx) >> sh;
+    cy0 = quantize(b.miny, loy, sy) >> sh;
+    cy1 = quantize(b.maxy, loy, sy) >> sh;
+    return true;
+}
+
+__global__ void cell_count_kernel(const vs_box* __restrict__ box, int64_t M, const double* __restrict__ fr, int L,
+                                  uint32_t* __restrict__ cnt, unsigned long long* __restrict__ total) {
+    unsigned long long t = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t x0, x1, y0, y1;
+        uint64_t c = 0;
+        if (cell_range(box[i], fr, L, x0, x1, y0, y1)) c = (uint64_t)(x1 - x0 + 1) * (uint64_t)(y1 - y0 + 1);
+        cnt[i] = c > 0xffffffffull ? 0xffffffffu : (uint32_t)c;
+        t += c;
+    }
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0 && t) atomicAdd(total, t);
+}
+
+__global__ void cell_emit_kernel(const vs_box* __restrict__ box, int64_t M, const double* __restrict__ fr, int L,
+                                 const uint32_t* __restrict__ off, uint32_t* __restrict__ keys,
+                                 uint32_t* __restrict__ vals) {
+    const int sh = 32 - L;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t x0, x1, y0, y1;
+        if (!cell_range(box[i], fr, L, x0, x1, y0, y1)) continue;
+        uint32_t o = off[i];
+        for (uint32_t cy = y0; cy <= y1; ++cy)
+            for (uint32_t cx = x0; cx <= x1; ++cx) {
+                keys[o] = (uint32_t)hilbert_key(cx << sh, cy << sh, L);
+                vals[o] = (uint32_t)i;
+                ++o;
+            }
+    }
+}
+
+__global__ void cell_flag_kernel(const uint32_t* __restrict__ keys, int64_t E, uint32_t* __restrict__ flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x)
+        flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+__global__ void cell_compact_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ id, int64_t E,
+                                    uint32_t* __restrict__ cell_keys, uint32_t* __restrict__ cell_start) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i == 0 || keys[i] != keys[i - 1]) {
+            cell_keys[id[i]] = keys[i];
+            cell_start[id[i]] = (uint32_t)i;
+        }
+    }
+}
+
+__global__ void occ_kernel(const uint32_t* __restrict__ cell_keys, int64_t n, int shift, uint32_t* __restrict__ occ) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = cell_keys[i] >> shift;
+        atomicOr(&occ[b >> 5], 1u << (b & 31));
+    }
+}
+
+// One warp per slot: origin, outward-rounded FP32 box, FP32 vertices and the
+// slot's rounding-error bound.
+__global__ void split_copy_kernel(const vs_box* __restrict__ box, int64_t M, const int32_t* __restrict__ geom_off,
+                                  const int32_t* __restrict__ part_off, const int32_t* __restrict__ ring_off,
+                                  const double2* __restrict__ xy, double2* __restrict__ origin,
+                                  float4* __restrict__ box32, float* __restrict__ err32, float2* __restrict__ xy32) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const double u64 = 1.1102230246251565e-16;  // 2^-53
+    for (int64_t s = warp; s < M; s += nw) {
+        const vs_box b = box[s];
+        const bool ok = b.minx <= b.maxx;
+        const double ox = ok ? 0.5 * b.minx + 0.5 * b.maxx : 0.0;
+        const double oy = ok ? 0.5 * b.miny + 0.5 * b.maxy : 0.0;
+        const int32_t c0 = ring_off[part_off[geom_off[s]]], c1 = ring_off[part_off[geom_off[s + 1]]];
+        double emax = 0.0;
+        for (int32_t c = c0 + lane; c < c1; c += 32) {
+            const double2 v = xy[c];
+            const double dx = v.x - ox, dy = v.y - oy;
+            const float fx = __double2float_rn(dx), fy = __double2float_rn(dy);
+            xy32[c] = make_float2(fx, fy);
+            const double ex = fabs((double)fx - dx) + fabs(dx) * u64;
+            const double ey = fabs((double)fy - dy) + fabs(dy) * u64;
+            emax = fmax(emax, fmax(ex, ey));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+        if (lane == 0) {
+            origin[s] = make_double2(ox, oy);
+            err32[s] = __double2float_ru(emax * (1.0 + 1e-6));
+            if (ok) {
+                const double a = b.minx - ox, c = b.miny - oy, d = b.maxx - ox, e = b.maxy - oy;
+                box32[s] = make_float4(__double2float_rd(a - fabs(a) * u64), __double2float_rd(c - fabs(c) * u64),
+                                       __double2float_ru(d + fabs(d) * u64), __double2float_ru(e + fabs(e) * u64));
+            } else {
+                box32[s] = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ RMI train ---
+__global__ void rmi_samples_kernel(const uint32_t* __restrict__ keys, int64_t n, int S, double key_lo, double key_scale,
+                                   float* __restrict__ xs, float* __restrict__ ts) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        const int64_t i = (int64_t)((double)s * (double)n / (double)S);
+        xs[s] = __double2float_rn(((double)keys[i] - key_lo) * key_scale);
+        ts[s] = (float)((double)i / (double)n);
+    }
+}
+
+// Full-batch gradient of the mean squared error over S samples.  A warp takes
+// one sample at a time with lane j owning hidden unit j; each block sums its
+// warps' gradients in shared memory and writes one partial row.
+__global__ void __launch_bounds__(kThreads) rmi_grad_kernel(const float* __restrict__ P, const float* __restrict__ xs,
+                                                            const float* __restrict__ ts, int S,
+                                                            float* __restrict__ partial, float* __restrict__ loss) {
+    __shared__ float g[kRmiP];
+    for (int i = threadIdx.x; i < kRmiP; i += blockDim.x) g[i] = 0.f;
+    __syncthreads();
+    const int j = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const float w1 = P[kOffW1 + j], b1 = P[kOffB1 + j], b2 = P[kOffB2 + j], w3 = P[kOffW3 + j], b3 = P[kOffB3];
+    float row[kRmiHidden], col[kRmiHidden], grow[kRmiHidden];
+#pragma unroll
+    for (int k = 0; k < kRmiHidden; ++k) {
+        row[k] = P[kOffW2 + j * kRmiHidden + k];
+        col[k] = P[kOffW2 + k * kRmiHidden + j];
+        grow[k] = 0.f;
+    }
+    float gw1 = 0.f, gb1 = 0.f, gb2 = 0.f, gw3 = 0.f, gb3 = 0.f, l2 = 0.f;
+    const float inv = 1.0f / (float)S;
+    for (int s = warp; s < S; s += nwarps) {
+        const float x = xs[s], t = ts[s];
+        const float z1 = fmaf(w1, x, b1);
+        const float h1 = fmaxf(z1, 0.f);
+        float z2 = b2;
+#pragma unroll
+        for (int k = 0; k < kRmiHidden; ++k) z2 = fmaf(row[k], __shfl_sync(0xffffffffu, h1, k), z2);
+        const float h2 = fmaxf(z2, 0.f);
+        float y = w3 * h2;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        y += b3;
+        const float err = y - t;
+        const float gy = 2.f * err * inv;
+        l2 += err * err * inv;
+        gw3 += gy * h2;
+        gb3 += gy;
+        const float d2 = z2 > 0.f ? gy * w3 : 0.f;
+        gb2 += d2;
+#pragma unroll
+        for (int k = 0; k < kRmiHidden; ++k) grow[k] = fmaf(d2, __shfl_sync(0xffffffffu, h1, k), grow[k]);
+        float dh1 = 0.f;
+#pragma unroll
+        for (int i = 0; i < kRmiHidden; ++i) dh1 = fmaf(__shfl_sync(0xffffffffu, d2, i), col[i], dh1);
+        const float d1 = z1 > 0.f ? dh1 : 0.f;
+        gw1 += d1 * x;
+        gb1 += d1;
+    }
+    atomicAdd(&g[kOffW1 + j], gw1);
+    atomicAdd(&g[kOffB1 + j], gb1);
+    atomicAdd(&g[kOffB2 + j], gb2);
+    atomicAdd(&g[kOffW3 + j], gw3);
+#pragma unroll
+    for (int k = 0; k < kRmiHidden; ++k) atomicAdd(&g[kOffW2 + j * kRmiHidden + k], grow[k]);
+    if (j == 0) {
+        atomicAdd(&g[kOffB3], gb3);
+        atomicAdd(loss, l2);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRmiP; i += blockDim.x) partial[(int64_t)blockIdx.x * kRmiP + i] = g[i];
+}
+
+__global__ void rmi_adam_kernel(float* __restrict__ P, float* __restrict__ m1, float* __restrict__ m2,
+                                const float* __restrict__ partial, int G, int step, float lr) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kRmiP) return;
+    float g = 0.f;
+    for (int b = 0; b < G; ++b) g += partial[(int64_t)b * kRmiP + p];
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float m = b1 * m1[p] + (1.f - b1) * g;
+    const float v = b2 * m2[p] + (1.f - b2) * g * g;
+    m1[p] = m;
+    m2[p] = v;
+    const float mh = m / (1.f - powf(b1, (float)step));
+    const float vh = v / (1.f - powf(b2, (float)step));
+    P[p] -= lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+__global__ void rmi_pack_kernel(const float* __restrict__ P, RmiModel* __restrict__ m, double key_lo, double key_scale,
+                                int n_leaves, int n_keys) {
+    for (int i = threadIdx.x; i < kRmiHidden * kRmiHidden; i += blockDim.x) m->w2[i] = P[kOffW2 + i];
+    for (int i = threadIdx.x; i < kRmiHidden; i += blockDim.x) {
+        m->w1[i] = P[kOffW1 + i];
+        m->b1[i] = P[kOffB1 + i];
+        m->b2[i] = P[kOffB2 + i];
+        m->w3[i] = P[kOffW3 + i];
+    }
+    if (threadIdx.x == 0) {
+        m->b3 = P[kOffB3];
+        m->key_lo = key_lo;
+        m->key_scale = key_scale;
+        m->n_leaves = n_leaves;
+        m->n_keys = n_keys;
+    }
+}
+
+// Route every stored key through the inference path (one warp per key).
+__global__ void __launch_bounds__(kThreads) rmi_route_kernel(const RmiModel* __restrict__ model,
+                                                             const uint32_t* __restrict__ keys, int64_t n,
+                                                             uint32_t* __restrict__ leaf_of) {
+    __shared__ RmiShared sm;
+    rmi_load_shared(&sm, model);
+    __syncthreads();
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < n; i += nw) {
+        const float y = rmi_root_warp(&sm, rmi_input(keys[i], &sm));
+        if ((threadIdx.x & 31) == 0) leaf_of[i] = (uint32_t)rmi_leaf(&sm, y);
+    }
+}
+
+__global__ void rmi_leaf_sums_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ leaf_of, int64_t n,
+                                     double key_lo, double* __restrict__ sums) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t l = leaf_of[i];
+        atomicAdd(&sums[3 * l + 0], 1.0);
+        atomicAdd(&sums[3 * l + 1], (double)keys[i] - key_lo);
+        atomicAdd(&sums[3 * l + 2], (double)i);
+    }
+}
+
+__global__ void rmi_leaf_cov_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ leaf_of, int64_t n,
+                                    double key_lo, const double* __restrict__ sums, double* __restrict__ cov) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t l = leaf_of[i];
+        const double c = sums[3 * l];
+        const double mx = sums[3 * l + 1] / c, my = sums[3 * l + 2] / c;
+        const double dx = (double)keys[i] - key_lo - mx, dy = (double)i - my;
+        atomicAdd(&cov[2 * l + 0], dx * dy);
+        atomicAdd(&cov[2 * l + 1], dx * dx);
+    }
+}
+
+__global__ void rmi_leaf_fit_kernel(const double* __restrict__ sums, const double* __restrict__ cov, int nl,
+                                    double2* __restrict__ ab, int2* __restrict__ err) {
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += gridDim.x * blockDim.x) {
+        const double c = sums[3 * l];
+        double a = 0.0, b = 0.0;
+        if (c > 0) {
+            const double mx = sums[3 * l + 1] / c, my = sums[3 * l + 2] / c;
+            b = cov[2 * l + 1] > 0 ? cov[2 * l + 0] / cov[2 * l + 1] : 0.0;
+            a = my - b * mx;
+        }
+        ab[l] = make_double2(a, b);
+        err[l] = make_int2(0x7fffffff, -0x7fffffff);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) rmi_err_kernel(const RmiModel* __restrict__ model,
+                                                           const uint32_t* __restrict__ keys,
+                                                           const uint32_t* __restrict__ leaf_of, int64_t n,
+                                                           const double2* __restrict__ ab, int2* __restrict__ err) {
+    __shared__ RmiShared sm;
+    rmi_load_shared(&sm, model);
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t l = leaf_of[i];
+        const long long pred = rmi_predict(ab[l], keys[i], &sm);
+        long long e = (long long)i - pred;
+        e = e < -0x7ffffffe ? -0x7ffffffe : (e > 0x7ffffffe ? 0x7ffffffe : e);
+        atomicMin(&err[l].x, (int)e);
+        atomicMax(&err[l].y, (int)e);
+    }
+}
+
+__global__ void rmi_window_stats_kernel(const uint32_t* __restrict__ leaf_of, int64_t n, const int2* __restrict__ err,
+                                        unsigned long long* __restrict__ acc) {
+    unsigned long long s = 0, mx = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int2 e = err[leaf_of[i]];
+        const unsigned long long w = (unsigned long long)((long long)e.y - (long long)e.x + 1);
+        s += w;
+        mx = mx > w ? mx : w;
+    }
+    s = warp_sum(s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = mx > t ? mx : t;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc[0], s);
+        atomicMax(&acc[1], mx);
+    }
+}
+
+// ----------------------------------------------------------------- query ---
+struct LearnedArgs {
+    const double* px;
+    const double* py;
+    const uint32_t* order;
+    const uint32_t* keys;      // sorted level-16 keys
+    const uint32_t* n_sorted;
+    int L;
+    int occ_shift;             // cell key >> occ_shift = occupancy bit
+    const uint32_t* occ;
+    const uint32_t* cell_keys;
+    const uint32_t* cell_start;
+    const uint32_t* entries;
+    int64_t n_cells;
+    const RmiModel* model;
+    const double2* leaf_ab;
+    const int2* leaf_err;
+    const vs_box* boxes;       // FP64 slot boxes (R-tree level 0)
+    const double2* origin;
+    const float4* box32;
+    const float* err32;
+    const float2* xy32;
+    const double2* xy;
+    const int32_t* item_geom;
+    const int32_t* geom_off;
+    const int32_t* part_off;
+    const int32_t* ring_off;
+    int accept_mask;
+    PairSink sink;
+    unsigned long long* counters;
+};
+
+// One edge in FP32 on tile-relative coordinates.  Returns false when some
+// decision the exact walk needs lies within the rounding-error bound `t`
+// (the caller then re-decides the edge in FP64 / exactly); otherwise applies
+// the same decision the exact walk would (the point cannot be on this edge).
+__device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, float by, float px, float py, float t,
+                                               bool& inside) {
+    const float A2 = __fsub_rn(ay, py), B2 = __fsub_rn(by, py);
+    if (fabsf(A2) <= t || fabsf(B2) <= t) return false;
+    const bool sA = A2 > 0.f, sB = B2 > 0.f;
+    if (sA == sB) return true;  // py strictly outside the edge's y-range
+    const float A1 = __fsub_rn(ax, px), B1 = __fsub_rn(bx, px);
+    if (A1 > t && B1 > t) {  // edge strictly right of the point: the +x ray crosses it
+        inside = !inside;
+        return true;
+    }
+    if (A1 < -t && B1 < -t) return true;  // strictly left
+    const float l = __fmul_rn(A1, B2), r = __fmul_rn(A2, B1);
+    const float det = __fsub_rn(l, r);
+    const float m = fmaxf(fmaxf(fabsf(A1), fabsf(A2)), fmaxf(fabsf(B1), fabsf(B2)));
+    const float e = __fmaf_ru(m, 6.0e-8f, t);
+    const float S = __fadd_ru(__fadd_ru(fabsf(A1), fabsf(A2)), __fadd_ru(fabsf(B1), fabsf(B2)));
+    float bound = __fmaf_ru(3.6e-7f, __fadd_ru(fabsf(l), fabsf(r)), __fmaf_ru(S, e, __fmul_ru(2.0f, __fmul_ru(e, e))));
+    bound = __fmaf_ru(bound, 1.01f, 1e-30f);
+    if (det > bound) {
+        if (sB) inside = !inside;  // o > 0 and, since the edge crosses, by > ay <=> sB
+        return true;
+    }
+    if (det < -bound) {
+        if (!sB) inside = !inside;
+        return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ int ring_location_split(double px, double py, float qx, float qy, float t,
+                                                   const float2* __restrict__ xy32, const double2* __restrict__ xy,
+                                                   int start, int end, unsigned& n_exact, unsigned& n32,
+                                                   unsigned& n64) {
+    if (end - start < 2) return LOC_OUTSIDE;
+    bool inside = false;
+    float2 a = xy32[end - 1];
+    int ia = end - 1;
+    for (int i = start; i < end; ++i) {
+        const float2 b = xy32[i];
+        if (edge_step_fp32(a.x, a.y, b.x, b.y, qx, qy, t, inside)) {
+            ++n32;
+        } else {
+            ++n64;
+            const double2 A = xy[ia], B = xy[i];
+            if (edge_step_exact(A.x, A.y, B.x, B.y, px, py, inside, n_exact)) return LOC_BOUNDARY;
+        }
+        a = b;
+        ia = i;
+    }
+    return inside ? LOC_INTERIOR : LOC_OUTSIDE;
+}
+
+__device__ __forceinline__ int geometry_location_split(double px, double py, float qx, float qy, float t,
+                                                       const LearnedArgs& a, int g, unsigned& n_exact, unsigned& n32,
+                                                       unsigned& n64) {
+    const int p0 = a.geom_off[g], p1 = a.geom_off[g + 1];
+    for (int part = p0; part < p1; ++part) {
+        bool inside = false;
+        const int r0 = a.part_off[part], r1 = a.part_off[part + 1];
+        for (int ring = r0; ring < r1; ++ring) {
+            const int k = ring_location_split(px, py, qx, qy, t, a.xy32, a.xy, a.ring_off[ring], a.ring_off[ring + 1],
+                                              n_exact, n32, n64);
+            if (k == LOC_BOUNDARY) return LOC_BOUNDARY;
+            if (k == LOC_INTERIOR) inside = !inside;
+        }
+        if (inside) return LOC_INTERIOR;
+    }
+    return LOC_OUTSIDE;
+}
+
+__global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArgs a) {
+    __shared__ RmiShared sm;
+    __shared__ int2 s_buf[kOutBuf];
+    __shared__ unsigned s_cnt, s_n;
+    __shared__ unsigned long long s_base;
+    rmi_load_shared(&sm, a.model);
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    const BlockOut out{s_buf, &s_cnt};
+    const int lane = threadIdx.x & 31;
+    const int64_t n = (int64_t)*a.n_sorted;
+    const int cell_shift = 32 - 2 * a.L;
+    unsigned long long n_cand = 0, n_binsearch = 0;
+    unsigned n_exact = 0, n32 = 0, n64 = 0;
+
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const bool active = i < n;
+        uint32_t cell = 0xffffffffu;
+        bool need = false;
+        if (active) {
+            cell = a.keys[i] >> cell_shift;
+            const uint32_t ob = cell >> a.occ_shift;
+            need = (a.occ[ob >> 5] >> (ob & 31)) & 1u;
+        }
+        // Phase 1: one RMI lookup per distinct cell of the warp.
+        uint32_t lo = 0, hi = 0;
+        unsigned pending = __ballot_sync(0xffffffffu, need);
+        while (pending) {
+            const int leader = __ffs(pending) - 1;
+            const uint32_t k = __shfl_sync(0xffffffffu, cell, leader);
+            const unsigned peers = __ballot_sync(0xffffffffu, need && cell == k);
+            pending &= ~peers;
+            const float y = rmi_root_warp(&sm, rmi_input(k, &sm));
+            const int leaf = rmi_leaf(&sm, y);
+            const int2 er = a.leaf_err[leaf];
+            long long found = -1;
+            if (er.x <= er.y) {
+                const long long pred = rmi_predict(a.leaf_ab[leaf], k, &sm);
+                long long wlo = pred + er.x, whi = pred + er.y;
+                wlo = wlo < 0 ? 0 : wlo;
+                whi = whi > a.n_cells - 1 ? a.n_cells - 1 : whi;
+                if (whi - wlo < 256) {
+                    for (long long b0 = wlo; b0 <= whi; b0 += 32) {
+                        const long long j = b0 + lane;
+                        const uint32_t kk = j <= whi ? a.cell_keys[j] : ~k;
+                        const unsigned m = __ballot_sync(0xffffffffu, kk == k);
+                        if (m) {
+                            found = b0 + __ffs(m) - 1;
+                            break;
+                        }
+                    }
+                } else {
+                    ++n_binsearch;
+                    long long l0 = wlo, h0 = whi + 1;
+                    while (l0 < h0) {
+                        const long long mid = (l0 + h0) >> 1;
+                        if (a.cell_keys[mid] < k) l0 = mid + 1;
+                        else h0 = mid;
+                    }
+                    if (l0 <= whi && a.cell_keys[l0] == k) found = l0;
+                }
+            }
+            if (found >= 0 && ((peers >> lane) & 1u)) {
+                lo = a.cell_start[found];
+                hi = a.cell_start[found + 1];
+            }
+        }
+        // Phase 2: each lane scans its own cell's polygons.
+        if (lo < hi) {
+            const int32_t row = (int32_t)a.order[i];
+            const double x = a.px[row], y = a.py[row];
+            for (uint32_t e = lo; e < hi; ++e) {
+                const int slot = (int)a.entries[e];
+                const double2 o = a.origin[slot];
+                const float qx = __double2float_rn(x - o.x), qy = __double2float_rn(y - o.y);
+                const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
+                const float4 b32 = a.box32[slot];
+                if (__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
+                    __fsub_rd(qy, dp) > b32.w)
+                    continue;  // certainly outside the box
+                const vs_box bb = a.boxes[slot];
+                if (!(x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy)) continue;
+                ++n_cand;
+                int loc = 0;
+                if (a.accept_mask) {
+                    const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
+                    loc = geometry_location_split(x, y, qx, qy, t, a, slot, n_exact, n32, n64);
+                }
+                if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) emit(out, a.sink, row, a.item_geom[slot]);
+            }
+        }
+        flush(out, a.sink, &s_base, &s_n);
+    }
+    add_counter(a.counters, 5, n_cand);
+    add_counter(a.counters, 1, n_exact);
+    add_counter(a.counters, 2, n32);
+    add_counter(a.counters, 3, n64);
+    add_counter(a.counters, 6, n_binsearch);
+}
+
+template <class T>
+int dalloc(T** p, size_t n, int64_t& bytes) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        set_error("cudaMalloc(%zu bytes) failed: %s", n * sizeof(T), cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? VS_E_OOM : VS_E_CUDA;
+    }
+    bytes += (int64_t)(n * sizeof(T));
+    return VS_OK;
+}
+
+int train_rmi(vs_context* ctx, vs_index* idx, int steps) {
+    LearnedIndex& li = idx->learned;
+    cudaStream_t s = ctx->stream;
+    const int64_t n = li.n_cells;
+    // key range and quantile knots (33 keys read back)
+    std::vector<uint32_t> q(33);
+    for (int j = 0; j <= 32; ++j) {
+        const int64_t pos = (int64_t)((double)j * (double)(n - 1) / 32.0);
+        VS_CUDA_TRY(cudaMemcpyAsync(&q[j], li.cell_keys + pos, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    }
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    const double key_lo = (double)q[0];
+    const double span = (double)q[32] - key_lo;
+    const double key_scale = span > 0 ? 1.0 / span : 0.0;
+    // Initial root: a piecewise-linear interpolant of the key CDF through the
+    // 33 quantile knots (h1_j = relu(x - c_j), W2 = I, w3_j = slope change).
+    std::vector<float> P(kRmiP, 0.f);
+    std::vector<double> c(33), yk(33);
+    for (int j = 0; j <= 32; ++j) {
+        c[j] = ((double)q[j] - key_lo) * key_scale;
+        yk[j] = (double)j / 32.0;
+    }
+    double prev_slope = 0.0;
+    for (int j = 0; j < 32; ++j) {
+        const double dx = c[j + 1] - c[j];
+        const double slope = dx > 1e-12 ? (yk[j + 1] - yk[j]) / dx : 0.0;
+        P[kOffW1 + j] = 1.0f;
+        P[kOffB1 + j] = (float)-c[j];
+        P[kOffW3 + j] = (float)(slope - prev_slope);
+        prev_slope = slope;
+        P[kOffW2 + j * kRmiHidden + j] = 1.0f;
+        P[kOffB2 + j] = 0.0f;
+    }
+    P[kOffB3] = 0.0f;
+    const int S = (int)std::min<int64_t>(n, 16384);
+    Scratch<float> dP, m1, m2, xs, ts, part, loss;
+    VS_TRY(dP.alloc(kRmiP, s));
+    VS_TRY(m1.alloc(kRmiP, s));
+    VS_TRY(m2.alloc(kRmiP, s));
+    VS_TRY(xs.alloc(S, s));
+    VS_TRY(ts.alloc(S, s));
+    VS_TRY(part.alloc((size_t)kTrainBlocks * kRmiP, s));
+    VS_TRY(loss.alloc(1, s));
+    VS_CUDA_TRY(cudaMemcpyAsync(dP.p, P.data(), kRmiP * sizeof(float), cudaMemcpyHostToDevice, s));
+    VS_CUDA_TRY(cudaMemsetAsync(m1.p, 0, kRmiP * sizeof(float), s));
+    VS_CUDA_TRY(cudaMemsetAsync(m2.p, 0, kRmiP * sizeof(float), s));
+    rmi_samples_kernel<<<div_up(S, 256), 256, 0, s>>>(li.cell_keys, n, S, key_lo, key_scale, xs.p, ts.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    for (int step = 1; step <= steps; ++step) {
+        VS_CUDA_TRY(cudaMemsetAsync(loss.p, 0, sizeof(float), s));
+        rmi_grad_kernel<<<kTrainBlocks, kThreads, 0, s>>>(dP.p, xs.p, ts.p, S, part.p, loss.p);
+        const float lr = 2e-3f * (step < steps / 2 ? 1.0f : 0.3f);
+        rmi_adam_kernel<<<div_up(kRmiP, 256), 256, 0, s>>>(dP.p, m1.p, m2.p, part.p, kTrainBlocks, step, lr);
+    }
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_CUDA_TRY(cudaMemcpyAsync(&li.rmi_final_loss, loss.p, sizeof(float), cudaMemcpyDeviceToHost, s));
+    int64_t& bytes = idx->device_bytes;
+    if (!li.model) VS_TRY(dalloc(&li.model, 1, bytes));
+    rmi_pack_kernel<<<1, 256, 0, s>>>(dP.p, li.model, key_lo, key_scale, li.n_leaves, (int)n);
+    VS_CUDA_TRY(cudaGetLastError());
+    return VS_OK;
+}
+
+int fit_leaves(vs_context* ctx, vs_index* idx) {
+    LearnedIndex& li = idx->learned;
+    cudaStream_t s = ctx->stream;
+    const int64_t n = li.n_cells;
+    const int nl = li.n_leaves;
+    int64_t& bytes = idx->device_bytes;
+    VS_TRY(dalloc(&li.leaf_ab, (size_t)nl, bytes));
+    VS_TRY(dalloc(&li.leaf_err, (size_t)nl, bytes));
+    Scratch<uint32_t> leaf_of;
+    Scratch<double> sums, cov;
+    Scratch<unsigned long long> acc;
+    VS_TRY(leaf_of.alloc((size_t)n, s));
+    VS_TRY(sums.alloc((size_t)3 * nl, s));
+    VS_TRY(cov.alloc((size_t)2 * nl, s));
+    VS_TRY(acc.alloc(2, s));
+    VS_CUDA_TRY(cudaMemsetAsync(sums.p, 0, 3 * nl * sizeof(double), s));
+    VS_CUDA_TRY(cudaMemsetAsync(cov.p, 0, 2 * nl * sizeof(double), s));
+    VS_CUDA_TRY(cudaMemsetAsync(acc.p, 0, 2 * sizeof(unsigned long long), s));
+    RmiModel hm;
+    VS_CUDA_TRY(cudaMemcpyAsync(&hm, li.model, sizeof(RmiModel), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    rmi_route_kernel<<<grid_for(n * 32, kThreads, 8), kThreads, 0, s>>>(li.model, li.cell_keys, n, leaf_of.p);
+    rmi_leaf_sums_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, hm.key_lo, sums.p);
+    rmi_leaf_cov_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, hm.key_lo, sums.p, cov.p);
+    rmi_leaf_fit_kernel<<<div_up(nl, 256), 256, 0, s>>>(sums.p, cov.p, nl, li.leaf_ab, li.leaf_err);
+    rmi_err_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(li.model, li.cell_keys, leaf_of.p, n, li.leaf_ab,
+                                                             li.leaf_err);
+    rmi_window_stats_kernel<<<grid_for(n, 256), 256, 0, s>>>(leaf_of.p, n, li.leaf_err, acc.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    unsigned long long h[2];
+    VS_CUDA_TRY(cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    li.mean_window = n > 0 ? (float)((double)h[0] / (double)n) : 0.f;
+    li.max_window = (int32_t)h[1];
+    return VS_OK;
+}
+
+}  // namespace
+
+void free_learned_index(vs_index* idx) {
+    LearnedIndex& li = idx->learned;
+    cudaFree(li.cell_keys);
+    cudaFree(li.cell_start);
+    cudaFree(li.entries);
+    cudaFree(li.occ);
+    cudaFree(li.model);
+    cudaFree(li.leaf_ab);
+    cudaFree(li.leaf_err);
+    cudaFree(li.origin);
+    cudaFree(li.box32);
+    cudaFree(li.err32);
+    cudaFree(li.xy32);
+    li = LearnedIndex{};
+}
+
+int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* opts) {
+    LearnedIndex& li = idx->learned;
+    cudaStream_t s = ctx->stream;
+    const int64_t M = idx->n_geoms;
+    int64_t& bytes = idx->device_bytes;
+    if (M == 0 || !(idx->h_frame[0] <= idx->h_frame[2])) return VS_OK;  // nothing to index: joins use the R-tree
+    const vs_box* boxes = idx->nodes;  // level 0 = slot boxes
+    // 1. grid level
+    int L = opts ? opts->cell_level : 0;
+    if (L <= 0) {
+        Scratch<double> acc;
+        VS_TRY(acc.alloc(2, s));
+        VS_CUDA_TRY(cudaMemsetAsync(acc.p, 0, 2 * sizeof(double), s));
+        box_side_kernel<<<grid_for(M, 256), 256, 0, s>>>(boxes, M, acc.p);
+        double h[2];
+        VS_CUDA_TRY(cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+        const double mean_side = h[1] > 0 ? h[0] / h[1] : 1.0;
+        const double extent = std::max(idx->h_frame[2] - idx->h_frame[0], idx->h_frame[3] - idx->h_frame[1]);
+        L = mean_side > 0 ? (int)std::lround(std::log2(extent / mean_side)) : 15;
+    }
+    L = std::max(1, std::min(L, 15));
+    // 2. registrations; coarsen while the entry count is out of proportion
+    Scratch<uint32_t> cnt;
+    Scratch<unsigned long long> tot;
+    VS_TRY(cnt.alloc((size_t)M, s));
+    VS_TRY(tot.alloc(1, s));
+    unsigned long long E = 0;
+    for (;;) {
+        VS_CUDA_TRY(cudaMemsetAsync(tot.p, 0, sizeof(unsigned long long), s));
+        cell_count_kernel<<<grid_for(M, 256), 256, 0, s>>>(boxes, M, idx->frame, L, cnt.p, tot.p);
+        VS_CUDA_TRY(cudaMemcpyAsync(&E, tot.p, sizeof(E), cudaMemcpyDeviceToHost, s));
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (L <= 1 || E <= (unsigned long long)(16 * M + (1 << 20))) break;
+        --L;
+    }
+    if (E >= 0x7fffffffull) {
+        set_error("learned index: too many cell registrations (%llu)", E);
+        return VS_E_ARG;
+    }
+    li.level = L;
+    li.n_entries = (int64_t)E;
+    Scratch<uint32_t> off, keys, flag;
+    VS_TRY(off.alloc((size_t)M, s));
+    VS_TRY(keys.alloc((size_t)E, s));
+    VS_TRY(flag.alloc((size_t)E, s));
+    VS_TRY(dalloc(&li.entries, (size_t)E, bytes));
+    VS_TRY(exclusive_scan_u32(cnt.p, off.p, M, nullptr, s));
+    cell_emit_kernel<<<grid_for(M, 256), 256, 0, s>>>(boxes, M, idx->frame, L, off.p, keys.p, li.entries);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(radix_sort_u32_u32(keys.p, li.entries, (int64_t)E, 2 * L, s));
+    // 3. unique cells + CSR
+    Scratch<uint32_t> ncell;
+    VS_TRY(ncell.alloc(1, s));
+    cell_flag_kernel<<<grid_for(E, 256), 256, 0, s>>>(keys.p, (int64_t)E, flag.p);
+    VS_TRY(exclusive_scan_u32(flag.p, flag.p, (int64_t)E, ncell.p, s));
+    uint32_t nc = 0;
+    VS_CUDA_TRY(cudaMemcpyAsync(&nc, ncell.p, sizeof(nc), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    li.n_cells = nc;
+    VS_TRY(dalloc(&li.cell_keys, (size_t)nc, bytes));
+    VS_TRY(dalloc(&li.cell_start, (size_t)nc + 1, bytes));
+    cell_compact_kernel<<<grid_for(E, 256), 256, 0, s>>>(keys.p, flag.p, (int64_t)E, li.cell_keys, li.cell_start);
+    const uint32_t Eu = (uint32_t)E;
+    VS_CUDA_TRY(cudaMemcpyAsync(li.cell_start + nc, &Eu, sizeof(Eu), cudaMemcpyHostToDevice, s));
+    // 4. occupancy bitmap
+    li.occ_level = std::min(L, 11);
+    const int64_t occ_bits = 1ll << (2 * li.occ_level);
+    VS_TRY(dalloc(&li.occ, (size_t)((occ_bits + 31) / 32), bytes));
+    VS_CUDA_TRY(cudaMemsetAsync(li.occ, 0, (size_t)((occ_bits + 31) / 32) * sizeof(uint32_t), s));
+    occ_kernel<<<grid_for(nc, 256), 256, 0, s>>>(li.cell_keys, nc, 2 * (L - li.occ_level), li.occ);
+    VS_CUDA_TRY(cudaGetLastError());
+    // 5. RMI
+    li.n_leaves = (opts && opts->rmi_leaves > 0) ? opts->rmi_leaves : 4096;
+    const int steps = (opts && opts->rmi_train_steps > 0) ? opts->rmi_train_steps : 300;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    int st = train_rmi(ctx, idx, steps);
+    if (st == VS_OK) st = fit_leaves(ctx, idx);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&li.rmi_train_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    VS_TRY(st);
+    // 6. FP32 tile-relative copies
+    VS_TRY(dalloc(&li.origin, (size_t)M, bytes));
+    VS_TRY(dalloc(&li.box32, (size_t)M, bytes));
+    VS_TRY(dalloc(&li.err32, (size_t)M, bytes));
+    VS_TRY(dalloc(&li.xy32, (size_t)std::max<int64_t>(idx->n_coords, 1), bytes));
+    split_copy_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
+                                                            idx->xy, li.origin, li.box32, li.err32, li.xy32);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    idx->has_learned = true;
+    return VS_OK;
+}
+
+int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, int32_t* d_left,
+                        int32_t* d_right, int64_t capacity) {
+    const LearnedIndex& li = idx->learned;
+    QueryOrder q;
+    VS_TRY(prepare_queries(ctx, idx, pts, q));
+    LearnedArgs a{};
+    a.px = pts->d_x;
+    a.py = pts->d_y;
+    a.order = q.order.p;
+    a.keys = q.keys.p;
+    a.n_sorted = q.n_valid.p;
+    a.L = li.level;
+    a.occ_shift = 2 * (li.level - li.occ_level);
+    a.occ = li.occ;
+    a.cell_keys = li.cell_keys;
+    a.cell_start = li.cell_start;
+    a.entries = li.entries;
+    a.n_cells = li.n_cells;
+    a.model = li.model;
+    a.leaf_ab = li.leaf_ab;
+    a.leaf_err = li.leaf_err;
+    a.boxes = idx->nodes;
+    a.origin = li.origin;
+    a.box32 = li.box32;
+    a.err32 = li.err32;
+    a.xy32 = li.xy32;
+    a.xy = idx->xy;
+    a.item_geom = idx->item_geom;
+    a.geom_off = idx->geom_off;
+    a.part_off = idx->part_off;
+    a.ring_off = idx->ring_off;
+    a.accept_mask = accept_mask;
+    a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
+    a.counters = ctx->d_counters;
+    join_learned_kernel<<<grid_for(pts->n, kThreads, 8), kThreads, 0, ctx->stream>>>(a);
+    VS_CUDA_TRY(cudaGetLastError());
+    return VS_OK;
+}
+
 }  // namespace vs

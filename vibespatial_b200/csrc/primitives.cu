@@ -129,9 +129,9 @@ constexpr int kRsRounds = 16;
 constexpr int kRsTile = kRsThreads * kRsRounds;  // 4096 keys per tile
 constexpr int kRadix = 256;
 
-__global__ void __launch_bounds__(kRsThreads) rs_histogram_kernel(const uint64_t* __restrict__ keys, int64_t n,
-                                                                  int shift, uint32_t* __restrict__ hist,
-                                                                  int ntiles) {
+template <class K>
+__global__ void __launch_bounds__(kRsThreads) rs_histogram_kernel(const K* __restrict__ keys, int64_t n, int shift,
+                                                                  uint32_t* __restrict__ hist, int ntiles) {
     __shared__ uint32_t h[kRadix];
     h[threadIdx.x] = 0;
     __syncthreads();
@@ -145,13 +145,11 @@ __global__ void __launch_bounds__(kRsThreads) rs_histogram_kernel(const uint64_t
     hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t* __restrict__ kin,
-                                                                const uint32_t* __restrict__ vin,
-                                                                uint64_t* __restrict__ kout,
-                                                                uint32_t* __restrict__ vout, int64_t n,
-                                                                int shift,
-                                                                const uint32_t* __restrict__ offsets,
-                                                                int ntiles) {
+template <class K>
+__global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                                K* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                                int64_t n, int shift,
+                                                                const uint32_t* __restrict__ offsets, int ntiles) {
     __shared__ uint32_t base[kRadix];
     __shared__ uint32_t wcnt[kRsWarps][kRadix];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -164,7 +162,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t* 
     for (int r = 0; r < kRsRounds; ++r) {
         const int64_t i = tile0 + (int64_t)r * kRsThreads + tid;
         const bool valid = i < n;
-        uint64_t key = 0;
+        K key = 0;
         uint32_t val = 0;
         unsigned d = kRadix;  // sentinel digit for out-of-range lanes
         if (valid) {
@@ -177,13 +175,11 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t* 
         if (valid && (__ffs(peers) - 1) == lane) wcnt[warp][d] = __popc(peers);
         __syncthreads();
         uint32_t acc = 0;
-        {
 #pragma unroll
-            for (int w = 0; w < kRsWarps; ++w) {
-                const uint32_t c = wcnt[w][tid];
-                wcnt[w][tid] = acc;
-                acc += c;
-            }
+        for (int w = 0; w < kRsWarps; ++w) {
+            const uint32_t c = wcnt[w][tid];
+            wcnt[w][tid] = acc;
+            acc += c;
         }
         __syncthreads();
         if (valid) {
@@ -199,6 +195,47 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t* 
     }
 }
 
+template <class K>
+int radix_sort_impl(K* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s) {
+    if (n <= 1) return VS_OK;
+    if (n > 0xffffffffLL) {
+        set_error("radix sort supports at most 2^32-1 items (got %lld)", (long long)n);
+        return VS_E_ARG;
+    }
+    const int max_bits = (int)(8 * sizeof(K));
+    if (key_bits <= 0 || key_bits > max_bits) key_bits = max_bits;
+    const int passes = (key_bits + 7) / 8;
+    const int ntiles = (int)((n + kRsTile - 1) / kRsTile);
+    Scratch<K> kalt;
+    Scratch<uint32_t> valt, hist;
+    VS_TRY(kalt.alloc((size_t)n, s));
+    VS_TRY(valt.alloc((size_t)n, s));
+    VS_TRY(hist.alloc((size_t)kRadix * ntiles, s));
+    K* ka = keys;
+    uint32_t* va = vals;
+    K* kb = kalt.p;
+    uint32_t* vb = valt.p;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        rs_histogram_kernel<K><<<ntiles, kRsThreads, 0, s>>>(ka, n, shift, hist.p, ntiles);
+        VS_CUDA_TRY(cudaGetLastError());
+        VS_TRY(exclusive_scan_u32(hist.p, hist.p, (int64_t)kRadix * ntiles, nullptr, s));
+        rs_scatter_kernel<K><<<ntiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist.p, ntiles);
+        VS_CUDA_TRY(cudaGetLastError());
+        K* tk = ka;
+        ka = kb;
+        kb = tk;
+        uint32_t* tv = va;
+        va = vb;
+        vb = tv;
+    }
+    if (ka != keys) {
+        VS_CUDA_TRY(cudaMemcpyAsync(keys, ka, (size_t)n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+        VS_CUDA_TRY(cudaMemcpyAsync(vals, va, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    }
+    return VS_OK;
+}
+
 }  // namespace
 
 int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* d_total, cudaStream_t s) {
@@ -209,42 +246,11 @@ int exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, uint64_t* d
 }
 
 int radix_sort_u64_u32(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s) {
-    if (n <= 1) return VS_OK;
-    if (n > 0xffffffffLL) {
-        set_error("radix sort supports at most 2^32-1 items (got %lld)", (long long)n);
-        return VS_E_ARG;
-    }
-    if (key_bits <= 0 || key_bits > 64) key_bits = 64;
-    const int passes = (key_bits + 7) / 8;
-    const int ntiles = (int)((n + kRsTile - 1) / kRsTile);
-    Scratch<uint64_t> kalt;
-    Scratch<uint32_t> valt, hist;
-    VS_TRY(kalt.alloc((size_t)n, s));
-    VS_TRY(valt.alloc((size_t)n, s));
-    VS_TRY(hist.alloc((size_t)kRadix * ntiles, s));
-    uint64_t* ka = keys;
-    uint32_t* va = vals;
-    uint64_t* kb = kalt.p;
-    uint32_t* vb = valt.p;
-    for (int p = 0; p < passes; ++p) {
-        const int shift = 8 * p;
-        rs_histogram_kernel<<<ntiles, kRsThreads, 0, s>>>(ka, n, shift, hist.p, ntiles);
-        VS_CUDA_TRY(cudaGetLastError());
-        VS_TRY(exclusive_scan_u32(hist.p, hist.p, (int64_t)kRadix * ntiles, nullptr, s));
-        rs_scatter_kernel<<<ntiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist.p, ntiles);
-        VS_CUDA_TRY(cudaGetLastError());
-        uint64_t* tk = ka;
-        ka = kb;
-        kb = tk;
-        uint32_t* tv = va;
-        va = vb;
-        vb = tv;
-    }
-    if (ka != keys) {
-        VS_CUDA_TRY(cudaMemcpyAsync(keys, ka, (size_t)n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
-        VS_CUDA_TRY(cudaMemcpyAsync(vals, va, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-    }
-    return VS_OK;
+    return radix_sort_impl<uint64_t>(keys, vals, n, key_bits, s);
+}
+
+int radix_sort_u32_u32(uint32_t* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s) {
+    return radix_sort_impl<uint32_t>(keys, vals, n, key_bits, s);
 }
 
 }  // namespace vs
