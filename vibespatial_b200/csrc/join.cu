@@ -73,6 +73,7 @@ __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ fr
     const double f0 = frame[0], f1 = frame[1], f2 = frame[2], f3 = frame[3];
     const double sx = f2 > f0 ? 4294967295.0 / (f2 - f0) : 0.0;
     const double sy = f3 > f1 ? 4294967295.0 / (f3 - f1) : 0.0;
+    uint32_t cnt = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += (int64_t)gridDim.x * blockDim.x) {
         const double x = p.d_x[i], y = p.d_y[i];
         const bool ok = (p.d_valid == nullptr || p.d_valid[i]) && x >= f0 && x <= f2 && y >= f1 && y <= f3;
@@ -83,8 +84,17 @@ __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ fr
         }
         keys[i] = k;
         idx[i] = (uint32_t)i;
-        const unsigned m = __ballot_sync(__activemask(), ok);
-        if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && m) atomicAdd(n_valid, (uint32_t)__popc(m));
+        cnt += ok ? 1u : 0u;
+    }
+    // one atomic per block
+    cnt = (uint32_t)warp_sum(cnt);
+    __shared__ uint32_t wsum[32];
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += wsum[w];
+        if (t) atomicAdd(n_valid, t);
     }
 }
 
@@ -290,7 +300,9 @@ int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
     VS_CUDA_TRY(cudaMemsetAsync(q.n_valid.p, 0, sizeof(uint32_t), s));
     point_sort_key_kernel<<<grid_for(n, 256, 16), 256, 0, s>>>(*pts, idx->frame, q.keys.p, q.order.p, q.n_valid.p);
     VS_CUDA_TRY(cudaGetLastError());
-    VS_TRY(radix_sort_u32_u32(q.keys.p, q.order.p, n, 32, s));
+    // Sorting by the top 24 key bits (a level-12 Hilbert cell) already makes
+    // a warp's 32 points spatially coherent; the low byte is left unsorted.
+    VS_TRY(radix_sort_u32_u32(q.keys.p, q.order.p, n, 32, s, 8));
     return VS_OK;
 }
 

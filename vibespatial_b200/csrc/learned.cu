@@ -526,28 +526,27 @@ __global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArg
             long long found = -1;
             if (er.x <= er.y) {
                 const long long pred = rmi_predict(a.leaf_ab[leaf], k, &sm);
-                long long wlo = pred + er.x, whi = pred + er.y;
-                wlo = wlo < 0 ? 0 : wlo;
-                whi = whi > a.n_cells - 1 ? a.n_cells - 1 : whi;
-                if (whi - wlo < 256) {
-                    for (long long b0 = wlo; b0 <= whi; b0 += 32) {
-                        const long long j = b0 + lane;
-                        const uint32_t kk = j <= whi ? a.cell_keys[j] : ~k;
-                        const unsigned m = __ballot_sync(0xffffffffu, kk == k);
-                        if (m) {
-                            found = b0 + __ffs(m) - 1;
-                            break;
-                        }
-                    }
-                } else {
-                    ++n_binsearch;
-                    long long l0 = wlo, h0 = whi + 1;
-                    while (l0 < h0) {
-                        const long long mid = (l0 + h0) >> 1;
-                        if (a.cell_keys[mid] < k) l0 = mid + 1;
-                        else h0 = mid;
-                    }
-                    if (l0 <= whi && a.cell_keys[l0] == k) found = l0;
+                long long lo0 = pred + er.x, hi0 = pred + er.y + 1;  // search [lo0, hi0)
+                lo0 = lo0 < 0 ? 0 : lo0;
+                hi0 = hi0 > a.n_cells ? a.n_cells : hi0;
+                if (hi0 - lo0 > 256) ++n_binsearch;
+                // 32-ary search: each round the lanes sample 32 evenly spaced
+                // keys; the count of samples below k narrows the range 32x.
+                while (hi0 - lo0 > 32) {
+                    const long long step = (hi0 - lo0 + 31) >> 5;
+                    const long long j = lo0 + (long long)lane * step;
+                    const bool below = j < hi0 && a.cell_keys[j] < k;
+                    const int c = __popc(__ballot_sync(0xffffffffu, below));
+                    const long long nlo = c == 0 ? lo0 : lo0 + (long long)(c - 1) * step + 1;
+                    const long long cap = lo0 + (long long)c * step + 1;
+                    hi0 = cap < hi0 ? cap : hi0;
+                    lo0 = nlo;
+                }
+                if (lo0 < hi0) {
+                    const long long j = lo0 + lane;
+                    const uint32_t kk = j < hi0 ? a.cell_keys[j] : ~k;
+                    const unsigned m = __ballot_sync(0xffffffffu, kk == k);
+                    if (m) found = lo0 + __ffs(m) - 1;
                 }
             }
             if (found >= 0 && ((peers >> lane) & 1u)) {

@@ -50,9 +50,9 @@ struct Scratch {
 int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* d_total, cudaStream_t s);
 int exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, uint64_t* d_total, cudaStream_t s);
 
-// Stable LSD radix sort of (key, value) pairs by the low `key_bits` bits of
-// key (8 bits per pass).  Sorted data ends in keys / vals.
-int radix_sort_u64_u32(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s);
-int radix_sort_u32_u32(uint32_t* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s);
+// Stable LSD radix sort of (key, value) pairs by key bits [begin_bit,
+// key_bits) (8 bits per pass).  Sorted data ends in keys / vals.
+int radix_sort_u64_u32(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s, int begin_bit = 0);
+int radix_sort_u32_u32(uint32_t* keys, uint32_t* vals, int64_t n, int key_bits, cudaStream_t s, int begin_bit = 0);
 
 }  // namespace vs
