@@ -71,6 +71,24 @@ int check_points(const vs_points* p) {
     return VS_OK;
 }
 
+int ensure_defer_capacity(vs_context* ctx, unsigned long long want) {
+    if (ctx->defer_cap >= want) return VS_OK;
+    if (ctx->defer_buf) {
+        VS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->defer_buf);
+        ctx->defer_buf = nullptr;
+        ctx->defer_cap = 0;
+    }
+    cudaError_t e = cudaMalloc((void**)&ctx->defer_buf, want * sizeof(int2));
+    if (e != cudaSuccess) {
+        ctx->defer_buf = nullptr;
+        set_error("cudaMalloc of the deferred-pair buffer (%llu pairs) failed: %s", want, cudaGetErrorString(e));
+        return VS_E_OOM;
+    }
+    ctx->defer_cap = want;
+    return VS_OK;
+}
+
 struct EventPair {
     cudaEvent_t a = nullptr, b = nullptr;
     EventPair() {
@@ -153,6 +171,7 @@ int vs_context_destroy(vs_context* ctx) {
     use_device(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->d_counters);
+    cudaFree(ctx->defer_buf);
     cudaFreeHost(ctx->h_counter);
     if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -265,18 +284,33 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
     VS_TRY(use_device(ctx->device));
     if (pts->n == 0 || idx->n_geoms == 0 || !(idx->h_frame[0] <= idx->h_frame[2])) return VS_OK;
     cudaStream_t s = ctx->stream;
-    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, 8 * sizeof(unsigned long long), s));
     EventPair ev;
-    cudaEventRecord(ev.a, s);
-    if (method == VS_METHOD_LEARNED)
-        VS_TRY(launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity));
-    else
-        VS_TRY(launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, d_left, d_right, capacity));
-    cudaEventRecord(ev.b, s);
-    VS_CUDA_TRY(cudaMemcpyAsync(ctx->h_counter, ctx->d_counters, 8 * sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost, s));
-    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    // Pairs the filters cannot certify go to the context's deferred buffer
+    // and are resolved exactly after the join kernel; if more were deferred
+    // than the buffer holds, the join runs once more with a buffer that fits.
+    unsigned long long want = (unsigned long long)(pts->n / 64 + 65536);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        VS_TRY(ensure_defer_capacity(ctx, want));
+        VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, 8 * sizeof(unsigned long long), s));
+        const DeferSink ds{ctx->defer_buf, ctx->defer_cap, &ctx->d_counters[7]};
+        cudaEventRecord(ev.a, s);
+        if (method == VS_METHOD_LEARNED)
+            VS_TRY(launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity, ds));
+        else
+            VS_TRY(launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, d_left, d_right, capacity, ds));
+        if (mask) VS_TRY(launch_resolve_deferred(ctx, idx, pts, mask, d_left, d_right, capacity, ds));
+        cudaEventRecord(ev.b, s);
+        VS_CUDA_TRY(cudaMemcpyAsync(ctx->h_counter, ctx->d_counters, 8 * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, s));
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (ctx->h_counter[7] <= ctx->defer_cap) break;
+        want = ctx->h_counter[7];
+    }
     const unsigned long long* c = ctx->h_counter;
+    if (c[7] > ctx->defer_cap) {
+        set_error("deferred-pair buffer did not converge (%llu pairs)", c[7]);
+        return VS_E_STATE;
+    }
     const int64_t n = (int64_t)c[0];
     *n_pairs = n;
     if (stats) {

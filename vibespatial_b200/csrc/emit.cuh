@@ -63,6 +63,68 @@ __device__ __forceinline__ void flush(const BlockOut& o, const PairSink& k, unsi
     __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// Warp-private buffering: the same idea without block barriers, so a warp
+// that finishes early never waits for the slowest warp of its block.
+// ---------------------------------------------------------------------------
+constexpr int kWarpBuf = 128;  // pairs buffered per warp
+
+struct WarpOut {
+    int2* buf;
+    unsigned* cnt;
+};
+
+__device__ __forceinline__ void wemit(const WarpOut& o, const PairSink& k, int32_t l, int32_t r) {
+    const unsigned pos = atomicAdd(o.cnt, 1u);
+    if (pos < (unsigned)kWarpBuf) {
+        o.buf[pos] = make_int2(l, r);
+    } else {
+        const unsigned long long gp = atomicAdd(k.counter, 1ull);
+        if (gp < k.capacity) {
+            k.out_left[gp] = l;
+            k.out_right[gp] = r;
+        }
+    }
+}
+
+// Call with the whole warp converged.  Flushes when at least half full, or
+// always when `force`.
+__device__ __forceinline__ void wflush(const WarpOut& o, const PairSink& k, bool force) {
+    __syncwarp();
+    const unsigned raw = *o.cnt;
+    const unsigned c = raw < (unsigned)kWarpBuf ? raw : (unsigned)kWarpBuf;
+    if (!force && raw < (unsigned)(kWarpBuf / 2)) return;
+    const int lane = threadIdx.x & 31;
+    unsigned long long b = 0;
+    if (lane == 0 && c) b = atomicAdd(k.counter, (unsigned long long)c);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    for (unsigned j = lane; j < c; j += 32) {
+        const unsigned long long gp = b + j;
+        if (gp < k.capacity) {
+            const int2 v = o.buf[j];
+            k.out_left[gp] = v.x;
+            k.out_right[gp] = v.y;
+        }
+    }
+    __syncwarp();
+    if (lane == 0) *o.cnt = 0;
+    __syncwarp();
+}
+
+// Pairs whose location the filters could not certify; resolved exactly by a
+// separate pass.  Entries beyond `capacity` are counted, not stored, and the
+// host re-runs the join with a larger buffer.
+struct DeferSink {
+    int2* buf;                    // (point row, polygon slot)
+    unsigned long long capacity;
+    unsigned long long* counter;
+};
+
+__device__ __forceinline__ void defer(const DeferSink& d, int32_t row, int32_t slot) {
+    const unsigned long long p = atomicAdd(d.counter, 1ull);
+    if (p < d.capacity) d.buf[p] = make_int2(row, slot);
+}
+
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -134,6 +134,76 @@ __device__ __forceinline__ bool edge_step_exact(double ax, double ay, double bx,
     return false;
 }
 
+// ---------------------------------------------------------------------------
+// Filtered variants for the hot join kernels: identical decisions, but an
+// orientation the stage-A filter cannot certify makes the whole pair
+// UNDECIDED instead of calling the exact stage in line.  The join defers such
+// pairs to a separate exact pass, which keeps the out-of-line call (and the
+// register spills around it) out of the hot loops.
+// ---------------------------------------------------------------------------
+enum : int { LOC_UNDECIDED = -1 };
+
+// +1 / -1 when the stage-A filter certifies the sign, 0 when it cannot.
+__device__ __forceinline__ int orient2d_filter(double ax, double ay, double bx, double by, double cx, double cy) {
+    const double acx = __dsub_rn(ax, cx), bcx = __dsub_rn(bx, cx);
+    const double acy = __dsub_rn(ay, cy), bcy = __dsub_rn(by, cy);
+    const double l = __dmul_rn(acx, bcy), r = __dmul_rn(acy, bcx);
+    const double det = __dsub_rn(l, r);
+    const double bound = __dmul_rn(kCcwErrBoundA, __dadd_rn(fabs(l), fabs(r)));
+    return det > bound ? 1 : (-det > bound ? -1 : 0);
+}
+
+// 0: decided, not on the edge; 1: on the edge (boundary); 2: undecided.
+__device__ __forceinline__ int edge_step_filtered(double ax, double ay, double bx, double by, double px, double py,
+                                                  bool& inside) {
+    const bool crosses = (ay > py) != (by > py);
+    const double minx = fmin(ax, bx), maxx = fmax(ax, bx);
+    const bool on_bbox = py >= fmin(ay, by) && py <= fmax(ay, by) && px >= minx && px <= maxx;
+    if (!crosses && !on_bbox) return 0;
+    if (crosses && px < minx) {
+        inside = !inside;
+        return 0;
+    }
+    if (crosses && px > maxx) return 0;
+    const int o = orient2d_filter(ax, ay, bx, by, px, py);
+    if (o == 0) return 2;
+    if (crosses && ((o > 0) == (by > ay))) inside = !inside;
+    return 0;
+}
+
+__device__ __forceinline__ int ring_location_filtered(double px, double py, const double2* __restrict__ xy, int start,
+                                                      int end) {
+    if (end - start < 2) return LOC_OUTSIDE;
+    bool inside = false;
+    double2 a = xy[end - 1];
+    for (int i = start; i < end; ++i) {
+        const double2 b = xy[i];
+        const int r = edge_step_filtered(a.x, a.y, b.x, b.y, px, py, inside);
+        if (r == 1) return LOC_BOUNDARY;
+        if (r == 2) return LOC_UNDECIDED;
+        a = b;
+    }
+    return inside ? LOC_INTERIOR : LOC_OUTSIDE;
+}
+
+__device__ __forceinline__ int geometry_location_filtered(double px, double py, const double2* __restrict__ xy,
+                                                          const int32_t* __restrict__ ring_off,
+                                                          const int32_t* __restrict__ part_off,
+                                                          const int32_t* __restrict__ geom_off, int g) {
+    const int p0 = geom_off[g], p1 = geom_off[g + 1];
+    for (int part = p0; part < p1; ++part) {
+        bool inside = false;
+        const int r0 = part_off[part], r1 = part_off[part + 1];
+        for (int ring = r0; ring < r1; ++ring) {
+            const int k = ring_location_filtered(px, py, xy, ring_off[ring], ring_off[ring + 1]);
+            if (k == LOC_BOUNDARY || k == LOC_UNDECIDED) return k;
+            if (k == LOC_INTERIOR) inside = !inside;
+        }
+        if (inside) return LOC_INTERIOR;
+    }
+    return LOC_OUTSIDE;
+}
+
 // Ring walk over interleaved vertices xy[start, end); the edge (end-1 -> start)
 // closes the ring exactly as in the reference's (i, j = i - 1) loop.
 __device__ __forceinline__ int ring_location(double px, double py, const double2* __restrict__ xy,

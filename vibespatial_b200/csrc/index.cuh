@@ -38,9 +38,16 @@ struct LearnedIndex {
     uint32_t* cell_start = nullptr;  // [n_cells + 1] CSR offsets into entries
     uint32_t* entries = nullptr;     // [n_entries] polygon slots (Hilbert order)
     uint32_t* occ = nullptr;         // occupancy bitmap of level occ_level
-    // RMI: root MLP + per-leaf linear model and error window
+    // RMI: root MLP + per-leaf linear model and error window.  The root's
+    // input is the cell's level-R ancestor key (R = root_level <= L), a
+    // finite domain of 4^R values, so the trained MLP is tabulated over that
+    // whole domain once (root_table[ancestor] = leaf).  Routing at build and
+    // query time reads the same table, which is what makes the per-leaf
+    // error windows exact bounds for every stored key.
     RmiModel* model = nullptr;       // device
-    double2* leaf_ab = nullptr;      // [n_leaves] position = a + b * (key - key_lo)
+    int32_t root_level = 0;
+    uint16_t* root_table = nullptr;  // [4^root_level] leaf of each ancestor cell
+    double2* leaf_ab = nullptr;      // [n_leaves] position = a + b * key
     int2* leaf_err = nullptr;        // [n_leaves] inclusive error window (lo, hi)
     int32_t n_leaves = 0;
     // FP32 tile-relative copies used by the split-precision filter

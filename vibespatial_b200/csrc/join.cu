@@ -16,8 +16,10 @@
 // upper levels from shared memory), test them against the packet's bounding
 // box and push the hits on a warp-shared stack in shared memory.  At the leaf
 // level every lane tests its own point against the hit item boxes and refines
-// each hit immediately with the exact location; accepted pairs go through the
-// block-buffered sink.  No candidate array, no count pass, no host fence.
+// each hit immediately (stage-A filtered orientation; a pair the filter cannot
+// certify is deferred to the exact pass); accepted pairs go through a
+// warp-private buffer.  No candidate array, no count pass, no host fence, no
+// block-wide barrier inside the loop.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -35,7 +37,7 @@ namespace {
 constexpr int kJoinThreads = 256;
 constexpr int kWarps = kJoinThreads / 32;
 constexpr int kStack = 112;            // > (fanout-1) * (max levels-2) + 1
-constexpr int kMaxStagedBoxes = 1365;  // 1 + 16 + 256 + 1092 FP64 boxes (~43 KB)
+constexpr int kMaxStagedBoxes = 273;   // 1 + 16 + 256 FP64 boxes (~8.5 KB)
 
 struct RtreeArgs {
     const double* px;
@@ -57,6 +59,7 @@ struct RtreeArgs {
     const double2* xy;
     int accept_mask;  // bit k: location k accepted; 0 = box candidates only
     PairSink sink;
+    DeferSink defer;
     unsigned long long* counters;
 };
 
@@ -100,25 +103,25 @@ __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ fr
 
 __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const RtreeArgs a) {
     extern __shared__ vs_box s_nodes[];
-    __shared__ int2 s_buf[kOutBuf];
-    __shared__ unsigned s_cnt, s_n;
-    __shared__ unsigned long long s_base;
+    __shared__ int2 s_buf[kWarps][kWarpBuf];
+    __shared__ unsigned s_cnt[kWarps];
     __shared__ int s_stack[kWarps][kStack];
     __shared__ vs_box s_items[kWarps][kFanout];
     const int64_t stage_base = a.level_off[a.stage_level];
     for (int k = threadIdx.x; k < a.staged; k += blockDim.x) s_nodes[k] = a.nodes[stage_base + k];
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    const BlockOut out{s_buf, &s_cnt};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncthreads();
+    const WarpOut out{s_buf[warp], &s_cnt[warp]};
     const unsigned lt = (1u << lane) - 1u;
     const int top = a.levels - 1;
     const int64_t n = (int64_t)*a.n_sorted;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long n_cand = 0;
-    unsigned n_exact = 0;
 
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t i = base + lane;
         const bool active = i < n;
         double x = 0.0, y = 0.0;
         int32_t row = -1;
@@ -136,91 +139,92 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
             y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
             y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
         }
-        if (__ballot_sync(0xffffffffu, active)) {
-            int sp = 0;
-            const vs_box root = s_nodes[a.level_off[top] - stage_base];
-            if (box_overlaps(root, x0, y0, x1, y1)) {
-                if (top == 0) {
-                    // a single polygon: the root is the item
-                    if (active && box_has(root, x, y)) {
-                        ++n_cand;
-                        const int loc = a.accept_mask ? geometry_location(x, y, a.xy, a.ring_off, a.part_off,
-                                                                          a.geom_off, 0, n_exact) : 0;
-                        if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) emit(out, a.sink, row, a.item_geom[0]);
-                    }
-                } else {
-                    if (lane == 0) s_stack[warp][0] = top;  // node 0 of the top level
-                    sp = 1;
+        int sp = 0;
+        const vs_box root = s_nodes[a.level_off[top] - stage_base];
+        if (box_overlaps(root, x0, y0, x1, y1)) {
+            if (top == 0) {
+                // a single polygon: the root is the item
+                if (active && box_has(root, x, y)) {
+                    ++n_cand;
+                    const int loc = a.accept_mask ? geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off,
+                                                                               a.geom_off, 0) : 0;
+                    if (loc == LOC_UNDECIDED) defer(a.defer, row, 0);
+                    else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) wemit(out, a.sink, row, a.item_geom[0]);
                 }
-            }
-            __syncwarp();
-            while (sp > 0) {
-                --sp;
-                const int e = s_stack[warp][sp];
-                __syncwarp();
-                const int cl = (e & 15) - 1;
-                const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
-                const bool in_range = lane < kFanout && c < a.level_size[cl];
-                vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
-                if (in_range)
-                    b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
-                const bool hit = in_range && box_overlaps(b, x0, y0, x1, y1);
-                const unsigned m = __ballot_sync(0xffffffffu, hit);
-                if (cl > 0) {
-                    if (hit) {
-                        const int pos = sp + __popc(m & lt);
-                        if (pos < kStack) s_stack[warp][pos] = (int)(c << 4) | cl;
-                    }
-                    int add = __popc(m);
-                    if (sp + add > kStack) {
-                        if (lane == 0) atomicOr(&a.counters[4], 1ull);  // cannot happen for < 2^31 items
-                        add = kStack - sp;
-                    }
-                    sp += add;
-                    __syncwarp();
-                } else {
-                    if (lane < kFanout) s_items[warp][lane] = b;
-                    __syncwarp();
-                    unsigned mm = m;
-                    const int64_t slot0 = (int64_t)(e >> 4) * kFanout;
-                    while (mm) {
-                        const int j = __ffs(mm) - 1;
-                        mm &= mm - 1;
-                        const vs_box ib = s_items[warp][j];
-                        if (active && box_has(ib, x, y)) {
-                            ++n_cand;
-                            const int slot = (int)(slot0 + j);
-                            int loc = 0;
-                            if (a.accept_mask)
-                                loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, n_exact);
-                            if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                                emit(out, a.sink, row, a.item_geom[slot]);
-                        }
-                    }
-                    __syncwarp();
-                }
+            } else {
+                if (lane == 0) s_stack[warp][0] = top;  // node 0 of the top level
+                sp = 1;
             }
         }
-        flush(out, a.sink, &s_base, &s_n);
+        __syncwarp();
+        while (sp > 0) {
+            --sp;
+            const int e = s_stack[warp][sp];
+            __syncwarp();
+            const int cl = (e & 15) - 1;
+            const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
+            const bool in_range = lane < kFanout && c < a.level_size[cl];
+            vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
+            if (in_range)
+                b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
+            const bool hit = in_range && box_overlaps(b, x0, y0, x1, y1);
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (cl > 0) {
+                if (hit) {
+                    const int pos = sp + __popc(m & lt);
+                    if (pos < kStack) s_stack[warp][pos] = (int)(c << 4) | cl;
+                }
+                int add = __popc(m);
+                if (sp + add > kStack) {
+                    if (lane == 0) atomicOr(&a.counters[4], 1ull);  // cannot happen for < 2^31 items
+                    add = kStack - sp;
+                }
+                sp += add;
+                __syncwarp();
+            } else {
+                if (lane < kFanout) s_items[warp][lane] = b;
+                __syncwarp();
+                unsigned mm = m;
+                const int64_t slot0 = (int64_t)(e >> 4) * kFanout;
+                while (mm) {
+                    const int j = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    const vs_box ib = s_items[warp][j];
+                    if (active && box_has(ib, x, y)) {
+                        ++n_cand;
+                        const int slot = (int)(slot0 + j);
+                        int loc = 0;
+                        if (a.accept_mask)
+                            loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot);
+                        if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
+                        else if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
+                            wemit(out, a.sink, row, a.item_geom[slot]);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        wflush(out, a.sink, false);
     }
+    wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
-    add_counter(a.counters, 1, n_exact);
 }
 
 // Every point against every polygon box, one thread per point in input order
 // (small joins and cross-checks).
 __global__ void __launch_bounds__(kJoinThreads) join_brute_kernel(const RtreeArgs a) {
-    __shared__ int2 s_buf[kOutBuf];
-    __shared__ unsigned s_cnt, s_n;
-    __shared__ unsigned long long s_base;
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    const BlockOut out{s_buf, &s_cnt};
+    __shared__ int2 s_buf[kWarps][kWarpBuf];
+    __shared__ unsigned s_cnt[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncwarp();
+    const WarpOut out{s_buf[warp], &s_cnt[warp]};
     const int64_t M = a.level_size[0];
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long n_cand = 0;
-    unsigned n_exact = 0;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < a.n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;
+    for (int64_t base = gw * 32; base < a.n; base += nw * 32) {
+        const int64_t i = base + lane;
         if (i < a.n && (a.pvalid == nullptr || a.pvalid[i])) {
             const double x = a.px[i], y = a.py[i];
             for (int64_t c = 0; c < M; ++c) {
@@ -228,13 +232,59 @@ __global__ void __launch_bounds__(kJoinThreads) join_brute_kernel(const RtreeArg
                 ++n_cand;
                 int loc = 0;
                 if (a.accept_mask)
-                    loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, (int)c, n_exact);
-                if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) emit(out, a.sink, (int32_t)i, a.item_geom[c]);
+                    loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, (int)c);
+                if (loc == LOC_UNDECIDED) defer(a.defer, (int32_t)i, (int32_t)c);
+                else if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
+                    wemit(out, a.sink, (int32_t)i, a.item_geom[c]);
             }
         }
-        flush(out, a.sink, &s_base, &s_n);
+        wflush(out, a.sink, false);
     }
+    wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
+}
+
+// Exact pass over the deferred (point row, polygon slot) pairs: the full
+// location with the exact orientation stage.
+struct ResolveArgs {
+    const double* px;
+    const double* py;
+    const int32_t* item_geom;
+    const int32_t* geom_off;
+    const int32_t* part_off;
+    const int32_t* ring_off;
+    const double2* xy;
+    int accept_mask;
+    const int2* pairs;
+    unsigned long long capacity;
+    const unsigned long long* count;
+    PairSink sink;
+    unsigned long long* counters;
+};
+
+__global__ void __launch_bounds__(kJoinThreads) resolve_deferred_kernel(const ResolveArgs a) {
+    __shared__ int2 s_buf[kWarps][kWarpBuf];
+    __shared__ unsigned s_cnt[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncwarp();
+    const WarpOut out{s_buf[warp], &s_cnt[warp]};
+    const unsigned long long cnt = *a.count;
+    const int64_t n = (int64_t)(cnt < a.capacity ? cnt : a.capacity);
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned n_exact = 0;
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t k = base + lane;
+        if (k < n) {
+            const int2 pr = a.pairs[k];
+            const double x = a.px[pr.x], y = a.py[pr.x];
+            const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, pr.y, n_exact);
+            if ((a.accept_mask >> loc) & 1) wemit(out, a.sink, pr.x, a.item_geom[pr.y]);
+        }
+        wflush(out, a.sink, false);
+    }
+    wflush(out, a.sink, true);
     add_counter(a.counters, 1, n_exact);
 }
 
@@ -307,7 +357,7 @@ int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
 }
 
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
-                      int32_t* d_left, int32_t* d_right, int64_t capacity) {
+                      int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
     RtreeArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
@@ -335,6 +385,7 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.xy = idx->xy;
     a.accept_mask = accept_mask;
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
+    a.defer = dsink;
     a.counters = ctx->d_counters;
     if (brute) {
         join_brute_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, 0, ctx->stream>>>(a);
@@ -348,6 +399,27 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     const size_t smem = (size_t)a.staged * sizeof(vs_box);
     VS_CUDA_TRY(cudaFuncSetAttribute(join_rtree_packet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     join_rtree_packet_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, smem, ctx->stream>>>(a);
+    VS_CUDA_TRY(cudaGetLastError());
+    return VS_OK;
+}
+
+int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
+                            int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
+    ResolveArgs a{};
+    a.px = pts->d_x;
+    a.py = pts->d_y;
+    a.item_geom = idx->item_geom;
+    a.geom_off = idx->geom_off;
+    a.part_off = idx->part_off;
+    a.ring_off = idx->ring_off;
+    a.xy = idx->xy;
+    a.accept_mask = accept_mask;
+    a.pairs = dsink.buf;
+    a.capacity = dsink.capacity;
+    a.count = dsink.counter;
+    a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
+    a.counters = ctx->d_counters;
+    resolve_deferred_kernel<<<kNumSMs * 4, kJoinThreads, 0, ctx->stream>>>(a);
     VS_CUDA_TRY(cudaGetLastError());
     return VS_OK;
 }

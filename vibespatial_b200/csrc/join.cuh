@@ -2,6 +2,7 @@
 #pragma once
 #include <stdint.h>
 
+#include "emit.cuh"
 #include "index.cuh"
 #include "primitives.cuh"
 #include "vs_common.cuh"
@@ -15,9 +16,12 @@ struct QueryOrder {
 int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q);
 int accept_mask_for(int predicate, int* mask);
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
-                      int32_t* d_left, int32_t* d_right, int64_t capacity);
+                      int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
-                        int32_t* d_left, int32_t* d_right, int64_t capacity);
+                        int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
+// Exact pass over the pairs the filtered kernels deferred (count read on device).
+int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
+                            int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
 int launch_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, uint8_t* d_out);
 int sort_pairs(vs_context* ctx, int32_t* d_left, int32_t* d_right, int64_t n, uint64_t max_left,
                uint64_t max_right);

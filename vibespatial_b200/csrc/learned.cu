@@ -8,18 +8,20 @@
 //   3. an occupancy bitmap at a coarser level lets empty regions skip lookups
 //   4. the RMI (FP32 MLP 1->32->32->1 root + linear leaves) is trained on the
 //      sorted cell keys with hand-written forward/backward and Adam kernels;
-//      every key is then routed through the same inference functions to fit
-//      the leaves and to measure each leaf's inclusive error window
+//      the root's input is the cell's level-R ancestor (R <= 10), so the
+//      trained MLP is tabulated over all 4^R ancestors; every stored key is
+//      routed through that table to fit the leaves and to measure each
+//      leaf's inclusive error window
 //   5. FP32 copies of every polygon relative to its own origin (box centre),
 //      with a per-polygon bound on the rounding error, for the split filter
 //
-// Query (points already keyed and sorted, see prepare_queries): for each
-// distinct cell among a warp's 32 points the warp evaluates the root MLP
-// cooperatively (lane = hidden unit), predicts the position with the leaf
-// model and searches the error window; each lane then scans its cell's
-// polygon list, filters boxes in FP32 (rounded outward), and refines with the
-// FP32 crossing test, re-deciding in FP64 (and exactly, if needed) only the
-// edges whose FP32 decision is within its rounding-error bound.
+// Query (points in input order, one thread each, no sort): the point's
+// level-L cell key -> occupancy bit -> root table -> leaf model -> binary
+// search inside the leaf's error window -> the cell's polygon list.  Each
+// candidate is box-filtered in FP32 (rounded outward) and refined with the
+// FP32 crossing test on tile-relative coordinates; only edges whose FP32
+// decision lies within the rounding-error bound are re-decided in FP64, and a
+// pair the FP64 filter cannot certify is deferred to the exact pass.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -183,11 +185,12 @@ __global__ void split_copy_kernel(const vs_box* __restrict__ box, int64_t M, con
 }
 
 // ------------------------------------------------------------ RMI train ---
-__global__ void rmi_samples_kernel(const uint32_t* __restrict__ keys, int64_t n, int S, double key_lo, double key_scale,
-                                   float* __restrict__ xs, float* __restrict__ ts) {
+// Training pairs: x = normalised ancestor key of stored cell i, t = i / n.
+__global__ void rmi_samples_kernel(const uint32_t* __restrict__ keys, int64_t n, int S, int anc_shift, double key_lo,
+                                   double key_scale, float* __restrict__ xs, float* __restrict__ ts) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
         const int64_t i = (int64_t)((double)s * (double)n / (double)S);
-        xs[s] = __double2float_rn(((double)keys[i] - key_lo) * key_scale);
+        xs[s] = __double2float_rn(((double)(keys[i] >> anc_shift) - key_lo) * key_scale);
         ts[s] = (float)((double)i / (double)n);
     }
 }
@@ -290,38 +293,43 @@ __global__ void rmi_pack_kernel(const float* __restrict__ P, RmiModel* __restric
     }
 }
 
-// Route every stored key through the inference path (one warp per key).
-__global__ void __launch_bounds__(kThreads) rmi_route_kernel(const RmiModel* __restrict__ model,
-                                                             const uint32_t* __restrict__ keys, int64_t n,
-                                                             uint32_t* __restrict__ leaf_of) {
+// Tabulate the trained root over every ancestor key (one warp per key).
+__global__ void __launch_bounds__(kThreads) rmi_table_kernel(const RmiModel* __restrict__ model, int64_t n_anc,
+                                                             uint16_t* __restrict__ table) {
     __shared__ RmiShared sm;
     rmi_load_shared(&sm, model);
     __syncthreads();
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = warp; i < n; i += nw) {
-        const float y = rmi_root_warp(&sm, rmi_input(keys[i], &sm));
-        if ((threadIdx.x & 31) == 0) leaf_of[i] = (uint32_t)rmi_leaf(&sm, y);
+    for (int64_t c = warp; c < n_anc; c += nw) {
+        const float y = rmi_root_warp(&sm, rmi_input((uint32_t)c, &sm));
+        if ((threadIdx.x & 31) == 0) table[c] = (uint16_t)rmi_leaf(sm.n_leaves, y);
     }
 }
 
+__global__ void rmi_route_kernel(const uint16_t* __restrict__ table, const uint32_t* __restrict__ keys, int64_t n,
+                                 int anc_shift, uint32_t* __restrict__ leaf_of) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        leaf_of[i] = table[keys[i] >> anc_shift];
+}
+
 __global__ void rmi_leaf_sums_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ leaf_of, int64_t n,
-                                     double key_lo, double* __restrict__ sums) {
+                                     double* __restrict__ sums) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t l = leaf_of[i];
         atomicAdd(&sums[3 * l + 0], 1.0);
-        atomicAdd(&sums[3 * l + 1], (double)keys[i] - key_lo);
+        atomicAdd(&sums[3 * l + 1], (double)keys[i]);
         atomicAdd(&sums[3 * l + 2], (double)i);
     }
 }
 
 __global__ void rmi_leaf_cov_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ leaf_of, int64_t n,
-                                    double key_lo, const double* __restrict__ sums, double* __restrict__ cov) {
+                                    const double* __restrict__ sums, double* __restrict__ cov) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t l = leaf_of[i];
         const double c = sums[3 * l];
         const double mx = sums[3 * l + 1] / c, my = sums[3 * l + 2] / c;
-        const double dx = (double)keys[i] - key_lo - mx, dy = (double)i - my;
+        const double dx = (double)keys[i] - mx, dy = (double)i - my;
         atomicAdd(&cov[2 * l + 0], dx * dy);
         atomicAdd(&cov[2 * l + 1], dx * dx);
     }
@@ -342,17 +350,13 @@ __global__ void rmi_leaf_fit_kernel(const double* __restrict__ sums, const doubl
     }
 }
 
-__global__ void __launch_bounds__(kThreads) rmi_err_kernel(const RmiModel* __restrict__ model,
-                                                           const uint32_t* __restrict__ keys,
-                                                           const uint32_t* __restrict__ leaf_of, int64_t n,
-                                                           const double2* __restrict__ ab, int2* __restrict__ err) {
-    __shared__ RmiShared sm;
-    rmi_load_shared(&sm, model);
-    __syncthreads();
+// Error window of each leaf, measured over every stored key with the same
+// routing table and leaf model the queries use.
+__global__ void rmi_err_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ leaf_of, int64_t n,
+                               const double2* __restrict__ ab, int2* __restrict__ err) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t l = leaf_of[i];
-        const long long pred = rmi_predict(ab[l], keys[i], &sm);
-        long long e = (long long)i - pred;
+        long long e = (long long)i - rmi_predict(ab[l], keys[i]);
         e = e < -0x7ffffffe ? -0x7ffffffe : (e > 0x7ffffffe ? 0x7ffffffe : e);
         atomicMin(&err[l].x, (int)e);
         atomicMax(&err[l].y, (int)e);
@@ -384,17 +388,18 @@ __global__ void rmi_window_stats_kernel(const uint32_t* __restrict__ leaf_of, in
 struct LearnedArgs {
     const double* px;
     const double* py;
-    const uint32_t* order;
-    const uint32_t* keys;      // sorted level-16 keys
-    const uint32_t* n_sorted;
+    const uint8_t* pvalid;
+    int64_t n;
+    const double* frame;
     int L;
     int occ_shift;             // cell key >> occ_shift = occupancy bit
+    int root_shift;            // cell key >> root_shift = root-table index
     const uint32_t* occ;
+    const uint16_t* root_table;
     const uint32_t* cell_keys;
     const uint32_t* cell_start;
     const uint32_t* entries;
     int64_t n_cells;
-    const RmiModel* model;
     const double2* leaf_ab;
     const int2* leaf_err;
     const vs_box* boxes;       // FP64 slot boxes (R-tree level 0)
@@ -409,13 +414,14 @@ struct LearnedArgs {
     const int32_t* ring_off;
     int accept_mask;
     PairSink sink;
+    DeferSink defer;
     unsigned long long* counters;
 };
 
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
 // decision the exact walk needs lies within the rounding-error bound `t`
-// (the caller then re-decides the edge in FP64 / exactly); otherwise applies
-// the same decision the exact walk would (the point cannot be on this edge).
+// (the caller then re-decides the edge in FP64); otherwise applies the same
+// decision the exact walk would (the point cannot be on this edge).
 __device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, float by, float px, float py, float t,
                                                bool& inside) {
     const float A2 = __fsub_rn(ay, py), B2 = __fsub_rn(by, py);
@@ -448,8 +454,7 @@ __device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, flo
 
 __device__ __forceinline__ int ring_location_split(double px, double py, float qx, float qy, float t,
                                                    const float2* __restrict__ xy32, const double2* __restrict__ xy,
-                                                   int start, int end, unsigned& n_exact, unsigned& n32,
-                                                   unsigned& n64) {
+                                                   int start, int end, unsigned& n32, unsigned& n64) {
     if (end - start < 2) return LOC_OUTSIDE;
     bool inside = false;
     float2 a = xy32[end - 1];
@@ -461,7 +466,9 @@ __device__ __forceinline__ int ring_location_split(double px, double py, float q
         } else {
             ++n64;
             const double2 A = xy[ia], B = xy[i];
-            if (edge_step_exact(A.x, A.y, B.x, B.y, px, py, inside, n_exact)) return LOC_BOUNDARY;
+            const int r = edge_step_filtered(A.x, A.y, B.x, B.y, px, py, inside);
+            if (r == 1) return LOC_BOUNDARY;
+            if (r == 2) return LOC_UNDECIDED;
         }
         a = b;
         ia = i;
@@ -470,16 +477,15 @@ __device__ __forceinline__ int ring_location_split(double px, double py, float q
 }
 
 __device__ __forceinline__ int geometry_location_split(double px, double py, float qx, float qy, float t,
-                                                       const LearnedArgs& a, int g, unsigned& n_exact, unsigned& n32,
-                                                       unsigned& n64) {
+                                                       const LearnedArgs& a, int g, unsigned& n32, unsigned& n64) {
     const int p0 = a.geom_off[g], p1 = a.geom_off[g + 1];
     for (int part = p0; part < p1; ++part) {
         bool inside = false;
         const int r0 = a.part_off[part], r1 = a.part_off[part + 1];
         for (int ring = r0; ring < r1; ++ring) {
             const int k = ring_location_split(px, py, qx, qy, t, a.xy32, a.xy, a.ring_off[ring], a.ring_off[ring + 1],
-                                              n_exact, n32, n64);
-            if (k == LOC_BOUNDARY) return LOC_BOUNDARY;
+                                              n32, n64);
+            if (k == LOC_BOUNDARY || k == LOC_UNDECIDED) return k;
             if (k == LOC_INTERIOR) inside = !inside;
         }
         if (inside) return LOC_INTERIOR;
@@ -487,77 +493,54 @@ __device__ __forceinline__ int geometry_location_split(double px, double py, flo
     return LOC_OUTSIDE;
 }
 
+// Points in input order, one thread each: key -> occupancy -> root table ->
+// leaf model -> bounded binary search -> the cell's polygon list.
 __global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArgs a) {
-    __shared__ RmiShared sm;
-    __shared__ int2 s_buf[kOutBuf];
-    __shared__ unsigned s_cnt, s_n;
-    __shared__ unsigned long long s_base;
-    rmi_load_shared(&sm, a.model);
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    const BlockOut out{s_buf, &s_cnt};
-    const int lane = threadIdx.x & 31;
-    const int64_t n = (int64_t)*a.n_sorted;
-    const int cell_shift = 32 - 2 * a.L;
-    unsigned long long n_cand = 0, n_binsearch = 0;
-    unsigned n_exact = 0, n32 = 0, n64 = 0;
+    __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
+    __shared__ unsigned s_cnt[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncwarp();
+    const WarpOut out{s_buf[warp], &s_cnt[warp]};
+    double lox, loy, sx, sy;
+    frame_q(a.frame, lox, loy, sx, sy);
+    const double fx1 = a.frame[2], fy1 = a.frame[3];
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long n_cand = 0, n_wide = 0;
+    unsigned n32 = 0, n64 = 0;
 
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;
-        const bool active = i < n;
-        uint32_t cell = 0xffffffffu;
-        bool need = false;
-        if (active) {
-            cell = a.keys[i] >> cell_shift;
-            const uint32_t ob = cell >> a.occ_shift;
-            need = (a.occ[ob >> 5] >> (ob & 31)) & 1u;
-        }
-        // Phase 1: one RMI lookup per distinct cell of the warp.
-        uint32_t lo = 0, hi = 0;
-        unsigned pending = __ballot_sync(0xffffffffu, need);
-        while (pending) {
-            const int leader = __ffs(pending) - 1;
-            const uint32_t k = __shfl_sync(0xffffffffu, cell, leader);
-            const unsigned peers = __ballot_sync(0xffffffffu, need && cell == k);
-            pending &= ~peers;
-            const float y = rmi_root_warp(&sm, rmi_input(k, &sm));
-            const int leaf = rmi_leaf(&sm, y);
-            const int2 er = a.leaf_err[leaf];
-            long long found = -1;
-            if (er.x <= er.y) {
-                const long long pred = rmi_predict(a.leaf_ab[leaf], k, &sm);
-                long long lo0 = pred + er.x, hi0 = pred + er.y + 1;  // search [lo0, hi0)
-                lo0 = lo0 < 0 ? 0 : lo0;
-                hi0 = hi0 > a.n_cells ? a.n_cells : hi0;
-                if (hi0 - lo0 > 256) ++n_binsearch;
-                // 32-ary search: each round the lanes sample 32 evenly spaced
-                // keys; the count of samples below k narrows the range 32x.
-                while (hi0 - lo0 > 32) {
-                    const long long step = (hi0 - lo0 + 31) >> 5;
-                    const long long j = lo0 + (long long)lane * step;
-                    const bool below = j < hi0 && a.cell_keys[j] < k;
-                    const int c = __popc(__ballot_sync(0xffffffffu, below));
-                    const long long nlo = c == 0 ? lo0 : lo0 + (long long)(c - 1) * step + 1;
-                    const long long cap = lo0 + (long long)c * step + 1;
-                    hi0 = cap < hi0 ? cap : hi0;
-                    lo0 = nlo;
-                }
-                if (lo0 < hi0) {
-                    const long long j = lo0 + lane;
-                    const uint32_t kk = j < hi0 ? a.cell_keys[j] : ~k;
-                    const unsigned m = __ballot_sync(0xffffffffu, kk == k);
-                    if (m) found = lo0 + __ffs(m) - 1;
+    for (int64_t base = gw * 32; base < a.n; base += nw * 32) {
+        const int64_t i = base + lane;
+        if (i < a.n) {
+            const double x = a.px[i], y = a.py[i];
+            const bool ok = (a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1;
+            uint32_t lo = 0, hi = 0;
+            if (ok) {
+                const uint32_t cell = (uint32_t)hilbert_key(quantize(x, lox, sx), quantize(y, loy, sy), a.L);
+                const uint32_t ob = cell >> a.occ_shift;
+                if ((a.occ[ob >> 5] >> (ob & 31)) & 1u) {
+                    const int leaf = a.root_table[cell >> a.root_shift];
+                    const int2 er = a.leaf_err[leaf];
+                    if (er.x <= er.y) {
+                        const long long pred = rmi_predict(a.leaf_ab[leaf], cell);
+                        long long l0 = pred + er.x, h0 = pred + er.y + 1;  // search [l0, h0)
+                        l0 = l0 < 0 ? 0 : l0;
+                        h0 = h0 > a.n_cells ? a.n_cells : h0;
+                        if (h0 - l0 > 256) ++n_wide;
+                        const long long h1 = h0;
+                        while (l0 < h0) {
+                            const long long mid = (l0 + h0) >> 1;
+                            if (a.cell_keys[mid] < cell) l0 = mid + 1;
+                            else h0 = mid;
+                        }
+                        if (l0 < h1 && a.cell_keys[l0] == cell) {
+                            lo = a.cell_start[l0];
+                            hi = a.cell_start[l0 + 1];
+                        }
+                    }
                 }
             }
-            if (found >= 0 && ((peers >> lane) & 1u)) {
-                lo = a.cell_start[found];
-                hi = a.cell_start[found + 1];
-            }
-        }
-        // Phase 2: each lane scans its own cell's polygons.
-        if (lo < hi) {
-            const int32_t row = (int32_t)a.order[i];
-            const double x = a.px[row], y = a.py[row];
             for (uint32_t e = lo; e < hi; ++e) {
                 const int slot = (int)a.entries[e];
                 const double2 o = a.origin[slot];
@@ -573,18 +556,20 @@ __global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArg
                 int loc = 0;
                 if (a.accept_mask) {
                     const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
-                    loc = geometry_location_split(x, y, qx, qy, t, a, slot, n_exact, n32, n64);
+                    loc = geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
                 }
-                if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) emit(out, a.sink, row, a.item_geom[slot]);
+                if (loc == LOC_UNDECIDED) defer(a.defer, (int32_t)i, slot);
+                else if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
+                    wemit(out, a.sink, (int32_t)i, a.item_geom[slot]);
             }
         }
-        flush(out, a.sink, &s_base, &s_n);
+        wflush(out, a.sink, false);
     }
+    wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
-    add_counter(a.counters, 1, n_exact);
     add_counter(a.counters, 2, n32);
     add_counter(a.counters, 3, n64);
-    add_counter(a.counters, 6, n_binsearch);
+    add_counter(a.counters, 6, n_wide);
 }
 
 template <class T>
@@ -604,13 +589,15 @@ int train_rmi(vs_context* ctx, vs_index* idx, int steps) {
     LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
     const int64_t n = li.n_cells;
-    // key range and quantile knots (33 keys read back)
+    const int anc_shift = 2 * (li.level - li.root_level);
+    // ancestor-key range and quantile knots (33 keys read back)
     std::vector<uint32_t> q(33);
     for (int j = 0; j <= 32; ++j) {
         const int64_t pos = (int64_t)((double)j * (double)(n - 1) / 32.0);
         VS_CUDA_TRY(cudaMemcpyAsync(&q[j], li.cell_keys + pos, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     }
     VS_CUDA_TRY(cudaStreamSynchronize(s));
+    for (auto& v : q) v >>= anc_shift;
     const double key_lo = (double)q[0];
     const double span = (double)q[32] - key_lo;
     const double key_scale = span > 0 ? 1.0 / span : 0.0;
@@ -646,7 +633,7 @@ int train_rmi(vs_context* ctx, vs_index* idx, int steps) {
     VS_CUDA_TRY(cudaMemcpyAsync(dP.p, P.data(), kRmiP * sizeof(float), cudaMemcpyHostToDevice, s));
     VS_CUDA_TRY(cudaMemsetAsync(m1.p, 0, kRmiP * sizeof(float), s));
     VS_CUDA_TRY(cudaMemsetAsync(m2.p, 0, kRmiP * sizeof(float), s));
-    rmi_samples_kernel<<<div_up(S, 256), 256, 0, s>>>(li.cell_keys, n, S, key_lo, key_scale, xs.p, ts.p);
+    rmi_samples_kernel<<<div_up(S, 256), 256, 0, s>>>(li.cell_keys, n, S, anc_shift, key_lo, key_scale, xs.p, ts.p);
     VS_CUDA_TRY(cudaGetLastError());
     for (int step = 1; step <= steps; ++step) {
         VS_CUDA_TRY(cudaMemsetAsync(loss.p, 0, sizeof(float), s));
@@ -660,6 +647,11 @@ int train_rmi(vs_context* ctx, vs_index* idx, int steps) {
     if (!li.model) VS_TRY(dalloc(&li.model, 1, bytes));
     rmi_pack_kernel<<<1, 256, 0, s>>>(dP.p, li.model, key_lo, key_scale, li.n_leaves, (int)n);
     VS_CUDA_TRY(cudaGetLastError());
+    // tabulate the root over all 4^R ancestor keys
+    const int64_t n_anc = 1ll << (2 * li.root_level);
+    VS_TRY(dalloc(&li.root_table, (size_t)n_anc, bytes));
+    rmi_table_kernel<<<grid_for(n_anc * 32, kThreads, 8), kThreads, 0, s>>>(li.model, n_anc, li.root_table);
+    VS_CUDA_TRY(cudaGetLastError());
     return VS_OK;
 }
 
@@ -668,6 +660,7 @@ int fit_leaves(vs_context* ctx, vs_index* idx) {
     cudaStream_t s = ctx->stream;
     const int64_t n = li.n_cells;
     const int nl = li.n_leaves;
+    const int anc_shift = 2 * (li.level - li.root_level);
     int64_t& bytes = idx->device_bytes;
     VS_TRY(dalloc(&li.leaf_ab, (size_t)nl, bytes));
     VS_TRY(dalloc(&li.leaf_err, (size_t)nl, bytes));
@@ -681,15 +674,11 @@ int fit_leaves(vs_context* ctx, vs_index* idx) {
     VS_CUDA_TRY(cudaMemsetAsync(sums.p, 0, 3 * nl * sizeof(double), s));
     VS_CUDA_TRY(cudaMemsetAsync(cov.p, 0, 2 * nl * sizeof(double), s));
     VS_CUDA_TRY(cudaMemsetAsync(acc.p, 0, 2 * sizeof(unsigned long long), s));
-    RmiModel hm;
-    VS_CUDA_TRY(cudaMemcpyAsync(&hm, li.model, sizeof(RmiModel), cudaMemcpyDeviceToHost, s));
-    VS_CUDA_TRY(cudaStreamSynchronize(s));
-    rmi_route_kernel<<<grid_for(n * 32, kThreads, 8), kThreads, 0, s>>>(li.model, li.cell_keys, n, leaf_of.p);
-    rmi_leaf_sums_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, hm.key_lo, sums.p);
-    rmi_leaf_cov_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, hm.key_lo, sums.p, cov.p);
+    rmi_route_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.root_table, li.cell_keys, n, anc_shift, leaf_of.p);
+    rmi_leaf_sums_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, sums.p);
+    rmi_leaf_cov_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, sums.p, cov.p);
     rmi_leaf_fit_kernel<<<div_up(nl, 256), 256, 0, s>>>(sums.p, cov.p, nl, li.leaf_ab, li.leaf_err);
-    rmi_err_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(li.model, li.cell_keys, leaf_of.p, n, li.leaf_ab,
-                                                             li.leaf_err);
+    rmi_err_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, li.leaf_ab, li.leaf_err);
     rmi_window_stats_kernel<<<grid_for(n, 256), 256, 0, s>>>(leaf_of.p, n, li.leaf_err, acc.p);
     VS_CUDA_TRY(cudaGetLastError());
     unsigned long long h[2];
@@ -709,6 +698,7 @@ void free_learned_index(vs_index* idx) {
     cudaFree(li.entries);
     cudaFree(li.occ);
     cudaFree(li.model);
+    cudaFree(li.root_table);
     cudaFree(li.leaf_ab);
     cudaFree(li.leaf_err);
     cudaFree(li.origin);
@@ -790,8 +780,9 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_CUDA_TRY(cudaMemsetAsync(li.occ, 0, (size_t)((occ_bits + 31) / 32) * sizeof(uint32_t), s));
     occ_kernel<<<grid_for(nc, 256), 256, 0, s>>>(li.cell_keys, nc, 2 * (L - li.occ_level), li.occ);
     VS_CUDA_TRY(cudaGetLastError());
-    // 5. RMI
-    li.n_leaves = (opts && opts->rmi_leaves > 0) ? opts->rmi_leaves : 4096;
+    // 5. RMI (root tabulated over level-R ancestors)
+    li.n_leaves = (opts && opts->rmi_leaves > 0) ? std::min(opts->rmi_leaves, 65535) : 4096;
+    li.root_level = std::min(L, 10);
     const int steps = (opts && opts->rmi_train_steps > 0) ? opts->rmi_train_steps : 300;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -819,24 +810,23 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
 }
 
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, int32_t* d_left,
-                        int32_t* d_right, int64_t capacity) {
+                        int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
     const LearnedIndex& li = idx->learned;
-    QueryOrder q;
-    VS_TRY(prepare_queries(ctx, idx, pts, q));
     LearnedArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
-    a.order = q.order.p;
-    a.keys = q.keys.p;
-    a.n_sorted = q.n_valid.p;
+    a.pvalid = pts->d_valid;
+    a.n = pts->n;
+    a.frame = idx->frame;
     a.L = li.level;
     a.occ_shift = 2 * (li.level - li.occ_level);
+    a.root_shift = 2 * (li.level - li.root_level);
     a.occ = li.occ;
+    a.root_table = li.root_table;
     a.cell_keys = li.cell_keys;
     a.cell_start = li.cell_start;
     a.entries = li.entries;
     a.n_cells = li.n_cells;
-    a.model = li.model;
     a.leaf_ab = li.leaf_ab;
     a.leaf_err = li.leaf_err;
     a.boxes = idx->nodes;
@@ -851,6 +841,7 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.ring_off = idx->ring_off;
     a.accept_mask = accept_mask;
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
+    a.defer = dsink;
     a.counters = ctx->d_counters;
     join_learned_kernel<<<grid_for(pts->n, kThreads, 8), kThreads, 0, ctx->stream>>>(a);
     VS_CUDA_TRY(cudaGetLastError());

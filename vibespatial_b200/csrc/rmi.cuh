@@ -1,10 +1,10 @@
-// Recursive model index (RMI) evaluation shared by training-time routing and
-// query-time lookups.  Exactness of the learned lookup rests on one fact: the
-// per-leaf error windows are measured by routing every stored key through the
-// very functions below, and queries route through the same functions, so a
-// stored key is always inside its leaf's window.  Each function fixes its
-// operation order with explicit round-to-nearest intrinsics (no contraction
-// differences between call sites).
+// Recursive model index (RMI) evaluation.
+//
+// The root MLP (FP32, 1 -> 32 -> 32 -> 1) maps a normalised ancestor-cell key
+// to [0, 1); leaf = floor(y * n_leaves).  It is evaluated by a full warp for
+// one input (lane j owns hidden unit j) when the root table is built; queries
+// only read the table.  Leaf models predict a position from the full cell key
+// in FP64.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -43,13 +43,13 @@ __device__ __forceinline__ void rmi_load_shared(RmiShared* s, const RmiModel* m)
     }
 }
 
-__device__ __forceinline__ float rmi_input(uint32_t key, const RmiShared* s) {
-    return __double2float_rn(__dmul_rn((double)key - s->key_lo, s->key_scale));
+// Normalised root input of an ancestor-cell key.
+__device__ __forceinline__ float rmi_input(uint32_t anc, const RmiShared* s) {
+    return __double2float_rn(__dmul_rn((double)anc - s->key_lo, s->key_scale));
 }
 
-// Root MLP 1 -> 32 -> 32 -> 1, evaluated by a full warp for ONE input: lane j
-// owns hidden unit j.  Layer 2 accumulates k = 0..31 in order with fmaf;
-// layer 3 is a xor-butterfly sum, so every lane ends with the same bits.
+// Root MLP for ONE input, evaluated by the whole warp (lane j = hidden unit
+// j); the xor-butterfly sum leaves the same bits in every lane.
 __device__ __forceinline__ float rmi_root_warp(const RmiShared* s, float x) {
     const int j = threadIdx.x & 31;
     const float h1 = fmaxf(__fmaf_rn(s->w1[j], x, s->b1[j]), 0.0f);
@@ -62,16 +62,16 @@ __device__ __forceinline__ float rmi_root_warp(const RmiShared* s, float x) {
     return __fadd_rn(t, s->b3);
 }
 
-__device__ __forceinline__ int rmi_leaf(const RmiShared* s, float y) {
-    const float f = floorf(__fmul_rn(y, (float)s->n_leaves));
+__device__ __forceinline__ int rmi_leaf(int n_leaves, float y) {
+    const float f = floorf(__fmul_rn(y, (float)n_leaves));
     // NaN lands in leaf 0 like any other value: routing only has to be deterministic.
-    return (f >= 0.0f) ? (f < (float)s->n_leaves ? (int)f : s->n_leaves - 1) : 0;
+    return (f >= 0.0f) ? (f < (float)n_leaves ? (int)f : n_leaves - 1) : 0;
 }
 
-// Leaf model: predicted position = floor(a + b * (key - key_lo)) in FP64,
-// clamped to +-2^40 so that adding an error bound cannot overflow.
-__device__ __forceinline__ long long rmi_predict(const double2 ab, uint32_t key, const RmiShared* s) {
-    const double p = floor(__fma_rn(ab.y, (double)key - s->key_lo, ab.x));
+// Leaf model: predicted position = floor(a + b * key) in FP64, clamped to
+// +-2^40 so that adding an error bound cannot overflow.
+__device__ __forceinline__ long long rmi_predict(const double2 ab, uint32_t key) {
+    const double p = floor(__fma_rn(ab.y, (double)key, ab.x));
     const double c = 1099511627776.0;
     return (long long)(p >= -c ? (p <= c ? p : c) : -c);
 }

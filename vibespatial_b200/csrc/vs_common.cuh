@@ -80,6 +80,10 @@ struct vs_context {
     unsigned long long* h_counter;
     // Device counters: [0] pair count, [1] exact-fallback count,
     // [2] fp32-filter decided edges, [3] edges sent past the fp32 filter,
-    // [4] error flags, [5] candidate (bbox) count, [6..7] spare.
+    // [4] error flags, [5] candidate (bbox) count, [6] wide learned-index
+    // windows, [7] deferred pairs.
     unsigned long long* d_counters;
+    // Pairs deferred to the exact pass (grown on demand).
+    int2* defer_buf;
+    unsigned long long defer_cap;
 };
