@@ -280,6 +280,7 @@ def run_ours(args, rank, world, local_rank):
                 ex.copy_(hx, non_blocking=True)
                 ey.copy_(hy, non_blocking=True)
                 n_e, _ = index.join_into(epts, pred, method, left, right)
+                assert n_e == n_pairs, (n_e, n_pairs)
                 hl[:n_e].copy_(left[:n_e], non_blocking=True)
                 hr[:n_e].copy_(right[:n_e], non_blocking=True)
                 b.record(stream)

@@ -129,7 +129,8 @@ int vs_version(void);
 const char* vs_last_error(void);
 
 /* A context = one device + one stream + a scratch arena.  `stream` is a
- * cudaStream_t (NULL: the context creates its own).  Not thread-safe: callers
+ * cudaStream_t (NULL: the context creates its own non-blocking stream; pass
+ * cudaStreamLegacy to run on the legacy default stream).  Not thread-safe: callers
  * serialise use of one context.  Replaces the reference's per-process runtime
  * (src/vibespatial/cuda/_runtime.py:1821-1852, launches on CuPy's stream). */
 int vs_context_create(int device, void* stream, vs_context** out);

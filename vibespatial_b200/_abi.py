@@ -167,8 +167,12 @@ class Context:
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
         self.torch_stream = stream
+        # torch reports its legacy default stream as handle 0, which the C-ABI
+        # reads as "create a private stream"; pass cudaStreamLegacy (0x1)
+        # instead so the join is ordered after torch's own copies.
+        handle = stream.cuda_stream or 0x1
         h = ctypes.c_void_p()
-        check(load().vs_context_create(self.device, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)))
+        check(load().vs_context_create(self.device, ctypes.c_void_p(handle), ctypes.byref(h)))
         self.handle = h
 
     def synchronize(self):
