@@ -15,13 +15,23 @@
 //   5. FP32 copies of every polygon relative to its own origin (box centre),
 //      with a per-polygon bound on the rounding error, for the split filter
 //
-// Query (points in input order, one thread each, no sort): the point's
-// level-L cell key -> occupancy bit -> root table -> leaf model -> binary
-// search inside the leaf's error window -> the cell's polygon list.  Each
-// candidate is box-filtered in FP32 (rounded outward) and refined with the
-// FP32 crossing test on tile-relative coordinates; only edges whose FP32
-// decision lies within the rounding-error bound are re-decided in FP64, and a
-// pair the FP64 filter cannot certify is deferred to the exact pass.
+// Query, three passes over the points:
+//   map      input order, one thread per point: level-L cell key ->
+//            occupancy bit -> root table -> leaf model -> binary search inside
+//            the leaf's error window -> cell index (or none), plus a
+//            warp-aggregated count of points per cell
+//   scatter  after an exclusive scan of the counts, points that fall in a
+//            stored cell are grouped by cell (coordinates copied beside their
+//            row), i.e. a counting sort on the learned index's own positions;
+//            points in empty cells are dropped here
+//   join     a warp takes 32 consecutive grouped points, which share one
+//            polygon list except at cell boundaries (broadcast list reads, no
+//            divergence between lanes of one cell); each candidate is
+//            box-filtered in FP32 (rounded outward) and refined with the FP32
+//            crossing test on tile-relative coordinates; only edges whose FP32
+//            decision lies within the rounding-error bound are re-decided in
+//            FP64, and a pair the FP64 filter cannot certify is deferred to
+//            the exact pass.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -416,6 +426,14 @@ struct LearnedArgs {
     PairSink sink;
     DeferSink defer;
     unsigned long long* counters;
+    // grouping scratch (per join)
+    int32_t* cell_of;          // [n] cell index of each point, -1 = none
+    uint32_t* cell_count;      // [n_cells] points per cell
+    uint32_t* cell_fill;       // [n_cells] running insert position (starts at the cell's offset)
+    double2* grp_xy;           // [n_grouped] coordinates grouped by cell
+    int32_t* grp_row;          // [n_grouped] original point row
+    int32_t* grp_cell;         // [n_grouped] cell index
+    const uint32_t* n_grouped;
 };
 
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
@@ -493,54 +511,93 @@ __device__ __forceinline__ int geometry_location_split(double px, double py, flo
     return LOC_OUTSIDE;
 }
 
-// Points in input order, one thread each: key -> occupancy -> root table ->
-// leaf model -> bounded binary search -> the cell's polygon list.
-__global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArgs a) {
+// Pass 1 (map), points in input order: level-L cell key -> occupancy bit ->
+// root table -> leaf model -> binary search inside the leaf's error window.
+// Writes the point's cell index (-1: no polygon can contain it) and counts
+// points per cell with warp-aggregated atomics.
+__device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, double y, double lox, double loy,
+                                              double sx, double sy, unsigned long long& n_wide) {
+    const uint32_t cell = (uint32_t)hilbert_key(quantize(x, lox, sx), quantize(y, loy, sy), a.L);
+    const uint32_t ob = cell >> a.occ_shift;
+    if (!((a.occ[ob >> 5] >> (ob & 31)) & 1u)) return -1;
+    const int leaf = a.root_table[cell >> a.root_shift];
+    const int2 er = a.leaf_err[leaf];
+    if (er.x > er.y) return -1;  // no stored key routes to this leaf
+    const long long pred = rmi_predict(a.leaf_ab[leaf], cell);
+    long long l0 = pred + er.x, h0 = pred + er.y + 1;  // search [l0, h0)
+    l0 = l0 < 0 ? 0 : l0;
+    h0 = h0 > a.n_cells ? a.n_cells : h0;
+    if (h0 - l0 > 256) ++n_wide;
+    const long long h1 = h0;
+    while (l0 < h0) {
+        const long long mid = (l0 + h0) >> 1;
+        if (a.cell_keys[mid] < cell) l0 = mid + 1;
+        else h0 = mid;
+    }
+    return (l0 < h1 && a.cell_keys[l0] == cell) ? (int)l0 : -1;
+}
+
+__global__ void __launch_bounds__(kThreads) learned_map_kernel(const LearnedArgs a) {
+    double lox, loy, sx, sy;
+    frame_q(a.frame, lox, loy, sx, sy);
+    const double fx1 = a.frame[2], fy1 = a.frame[3];
+    unsigned long long n_wide = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = a.px[i], y = a.py[i];
+        int c = -1;
+        if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1)
+            c = learned_lookup(a, x, y, lox, loy, sx, sy, n_wide);
+        a.cell_of[i] = c;
+        if (c >= 0) {
+            const unsigned peers = __match_any_sync(__activemask(), c);
+            if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&a.cell_count[c], (uint32_t)__popc(peers));
+        }
+    }
+    add_counter(a.counters, 6, n_wide);
+}
+
+// Pass 2 (scatter): points grouped by cell, coordinates copied next to their
+// row and cell so that pass 3 reads them coalesced.
+__global__ void __launch_bounds__(kThreads) learned_scatter_kernel(const LearnedArgs a) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = a.cell_of[i];
+        if (c >= 0) {
+            const unsigned peers = __match_any_sync(__activemask(), c);
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&a.cell_fill[c], (uint32_t)__popc(peers));
+            base = __shfl_sync(peers, base, leader);
+            const uint32_t pos = base + __popc(peers & ((1u << lane) - 1u));
+            a.grp_xy[pos] = make_double2(a.px[i], a.py[i]);
+            a.grp_row[pos] = (int32_t)i;
+            a.grp_cell[pos] = c;
+        }
+    }
+}
+
+// Pass 3 (join): a warp takes 32 consecutive grouped points, which share a
+// cell (and so a polygon list) except at cell boundaries.
+__global__ void __launch_bounds__(kThreads) learned_join_kernel(const LearnedArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
     __shared__ unsigned s_cnt[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) s_cnt[warp] = 0;
     __syncwarp();
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
-    double lox, loy, sx, sy;
-    frame_q(a.frame, lox, loy, sx, sy);
-    const double fx1 = a.frame[2], fy1 = a.frame[3];
+    const int64_t n = (int64_t)*a.n_grouped;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    unsigned long long n_cand = 0, n_wide = 0;
+    unsigned long long n_cand = 0;
     unsigned n32 = 0, n64 = 0;
-
-    for (int64_t base = gw * 32; base < a.n; base += nw * 32) {
-        const int64_t i = base + lane;
-        if (i < a.n) {
-            const double x = a.px[i], y = a.py[i];
-            const bool ok = (a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1;
-            uint32_t lo = 0, hi = 0;
-            if (ok) {
-                const uint32_t cell = (uint32_t)hilbert_key(quantize(x, lox, sx), quantize(y, loy, sy), a.L);
-                const uint32_t ob = cell >> a.occ_shift;
-                if ((a.occ[ob >> 5] >> (ob & 31)) & 1u) {
-                    const int leaf = a.root_table[cell >> a.root_shift];
-                    const int2 er = a.leaf_err[leaf];
-                    if (er.x <= er.y) {
-                        const long long pred = rmi_predict(a.leaf_ab[leaf], cell);
-                        long long l0 = pred + er.x, h0 = pred + er.y + 1;  // search [l0, h0)
-                        l0 = l0 < 0 ? 0 : l0;
-                        h0 = h0 > a.n_cells ? a.n_cells : h0;
-                        if (h0 - l0 > 256) ++n_wide;
-                        const long long h1 = h0;
-                        while (l0 < h0) {
-                            const long long mid = (l0 + h0) >> 1;
-                            if (a.cell_keys[mid] < cell) l0 = mid + 1;
-                            else h0 = mid;
-                        }
-                        if (l0 < h1 && a.cell_keys[l0] == cell) {
-                            lo = a.cell_start[l0];
-                            hi = a.cell_start[l0 + 1];
-                        }
-                    }
-                }
-            }
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t j = base + lane;
+        if (j < n) {
+            const double2 p = a.grp_xy[j];
+            const double x = p.x, y = p.y;
+            const int32_t row = a.grp_row[j];
+            const int c = a.grp_cell[j];
+            const uint32_t lo = a.cell_start[c], hi = a.cell_start[c + 1];
             for (uint32_t e = lo; e < hi; ++e) {
                 const int slot = (int)a.entries[e];
                 const double2 o = a.origin[slot];
@@ -558,9 +615,9 @@ __global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArg
                     const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
                     loc = geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
                 }
-                if (loc == LOC_UNDECIDED) defer(a.defer, (int32_t)i, slot);
+                if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
                 else if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                    wemit(out, a.sink, (int32_t)i, a.item_geom[slot]);
+                    wemit(out, a.sink, row, a.item_geom[slot]);
             }
         }
         wflush(out, a.sink, false);
@@ -569,7 +626,6 @@ __global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArg
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 2, n32);
     add_counter(a.counters, 3, n64);
-    add_counter(a.counters, 6, n_wide);
 }
 
 template <class T>
@@ -812,11 +868,23 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, int32_t* d_left,
                         int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
     const LearnedIndex& li = idx->learned;
+    cudaStream_t s = ctx->stream;
+    const int64_t n = pts->n;
+    Scratch<int32_t> cell_of, grp_row, grp_cell;
+    Scratch<uint32_t> cell_count, n_grouped;
+    Scratch<double2> grp_xy;
+    VS_TRY(cell_of.alloc((size_t)n, s));
+    VS_TRY(grp_row.alloc((size_t)n, s));
+    VS_TRY(grp_cell.alloc((size_t)n, s));
+    VS_TRY(grp_xy.alloc((size_t)n, s));
+    VS_TRY(cell_count.alloc((size_t)li.n_cells, s));
+    VS_TRY(n_grouped.alloc(1, s));
+    VS_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, (size_t)li.n_cells * sizeof(uint32_t), s));
     LearnedArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
     a.pvalid = pts->d_valid;
-    a.n = pts->n;
+    a.n = n;
     a.frame = idx->frame;
     a.L = li.level;
     a.occ_shift = 2 * (li.level - li.occ_level);
@@ -843,7 +911,20 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.defer = dsink;
     a.counters = ctx->d_counters;
-    join_learned_kernel<<<grid_for(pts->n, kThreads, 8), kThreads, 0, ctx->stream>>>(a);
+    a.cell_of = cell_of.p;
+    a.cell_count = cell_count.p;
+    a.cell_fill = cell_count.p;  // scanned in place: counts -> insert positions
+    a.grp_xy = grp_xy.p;
+    a.grp_row = grp_row.p;
+    a.grp_cell = grp_cell.p;
+    a.n_grouped = n_grouped.p;
+    const int grid = grid_for(n, kThreads, 8);
+    learned_map_kernel<<<grid, kThreads, 0, s>>>(a);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(exclusive_scan_u32(cell_count.p, cell_count.p, li.n_cells, n_grouped.p, s));
+    learned_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
+    VS_CUDA_TRY(cudaGetLastError());
+    learned_join_kernel<<<grid, kThreads, 0, s>>>(a);
     VS_CUDA_TRY(cudaGetLastError());
     return VS_OK;
 }
