@@ -15,23 +15,18 @@
 //   5. FP32 copies of every polygon relative to its own origin (box centre),
 //      with a per-polygon bound on the rounding error, for the split filter
 //
-// Query, three passes over the points:
-//   map      input order, one thread per point: level-L cell key ->
-//            occupancy bit -> root table -> leaf model -> binary search inside
-//            the leaf's error window -> cell index (or none), plus a
-//            warp-aggregated count of points per cell
-//   scatter  after an exclusive scan of the counts, points that fall in a
-//            stored cell are grouped by cell (coordinates copied beside their
-//            row), i.e. a counting sort on the learned index's own positions;
-//            points in empty cells are dropped here
-//   join     a warp takes 32 consecutive grouped points, which share one
-//            polygon list except at cell boundaries (broadcast list reads, no
-//            divergence between lanes of one cell); each candidate is
-//            box-filtered in FP32 (rounded outward) and refined with the FP32
-//            crossing test on tile-relative coordinates; only edges whose FP32
-//            decision lies within the rounding-error bound are re-decided in
-//            FP64, and a pair the FP64 filter cannot certify is deferred to
-//            the exact pass.
+// Query, one fused kernel over the points in input order (no sort):
+//   1. each lane looks up its point: level-L cell key -> occupancy bit ->
+//      root table -> leaf model -> binary search inside the leaf's error
+//      window -> the cell's polygon list [lo, hi)
+//   2. a warp scan of the list lengths lays out the warp's (point, entry)
+//      candidates in one index space, and the 32 lanes stride over it, so
+//      lanes never idle behind a neighbour's long list
+//   3. each candidate is box-filtered in FP32 (rounded outward) and refined
+//      with the FP32 crossing test on tile-relative coordinates; only edges
+//      whose FP32 decision lies within the rounding-error bound are re-decided
+//      in FP64, and a pair the FP64 filter cannot certify is deferred to the
+//      exact pass.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -426,14 +421,6 @@ struct LearnedArgs {
     PairSink sink;
     DeferSink defer;
     unsigned long long* counters;
-    // grouping scratch (per join)
-    int32_t* cell_of;          // [n] cell index of each point, -1 = none
-    uint32_t* cell_count;      // [n_cells] points per cell
-    uint32_t* cell_fill;       // [n_cells] running insert position (starts at the cell's offset)
-    double2* grp_xy;           // [n_grouped] coordinates grouped by cell
-    int32_t* grp_row;          // [n_grouped] original point row
-    int32_t* grp_cell;         // [n_grouped] cell index
-    const uint32_t* n_grouped;
 };
 
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
@@ -511,10 +498,10 @@ __device__ __forceinline__ int geometry_location_split(double px, double py, flo
     return LOC_OUTSIDE;
 }
 
-// Pass 1 (map), points in input order: level-L cell key -> occupancy bit ->
-// root table -> leaf model -> binary search inside the leaf's error window.
-// Writes the point's cell index (-1: no polygon can contain it) and counts
-// points per cell with warp-aggregated atomics.
+// Exact lookup of a point's cell in the learned index: level-L cell key ->
+// occupancy bit -> root table -> leaf model -> binary search inside the
+// leaf's error window.  Returns the cell's index, or -1 when no stored cell
+// matches (no polygon box overlaps the point's cell).
 __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, double y, double lox, double loy,
                                               double sx, double sy, unsigned long long& n_wide) {
     const uint32_t cell = (uint32_t)hilbert_key(quantize(x, lox, sx), quantize(y, loy, sy), a.L);
@@ -537,88 +524,85 @@ __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, do
     return (l0 < h1 && a.cell_keys[l0] == cell) ? (int)l0 : -1;
 }
 
-__global__ void __launch_bounds__(kThreads) learned_map_kernel(const LearnedArgs a) {
-    double lox, loy, sx, sy;
-    frame_q(a.frame, lox, loy, sx, sy);
-    const double fx1 = a.frame[2], fy1 = a.frame[3];
-    unsigned long long n_wide = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double x = a.px[i], y = a.py[i];
-        int c = -1;
-        if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1)
-            c = learned_lookup(a, x, y, lox, loy, sx, sy, n_wide);
-        a.cell_of[i] = c;
-        if (c >= 0) {
-            const unsigned peers = __match_any_sync(__activemask(), c);
-            if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&a.cell_count[c], (uint32_t)__popc(peers));
-        }
-    }
-    add_counter(a.counters, 6, n_wide);
-}
-
-// Pass 2 (scatter): points grouped by cell, coordinates copied next to their
-// row and cell so that pass 3 reads them coalesced.
-__global__ void __launch_bounds__(kThreads) learned_scatter_kernel(const LearnedArgs a) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int c = a.cell_of[i];
-        if (c >= 0) {
-            const unsigned peers = __match_any_sync(__activemask(), c);
-            const int leader = __ffs(peers) - 1;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(&a.cell_fill[c], (uint32_t)__popc(peers));
-            base = __shfl_sync(peers, base, leader);
-            const uint32_t pos = base + __popc(peers & ((1u << lane) - 1u));
-            a.grp_xy[pos] = make_double2(a.px[i], a.py[i]);
-            a.grp_row[pos] = (int32_t)i;
-            a.grp_cell[pos] = c;
-        }
-    }
-}
-
-// Pass 3 (join): a warp takes 32 consecutive grouped points, which share a
-// cell (and so a polygon list) except at cell boundaries.
-__global__ void __launch_bounds__(kThreads) learned_join_kernel(const LearnedArgs a) {
-    __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
-    __shared__ unsigned s_cnt[kThreads / 32];
+// Points in input order.  Each warp: (1) every lane looks up its point's
+// cell and polygon list [lo, hi); (2) a warp scan of the list lengths lays
+// the warp's (point, list entry) candidates out in one index space; (3) the
+// lanes stride over that space, so the box tests and refinements of the whole
+// warp are spread evenly over its 32 lanes whatever the list lengths are.
+__global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArgs a) {
+    constexpr int W = kThreads / 32;
+    __shared__ int2 s_buf[W][kWarpBuf];
+    __shared__ unsigned s_cnt[W];
+    __shared__ double2 s_pt[W][32];
+    __shared__ uint32_t s_seg[W][32];  // first candidate index of each lane's list
+    __shared__ uint32_t s_lo[W][32];   // each lane's first list entry
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) s_cnt[warp] = 0;
     __syncwarp();
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
-    const int64_t n = (int64_t)*a.n_grouped;
+    double lox, loy, sx, sy;
+    frame_q(a.frame, lox, loy, sx, sy);
+    const double fx1 = a.frame[2], fy1 = a.frame[3];
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    unsigned long long n_cand = 0;
+    unsigned long long n_cand = 0, n_wide = 0;
     unsigned n32 = 0, n64 = 0;
-    for (int64_t base = gw * 32; base < n; base += nw * 32) {
-        const int64_t j = base + lane;
-        if (j < n) {
-            const double2 p = a.grp_xy[j];
-            const double x = p.x, y = p.y;
-            const int32_t row = a.grp_row[j];
-            const int c = a.grp_cell[j];
-            const uint32_t lo = a.cell_start[c], hi = a.cell_start[c + 1];
-            for (uint32_t e = lo; e < hi; ++e) {
-                const int slot = (int)a.entries[e];
-                const double2 o = a.origin[slot];
-                const float qx = __double2float_rn(x - o.x), qy = __double2float_rn(y - o.y);
-                const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-                const float4 b32 = a.box32[slot];
-                if (__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
-                    __fsub_rd(qy, dp) > b32.w)
-                    continue;  // certainly outside the box
-                const vs_box bb = a.boxes[slot];
-                if (!(x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy)) continue;
-                ++n_cand;
-                int loc = 0;
-                if (a.accept_mask) {
-                    const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
-                    loc = geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
+
+    for (int64_t base = gw * 32; base < a.n; base += nw * 32) {
+        const int64_t i = base + lane;
+        double x = 0.0, y = 0.0;
+        uint32_t lo = 0, hi = 0;
+        if (i < a.n) {
+            x = a.px[i];
+            y = a.py[i];
+            if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1) {
+                const int c = learned_lookup(a, x, y, lox, loy, sx, sy, n_wide);
+                if (c >= 0) {
+                    lo = a.cell_start[c];
+                    hi = a.cell_start[c + 1];
                 }
-                if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
-                else if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                    wemit(out, a.sink, row, a.item_geom[slot]);
             }
+        }
+        // lay the warp's candidates out: lane j owns [seg_j, seg_j + hi_j - lo_j)
+        const uint32_t cnt = hi - lo;
+        uint32_t inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+        s_pt[warp][lane] = make_double2(x, y);
+        s_seg[warp][lane] = inc - cnt;
+        s_lo[warp][lane] = lo;
+        __syncwarp();
+        for (uint32_t k = lane; k < total; k += 32) {
+            // owner: the last lane whose segment starts at or before k
+            int j = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (s_seg[warp][j + step] <= k) j += step;
+            const uint32_t e = s_lo[warp][j] + (k - s_seg[warp][j]);
+            const double2 p = s_pt[warp][j];
+            const int32_t row = (int32_t)(base + j);
+            const int slot = (int)a.entries[e];
+            const double2 o = a.origin[slot];
+            const float qx = __double2float_rn(p.x - o.x), qy = __double2float_rn(p.y - o.y);
+            const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
+            const float4 b32 = a.box32[slot];
+            if (__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
+                __fsub_rd(qy, dp) > b32.w)
+                continue;  // certainly outside the box
+            const vs_box bb = a.boxes[slot];
+            if (!(p.x >= bb.minx && p.x <= bb.maxx && p.y >= bb.miny && p.y <= bb.maxy)) continue;
+            ++n_cand;
+            int loc = 0;
+            if (a.accept_mask) {
+                const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
+                loc = geometry_location_split(p.x, p.y, qx, qy, t, a, slot, n32, n64);
+            }
+            if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
+            else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) wemit(out, a.sink, row, a.item_geom[slot]);
         }
         wflush(out, a.sink, false);
     }
@@ -626,6 +610,7 @@ __global__ void __launch_bounds__(kThreads) learned_join_kernel(const LearnedArg
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 2, n32);
     add_counter(a.counters, 3, n64);
+    add_counter(a.counters, 6, n_wide);
 }
 
 template <class T>
@@ -870,16 +855,6 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     const LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
     const int64_t n = pts->n;
-    Scratch<int32_t> cell_of, grp_row, grp_cell;
-    Scratch<uint32_t> cell_count, n_grouped;
-    Scratch<double2> grp_xy;
-    VS_TRY(cell_of.alloc((size_t)n, s));
-    VS_TRY(grp_row.alloc((size_t)n, s));
-    VS_TRY(grp_cell.alloc((size_t)n, s));
-    VS_TRY(grp_xy.alloc((size_t)n, s));
-    VS_TRY(cell_count.alloc((size_t)li.n_cells, s));
-    VS_TRY(n_grouped.alloc(1, s));
-    VS_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, (size_t)li.n_cells * sizeof(uint32_t), s));
     LearnedArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
@@ -911,20 +886,7 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.defer = dsink;
     a.counters = ctx->d_counters;
-    a.cell_of = cell_of.p;
-    a.cell_count = cell_count.p;
-    a.cell_fill = cell_count.p;  // scanned in place: counts -> insert positions
-    a.grp_xy = grp_xy.p;
-    a.grp_row = grp_row.p;
-    a.grp_cell = grp_cell.p;
-    a.n_grouped = n_grouped.p;
-    const int grid = grid_for(n, kThreads, 8);
-    learned_map_kernel<<<grid, kThreads, 0, s>>>(a);
-    VS_CUDA_TRY(cudaGetLastError());
-    VS_TRY(exclusive_scan_u32(cell_count.p, cell_count.p, li.n_cells, n_grouped.p, s));
-    learned_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
-    VS_CUDA_TRY(cudaGetLastError());
-    learned_join_kernel<<<grid, kThreads, 0, s>>>(a);
+    join_learned_kernel<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(a);
     VS_CUDA_TRY(cudaGetLastError());
     return VS_OK;
 }
