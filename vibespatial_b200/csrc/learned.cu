@@ -15,18 +15,23 @@
 //   5. FP32 copies of every polygon relative to its own origin (box centre),
 //      with a per-polygon bound on the rounding error, for the split filter
 //
-// Query, one fused kernel over the points in input order (no sort):
-//   1. each lane looks up its point: level-L cell key -> occupancy bit ->
-//      root table -> leaf model -> binary search inside the leaf's error
-//      window -> the cell's polygon list [lo, hi)
-//   2. a warp scan of the list lengths lays out the warp's (point, entry)
-//      candidates in one index space, and the 32 lanes stride over it, so
-//      lanes never idle behind a neighbour's long list
-//   3. each candidate is box-filtered in FP32 (rounded outward) and refined
-//      with the FP32 crossing test on tile-relative coordinates; only edges
-//      whose FP32 decision lies within the rounding-error bound are re-decided
-//      in FP64, and a pair the FP64 filter cannot certify is deferred to the
-//      exact pass.
+// Query, three passes over the points (a counting sort keyed by the learned
+// index's own positions, so no general sort is needed):
+//   map      input order: level-L cell key -> occupancy bit -> root table ->
+//            leaf model -> binary search inside the leaf's error window ->
+//            cell index (or none); warp-aggregated atomics on the per-cell
+//            counts return each point's rank within its cell
+//   scatter  after an exclusive scan of the counts, each matched point
+//            writes one aligned 32-byte record (x, y, row, cell) at
+//            start[cell] + rank; points in empty cells drop out
+//   join     a warp takes 32 consecutive records, which share a polygon list
+//            except at cell boundaries, so the lanes read each polygon's data
+//            together (broadcast); each candidate is box-filtered in FP32
+//            (rounded outward) and refined with the FP32 crossing test on
+//            tile-relative coordinates; only edges whose FP32 decision lies
+//            within the rounding-error bound are re-decided in FP64, and a
+//            pair the FP64 filter cannot certify is deferred to the exact
+//            pass.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -390,6 +395,15 @@ __global__ void rmi_window_stats_kernel(const uint32_t* __restrict__ leaf_of, in
 }
 
 // ----------------------------------------------------------------- query ---
+// One grouped point: a full 32-byte sector, so the scatter writes whole
+// sectors (no read-modify-write of partially written ones).
+struct __align__(32) GroupedPoint {
+    double x, y;
+    int32_t row;
+    int32_t cell;
+    int64_t pad;
+};
+
 struct LearnedArgs {
     const double* px;
     const double* py;
@@ -421,6 +435,11 @@ struct LearnedArgs {
     PairSink sink;
     DeferSink defer;
     unsigned long long* counters;
+    // grouping scratch (per join)
+    int2* point_cell;          // [n] (cell index or -1, rank within the cell)
+    uint32_t* cell_count;      // [n_cells] counts, then (after the scan) start offsets
+    GroupedPoint* grouped;     // [n_grouped] points grouped by cell
+    const uint32_t* n_grouped;
 };
 
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
@@ -524,85 +543,92 @@ __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, do
     return (l0 < h1 && a.cell_keys[l0] == cell) ? (int)l0 : -1;
 }
 
-// Points in input order.  Each warp: (1) every lane looks up its point's
-// cell and polygon list [lo, hi); (2) a warp scan of the list lengths lays
-// the warp's (point, list entry) candidates out in one index space; (3) the
-// lanes stride over that space, so the box tests and refinements of the whole
-// warp are spread evenly over its 32 lanes whatever the list lengths are.
-__global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArgs a) {
-    constexpr int W = kThreads / 32;
-    __shared__ int2 s_buf[W][kWarpBuf];
-    __shared__ unsigned s_cnt[W];
-    __shared__ double2 s_pt[W][32];
-    __shared__ uint32_t s_seg[W][32];  // first candidate index of each lane's list
-    __shared__ uint32_t s_lo[W][32];   // each lane's first list entry
+// Pass 1 (map), points in input order: each point's cell and its rank among
+// the cell's points (warp-aggregated atomics on the per-cell counts).
+__global__ void __launch_bounds__(kThreads) learned_map_kernel(const LearnedArgs a) {
+    double lox, loy, sx, sy;
+    frame_q(a.frame, lox, loy, sx, sy);
+    const double fx1 = a.frame[2], fy1 = a.frame[3];
+    unsigned long long n_wide = 0;
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    // Warp-uniform loop: the whole warp reaches the match and shuffle together.
+    for (int64_t b0 = gw * 32; b0 < a.n; b0 += nw * 32) {
+        const int64_t i = b0 + lane;
+        int c = -1;
+        if (i < a.n) {
+            const double x = a.px[i], y = a.py[i];
+            if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1)
+                c = learned_lookup(a, x, y, lox, loy, sx, sy, n_wide);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (c >= 0 && lane == leader) base = atomicAdd(&a.cell_count[c], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (i < a.n) a.point_cell[i] = make_int2(c, (int)(base + __popc(peers & ((1u << lane) - 1u))));
+    }
+    add_counter(a.counters, 6, n_wide);
+}
+
+// Pass 2 (scatter): after the exclusive scan of the counts, each matched
+// point writes one aligned 32-byte record at start[cell] + rank.  Points in
+// empty cells are dropped here.
+__global__ void __launch_bounds__(kThreads) learned_scatter_kernel(const LearnedArgs a) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int2 cr = a.point_cell[i];
+        if (cr.x >= 0) {
+            GroupedPoint g;
+            g.x = a.px[i];
+            g.y = a.py[i];
+            g.row = (int32_t)i;
+            g.cell = cr.x;
+            a.grouped[a.cell_count[cr.x] + (uint32_t)cr.y] = g;
+        }
+    }
+}
+
+// Pass 3 (join): a warp takes 32 consecutive grouped points, which share a
+// cell (and so a polygon list: broadcast reads) except at cell boundaries.
+__global__ void __launch_bounds__(kThreads) learned_join_kernel(const LearnedArgs a) {
+    __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
+    __shared__ unsigned s_cnt[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) s_cnt[warp] = 0;
     __syncwarp();
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
-    double lox, loy, sx, sy;
-    frame_q(a.frame, lox, loy, sx, sy);
-    const double fx1 = a.frame[2], fy1 = a.frame[3];
+    const int64_t n = (int64_t)*a.n_grouped;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    unsigned long long n_cand = 0, n_wide = 0;
+    unsigned long long n_cand = 0;
     unsigned n32 = 0, n64 = 0;
-
-    for (int64_t base = gw * 32; base < a.n; base += nw * 32) {
-        const int64_t i = base + lane;
-        double x = 0.0, y = 0.0;
-        uint32_t lo = 0, hi = 0;
-        if (i < a.n) {
-            x = a.px[i];
-            y = a.py[i];
-            if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1) {
-                const int c = learned_lookup(a, x, y, lox, loy, sx, sy, n_wide);
-                if (c >= 0) {
-                    lo = a.cell_start[c];
-                    hi = a.cell_start[c + 1];
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t j = base + lane;
+        if (j < n) {
+            const GroupedPoint g = a.grouped[j];
+            const double x = g.x, y = g.y;
+            const uint32_t lo = a.cell_start[g.cell], hi = a.cell_start[g.cell + 1];
+            for (uint32_t e = lo; e < hi; ++e) {
+                const int slot = (int)a.entries[e];
+                const double2 o = a.origin[slot];
+                const float qx = __double2float_rn(x - o.x), qy = __double2float_rn(y - o.y);
+                const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
+                const float4 b32 = a.box32[slot];
+                if (__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
+                    __fsub_rd(qy, dp) > b32.w)
+                    continue;  // certainly outside the box
+                const vs_box bb = a.boxes[slot];
+                if (!(x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy)) continue;
+                ++n_cand;
+                int loc = 0;
+                if (a.accept_mask) {
+                    const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
+                    loc = geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
                 }
+                if (loc == LOC_UNDECIDED) defer(a.defer, g.row, slot);
+                else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) wemit(out, a.sink, g.row, a.item_geom[slot]);
             }
-        }
-        // lay the warp's candidates out: lane j owns [seg_j, seg_j + hi_j - lo_j)
-        const uint32_t cnt = hi - lo;
-        uint32_t inc = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += t;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-        s_pt[warp][lane] = make_double2(x, y);
-        s_seg[warp][lane] = inc - cnt;
-        s_lo[warp][lane] = lo;
-        __syncwarp();
-        for (uint32_t k = lane; k < total; k += 32) {
-            // owner: the last lane whose segment starts at or before k
-            int j = 0;
-#pragma unroll
-            for (int step = 16; step > 0; step >>= 1)
-                if (s_seg[warp][j + step] <= k) j += step;
-            const uint32_t e = s_lo[warp][j] + (k - s_seg[warp][j]);
-            const double2 p = s_pt[warp][j];
-            const int32_t row = (int32_t)(base + j);
-            const int slot = (int)a.entries[e];
-            const double2 o = a.origin[slot];
-            const float qx = __double2float_rn(p.x - o.x), qy = __double2float_rn(p.y - o.y);
-            const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-            const float4 b32 = a.box32[slot];
-            if (__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
-                __fsub_rd(qy, dp) > b32.w)
-                continue;  // certainly outside the box
-            const vs_box bb = a.boxes[slot];
-            if (!(p.x >= bb.minx && p.x <= bb.maxx && p.y >= bb.miny && p.y <= bb.maxy)) continue;
-            ++n_cand;
-            int loc = 0;
-            if (a.accept_mask) {
-                const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
-                loc = geometry_location_split(p.x, p.y, qx, qy, t, a, slot, n32, n64);
-            }
-            if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
-            else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) wemit(out, a.sink, row, a.item_geom[slot]);
         }
         wflush(out, a.sink, false);
     }
@@ -610,7 +636,6 @@ __global__ void __launch_bounds__(kThreads) join_learned_kernel(const LearnedArg
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 2, n32);
     add_counter(a.counters, 3, n64);
-    add_counter(a.counters, 6, n_wide);
 }
 
 template <class T>
@@ -855,6 +880,14 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     const LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
     const int64_t n = pts->n;
+    Scratch<int2> point_cell;
+    Scratch<uint32_t> cell_count, n_grouped;
+    Scratch<GroupedPoint> grouped;
+    VS_TRY(point_cell.alloc((size_t)n, s));
+    VS_TRY(grouped.alloc((size_t)n, s));
+    VS_TRY(cell_count.alloc((size_t)li.n_cells, s));
+    VS_TRY(n_grouped.alloc(1, s));
+    VS_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, (size_t)li.n_cells * sizeof(uint32_t), s));
     LearnedArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
@@ -886,7 +919,17 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.defer = dsink;
     a.counters = ctx->d_counters;
-    join_learned_kernel<<<grid_for(n, kThreads, 8), kThreads, 0, s>>>(a);
+    a.point_cell = point_cell.p;
+    a.cell_count = cell_count.p;
+    a.grouped = grouped.p;
+    a.n_grouped = n_grouped.p;
+    const int grid = grid_for(n, kThreads, 8);
+    learned_map_kernel<<<grid, kThreads, 0, s>>>(a);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(exclusive_scan_u32(cell_count.p, cell_count.p, li.n_cells, n_grouped.p, s));
+    learned_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
+    VS_CUDA_TRY(cudaGetLastError());
+    learned_join_kernel<<<grid, kThreads, 0, s>>>(a);
     VS_CUDA_TRY(cudaGetLastError());
     return VS_OK;
 }
