@@ -74,26 +74,8 @@ struct WarpOut {
     unsigned* cnt;
 };
 
-__device__ __forceinline__ void wemit(const WarpOut& o, const PairSink& k, int32_t l, int32_t r) {
-    const unsigned pos = atomicAdd(o.cnt, 1u);
-    if (pos < (unsigned)kWarpBuf) {
-        o.buf[pos] = make_int2(l, r);
-    } else {
-        const unsigned long long gp = atomicAdd(k.counter, 1ull);
-        if (gp < k.capacity) {
-            k.out_left[gp] = l;
-            k.out_right[gp] = r;
-        }
-    }
-}
-
-// Call with the whole warp converged.  Flushes when at least half full, or
-// always when `force`.
-__device__ __forceinline__ void wflush(const WarpOut& o, const PairSink& k, bool force) {
-    __syncwarp();
-    const unsigned raw = *o.cnt;
-    const unsigned c = raw < (unsigned)kWarpBuf ? raw : (unsigned)kWarpBuf;
-    if (!force && raw < (unsigned)(kWarpBuf / 2)) return;
+// Copy `c` buffered pairs out with one global atomic.  Whole warp, converged.
+__device__ __forceinline__ void wdrain(const WarpOut& o, const PairSink& k, unsigned c) {
     const int lane = threadIdx.x & 31;
     unsigned long long b = 0;
     if (lane == 0 && c) b = atomicAdd(k.counter, (unsigned long long)c);
@@ -107,7 +89,36 @@ __device__ __forceinline__ void wflush(const WarpOut& o, const PairSink& k, bool
         }
     }
     __syncwarp();
-    if (lane == 0) *o.cnt = 0;
+}
+
+// Warp-synchronous emission: every lane of the warp calls it at a converged
+// point; the lanes with `want` set append (l, r).  Positions come from a
+// ballot, so the buffer count is only ever written by lane 0 between
+// __syncwarp()s and there are no shared-memory atomics in divergent code.
+__device__ __forceinline__ void wemit_sync(const WarpOut& o, const PairSink& k, bool want, int32_t l, int32_t r) {
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (m == 0u) return;
+    const int lane = threadIdx.x & 31;
+    unsigned base = *o.cnt;
+    const unsigned add = (unsigned)__popc(m);
+    if (base + add > (unsigned)kWarpBuf) {
+        wdrain(o, k, base);
+        base = 0;
+    }
+    if (want) o.buf[base + (unsigned)__popc(m & ((1u << lane) - 1u))] = make_int2(l, r);
+    __syncwarp();
+    if (lane == 0) *o.cnt = base + add;
+    __syncwarp();
+}
+
+// Call with the whole warp converged.  Drains when at least half full, or
+// always when `force`.
+__device__ __forceinline__ void wflush(const WarpOut& o, const PairSink& k, bool force) {
+    __syncwarp();
+    const unsigned c = *o.cnt;
+    if (c == 0u || (!force && c < (unsigned)(kWarpBuf / 2))) return;
+    wdrain(o, k, c);
+    if ((threadIdx.x & 31) == 0) *o.cnt = 0;
     __syncwarp();
 }
 

@@ -144,13 +144,15 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
         if (box_overlaps(root, x0, y0, x1, y1)) {
             if (top == 0) {
                 // a single polygon: the root is the item
+                bool want = false;
                 if (active && box_has(root, x, y)) {
                     ++n_cand;
                     const int loc = a.accept_mask ? geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off,
                                                                                a.geom_off, 0) : 0;
                     if (loc == LOC_UNDECIDED) defer(a.defer, row, 0);
-                    else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) wemit(out, a.sink, row, a.item_geom[0]);
+                    else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                 }
+                wemit_sync(out, a.sink, want, row, a.item_geom[0]);
             } else {
                 if (lane == 0) s_stack[warp][0] = top;  // node 0 of the top level
                 sp = 1;
@@ -190,16 +192,17 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
                     const int j = __ffs(mm) - 1;
                     mm &= mm - 1;
                     const vs_box ib = s_items[warp][j];
+                    const int slot = (int)(slot0 + j);
+                    bool want = false;
                     if (active && box_has(ib, x, y)) {
                         ++n_cand;
-                        const int slot = (int)(slot0 + j);
                         int loc = 0;
                         if (a.accept_mask)
                             loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot);
                         if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
-                        else if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                            wemit(out, a.sink, row, a.item_geom[slot]);
+                        else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                     }
+                    wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
                 }
                 __syncwarp();
             }
@@ -225,18 +228,19 @@ __global__ void __launch_bounds__(kJoinThreads) join_brute_kernel(const RtreeArg
     unsigned long long n_cand = 0;
     for (int64_t base = gw * 32; base < a.n; base += nw * 32) {
         const int64_t i = base + lane;
-        if (i < a.n && (a.pvalid == nullptr || a.pvalid[i])) {
-            const double x = a.px[i], y = a.py[i];
-            for (int64_t c = 0; c < M; ++c) {
-                if (!box_has(a.nodes[c], x, y)) continue;
+        const bool act = i < a.n && (a.pvalid == nullptr || a.pvalid[i]);
+        const double x = act ? a.px[i] : 0.0, y = act ? a.py[i] : 0.0;
+        for (int64_t c = 0; c < M; ++c) {  // the same trip count in every lane
+            bool want = false;
+            if (act && box_has(a.nodes[c], x, y)) {
                 ++n_cand;
                 int loc = 0;
                 if (a.accept_mask)
                     loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, (int)c);
                 if (loc == LOC_UNDECIDED) defer(a.defer, (int32_t)i, (int32_t)c);
-                else if (!a.accept_mask || ((a.accept_mask >> loc) & 1))
-                    wemit(out, a.sink, (int32_t)i, a.item_geom[c]);
+                else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
             }
+            wemit_sync(out, a.sink, want, (int32_t)i, a.item_geom[c]);
         }
         wflush(out, a.sink, false);
     }
@@ -276,12 +280,15 @@ __global__ void __launch_bounds__(kJoinThreads) resolve_deferred_kernel(const Re
     unsigned n_exact = 0;
     for (int64_t base = gw * 32; base < n; base += nw * 32) {
         const int64_t k = base + lane;
+        bool want = false;
+        int2 pr = make_int2(0, 0);
         if (k < n) {
-            const int2 pr = a.pairs[k];
+            pr = a.pairs[k];
             const double x = a.px[pr.x], y = a.py[pr.x];
             const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, pr.y, n_exact);
-            if ((a.accept_mask >> loc) & 1) wemit(out, a.sink, pr.x, a.item_geom[pr.y]);
+            want = (a.accept_mask >> loc) & 1;
         }
+        wemit_sync(out, a.sink, want, pr.x, want ? a.item_geom[pr.y] : 0);
         wflush(out, a.sink, false);
     }
     wflush(out, a.sink, true);
@@ -349,7 +356,7 @@ int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
     VS_TRY(q.n_valid.alloc(1, s));
     VS_CUDA_TRY(cudaMemsetAsync(q.n_valid.p, 0, sizeof(uint32_t), s));
     point_sort_key_kernel<<<grid_for(n, 256, 16), 256, 0, s>>>(*pts, idx->frame, q.keys.p, q.order.p, q.n_valid.p);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("point_sort_key", s);
     // Sorting by the top 24 key bits (a level-12 Hilbert cell) already makes
     // a warp's 32 points spatially coherent; the low byte is left unsorted.
     VS_TRY(radix_sort_u32_u32(q.keys.p, q.order.p, n, 32, s, 8));
@@ -399,7 +406,7 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     const size_t smem = (size_t)a.staged * sizeof(vs_box);
     VS_CUDA_TRY(cudaFuncSetAttribute(join_rtree_packet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     join_rtree_packet_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, smem, ctx->stream>>>(a);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("join_rtree_packet", ctx->stream);
     return VS_OK;
 }
 
@@ -420,7 +427,7 @@ int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_point
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.counters = ctx->d_counters;
     resolve_deferred_kernel<<<kNumSMs * 4, kJoinThreads, 0, ctx->stream>>>(a);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("resolve_deferred", ctx->stream);
     return VS_OK;
 }
 

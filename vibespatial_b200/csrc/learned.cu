@@ -605,30 +605,52 @@ __global__ void __launch_bounds__(kThreads) learned_join_kernel(const LearnedArg
     unsigned n32 = 0, n64 = 0;
     for (int64_t base = gw * 32; base < n; base += nw * 32) {
         const int64_t j = base + lane;
+        GroupedPoint g{0.0, 0.0, 0, 0, 0};
+        uint32_t lo = 0, hi = 0;
         if (j < n) {
-            const GroupedPoint g = a.grouped[j];
-            const double x = g.x, y = g.y;
-            const uint32_t lo = a.cell_start[g.cell], hi = a.cell_start[g.cell + 1];
-            for (uint32_t e = lo; e < hi; ++e) {
-                const int slot = (int)a.entries[e];
+            g = a.grouped[j];
+            lo = a.cell_start[g.cell];
+            hi = a.cell_start[g.cell + 1];
+        }
+        const double x = g.x, y = g.y;
+        // Candidate loop with one trip count for the whole warp (the longest
+        // list among its lanes; in grouped order the lanes mostly share one).
+        uint32_t len = hi - lo, maxlen = len;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
+            maxlen = t > maxlen ? t : maxlen;
+        }
+        for (uint32_t k = 0; k < maxlen; ++k) {
+            bool want = false;
+            int32_t right = 0;
+            if (k < len) {
+                const int slot = (int)a.entries[lo + k];
                 const double2 o = a.origin[slot];
                 const float qx = __double2float_rn(x - o.x), qy = __double2float_rn(y - o.y);
                 const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
                 const float4 b32 = a.box32[slot];
-                if (__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
-                    __fsub_rd(qy, dp) > b32.w)
-                    continue;  // certainly outside the box
-                const vs_box bb = a.boxes[slot];
-                if (!(x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy)) continue;
-                ++n_cand;
-                int loc = 0;
-                if (a.accept_mask) {
-                    const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
-                    loc = geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
+                // FP32 box filter (rounded outward), then the exact FP64 box test
+                if (!(__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
+                      __fsub_rd(qy, dp) > b32.w)) {
+                    const vs_box bb = a.boxes[slot];
+                    if (x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy) {
+                        ++n_cand;
+                        int loc = 0;
+                        if (a.accept_mask) {
+                            const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
+                            loc = geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
+                        }
+                        if (loc == LOC_UNDECIDED) {
+                            defer(a.defer, g.row, slot);
+                        } else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) {
+                            want = true;
+                            right = a.item_geom[slot];
+                        }
+                    }
                 }
-                if (loc == LOC_UNDECIDED) defer(a.defer, g.row, slot);
-                else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) wemit(out, a.sink, g.row, a.item_geom[slot]);
             }
+            wemit_sync(out, a.sink, want, g.row, right);
         }
         wflush(out, a.sink, false);
     }
@@ -925,12 +947,13 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.n_grouped = n_grouped.p;
     const int grid = grid_for(n, kThreads, 8);
     learned_map_kernel<<<grid, kThreads, 0, s>>>(a);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("learned_map", s);
     VS_TRY(exclusive_scan_u32(cell_count.p, cell_count.p, li.n_cells, n_grouped.p, s));
+    VS_LAUNCHED("cell scan", s);
     learned_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("learned_scatter", s);
     learned_join_kernel<<<grid, kThreads, 0, s>>>(a);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("learned_join", s);
     return VS_OK;
 }
 

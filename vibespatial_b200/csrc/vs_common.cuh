@@ -20,6 +20,22 @@ void set_error(const char* fmt, ...);
         }                                                                        \
     } while (0)
 
+// After a kernel launch: report launch errors.  Debug builds compiled with
+// -DVS_DEBUG_SYNC also wait for the kernel and name it in the error message.
+#ifdef VS_DEBUG_SYNC
+#define VS_LAUNCHED(name, stream)                                                        \
+    do {                                                                                 \
+        cudaError_t _e = cudaGetLastError();                                             \
+        if (_e == cudaSuccess) _e = cudaStreamSynchronize(stream);                       \
+        if (_e != cudaSuccess) {                                                         \
+            ::vs::set_error("kernel %s failed: %s", name, cudaGetErrorString(_e));       \
+            return VS_E_CUDA;                                                            \
+        }                                                                                \
+    } while (0)
+#else
+#define VS_LAUNCHED(name, stream) VS_CUDA_TRY(cudaGetLastError())
+#endif
+
 #define VS_TRY(expr)                 \
     do {                             \
         int _s = (expr);             \
