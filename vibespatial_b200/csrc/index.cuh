@@ -18,6 +18,25 @@ constexpr int kMaxLevels = 16;   // 16^15 > 2^31 items
 // error window bounds the search, so every lookup is exact.
 constexpr int kRmiHidden = 32;
 
+// Everything the learned join needs about one polygon slot, in three 16-byte
+// words: the FP64 origin, the FP32 box relative to it (rounded outward), the
+// bound on the FP32 vertex rounding error, the original row, and for a
+// single-ring polygon its coordinate range (c0 = -1 for multi-ring shapes).
+struct __align__(16) SlotRecord {
+    double ox, oy;
+    float4 box;
+    float err;
+    int32_t geom;
+    int32_t c0, c1;
+};
+
+// Leaf of the RMI: position = floor(a + b * key), error window [lo, hi].
+struct __align__(16) RmiLeaf {
+    double a, b;
+    int32_t lo, hi;
+    int32_t pad0, pad1;
+};
+
 struct RmiModel {
     // root MLP weights (FP32): h1 = relu(w1 * x + b1); h2 = relu(W2 h1 + b2); y = w3 . h2 + b3
     float w1[kRmiHidden], b1[kRmiHidden];
@@ -49,7 +68,9 @@ struct LearnedIndex {
     uint16_t* root_table = nullptr;  // [4^root_level] leaf of each ancestor cell
     double2* leaf_ab = nullptr;      // [n_leaves] position = a + b * key
     int2* leaf_err = nullptr;        // [n_leaves] inclusive error window (lo, hi)
+    RmiLeaf* leaves = nullptr;       // [n_leaves] the two above packed for queries
     int32_t n_leaves = 0;
+    SlotRecord* slots = nullptr;     // [n_geoms] packed per-slot data for queries
     // FP32 tile-relative copies used by the split-precision filter
     double2* origin = nullptr;       // [n_geoms] slot origin (box centre, FP64)
     float4* box32 = nullptr;         // [n_geoms] slot box relative to the origin, rounded outward

@@ -194,6 +194,41 @@ __global__ void split_copy_kernel(const vs_box* __restrict__ box, int64_t M, con
     }
 }
 
+__global__ void pack_slots_kernel(int64_t M, const double2* __restrict__ origin, const float4* __restrict__ box32,
+                                  const float* __restrict__ err32, const int32_t* __restrict__ item_geom,
+                                  const int32_t* __restrict__ geom_off, const int32_t* __restrict__ part_off,
+                                  const int32_t* __restrict__ ring_off, SlotRecord* __restrict__ out) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M; s += (int64_t)gridDim.x * blockDim.x) {
+        SlotRecord r;
+        r.ox = origin[s].x;
+        r.oy = origin[s].y;
+        r.box = box32[s];
+        r.err = err32[s];
+        r.geom = item_geom[s];
+        const int32_t p0 = geom_off[s], p1 = geom_off[s + 1];
+        r.c0 = -1;
+        r.c1 = -1;
+        if (p1 - p0 == 1 && part_off[p0 + 1] - part_off[p0] == 1) {
+            r.c0 = ring_off[part_off[p0]];
+            r.c1 = ring_off[part_off[p0] + 1];
+        }
+        out[s] = r;
+    }
+}
+
+__global__ void pack_leaves_kernel(int nl, const double2* __restrict__ ab, const int2* __restrict__ err,
+                                   RmiLeaf* __restrict__ out) {
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += gridDim.x * blockDim.x) {
+        RmiLeaf f;
+        f.a = ab[l].x;
+        f.b = ab[l].y;
+        f.lo = err[l].x;
+        f.hi = err[l].y;
+        f.pad0 = f.pad1 = 0;
+        out[l] = f;
+    }
+}
+
 // ------------------------------------------------------------ RMI train ---
 // Training pairs: x = normalised ancestor key of stored cell i, t = i / n.
 __global__ void rmi_samples_kernel(const uint32_t* __restrict__ keys, int64_t n, int S, int anc_shift, double key_lo,
@@ -419,8 +454,8 @@ struct LearnedArgs {
     const uint32_t* cell_start;
     const uint32_t* entries;
     int64_t n_cells;
-    const double2* leaf_ab;
-    const int2* leaf_err;
+    const RmiLeaf* leaves;
+    const SlotRecord* slots;
     const vs_box* boxes;       // FP64 slot boxes (R-tree level 0)
     const double2* origin;
     const float4* box32;
@@ -526,11 +561,10 @@ __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, do
     const uint32_t cell = (uint32_t)hilbert_key(quantize(x, lox, sx), quantize(y, loy, sy), a.L);
     const uint32_t ob = cell >> a.occ_shift;
     if (!((a.occ[ob >> 5] >> (ob & 31)) & 1u)) return -1;
-    const int leaf = a.root_table[cell >> a.root_shift];
-    const int2 er = a.leaf_err[leaf];
-    if (er.x > er.y) return -1;  // no stored key routes to this leaf
-    const long long pred = rmi_predict(a.leaf_ab[leaf], cell);
-    long long l0 = pred + er.x, h0 = pred + er.y + 1;  // search [l0, h0)
+    const RmiLeaf lf = a.leaves[a.root_table[cell >> a.root_shift]];
+    if (lf.lo > lf.hi) return -1;  // no stored key routes to this leaf
+    const long long pred = rmi_predict(make_double2(lf.a, lf.b), cell);
+    long long l0 = pred + lf.lo, h0 = pred + lf.hi + 1;  // search [l0, h0)
     l0 = l0 < 0 ? 0 : l0;
     h0 = h0 > a.n_cells ? a.n_cells : h0;
     if (h0 - l0 > 256) ++n_wide;
@@ -545,7 +579,7 @@ __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, do
 
 // Pass 1 (map), points in input order: each point's cell and its rank among
 // the cell's points (warp-aggregated atomics on the per-cell counts).
-__global__ void __launch_bounds__(kThreads) learned_map_kernel(const LearnedArgs a) {
+__global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LearnedArgs a) {
     double lox, loy, sx, sy;
     frame_q(a.frame, lox, loy, sx, sy);
     const double fx1 = a.frame[2], fy1 = a.frame[3];
@@ -591,7 +625,7 @@ __global__ void __launch_bounds__(kThreads) learned_scatter_kernel(const Learned
 
 // Pass 3 (join): a warp takes 32 consecutive grouped points, which share a
 // cell (and so a polygon list: broadcast reads) except at cell boundaries.
-__global__ void __launch_bounds__(kThreads) learned_join_kernel(const LearnedArgs a) {
+__global__ void __launch_bounds__(kThreads, 5) learned_join_kernel(const LearnedArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
     __shared__ unsigned s_cnt[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -626,26 +660,31 @@ __global__ void __launch_bounds__(kThreads) learned_join_kernel(const LearnedArg
             int32_t right = 0;
             if (k < len) {
                 const int slot = (int)a.entries[lo + k];
-                const double2 o = a.origin[slot];
-                const float qx = __double2float_rn(x - o.x), qy = __double2float_rn(y - o.y);
+                const SlotRecord r = a.slots[slot];
+                const float qx = __double2float_rn(x - r.ox), qy = __double2float_rn(y - r.oy);
                 const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-                const float4 b32 = a.box32[slot];
-                // FP32 box filter (rounded outward), then the exact FP64 box test
-                if (!(__fadd_ru(qx, dp) < b32.x || __fsub_rd(qx, dp) > b32.z || __fadd_ru(qy, dp) < b32.y ||
-                      __fsub_rd(qy, dp) > b32.w)) {
-                    const vs_box bb = a.boxes[slot];
-                    if (x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy) {
+                // FP32 box filter (rounded outward: never rejects a point of the box)
+                if (!(__fadd_ru(qx, dp) < r.box.x || __fsub_rd(qx, dp) > r.box.z || __fadd_ru(qy, dp) < r.box.y ||
+                      __fsub_rd(qy, dp) > r.box.w)) {
+                    bool cand = true;
+                    int loc = 0;
+                    if (a.accept_mask) {
+                        // The exact location rejects points outside the box by itself.
+                        const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
+                        loc = r.c0 >= 0 ? ring_location_split(x, y, qx, qy, t, a.xy32, a.xy, r.c0, r.c1, n32, n64)
+                                        : geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
+                    } else {
+                        // Box candidates only: decide the box exactly in FP64.
+                        const vs_box bb = a.boxes[slot];
+                        cand = x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy;
+                    }
+                    if (cand) {
                         ++n_cand;
-                        int loc = 0;
-                        if (a.accept_mask) {
-                            const float t = __fmul_ru(__fadd_ru(a.err32[slot], dp), 1.0001f);
-                            loc = geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
-                        }
                         if (loc == LOC_UNDECIDED) {
                             defer(a.defer, g.row, slot);
                         } else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) {
                             want = true;
-                            right = a.item_geom[slot];
+                            right = r.geom;
                         }
                     }
                 }
@@ -768,6 +807,8 @@ int fit_leaves(vs_context* ctx, vs_index* idx) {
     rmi_leaf_fit_kernel<<<div_up(nl, 256), 256, 0, s>>>(sums.p, cov.p, nl, li.leaf_ab, li.leaf_err);
     rmi_err_kernel<<<grid_for(n, 256), 256, 0, s>>>(li.cell_keys, leaf_of.p, n, li.leaf_ab, li.leaf_err);
     rmi_window_stats_kernel<<<grid_for(n, 256), 256, 0, s>>>(leaf_of.p, n, li.leaf_err, acc.p);
+    VS_TRY(dalloc(&li.leaves, (size_t)nl, bytes));
+    pack_leaves_kernel<<<div_up(nl, 256), 256, 0, s>>>(nl, li.leaf_ab, li.leaf_err, li.leaves);
     VS_CUDA_TRY(cudaGetLastError());
     unsigned long long h[2];
     VS_CUDA_TRY(cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -793,6 +834,8 @@ void free_learned_index(vs_index* idx) {
     cudaFree(li.box32);
     cudaFree(li.err32);
     cudaFree(li.xy32);
+    cudaFree(li.leaves);
+    cudaFree(li.slots);
     li = LearnedIndex{};
 }
 
@@ -892,6 +935,10 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     split_copy_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
                                                             idx->xy, li.origin, li.box32, li.err32, li.xy32);
     VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(dalloc(&li.slots, (size_t)M, bytes));
+    pack_slots_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, li.origin, li.box32, li.err32, idx->item_geom, idx->geom_off,
+                                                       idx->part_off, idx->ring_off, li.slots);
+    VS_CUDA_TRY(cudaGetLastError());
     VS_CUDA_TRY(cudaStreamSynchronize(s));
     idx->has_learned = true;
     return VS_OK;
@@ -925,8 +972,8 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.cell_start = li.cell_start;
     a.entries = li.entries;
     a.n_cells = li.n_cells;
-    a.leaf_ab = li.leaf_ab;
-    a.leaf_err = li.leaf_err;
+    a.leaves = li.leaves;
+    a.slots = li.slots;
     a.boxes = idx->nodes;
     a.origin = li.origin;
     a.box32 = li.box32;
