@@ -34,6 +34,46 @@ __host__ __device__ __forceinline__ uint64_t hilbert_key(uint32_t x, uint32_t y,
     return d;
 }
 
+// Table-driven form of the same curve, four levels per step.  The walk above
+// only ever swaps x/y and/or complements both, so after any prefix the
+// remaining bits are read through one of four transforms (state = swap |
+// complement << 1).  Entry [state][4 bits of x][4 bits of y] holds the 8 key
+// bits of those four levels and the next state (bits 8-9).  Each block builds
+// the 1024 entries in shared memory from the per-level rule.
+constexpr int kHilbertLutSize = 1024;
+
+__device__ __forceinline__ void hilbert_lut_init(uint16_t* lut) {
+    for (int e = threadIdx.x; e < kHilbertLutSize; e += blockDim.x) {
+        uint32_t sw = (uint32_t)(e >> 8) & 1u, inv = (uint32_t)(e >> 9) & 1u;
+        const uint32_t bx = (uint32_t)(e >> 4) & 15u, by = (uint32_t)e & 15u;
+        uint32_t d = 0;
+        for (int lv = 3; lv >= 0; --lv) {
+            const uint32_t x0 = (bx >> lv) & 1u, y0 = (by >> lv) & 1u;
+            const uint32_t rx = (sw ? y0 : x0) ^ inv, ry = (sw ? x0 : y0) ^ inv;
+            d = (d << 2) | ((3u * rx) ^ ry);
+            if (ry == 0) {
+                if (rx == 1) inv ^= 1u;
+                sw ^= 1u;
+            }
+        }
+        lut[e] = (uint16_t)(d | ((sw | (inv << 1)) << 8));
+    }
+}
+
+// Top 2*levels bits of the Hilbert key (levels <= 16), equal to
+// hilbert_key(x, y, levels).
+__device__ __forceinline__ uint32_t hilbert_key_lut(uint32_t x, uint32_t y, int levels, const uint16_t* lut) {
+    const int chunks = (levels + 3) >> 2;
+    uint32_t d = 0, state = 0;
+    for (int c = 0; c < chunks; ++c) {
+        const int sh = 28 - 4 * c;
+        const uint32_t e = lut[(state << 8) | (((x >> sh) & 15u) << 4) | ((y >> sh) & 15u)];
+        d = (d << 8) | (e & 255u);
+        state = e >> 8;
+    }
+    return d >> (2 * (4 * chunks - levels));
+}
+
 // Quantise a coordinate to the 2^32 grid spanning [lo, lo + span] with scale
 // = (2^32 - 1) / span; values outside clamp to the border cells.
 __host__ __device__ __forceinline__ uint32_t quantize(double v, double lo, double scale) {

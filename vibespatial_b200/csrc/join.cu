@@ -73,6 +73,9 @@ __device__ __forceinline__ bool box_overlaps(const vs_box& b, double x0, double 
 
 __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ frame, uint32_t* __restrict__ keys,
                                       uint32_t* __restrict__ idx, uint32_t* __restrict__ n_valid) {
+    __shared__ uint16_t s_lut[kHilbertLutSize];
+    hilbert_lut_init(s_lut);
+    __syncthreads();
     const double f0 = frame[0], f1 = frame[1], f2 = frame[2], f3 = frame[3];
     const double sx = f2 > f0 ? 4294967295.0 / (f2 - f0) : 0.0;
     const double sy = f3 > f1 ? 4294967295.0 / (f3 - f1) : 0.0;
@@ -82,7 +85,7 @@ __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ fr
         const bool ok = (p.d_valid == nullptr || p.d_valid[i]) && x >= f0 && x <= f2 && y >= f1 && y <= f3;
         uint32_t k = 0xffffffffu;
         if (ok) {
-            k = (uint32_t)hilbert_key(quantize(x, f0, sx), quantize(y, f1, sy), 16);
+            k = hilbert_key_lut(quantize(x, f0, sx), quantize(y, f1, sy), 16, s_lut);
             if (k == 0xffffffffu) k = 0xfffffffeu;  // keep the sentinel unique
         }
         keys[i] = k;

@@ -557,8 +557,9 @@ __device__ __forceinline__ int geometry_location_split(double px, double py, flo
 // leaf's error window.  Returns the cell's index, or -1 when no stored cell
 // matches (no polygon box overlaps the point's cell).
 __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, double y, double lox, double loy,
-                                              double sx, double sy, unsigned long long& n_wide) {
-    const uint32_t cell = (uint32_t)hilbert_key(quantize(x, lox, sx), quantize(y, loy, sy), a.L);
+                                              double sx, double sy, const uint16_t* lut,
+                                              unsigned long long& n_wide) {
+    const uint32_t cell = hilbert_key_lut(quantize(x, lox, sx), quantize(y, loy, sy), a.L, lut);
     const uint32_t ob = cell >> a.occ_shift;
     if (!((a.occ[ob >> 5] >> (ob & 31)) & 1u)) return -1;
     const RmiLeaf lf = a.leaves[a.root_table[cell >> a.root_shift]];
@@ -580,6 +581,9 @@ __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, do
 // Pass 1 (map), points in input order: each point's cell and its rank among
 // the cell's points (warp-aggregated atomics on the per-cell counts).
 __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LearnedArgs a) {
+    __shared__ uint16_t s_lut[kHilbertLutSize];
+    hilbert_lut_init(s_lut);
+    __syncthreads();
     double lox, loy, sx, sy;
     frame_q(a.frame, lox, loy, sx, sy);
     const double fx1 = a.frame[2], fy1 = a.frame[3];
@@ -594,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LearnedA
         if (i < a.n) {
             const double x = a.px[i], y = a.py[i];
             if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1)
-                c = learned_lookup(a, x, y, lox, loy, sx, sy, n_wide);
+                c = learned_lookup(a, x, y, lox, loy, sx, sy, s_lut, n_wide);
         }
         const unsigned peers = __match_any_sync(0xffffffffu, c);
         const int leader = __ffs(peers) - 1;
