@@ -1,0 +1,209 @@
+"""The GeoPandas-compatible surface: sjoin, GeoSeries.within/contains, sindex.query.
+
+Each test runs twice: with the CPU oracle as the pair / location source
+(checks the host logic: predicate routing, frame assembly, index naming,
+suffixes, how='left'/'right'/'outer', on_attribute) and on the GPU through
+the C-ABI (marked gpu).  Expected shapes and values come from the reference's
+vendored GeoPandas test-suite (tests/upstream/geopandas/tools/tests/test_sjoin.py).
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pandas as pd
+import pytest
+
+import vibespatial_b200 as vs
+from vibespatial_b200 import predicates as vs_predicates
+from vibespatial_b200 import query as vs_query
+from vibespatial_b200.geometry import GeometryArray
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+EXP = json.loads((GOLDEN / "expected.json").read_text())
+
+
+@pytest.fixture(params=["oracle", pytest.param("gpu", marks=pytest.mark.gpu)])
+def backend(request, monkeypatch, oracle):
+    if request.param == "oracle":
+        def pairs(points, polygons, predicate):
+            px, py, pv = points.point_buffers()
+            pb = polygons.polygon_buffers()
+            P = oracle.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
+            left, right = oracle.join(px, py, pv, P, predicate)
+            return left.astype(np.intp), right.astype(np.intp)
+
+        def locate(points, polygons):
+            px, py, pv = points.point_buffers()
+            pb = polygons.polygon_buffers()
+            P = oracle.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
+            return oracle.locate_aligned(px, py, pv, P)
+
+        monkeypatch.setattr(vs_query, "_pairs_backend", pairs)
+        monkeypatch.setattr(vs_predicates, "_locate_backend", locate)
+    return request.param
+
+
+def nybb_frames():
+    d = dict(np.load(GOLDEN / "nybb.npz"))
+    geoms = GeometryArray.from_polygon_buffers(d["x"], d["y"], d["ring_off"], d["part_off"], d["geom_off"],
+                                               geom_type=d["geom_type"])
+    polydf = vs.GeoDataFrame({"BoroCode": d["attr_BoroCode"], "BoroName": d["attr_BoroName"],
+                              "Shape_Leng": d["attr_Shape_Leng"], "Shape_Area": d["attr_Shape_Area"]},
+                             geometry=geoms, crs="EPSG:2263")
+    b = [int(v) for v in polydf.total_bounds]
+    n = 20
+    xs = list(range(b[0], b[2], int((b[2] - b[0]) / n)))
+    ys = list(range(b[1], b[3], int((b[3] - b[1]) / n)))
+    pts = list(zip(xs, ys))
+    pointdf = vs.GeoDataFrame({"geometry": [vs.Point(x, y) for x, y in pts],
+                               "pointattr1": [x + y for x, y in pts], "pointattr2": [x - y for x, y in pts]},
+                              crs="EPSG:2263")
+    return pointdf, polydf
+
+
+def test_nybb_left_within(backend):
+    pointdf, polydf = nybb_frames()
+    df = vs.sjoin(pointdf, polydf, how="left", predicate="within")
+    assert list(df.shape) == EXP["nybb_within_left_shape"]["value"]
+    assert df.loc[1]["BoroName"] == EXP["nybb_within_left_row1_boro"]["value"]
+    assert set(df.geometry.geom_type) == {"Point"}
+    assert "pointattr1" in df.columns and "BoroCode" in df.columns and "index_right" in df.columns
+    # points contain polygons? never: all right columns missing
+    df2 = vs.sjoin(pointdf, polydf, how="left", predicate="contains")
+    assert df2.shape == (21, 8) and np.isnan(df2.loc[1]["Shape_Area"])
+
+
+def test_nybb_inner_and_right(backend):
+    pointdf, polydf = nybb_frames()
+    assert list(vs.sjoin(pointdf, polydf, how="inner").shape) == EXP["nybb_inner_intersects_shape"]["value"]
+    df = vs.sjoin(pointdf, polydf, how="right")
+    df2 = vs.sjoin(polydf, pointdf, how="left")
+    assert list(df.shape) == EXP["nybb_right_intersects_shape"]["value"]
+    assert df.shape == df2.shape
+    assert set(df.geometry.geom_type) == {"MultiPolygon"}
+    assert set(df2.geometry.geom_type) == {"MultiPolygon"}
+    assert list(df.columns[:1]) == ["index_left"]
+
+
+def test_nybb_geometry_name_and_duplicate_columns(backend):
+    pointdf, polydf = nybb_frames()
+    renamed = polydf.rename_geometry("new_geom")
+    res = vs.sjoin(renamed, pointdf, how="left")
+    assert res.geometry.name == "new_geom"
+    pointdf2 = pointdf.rename(columns={"pointattr1": "Shape_Area"})
+    df = vs.sjoin(pointdf2, polydf, how="left")
+    assert "Shape_Area_left" in df.columns and "Shape_Area_right" in df.columns
+    with pytest.raises(ValueError):
+        vs.sjoin(pointdf, polydf, how="left", predicate="spandex")
+    with pytest.raises(ValueError, match="`how` was"):
+        vs.sjoin(pointdf, polydf, how="abcde")
+    with pytest.raises(TypeError):
+        vs.sjoin(pointdf, polydf, unknown=1)
+
+
+def test_no_valid_geoms(backend):
+    pointdf, polydf = nybb_frames()
+    empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([]), crs=pointdf.crs)
+    for predicate in ("intersects", "within", "contains"):
+        assert vs.sjoin(pointdf, empty, how="inner", predicate=predicate).empty
+        assert vs.sjoin(pointdf, empty, how="right", predicate=predicate).empty
+        assert vs.sjoin(empty, pointdf, how="inner", predicate=predicate).empty
+        assert vs.sjoin(empty, pointdf, how="left", predicate=predicate).empty
+
+
+def test_cities_countries(backend):
+    w = dict(np.load(GOLDEN / "naturalearth_lowres.npz"))
+    c = dict(np.load(GOLDEN / "naturalearth_cities.npz"))
+    world = vs.GeoDataFrame({"name": w["attr_name"]},
+                            geometry=GeometryArray.from_polygon_buffers(w["x"], w["y"], w["ring_off"], w["part_off"],
+                                                                        w["geom_off"], geom_type=w["geom_type"]))
+    cities = vs.GeoDataFrame({"name": c["attr_name"]}, geometry=vs.points_from_xy(c["x"], c["y"]))
+    countries = world[["geometry", "name"]].rename(columns={"name": "country"})
+    out = vs.sjoin(cities, countries, how="inner", predicate="intersects")
+    assert list(out.shape) == EXP["cities_countries_inner_intersects_shape"]["value"]
+    # within == contains with the sides swapped
+    a = vs.sjoin(cities, countries, predicate="within")
+    b = vs.sjoin(countries, cities, predicate="contains")
+    assert sorted(zip(a.index, a["index_right"])) == sorted(zip(b["index_right"], b.index))
+
+
+def _small_frames(index_kind):
+    polys = vs.GeoDataFrame({"geometry": [vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11)],
+                             "df2": [3, 4, 5]})
+    pts = vs.GeoDataFrame({"geometry": [vs.Point(1, 1), vs.Point(4, 4), vs.Point(20, 20), vs.Point(5, 5)],
+                           "df1": [0, 1, 2, 3]})
+    if index_kind == "string-index":
+        pts.index = ["a", "b", "c", "d"]
+        polys.index = ["e", "f", "g"]
+    elif index_kind == "named-index":
+        pts.index.name = "df1_ix"
+        polys.index.name = "df2_ix"
+    elif index_kind == "multi-index":
+        pts = pts.set_index([["a", "b", "c", "d"], ["p", "q", "r", "s"]])
+        polys = polys.set_index([["e", "f", "g"], ["x", "y", "z"]])
+    return pts, polys
+
+
+@pytest.mark.parametrize("index_kind", ["default-index", "string-index", "named-index", "multi-index"])
+def test_index_naming_and_pairs(backend, index_kind):
+    pts, polys = _small_frames(index_kind)
+    res = vs.sjoin(pts, polys, how="inner", predicate="intersects")
+    # (1,1) in box0; (4,4) in box0 and box1; (5,5) on the boundary of box0, inside box1
+    assert res["df1"].tolist() == [0, 1, 1, 3, 3]
+    assert res["df2"].tolist() == [3, 3, 4, 3, 4]
+    within = vs.sjoin(pts, polys, how="inner", predicate="within")
+    assert within["df1"].tolist() == [0, 1, 1, 3]  # (5,5) is on box0's boundary: not within
+    if index_kind == "default-index":
+        assert "index_right" in res.columns and list(res.index) == [0, 1, 1, 3, 3]
+    elif index_kind == "named-index":
+        assert res.index.name == "df1_ix" and "df2_ix" in res.columns
+    elif index_kind == "multi-index":
+        assert res.index.nlevels == 2 and "index_right0" in res.columns and "index_right1" in res.columns
+    left = vs.sjoin(pts, polys, how="left", predicate="within")
+    assert len(left) == 5 and left["df2"].isna().sum() == 1
+    right = vs.sjoin(pts, polys, how="right", predicate="within")
+    assert len(right) == 5 and right["df1"].isna().sum() == 1  # box2 has no point
+    outer = vs.sjoin(pts, polys, how="outer", predicate="within")
+    assert len(outer) == 6  # 4 matches + point (20,20) alone + box2 alone
+    assert outer.geometry.isna().sum() == 0
+
+
+def test_on_attribute(backend):
+    pts = vs.GeoDataFrame({"geometry": [vs.Point(1, 1), vs.Point(4, 4)], "city": ["a", "b"]})
+    polys = vs.GeoDataFrame({"geometry": [vs.box(0, 0, 5, 5), vs.box(0, 0, 5, 5)], "city": ["a", "b"]})
+    res = vs.sjoin(pts, polys, predicate="within", on_attribute="city")
+    assert list(zip(res.index, res["index_right"])) == [(0, 0), (1, 1)]
+    with pytest.raises(ValueError, match="missing"):
+        vs.sjoin(pts, polys, on_attribute="nope")
+
+
+def test_elementwise_within_contains(backend):
+    polys = vs.GeoSeries([vs.box(0, 0, 2, 2), vs.Polygon(), None, vs.box(5, 1, 9, 3),
+                          vs.Polygon([(0, 0), (4, 0), (4, 4), (0, 4)])])
+    pts = vs.GeoSeries([None, vs.Point(), vs.Point(1, 1), vs.Point(8, 2), vs.Point(4, 2)])
+    # nulls / empties are False; (4, 2) is on the boundary: covered_by but not within
+    assert pts.within(polys).tolist() == [False, False, False, True, False]
+    assert pts.covered_by(polys).tolist() == [False, False, False, True, True]
+    assert polys.contains(pts).tolist() == [False, False, False, True, False]
+    assert polys.covers(pts).tolist() == [False, False, False, True, True]
+    assert pts.touches(polys).tolist() == [False, False, False, False, True]
+    # scalar broadcast and index alignment
+    s = vs.GeoSeries([vs.Point(1, 1), vs.Point(3, 3)], index=[10, 20])
+    assert s.within(vs.box(0, 0, 2, 2)).tolist() == [True, False]
+    p = vs.GeoSeries([vs.box(0, 0, 2, 2)], index=[20])
+    aligned = s.within(p)
+    assert aligned.index.tolist() == [10, 20] and aligned.tolist() == [False, False]
+
+
+def test_sindex_query(backend):
+    tree = vs.GeometryArray.from_shapes([vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11)])
+    q = vs.GeometryArray.from_shapes([vs.Point(1, 1), vs.Point(4, 4), vs.Point(20, 20)])
+    res = tree.sindex.query(q, predicate="intersects")
+    # tests/test_spatial_query.py:2787-2848
+    assert res[0].tolist() == [0, 1, 1] and res[1].tolist() == [0, 0, 1]
+    # points as the tree, polygons as the input: contains
+    res2 = q.sindex.query(tree, predicate="contains")
+    assert res2[0].tolist() == [0, 0, 1] and res2[1].tolist() == [0, 1, 1]
+    assert tree.sindex.query(q, predicate="contains").shape == (2, 0)
+    with pytest.raises(NotImplementedError):
+        tree.sindex.query(tree, predicate="intersects")

@@ -1,0 +1,36 @@
+"""vibespatial_b200: B200-native point-by-polygon spatial join.
+
+A drop-in for ``sjoin(points, polygons, predicate='within'|'intersects')``
+and ``GeometryArray.within/contains`` of vibeSpatial's GeoPandas-compatible
+API.  Pairs are computed on the GPU by hand-written sm_100a kernels behind a
+C-ABI (``libvsjoin.so``, declared in ``include/vsjoin.h``): an exact
+point-in-polygon refine on a packed Hilbert R-tree, or on a learned cell
+index with an FP32 tile-relative filter.  There is no CPU fallback.
+"""
+from .frame import GeoDataFrame, GeoSeries
+from .geometry import (
+    GeometryArray,
+    GeometryDtype,
+    MultiPolygon,
+    Point,
+    Polygon,
+    box,
+    points_from_xy,
+)
+from .query import SpatialIndex, query_spatial_index
+from .sjoin import sjoin
+
+__all__ = [
+    "GeoDataFrame",
+    "GeoSeries",
+    "GeometryArray",
+    "GeometryDtype",
+    "MultiPolygon",
+    "Point",
+    "Polygon",
+    "SpatialIndex",
+    "box",
+    "points_from_xy",
+    "query_spatial_index",
+    "sjoin",
+]

@@ -1,0 +1,99 @@
+"""Host <-> device bridge between GeometryArrays and the C-ABI library.
+
+GeometryArray buffers are uploaded once and cached on the array (the
+reference does the same with its owned device state, ``move_to``:
+src/vibespatial/geometry/owned.py).  The polygon side's index is built once
+per array and per method and reused by later joins, as the reference caches
+its flat index on the tree array (``owned_flat_sindex``,
+src/vibespatial/api/tools/sjoin.py:566-571).
+
+There is no CPU fallback: every entry point raises when no CUDA device or no
+built library is available.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _abi
+
+PREDICATE_CODES = {
+    None: _abi.PRED_BBOX,
+    "intersects": _abi.PRED_INTERSECTS,
+    "within": _abi.PRED_WITHIN,
+    "covered_by": _abi.PRED_COVERED_BY,
+    "touches": _abi.PRED_TOUCHES,
+}
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("vibespatial_b200 needs a CUDA device (B200); none is visible and there is no CPU path")
+    return torch
+
+
+def _dev(a, torch, device):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device)
+
+
+def device_points(ga, device: int = 0):
+    """(vs_points struct, keep-alive tensors) for a point GeometryArray."""
+    cached = ga._cache.get(("dpoints", device))
+    if cached is None:
+        torch = _torch()
+        x, y, valid = ga.point_buffers()
+        t = dict(x=_dev(x, torch, device), y=_dev(y, torch, device), valid=_dev(valid, torch, device))
+        cached = (_abi.make_points(t["x"], t["y"], t["valid"]), t)
+        ga._cache[("dpoints", device)] = cached
+    return cached
+
+
+def device_polygons(ga, device: int = 0):
+    cached = ga._cache.get(("dpolys", device))
+    if cached is None:
+        torch = _torch()
+        pb = ga.polygon_buffers()
+        t = dict(x=_dev(pb.x, torch, device), y=_dev(pb.y, torch, device),
+                 ring_off=_dev(pb.ring_off, torch, device), part_off=_dev(pb.part_off, torch, device),
+                 geom_off=_dev(pb.geom_off, torch, device), valid=_dev(pb.valid, torch, device))
+        cached = (_abi.make_polygons(t["x"], t["y"], t["ring_off"], t["part_off"], t["geom_off"], t["valid"]), t)
+        ga._cache[("dpolys", device)] = cached
+    return cached
+
+
+def polygon_index(ga, learned: bool = True, device: int = 0) -> "_abi.DeviceIndex":
+    key = ("index", device, learned)
+    idx = ga._cache.get(key)
+    if idx is None:
+        ctx = _abi.default_context(device)
+        P, _ = device_polygons(ga, device)
+        idx = ga._cache[key] = _abi.DeviceIndex(ctx, P, learned=learned)
+    return idx
+
+
+def join_pairs(points, polygons, predicate, *, method: str = "learned", device: int = 0):
+    """Sorted (point row, polygon row) pairs satisfying ``predicate`` (point on the left)."""
+    code = PREDICATE_CODES[predicate]
+    if len(points) == 0 or len(polygons) == 0:
+        return np.empty(0, np.intp), np.empty(0, np.intp)
+    learned = method == "learned"
+    index = polygon_index(polygons, learned=learned, device=device)
+    pts, _ = device_points(points, device)
+    m = _abi.METHOD_LEARNED if learned else (_abi.METHOD_BRUTE if method == "brute" else _abi.METHOD_RTREE)
+    left, right, _ = index.join(pts, code, m, sort=True)
+    return left.cpu().numpy().astype(np.intp), right.cpu().numpy().astype(np.intp)
+
+
+def locate_aligned(points, polygons, device: int = 0) -> np.ndarray:
+    """Row-wise location codes 0 outside / 1 boundary / 2 interior / 255 null-or-empty."""
+    torch = _torch()
+    n = len(points)
+    if n == 0:
+        return np.empty(0, np.uint8)
+    ctx = _abi.default_context(device)
+    pts, _ = device_points(points, device)
+    P, _ = device_polygons(polygons, device)
+    out = torch.empty(n, dtype=torch.uint8, device=device)
+    _abi.locate_aligned(ctx, pts, P, out)
+    return out.cpu().numpy()

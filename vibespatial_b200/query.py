@@ -1,0 +1,108 @@
+"""The operator seam of the join: ``query_spatial_index`` and ``SpatialIndex``.
+
+Mirrors the reference's query_spatial_index(tree, flat_index, geometry, *,
+predicate, sort, ...) (src/vibespatial/spatial/query.py:247-261) and the
+``sindex.query`` contract it serves (src/vibespatial/api/sindex.py:144): the
+result is a (2, K) intp array of (input geometry row, tree row) pairs for
+which ``predicate(input geometry, tree geometry)`` holds.  Only point x
+polygon combinations run here; whichever side holds the points becomes the
+query side of the CUDA join, and the pairs are swapped back when the tree
+holds the points (the reference swaps ``within`` <-> ``contains`` the same
+way on its host path, src/vibespatial/api/tools/sjoin.py:1049-1082).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+VALID_PREDICATES = {None, "intersects", "within", "contains", "contains_properly", "covers", "covered_by",
+                    "touches", "overlaps", "crosses", "dwithin"}
+
+# (points are the INPUT side) -> device predicate, or "empty" when the
+# predicate can never hold between a point and a polygon
+_INPUT_POINTS = {None: None, "intersects": "intersects", "within": "within", "covered_by": "covered_by",
+                 "touches": "touches", "contains": "empty", "contains_properly": "empty", "covers": "empty",
+                 "overlaps": "empty", "crosses": "empty"}
+# (points are the TREE side)
+_TREE_POINTS = {None: None, "intersects": "intersects", "contains": "within", "contains_properly": "within",
+                "covers": "covered_by", "touches": "touches", "within": "empty", "covered_by": "empty",
+                "overlaps": "empty", "crosses": "empty"}
+
+# Pair generator: the CUDA join.  Tests of the host logic substitute the CPU
+# oracle here; the package itself never does.
+_pairs_backend = None
+
+
+def _pairs(points, polygons, predicate, method):
+    if _pairs_backend is not None:
+        return _pairs_backend(points, polygons, predicate)
+    from ._device import join_pairs
+
+    return join_pairs(points, polygons, predicate, method=method)
+
+
+def query_spatial_index(tree, geometry, *, predicate=None, sort=False, distance=None, method="learned"):
+    """(2, K) intp array of (geometry row, tree row) pairs satisfying ``predicate``.
+
+    ``tree`` and ``geometry`` are GeometryArrays; one must hold points and the
+    other polygons/multipolygons.  ``sort`` orders the pairs by (geometry row,
+    tree row) (the CUDA join always returns them sorted).
+    """
+    from .geometry import GeometryArray
+
+    if predicate not in VALID_PREDICATES:
+        raise ValueError(f"Got predicate='{predicate}'; `predicate` must be one of {sorted(map(str, VALID_PREDICATES))}")
+    if predicate == "dwithin" or distance is not None:
+        raise NotImplementedError("the dwithin predicate is outside this point-in-polygon join")
+    if not isinstance(tree, GeometryArray) or not isinstance(geometry, GeometryArray):
+        raise TypeError("query_spatial_index expects GeometryArrays")
+    empty = np.empty((2, 0), dtype=np.intp)
+    if len(tree) == 0 or len(geometry) == 0:
+        return empty
+    if geometry.is_points() and tree.is_polygonal():
+        pred = _INPUT_POINTS[predicate]
+        if pred == "empty":
+            return empty
+        left, right = _pairs(geometry, tree, pred, method)
+        return np.vstack([left, right]).astype(np.intp)
+    if geometry.is_polygonal() and tree.is_points():
+        pred = _TREE_POINTS[predicate]
+        if pred == "empty":
+            return empty
+        pt, poly = _pairs(tree, geometry, pred, method)
+        out = np.vstack([poly, pt]).astype(np.intp)
+        if out.shape[1]:
+            order = np.lexsort((out[1], out[0]))
+            out = out[:, order]
+        return out
+    raise NotImplementedError(
+        "vibespatial_b200 joins points with polygons/multipolygons only "
+        f"(tree families {sorted(tree.families())}, input families {sorted(geometry.families())})")
+
+
+class SpatialIndex:
+    """``GeometryArray.sindex``: a reusable index over the array (the tree side)."""
+
+    valid_query_predicates = {p for p in VALID_PREDICATES if p != "dwithin"}
+
+    def __init__(self, geometry):
+        self.geometry = geometry
+
+    def __len__(self):
+        return len(self.geometry)
+
+    @property
+    def is_empty(self):
+        return len(self.geometry) == 0
+
+    def query(self, geometry, predicate=None, sort=False, distance=None, method="learned"):
+        from .geometry import BaseGeometry, GeometryArray
+
+        if isinstance(geometry, BaseGeometry):
+            res = query_spatial_index(self.geometry, GeometryArray.from_shapes([geometry]), predicate=predicate,
+                                      sort=sort, distance=distance, method=method)
+            return res[1]
+        geometry = getattr(geometry, "values", geometry)
+        if not isinstance(geometry, GeometryArray):
+            geometry = GeometryArray.from_shapes(list(geometry))
+        return query_spatial_index(self.geometry, geometry, predicate=predicate, sort=sort, distance=distance,
+                                   method=method)
