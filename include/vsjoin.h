@@ -181,6 +181,23 @@ int vs_radix_sort_pairs(vs_context* ctx, uint64_t* d_keys, uint32_t* d_vals, int
 int vs_hilbert_keys(vs_context* ctx, const double* d_x, const double* d_y, int64_t n,
                     double minx, double miny, double maxx, double maxy, uint64_t* d_keys);
 
+/* Brute-force point x polygon join that allocates no device memory, for
+ * callers that cannot allocate (a host that owns all device memory in a
+ * fixed arena, a hard memory budget, a loop that cannot afford an
+ * allocation's synchronisation).  No counterpart in the reference: it has no
+ * allocation-free join.  Inputs and the pair buffers are the caller's; the
+ * kernels' only scratch (one box per polygon and a pair counter) is a fixed
+ * 2 MiB device array inside the library, held by every GPU that loads it.
+ * At most 65,536 polygon rows (larger inputs: VS_E_ARG).  Runs on `stream`
+ * (a cudaStream_t, NULL = legacy default) of the current device; the first
+ * call on a device resolves the array's address (cudaGetSymbolAddress), so
+ * make it before any stream capture.  Calls that overlap on the GPU share the
+ * array and race: serialise them.  Pairs come back unordered; VS_E_CAPACITY
+ * reports the required size in *n_pairs. */
+int vs_join_brute_noalloc(const vs_points* pts, const vs_polygons* polys, int32_t predicate,
+                          int32_t* d_left, int32_t* d_right, int64_t capacity, int64_t* n_pairs,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

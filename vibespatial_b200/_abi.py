@@ -25,6 +25,7 @@ EXPORTED = (
     "vs_version", "vs_last_error", "vs_context_create", "vs_context_destroy",
     "vs_context_synchronize", "vs_index_build", "vs_index_info_get", "vs_index_free",
     "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
+    "vs_join_brute_noalloc",
 )
 
 
@@ -123,6 +124,8 @@ def load(path: Path | str | None = None):
             "vs_radix_sort_pairs": (ctypes.c_int, [vp, vp, vp, i64, i32]),
             "vs_hilbert_keys": (ctypes.c_int, [vp, vp, vp, i64, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_double, vp]),
+            "vs_join_brute_noalloc": (ctypes.c_int, [ctypes.POINTER(Points), ctypes.POINTER(Polygons), i32, vp, vp,
+                                                     i64, ctypes.POINTER(i64), vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -272,6 +275,21 @@ class DeviceIndex:
 
 def locate_aligned(ctx: Context, pts: Points, polys: Polygons, out) -> None:
     check(load().vs_locate_aligned(ctx.handle, ctypes.byref(pts), ctypes.byref(polys), _ptr(out)))
+
+
+def join_brute_noalloc(pts: Points, polys: Polygons, predicate: int, left, right, stream: int = 0) -> int:
+    """Allocation-free brute-force join (see vs_join_brute_noalloc); returns the pair count.
+
+    For callers that cannot allocate device memory: the pairs go to the
+    caller's ``left`` / ``right`` buffers and the library's only scratch is a
+    fixed device array (at most 65,536 polygons).  Pairs are unordered.
+    """
+    n = ctypes.c_int64(0)
+    cap = 0 if left is None else int(left.numel())
+    status = load().vs_join_brute_noalloc(ctypes.byref(pts), ctypes.byref(polys), int(predicate), _ptr(left),
+                                          _ptr(right), cap, ctypes.byref(n), ctypes.c_void_p(stream))
+    check(status, required=int(n.value))
+    return int(n.value)
 
 
 def sort_pairs(ctx: Context, left, right) -> None:
