@@ -1,0 +1,88 @@
+"""Sharded join across ranks (gloo, world size 2, CPU): the union of the ranks'
+pairs equals the single-process join, and the gathered counts locate them."""
+import os
+import socket
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def test_shard_range_covers_everything_once():
+    from vibespatial_b200.sharding import shard_range
+
+    for n in (0, 1, 7, 100, 1001):
+        for world in (1, 2, 3, 8):
+            spans = [shard_range(n, r, world) for r in range(world)]
+            assert spans[0][0] == 0 and spans[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+            sizes = [b - a for a, b in spans]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        shard_range(10, 2, 2)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out_dir):
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle as O
+    from vibespatial_b200.geometry import GeometryArray
+    from vibespatial_b200.sharding import sharded_join
+    from vibespatial_b200.testing import synthetic as syn
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        w = syn.star_join(seed=31, n_points=30_001, n_polys=300)
+        points = GeometryArray.from_points(w.px, w.py)
+        polys = GeometryArray.from_polygon_buffers(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off,
+                                                   w.polys.geom_off)
+
+        def pairs_fn(pts, pg, predicate):  # the CPU oracle stands in for the GPU join here
+            px, py, pv = pts.point_buffers()
+            pb = pg.polygon_buffers()
+            return O.join(px, py, pv, O.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid),
+                          predicate)
+
+        left, right, counts = sharded_join(points, polys, "within", pairs_fn=pairs_fn)
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), left=left, right=right, counts=counts)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_sharded_join(tmp_path, oracle):
+    import torch.multiprocessing as mp
+
+    from vibespatial_b200.testing import synthetic as syn
+
+    world = 2
+    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    parts = [np.load(tmp_path / f"rank{r}.npz") for r in range(world)]
+    counts = parts[0]["counts"]
+    assert np.array_equal(counts, parts[1]["counts"])
+    assert [len(p["left"]) for p in parts] == counts.tolist()
+    left = np.concatenate([p["left"] for p in parts])
+    right = np.concatenate([p["right"] for p in parts])
+    w = syn.star_join(seed=31, n_points=30_001, n_polys=300)
+    el, er = oracle.join(w.px, w.py, None, oracle.Polygons(w.polys.x, w.polys.y, w.polys.ring_off,
+                                                          w.polys.part_off, w.polys.geom_off), "within")
+    o = np.lexsort((right, left))
+    np.testing.assert_array_equal(left[o], el)
+    np.testing.assert_array_equal(right[o], er)
+    # rank 0 holds the lower half of the points
+    assert parts[0]["left"].max() < parts[1]["left"].min()
