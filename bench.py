@@ -117,11 +117,19 @@ def make_workload(name: str, rank: int = 0, scale: float = 1.0):
     raise ValueError(name)
 
 
+def make_batched(rank: int = 0, scale: float = 1.0):
+    from vibespatial_b200.testing import synthetic as syn
+
+    return syn.batched_jobs(seed=2 + 1000 * rank, n_jobs=max(1, int(round(256 * scale))))
+
+
 WORKLOAD_DESC = {
     "zipf": "zipf_join: 50M FP64 points x 1M footprints, Zipf(s=1.1) clusters over 1024 sites in [0,1000]^2",
     "utm": "utm_join: 10M FP64 points (64-component GMM) x 100k footprints, UTM-like frame",
     "star": "star_join: 100k points x 1k star polygons in [0,1000]^2",
     "degenerate": "degenerate_join: 20M points x 200k polygons with holes/multiparts, on-edge and 1-ulp points",
+    "batched": "batched_jobs: 256 independent star joins, points logU[1k,2M] (69.6M total), polygons "
+               "logU[10,50k] (1.38M total), one persistent launch replayed from a CUDA graph",
 }
 
 
@@ -130,12 +138,6 @@ def algorithmic_bytes(w, n_pairs: int) -> int:
     p = w.polys
     return int(16 * w.n_points + 16 * p.n_coords + 4 * (len(p.ring_off) + len(p.part_off) + len(p.geom_off))
                + 8 * n_pairs)
-
-
-def launches_per_join(method: int) -> int:
-    """Kernels of ours one vs_join launches: point keys, 4 radix passes x
-    (histogram + 2 scan kernels + scatter), the join kernel."""
-    return 1 + 4 * 4 + 1
 
 
 def cpu_sample_rate(w, predicate: str, threads: int, target_s: float = 10.0):
@@ -157,8 +159,74 @@ def cpu_sample_rate(w, predicate: str, threads: int, target_s: float = 10.0):
     return n2 / dt2, n2, dt2
 
 
+def cpu_sample_batched(jobs, predicate: str, threads: int, target_s: float = 10.0):
+    """Oracle (all host threads) job after job until ~target_s of work; points/sec."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    n = 0
+    dt = 0.0
+    k = 0
+    for w in jobs:
+        P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+        t0 = time.perf_counter()
+        O.join(w.px, w.py, None, P, predicate, threads)
+        dt += time.perf_counter() - t0
+        n += w.n_points
+        k += 1
+        if dt >= target_s:
+            break
+    return n / dt, n, dt, k
+
+
+def run_reference_batched(args, world):
+    jobs = make_batched(0, args.scale)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    # a bounded sample: the first jobs up to --ref-sample points
+    sample, n = [], 0
+    for w in jobs:
+        if n >= args.ref_sample and sample:
+            break
+        sample.append((w, O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)))
+        n += w.n_points
+
+    def step():
+        for w, P in sample:
+            O.join(w.px, w.py, None, P, args.predicate, threads)
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = n * len(times) / tot
+    line = {
+        "impl": "reference", "metric": "query points/sec", "value": value, "unit": "points/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate, "sample_points": n,
+                   "sample_jobs": len(sample)},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
+                         "sample": f"first {len(sample)} of {len(jobs)} jobs ({n} points), exact CPU oracle "
+                                   "(C + OpenMP): Shapely/GEOS is not installable here"},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
+        return
+    if args.workload == "batched":
+        run_reference_batched(args, world)
         return
     w = make_workload(args.workload, 0, args.scale)
     threads = os.cpu_count() or 1
@@ -244,6 +312,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     kernel_ms = []
+    launches = 0
     with ClockSampler(dev) as clk:
         if args.profile:
             torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
@@ -252,6 +321,7 @@ def run_ours(args, rank, world, local_rank):
             n_k, st = index.join_into(pts, pred, method, left, right)
             ev[k][1].record(stream)
             kernel_ms.append(st["kernel_ms"])
+            launches += st["kernel_launches"]
             assert n_k == n_pairs
         torch.cuda.synchronize()
         if args.profile:
@@ -330,13 +400,179 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
                 "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int(8 * n_pairs)},
-        "gpu_launches": args.steps * launches_per_join(method),
+        "gpu_launches": launches,
         "join_stats": stats,
         "index_info": info,
     }
     if plain is not None:
         line["plain_rtree_ms"] = plain
         line["learned_vs_plain"] = plain / kmed
+    line["clocks"] = clk.summary()
+    print(json.dumps(line), flush=True)
+
+
+def run_batched(args, rank, world, local_rank):
+    """Batched joins: all jobs in one persistent launch, replayed from a CUDA graph."""
+    import torch
+
+    from vibespatial_b200 import _abi, autotune
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    jobs = make_batched(rank, args.scale)
+    ctx = _abi.Context(dev)
+    stream = ctx.torch_stream
+    pred = {"within": _abi.PRED_WITHIN, "intersects": _abi.PRED_INTERSECTS}[args.predicate]
+    t0 = time.perf_counter()
+    indexes, build_ms, n_polys = [], 0.0, 0
+    for w in jobs:
+        d = {k: torch.from_numpy(np.ascontiguousarray(getattr(w.polys, k))).to(dev)
+             for k in ("x", "y", "ring_off", "part_off", "geom_off")}
+        ix = _abi.DeviceIndex(ctx, _abi.make_polygons(d["x"], d["y"], d["ring_off"], d["part_off"], d["geom_off"]))
+        indexes.append(ix)
+        build_ms += ix.info()["build_ms"]
+        n_polys += len(w.polys)
+    build_wall = time.perf_counter() - t0
+    px = np.concatenate([w.px for w in jobs])
+    py = np.concatenate([w.py for w in jobs])
+    job_start = np.concatenate([[0], np.cumsum([w.n_points for w in jobs])]).astype(np.int64)
+    N = len(px)
+    dx = torch.from_numpy(px).to(dev)
+    dy = torch.from_numpy(py).to(dev)
+    pts = _abi.make_points(dx, dy)
+    # exact pair count from a first direct run, then buffers of that size
+    probe = _abi.BatchPlan(ctx, indexes, pts, job_start)
+    probe_l, _, _ = probe.run(pred, use_graph=False)
+    n_pairs = int(probe_l.numel())
+    del probe_l
+    probe.close()
+    cap = max(1024, n_pairs)
+    left = torch.empty(cap, dtype=torch.int32, device=dev)
+    right = torch.empty(cap, dtype=torch.int32, device=dev)
+    name, sms = autotune.device_identity(dev)
+    key = autotune.cache_key(name, sms, autotune.shape_class(len(jobs), N, n_polys), pred)
+    tune_s = None
+    if args.autotune:
+        t1 = time.perf_counter()
+        opts = autotune.tuned_options(ctx, indexes, pts, job_start, pred, n_polys, left=left, right=right,
+                                      use_cache=False)
+        tune_s = time.perf_counter() - t1
+        opts_src = "searched"
+    else:
+        opts = autotune.lookup(key)
+        opts_src = "cache" if opts else "defaults"
+        opts = opts or dict(autotune.DEFAULTS)
+    plan = _abi.BatchPlan(ctx, indexes, pts, job_start, options=opts)
+    for _ in range(args.warmup):
+        n_w, _ = plan.run_into(pred, left, right, use_graph=True)
+        assert n_w == n_pairs, (n_w, n_pairs)
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms, launches = [], 0
+    with ClockSampler(dev) as clk:
+        if args.profile:
+            torch.cuda.profiler.start()
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            n_k, st = plan.run_into(pred, left, right, use_graph=True)
+            ev[k][1].record(stream)
+            kernel_ms.append(st["kernel_ms"])
+            launches += st["kernel_launches"]
+            assert n_k == n_pairs
+        torch.cuda.synchronize()
+        if args.profile:
+            torch.cuda.profiler.stop()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        # the same jobs one vs_join call at a time (how a caller without the
+        # batch API runs them), after the timed region
+        loop_ms = []
+        views = [(_abi.make_points(dx[a:b], dy[a:b]), a) for a, b in zip(job_start[:-1], job_start[1:])]
+        for _ in range(3):
+            a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a_ev.record(stream)
+            off = 0
+            for ix, (pv, _a) in zip(indexes, views):
+                n_j, _ = ix.join_into(pv, pred, _abi.METHOD_RTREE, left[off:], right[off:])
+                off += n_j
+            b_ev.record(stream)
+            torch.cuda.synchronize()
+            assert off == n_pairs, (off, n_pairs)
+            loop_ms.append(a_ev.elapsed_time(b_ev))
+        # e2e through the C-ABI with host buffers: H2D points, batched join, D2H pairs
+        hx = torch.from_numpy(px).pin_memory()
+        hy = torch.from_numpy(py).pin_memory()
+        hl = torch.empty(cap, dtype=torch.int32).pin_memory()
+        hr = torch.empty(cap, dtype=torch.int32).pin_memory()
+        e2e_ms = []
+        for _ in range(max(3, args.steps)):
+            a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                a_ev.record(stream)
+                dx.copy_(hx, non_blocking=True)
+                dy.copy_(hy, non_blocking=True)
+                n_e, _ = plan.run_into(pred, left, right, use_graph=True)
+                assert n_e == n_pairs, (n_e, n_pairs)
+                hl[:n_e].copy_(left[:n_e], non_blocking=True)
+                hr[:n_e].copy_(right[:n_e], non_blocking=True)
+                b_ev.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms.append(a_ev.elapsed_time(b_ev))
+    total_ms = float(sum(step_ms))
+    if dist:
+        t = torch.tensor([total_ms, float(np.median(e2e_ms))], device=dev, dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        total_ms, e2e_med = float(t[0]), float(t[1])
+    else:
+        e2e_med = float(np.median(e2e_ms))
+    value = world * N * args.steps / (total_ms / 1e3)
+    plan.close()
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    kmed = float(np.median(kernel_ms))
+    B = sum(algorithmic_bytes(w, 0) for w in jobs) + 8 * n_pairs
+    achieved = B / (kmed / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "traffic_batched_rtree.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("traffic_bytes_per_launch")
+        except Exception:
+            traffic = None
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        threads = os.cpu_count() or 1
+        rate, n_s, dt, k = cpu_sample_batched(jobs, args.predicate, threads, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "points/s", "cores": threads, "kind": "port",
+               "sample": f"first {k} of {len(jobs)} jobs ({n_s} points, {dt:.1f} s), exact CPU oracle "
+                         "(C + OpenMP); Shapely/GEOS is not installable here"}
+    loop_med = float(np.median(loop_ms))
+    line = {
+        "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate, "method": "rtree, batched",
+                   "n_jobs": len(jobs), "n_points_per_gpu": N, "n_polygons": n_polys, "n_pairs": n_pairs,
+                   "parallelism": f"jobs replicated per GPU ({world} GPU(s)), independent",
+                   "l2": "inputs (1.1 GB of points) larger than L2; no flush",
+                   "launch_shape": opts, "launch_shape_source": opts_src, "autotune_s": tune_s,
+                   "index_build_ms": build_ms, "index_build_wall_s": build_wall},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel_ms": kmed,
+                     "algorithmic_bytes_per_launch": B},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
+                "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int(8 * n_pairs)},
+        "gpu_launches": launches,
+        "join_stats": st,
+        "per_job_loop_ms": loop_med,
+        "batched_vs_loop": loop_med / kmed,
+    }
     line["clocks"] = clk.summary()
     print(json.dumps(line), flush=True)
 
@@ -354,6 +590,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-sample", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="batched workload: search the launch shape now instead of using the cache/defaults")
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
@@ -374,7 +612,10 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                  device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "batched":
+            run_batched(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as tdist

@@ -104,6 +104,7 @@ typedef struct vs_join_stats {
     int64_t rmi_fallbacks;    /* learned-index lookups whose error window exceeded 256 cells (binary search) */
     float kernel_ms;          /* device time of the join kernels */
     float sort_ms;            /* device time of the optional pair sort */
+    int64_t kernel_launches;  /* kernels the call enqueued (a graph replay: the kernels in the graph) */
 } vs_join_stats;
 
 typedef struct vs_index_info {
@@ -180,6 +181,41 @@ int vs_radix_sort_pairs(vs_context* ctx, uint64_t* d_keys, uint32_t* d_vals, int
  * (replaces morton_keys_from_bounds, src/vibespatial/spatial/indexing_kernels.py:20-49). */
 int vs_hilbert_keys(vs_context* ctx, const double* d_x, const double* d_y, int64_t n,
                     double minx, double miny, double maxx, double maxy, uint64_t* d_keys);
+
+/* ---------------------------------------------------------------------- */
+/* Batched joins: many independent point x polygon joins of uneven sizes run
+ * as one persistent launch, replayed from a CUDA graph.  The reference runs
+ * such work as one query_spatial_index call per job
+ * (src/vibespatial/spatial/query.py:247), each with its own launches and host
+ * fences (count_scatter_total, src/vibespatial/cuda/_runtime.py:2015-2038);
+ * here the whole batch is key -> sort -> traversal -> exact pass on the
+ * device with no host round trip, and the pair sizes are checked after the
+ * graph.  Job j joins points [h_job_start[j], h_job_start[j+1]) of `pts`
+ * against indexes[j]; a pair is (left = row in `pts`, right = polygon row of
+ * job j's index).  Pairs come back unordered.  The plan borrows `pts` and
+ * the indexes for its lifetime. */
+typedef struct vs_batch_plan vs_batch_plan;
+
+typedef struct vs_batch_options {
+    int32_t blocks_per_sm;    /* join kernel blocks per SM, 1..8 (0 = 4) */
+    int32_t packets_per_grab; /* 32-point packets a warp takes per work-counter grab (0 = 4) */
+    int32_t sort_levels;      /* Hilbert levels the points of a job are sorted by (0 = 8) */
+    int32_t reserved;
+} vs_batch_options;
+
+/* At most 4096 jobs and 2^31-1 points in total. */
+int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_t n_jobs,
+                         const vs_points* pts, const int64_t* h_job_start,
+                         const vs_batch_options* opts, vs_batch_plan** out);
+
+/* One batched join.  use_graph != 0 replays a CUDA graph captured on the
+ * first call (and again whenever predicate or the pair buffers change);
+ * 0 launches the same kernels directly.  VS_E_CAPACITY: *n_pairs holds the
+ * required size.  stats->kernel_ms is the device time of the batch. */
+int vs_batch_run(vs_batch_plan* plan, int32_t predicate, int32_t* d_left, int32_t* d_right,
+                 int64_t capacity, int32_t use_graph, int64_t* n_pairs, vs_join_stats* stats);
+
+int vs_batch_plan_free(vs_batch_plan* plan);
 
 /* Brute-force point x polygon join that allocates no device memory, for
  * callers that cannot allocate (a host that owns all device memory in a

@@ -25,7 +25,7 @@ EXPORTED = (
     "vs_version", "vs_last_error", "vs_context_create", "vs_context_destroy",
     "vs_context_synchronize", "vs_index_build", "vs_index_info_get", "vs_index_free",
     "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
-    "vs_join_brute_noalloc",
+    "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
 )
 
 
@@ -70,11 +70,19 @@ class JoinStats(ctypes.Structure):
         ("candidates", ctypes.c_int64), ("exact_fallbacks", ctypes.c_int64),
         ("fp32_edges", ctypes.c_int64), ("fp64_edges", ctypes.c_int64),
         ("rmi_fallbacks", ctypes.c_int64), ("kernel_ms", ctypes.c_float),
-        ("sort_ms", ctypes.c_float),
+        ("sort_ms", ctypes.c_float), ("kernel_launches", ctypes.c_int64),
     ]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("blocks_per_sm", ctypes.c_int32), ("packets_per_grab", ctypes.c_int32),
+                ("sort_levels", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
 class IndexInfo(ctypes.Structure):
@@ -126,6 +134,12 @@ def load(path: Path | str | None = None):
                                                ctypes.c_double, ctypes.c_double, vp]),
             "vs_join_brute_noalloc": (ctypes.c_int, [ctypes.POINTER(Points), ctypes.POINTER(Polygons), i32, vp, vp,
                                                      i64, ctypes.POINTER(i64), vp]),
+            "vs_batch_plan_create": (ctypes.c_int, [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Points),
+                                                    ctypes.POINTER(i64), ctypes.POINTER(BatchOptions),
+                                                    ctypes.POINTER(vp)]),
+            "vs_batch_run": (ctypes.c_int, [vp, i32, vp, vp, i64, i32, ctypes.POINTER(i64),
+                                            ctypes.POINTER(JoinStats)]),
+            "vs_batch_plan_free": (ctypes.c_int, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -271,6 +285,71 @@ class DeviceIndex:
             except CapacityError as e:
                 cap = max(e.required, 1)
         raise RuntimeError("pair buffer sizing did not converge")
+
+
+class BatchPlan:
+    """Owned handle of a batched join plan (vs_batch_plan*).
+
+    Job j joins points ``job_start[j]:job_start[j+1]`` of ``pts`` against
+    ``indexes[j]``.  The plan borrows the point buffers and the indexes: keep
+    them alive while the plan is used (this object holds references).
+    """
+
+    def __init__(self, ctx: Context, indexes, pts: Points, job_start, *, options: dict | None = None,
+                 keepalive=()):
+        self.ctx = ctx
+        self.indexes = list(indexes)
+        self.pts = pts
+        self._keepalive = keepalive
+        js = np.ascontiguousarray(np.asarray(job_start, dtype=np.int64))
+        if len(js) != len(self.indexes) + 1:
+            raise ValueError("job_start needs one entry more than there are jobs")
+        self.job_start = js
+        o = BatchOptions(**(options or {}))
+        self.options = o.as_dict()
+        arr = (ctypes.c_void_p * len(self.indexes))(*[ix.handle.value for ix in self.indexes])
+        h = ctypes.c_void_p()
+        check(load().vs_batch_plan_create(ctx.handle, arr, len(self.indexes), ctypes.byref(pts),
+                                          js.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(o),
+                                          ctypes.byref(h)))
+        self.handle = h
+
+    def run_into(self, predicate: int, left, right, *, use_graph: bool = True):
+        """One batched join into caller buffers; returns (n_pairs, stats dict)."""
+        n = ctypes.c_int64(0)
+        st = JoinStats()
+        cap = 0 if left is None else int(left.numel())
+        status = load().vs_batch_run(self.handle, int(predicate), _ptr(left), _ptr(right), cap,
+                                     1 if use_graph else 0, ctypes.byref(n), ctypes.byref(st))
+        check(status, required=int(n.value))
+        return int(n.value), st.as_dict()
+
+    def run(self, predicate: int, *, use_graph: bool = True, capacity: int | None = None):
+        """Batched join into fresh int32 device tensors (grown once if too small)."""
+        import torch
+
+        dev = torch.device("cuda", self.ctx.device)
+        cap = int(capacity) if capacity is not None else max(1024, int(self.pts.n))
+        for _ in range(2):
+            left = torch.empty(cap, dtype=torch.int32, device=dev)
+            right = torch.empty(cap, dtype=torch.int32, device=dev)
+            try:
+                n, stats = self.run_into(predicate, left, right, use_graph=use_graph)
+                return left[:n], right[:n], stats
+            except CapacityError as e:
+                cap = max(e.required, 1)
+        raise RuntimeError("pair buffer sizing did not converge")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().vs_batch_plan_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def locate_aligned(ctx: Context, pts: Points, polys: Polygons, out) -> None:

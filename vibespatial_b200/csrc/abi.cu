@@ -14,6 +14,7 @@
 namespace vs {
 
 static thread_local char g_err[1024] = "";
+thread_local long long g_launches = 0;
 
 void set_error(const char* fmt, ...) {
     va_list ap;
@@ -21,8 +22,6 @@ void set_error(const char* fmt, ...) {
     vsnprintf(g_err, sizeof(g_err), fmt, ap);
     va_end(ap);
 }
-
-namespace {
 
 int use_device(int device) {
     int cur = -1;
@@ -70,6 +69,8 @@ int check_points(const vs_points* p) {
     }
     return VS_OK;
 }
+
+namespace {
 
 int ensure_defer_capacity(vs_context* ctx, unsigned long long want) {
     if (ctx->defer_cap >= want) return VS_OK;
@@ -154,7 +155,7 @@ int vs_context_create(int device, void* stream, vs_context** out) {
         uint64_t thr = ~0ull;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
-    if (cudaMallocHost((void**)&ctx->h_counter, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+    if (cudaMallocHost((void**)&ctx->h_counter, kHostCounters * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc((void**)&ctx->d_counters, 8 * sizeof(unsigned long long)) != cudaSuccess) {
         set_error("context buffer allocation failed");
         if (ctx->h_counter) cudaFreeHost(ctx->h_counter);
@@ -284,6 +285,7 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
     VS_TRY(use_device(ctx->device));
     if (pts->n == 0 || idx->n_geoms == 0 || !(idx->h_frame[0] <= idx->h_frame[2])) return VS_OK;
     cudaStream_t s = ctx->stream;
+    const long long launches0 = g_launches;
     EventPair ev;
     // Pairs the filters cannot certify go to the context's deferred buffer
     // and are resolved exactly after the join kernel; if more were deferred
@@ -320,6 +322,7 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
         stats->candidates = (int64_t)c[5];
         stats->rmi_fallbacks = (int64_t)c[6];
         stats->kernel_ms = ev.ms();
+        stats->kernel_launches = g_launches - launches0;
     }
     if (c[4] != 0) {
         set_error("device-side consistency check failed (flags 0x%llx)", (unsigned long long)c[4]);
@@ -335,7 +338,10 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
         VS_TRY(sort_pairs(ctx, d_left, d_right, n, (uint64_t)pts->n, (uint64_t)idx->n_geoms));
         cudaEventRecord(es.b, s);
         VS_CUDA_TRY(cudaStreamSynchronize(s));
-        if (stats) stats->sort_ms = es.ms();
+        if (stats) {
+            stats->sort_ms = es.ms();
+            stats->kernel_launches = g_launches - launches0;
+        }
     }
     return VS_OK;
 }

@@ -399,7 +399,7 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.counters = ctx->d_counters;
     if (brute) {
         join_brute_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, 0, ctx->stream>>>(a);
-        VS_CUDA_TRY(cudaGetLastError());
+        VS_LAUNCHED("join_brute", ctx->stream);
         return VS_OK;
     }
     QueryOrder q;
@@ -437,7 +437,7 @@ int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_point
 int launch_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, uint8_t* d_out) {
     if (pts->n == 0) return VS_OK;
     locate_aligned_kernel<<<grid_for(pts->n, 256, 16), 256, 0, ctx->stream>>>(*pts, *polys, d_out, ctx->d_counters);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("locate_aligned", ctx->stream);
     return VS_OK;
 }
 
@@ -456,10 +456,10 @@ int sort_pairs(vs_context* ctx, int32_t* d_left, int32_t* d_right, int64_t n, ui
     VS_TRY(keys.alloc((size_t)n, s));
     VS_TRY(vals.alloc((size_t)n, s));
     pack_pairs_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_left, d_right, n, rbits, keys.p, vals.p);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("pack_pairs", s);
     VS_TRY(radix_sort_u64_u32(keys.p, vals.p, n, rbits + lbits, s));
     unpack_pairs_kernel<<<grid_for(n, 256), 256, 0, s>>>(keys.p, n, rbits, d_left, d_right);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("unpack_pairs", s);
     return VS_OK;
 }
 

@@ -1000,7 +1000,6 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     learned_map_kernel<<<grid, kThreads, 0, s>>>(a);
     VS_LAUNCHED("learned_map", s);
     VS_TRY(exclusive_scan_u32(cell_count.p, cell_count.p, li.n_cells, n_grouped.p, s));
-    VS_LAUNCHED("cell scan", s);
     learned_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
     VS_LAUNCHED("learned_scatter", s);
     learned_join_kernel<<<grid, kThreads, 0, s>>>(a);

@@ -109,16 +109,16 @@ int exclusive_scan_impl(const T* in, T* out, int64_t n, T* d_total, cudaStream_t
     }
     if (nb == 1) {
         scan_downsweep_kernel<T><<<1, kScanThreads, 0, s>>>(in, out, n, nullptr, d_total);
-        VS_CUDA_TRY(cudaGetLastError());
+        VS_LAUNCHED("scan_downsweep", s);
         return VS_OK;
     }
     Scratch<T> sums;
     VS_TRY(sums.alloc((size_t)nb, s));
     scan_reduce_kernel<T><<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, sums.p);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("scan_reduce", s);
     VS_TRY(exclusive_scan_impl<T>(sums.p, sums.p, nb, (T*)nullptr, s));
     scan_downsweep_kernel<T><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, sums.p, d_total);
-    VS_CUDA_TRY(cudaGetLastError());
+    VS_LAUNCHED("scan_downsweep", s);
     return VS_OK;
 }
 
@@ -273,10 +273,10 @@ int radix_sort_impl(K* keys, uint32_t* vals, int64_t n, int begin_bit, int end_b
         int shift = begin_bit + 8 * p;
         if (shift + 8 > max_bits) shift = max_bits - 8;
         rs_histogram_kernel<K><<<ntiles, kRsThreads, 0, s>>>(ka, n, shift, hist.p, ntiles);
-        VS_CUDA_TRY(cudaGetLastError());
+        VS_LAUNCHED("rs_histogram", s);
         VS_TRY(exclusive_scan_u32(hist.p, hist.p, (int64_t)kRadix * ntiles, nullptr, s));
         rs_scatter_kernel<K><<<ntiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist.p, ntiles);
-        VS_CUDA_TRY(cudaGetLastError());
+        VS_LAUNCHED("rs_scatter", s);
         K* tk = ka;
         ka = kb;
         kb = tk;

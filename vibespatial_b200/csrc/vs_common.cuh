@@ -10,6 +10,16 @@ namespace vs {
 // Thread-local last-error message, exported through vs_last_error().
 void set_error(const char* fmt, ...);
 
+// Make `device` current (VS_OK or VS_E_CUDA).
+int use_device(int device);
+// Argument checks shared by the entry points (VS_OK or VS_E_ARG).
+int check_points(const vs_points* p);
+int check_polygons(const vs_polygons* p);
+
+// Pinned host words of a context (read-back of the device counters and of
+// per-call extras).
+constexpr int kHostCounters = 16;
+
 #define VS_CUDA_TRY(expr)                                                        \
     do {                                                                         \
         cudaError_t _e = (expr);                                                 \
@@ -20,11 +30,16 @@ void set_error(const char* fmt, ...);
         }                                                                        \
     } while (0)
 
-// After a kernel launch: report launch errors.  Debug builds compiled with
+// Kernels this thread has enqueued (every launch site ends in VS_LAUNCHED);
+// entry points report the difference as vs_join_stats.kernel_launches.
+extern thread_local long long g_launches;
+
+// After a kernel launch: count it and report launch errors.  Debug builds compiled with
 // -DVS_DEBUG_SYNC also wait for the kernel and name it in the error message.
 #ifdef VS_DEBUG_SYNC
 #define VS_LAUNCHED(name, stream)                                                        \
     do {                                                                                 \
+        ++::vs::g_launches;                                                              \
         cudaError_t _e = cudaGetLastError();                                             \
         if (_e == cudaSuccess) _e = cudaStreamSynchronize(stream);                       \
         if (_e != cudaSuccess) {                                                         \
@@ -33,7 +48,11 @@ void set_error(const char* fmt, ...);
         }                                                                                \
     } while (0)
 #else
-#define VS_LAUNCHED(name, stream) VS_CUDA_TRY(cudaGetLastError())
+#define VS_LAUNCHED(name, stream) \
+    do {                          \
+        ++::vs::g_launches;       \
+        VS_CUDA_TRY(cudaGetLastError()); \
+    } while (0)
 #endif
 
 #define VS_TRY(expr)                 \
@@ -92,7 +111,7 @@ struct vs_context {
     cudaStream_t stream;
     bool owns_stream;
     vs::Arena arena;
-    // Pinned host word used to read back pair counts.
+    // Pinned host words (kHostCounters) used to read back counts.
     unsigned long long* h_counter;
     // Device counters: [0] pair count, [1] exact-fallback count,
     // [2] fp32-filter decided edges, [3] edges sent past the fp32 filter,
