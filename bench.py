@@ -117,6 +117,9 @@ def make_workload(name: str, rank: int = 0, scale: float = 1.0):
     raise ValueError(name)
 
 
+PHASES = ("locate", "group", "refine", "exact")
+
+
 def make_batched(rank: int = 0, scale: float = 1.0):
     from vibespatial_b200.testing import synthetic as syn
 
@@ -311,8 +314,9 @@ def run_ours(args, rank, world, local_rank):
         tdist.barrier()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kernel_ms = []
+    kernel_ms, phases = [], []
     launches = 0
+    plain_phases = None
     with ClockSampler(dev) as clk:
         if args.profile:
             torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
@@ -321,6 +325,7 @@ def run_ours(args, rank, world, local_rank):
             n_k, st = index.join_into(pts, pred, method, left, right)
             ev[k][1].record(stream)
             kernel_ms.append(st["kernel_ms"])
+            phases.append(st["phase_ms"])
             launches += st["kernel_launches"]
             assert n_k == n_pairs
         torch.cuda.synchronize()
@@ -329,11 +334,13 @@ def run_ours(args, rank, world, local_rank):
         step_ms = [a.elapsed_time(b) for a, b in ev]
         # plain method timing (same GPU, same buffers) after the timed region
         if method == _abi.METHOD_LEARNED:
-            pm = []
+            pm, pph = [], []
             for _ in range(max(3, args.steps // 2)):
                 _, stp = index.join_into(pts, pred, _abi.METHOD_RTREE, left, right)
                 pm.append(stp["kernel_ms"])
+                pph.append(stp["phase_ms"])
             plain = float(np.median(pm))
+            plain_phases = [float(v) for v in np.median(np.array(pph), axis=0)]
         # e2e through the C-ABI with host buffers: H2D points, join, D2H pairs
         hx = torch.from_numpy(w.px).pin_memory()
         hy = torch.from_numpy(w.py).pin_memory()
@@ -401,11 +408,13 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
                 "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int(8 * n_pairs)},
         "gpu_launches": launches,
-        "join_stats": stats,
+        "phases_ms": dict(zip(PHASES, (float(v) for v in np.median(np.array(phases), axis=0)))),
+        "join_stats": st,
         "index_info": info,
     }
     if plain is not None:
         line["plain_rtree_ms"] = plain
+        line["plain_phases_ms"] = dict(zip(PHASES, plain_phases))
         line["learned_vs_plain"] = plain / kmed
     line["clocks"] = clk.summary()
     print(json.dumps(line), flush=True)

@@ -105,6 +105,9 @@ typedef struct vs_join_stats {
     float kernel_ms;          /* device time of the join kernels */
     float sort_ms;            /* device time of the optional pair sort */
     int64_t kernel_launches;  /* kernels the call enqueued (a graph replay: the kernels in the graph) */
+    float phase_ms[4];        /* device time per phase: [0] locate (learned: cell lookup; R-tree: point
+                                 keys + sort), [1] group (learned: points scattered by cell), [2] refine
+                                 (traversal / candidate loop with the filtered tests), [3] exact pass */
 } vs_join_stats;
 
 typedef struct vs_index_info {

@@ -71,10 +71,13 @@ class JoinStats(ctypes.Structure):
         ("fp32_edges", ctypes.c_int64), ("fp64_edges", ctypes.c_int64),
         ("rmi_fallbacks", ctypes.c_int64), ("kernel_ms", ctypes.c_float),
         ("sort_ms", ctypes.c_float), ("kernel_launches", ctypes.c_int64),
+        ("phase_ms", ctypes.c_float * 4),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["phase_ms"] = [float(v) for v in self.phase_ms]
+        return d
 
 
 class BatchOptions(ctypes.Structure):

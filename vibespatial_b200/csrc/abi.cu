@@ -155,9 +155,15 @@ int vs_context_create(int device, void* stream, vs_context** out) {
         uint64_t thr = ~0ull;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
-    if (cudaMallocHost((void**)&ctx->h_counter, kHostCounters * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc((void**)&ctx->d_counters, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+    bool ok = cudaMallocHost((void**)&ctx->h_counter, kHostCounters * sizeof(unsigned long long)) == cudaSuccess &&
+              cudaMalloc((void**)&ctx->d_counters, kDevCounters * sizeof(unsigned long long)) == cudaSuccess;
+    for (int k = 0; k < 5 && ok; ++k) ok = cudaEventCreate(&ctx->phase_ev[k]) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
         set_error("context buffer allocation failed");
+        for (int k = 0; k < 5; ++k)
+            if (ctx->phase_ev[k]) cudaEventDestroy(ctx->phase_ev[k]);
+        if (ctx->d_counters) cudaFree(ctx->d_counters);
         if (ctx->h_counter) cudaFreeHost(ctx->h_counter);
         if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
@@ -174,6 +180,7 @@ int vs_context_destroy(vs_context* ctx) {
     cudaFree(ctx->d_counters);
     cudaFree(ctx->defer_buf);
     cudaFreeHost(ctx->h_counter);
+    for (int k = 0; k < 5; ++k) cudaEventDestroy(ctx->phase_ev[k]);
     if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return VS_OK;
@@ -293,14 +300,21 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
     unsigned long long want = (unsigned long long)(pts->n / 64 + 65536);
     for (int attempt = 0; attempt < 2; ++attempt) {
         VS_TRY(ensure_defer_capacity(ctx, want));
-        VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, 8 * sizeof(unsigned long long), s));
+        VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, kDevCounters * sizeof(unsigned long long), s));
         const DeferSink ds{ctx->defer_buf, ctx->defer_cap, &ctx->d_counters[7]};
+        ctx->phase_on = stats != nullptr;
         cudaEventRecord(ev.a, s);
+        phase_mark(ctx, 0);
+        int st;
         if (method == VS_METHOD_LEARNED)
-            VS_TRY(launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity, ds));
+            st = launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity, ds);
         else
-            VS_TRY(launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, d_left, d_right, capacity, ds));
-        if (mask) VS_TRY(launch_resolve_deferred(ctx, idx, pts, mask, d_left, d_right, capacity, ds));
+            st = launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, d_left, d_right, capacity, ds);
+        phase_mark(ctx, 3);
+        if (st == VS_OK && mask) st = launch_resolve_deferred(ctx, idx, pts, mask, d_left, d_right, capacity, ds);
+        phase_mark(ctx, 4);
+        ctx->phase_on = false;
+        VS_TRY(st);
         cudaEventRecord(ev.b, s);
         VS_CUDA_TRY(cudaMemcpyAsync(ctx->h_counter, ctx->d_counters, 8 * sizeof(unsigned long long),
                                     cudaMemcpyDeviceToHost, s));
@@ -323,6 +337,7 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
         stats->rmi_fallbacks = (int64_t)c[6];
         stats->kernel_ms = ev.ms();
         stats->kernel_launches = g_launches - launches0;
+        for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&stats->phase_ms[k], ctx->phase_ev[k], ctx->phase_ev[k + 1]);
     }
     if (c[4] != 0) {
         set_error("device-side consistency check failed (flags 0x%llx)", (unsigned long long)c[4]);
@@ -362,7 +377,7 @@ int vs_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* 
         return VS_E_ARG;
     }
     VS_TRY(use_device(ctx->device));
-    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, kDevCounters * sizeof(unsigned long long), ctx->stream));
     VS_TRY(launch_locate_aligned(ctx, pts, polys, d_out));
     VS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return VS_OK;

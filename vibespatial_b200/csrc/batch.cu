@@ -374,17 +374,20 @@ BatchArgs plan_args(vs_batch_plan* p, int mask, int32_t* left, int32_t* right, i
 // synchronisation, scratch from the stream-ordered allocator).
 int enqueue_batch(vs_batch_plan* p, cudaStream_t s, int mask, int32_t* left, int32_t* right, int64_t capacity) {
     const BatchArgs a = plan_args(p, mask, left, right, capacity);
-    VS_CUDA_TRY(cudaMemsetAsync(p->ctx->d_counters, 0, 8 * sizeof(unsigned long long), s));
+    VS_CUDA_TRY(cudaMemsetAsync(p->ctx->d_counters, 0, kDevCounters * sizeof(unsigned long long), s));
     VS_CUDA_TRY(cudaMemsetAsync(p->d_work, 0, 2 * sizeof(unsigned long long), s));
     VS_CUDA_TRY(cudaMemsetAsync(p->d_n_valid, 0, sizeof(uint32_t), s));
     const size_t smem = (size_t)(p->n_jobs + 1) * sizeof(int64_t);
-    batch_key_kernel<<<grid_for(p->n_points, 256, 16), 256, smem, s>>>(a, p->n_points);
+    batch_key_kernel<<<resident_grid(batch_key_kernel, p->n_points, 256, smem), 256, smem, s>>>(a, p->n_points);
     VS_LAUNCHED("batch_key", s);
     VS_TRY(radix_sort_u32_u32(p->keys, p->order, p->n_points, 32, s, p->sort_begin));
-    batch_join_kernel<<<kNumSMs * p->opts.blocks_per_sm, kBThreads, 0, s>>>(a);
+    // blocks per SM from the launch shape, capped at what can be resident
+    const int resident = resident_grid(batch_join_kernel, (int64_t)1 << 30, kBThreads) / kNumSMs;
+    const int per_sm = p->opts.blocks_per_sm < resident ? p->opts.blocks_per_sm : resident;
+    batch_join_kernel<<<kNumSMs * per_sm, kBThreads, 0, s>>>(a);
     VS_LAUNCHED("batch_join", s);
     if (mask) {
-        batch_resolve_kernel<<<kNumSMs * 4, kBThreads, 0, s>>>(a);
+        batch_resolve_kernel<<<resident_grid(batch_resolve_kernel, (int64_t)1 << 30, kBThreads), kBThreads, 0, s>>>(a);
         VS_LAUNCHED("batch_resolve", s);
     }
     return VS_OK;

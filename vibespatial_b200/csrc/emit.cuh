@@ -136,6 +136,16 @@ __device__ __forceinline__ void defer(const DeferSink& d, int32_t row, int32_t s
     if (p < d.capacity) d.buf[p] = make_int2(row, slot);
 }
 
+// Warp-level dynamic work queue: lane 0 takes `grab` consecutive items from
+// *counter and the first one is broadcast to the warp (>= the item count
+// once the queue is drained).  Warps that finish early keep taking work, so
+// uneven per-item costs do not leave SMs idle at the end of a launch.
+__device__ __forceinline__ int64_t warp_grab(unsigned long long* counter, int64_t grab) {
+    unsigned long long b = 0;
+    if ((threadIdx.x & 31) == 0) b = atomicAdd(counter, (unsigned long long)grab);
+    return (int64_t)__shfl_sync(0xffffffffu, b, 0);
+}
+
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

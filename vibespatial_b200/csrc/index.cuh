@@ -20,13 +20,15 @@ constexpr int kRmiHidden = 32;
 
 // Everything the learned join needs about one polygon slot, in three 16-byte
 // words: the FP64 origin, the FP32 box relative to it (rounded outward), the
-// bound on the FP32 vertex rounding error, the original row, and for a
-// single-ring polygon its coordinate range (c0 = -1 for multi-ring shapes).
+// bound on the FP32 vertex rounding error, the slot (its original row is
+// item_geom[slot]), and for a single-ring polygon its coordinate range
+// (c0 = -1 for multi-ring shapes).  The learned index stores one record per
+// (cell, polygon) entry, in cell order, so a candidate is one 48-byte read.
 struct __align__(16) SlotRecord {
     double ox, oy;
     float4 box;
     float err;
-    int32_t geom;
+    int32_t slot;
     int32_t c0, c1;
 };
 
@@ -70,7 +72,7 @@ struct LearnedIndex {
     int2* leaf_err = nullptr;        // [n_leaves] inclusive error window (lo, hi)
     RmiLeaf* leaves = nullptr;       // [n_leaves] the two above packed for queries
     int32_t n_leaves = 0;
-    SlotRecord* slots = nullptr;     // [n_geoms] packed per-slot data for queries
+    SlotRecord* recs = nullptr;      // [n_entries] record of each entry's slot, cell order
     // FP32 tile-relative copies used by the split-precision filter
     double2* origin = nullptr;       // [n_geoms] slot origin (box centre, FP64)
     float4* box32 = nullptr;         // [n_geoms] slot box relative to the origin, rounded outward

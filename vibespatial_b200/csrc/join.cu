@@ -61,7 +61,13 @@ struct RtreeArgs {
     PairSink sink;
     DeferSink defer;
     unsigned long long* counters;
+    unsigned long long* work;  // traversal work queue (sorted points handed out)
 };
+
+#ifndef VS_RTREE_GRAB
+#define VS_RTREE_GRAB 64
+#endif
+constexpr int64_t kRtreeGrab = VS_RTREE_GRAB;  // sorted points per work-queue grab (multiple of 32)
 
 __device__ __forceinline__ bool box_has(const vs_box& b, double x, double y) {
     return x >= b.minx && x <= b.maxx && y >= b.miny && y <= b.maxy;
@@ -119,98 +125,100 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
     const unsigned lt = (1u << lane) - 1u;
     const int top = a.levels - 1;
     const int64_t n = (int64_t)*a.n_sorted;
-    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long n_cand = 0;
-
-    for (int64_t base = gw * 32; base < n; base += nw * 32) {
-        const int64_t i = base + lane;
-        const bool active = i < n;
-        double x = 0.0, y = 0.0;
-        int32_t row = -1;
-        if (active) {
-            row = (int32_t)a.order[i];
-            x = a.px[row];
-            y = a.py[row];
-        }
-        double x0 = active ? x : INFINITY, x1 = active ? x : -INFINITY;
-        double y0 = active ? y : INFINITY, y1 = active ? y : -INFINITY;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            x0 = fmin(x0, __shfl_xor_sync(0xffffffffu, x0, o));
-            x1 = fmax(x1, __shfl_xor_sync(0xffffffffu, x1, o));
-            y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
-            y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
-        }
-        int sp = 0;
-        const vs_box root = s_nodes[a.level_off[top] - stage_base];
-        if (box_overlaps(root, x0, y0, x1, y1)) {
-            if (top == 0) {
-                // a single polygon: the root is the item
-                bool want = false;
-                if (active && box_has(root, x, y)) {
-                    ++n_cand;
-                    const int loc = a.accept_mask ? geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off,
-                                                                               a.geom_off, 0) : 0;
-                    if (loc == LOC_UNDECIDED) defer(a.defer, row, 0);
-                    else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
-                }
-                wemit_sync(out, a.sink, want, row, a.item_geom[0]);
-            } else {
-                if (lane == 0) s_stack[warp][0] = top;  // node 0 of the top level
-                sp = 1;
+    for (;;) {
+        const int64_t b0 = warp_grab(a.work, kRtreeGrab);
+        if (b0 >= n) break;
+        const int64_t e0 = b0 + kRtreeGrab < n ? b0 + kRtreeGrab : n;
+        for (int64_t base = b0; base < e0; base += 32) {
+            const int64_t i = base + lane;
+            const bool active = i < e0;
+            double x = 0.0, y = 0.0;
+            int32_t row = -1;
+            if (active) {
+                row = (int32_t)a.order[i];
+                x = a.px[row];
+                y = a.py[row];
             }
-        }
-        __syncwarp();
-        while (sp > 0) {
-            --sp;
-            const int e = s_stack[warp][sp];
-            __syncwarp();
-            const int cl = (e & 15) - 1;
-            const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
-            const bool in_range = lane < kFanout && c < a.level_size[cl];
-            vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
-            if (in_range)
-                b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
-            const bool hit = in_range && box_overlaps(b, x0, y0, x1, y1);
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (cl > 0) {
-                if (hit) {
-                    const int pos = sp + __popc(m & lt);
-                    if (pos < kStack) s_stack[warp][pos] = (int)(c << 4) | cl;
-                }
-                int add = __popc(m);
-                if (sp + add > kStack) {
-                    if (lane == 0) atomicOr(&a.counters[4], 1ull);  // cannot happen for < 2^31 items
-                    add = kStack - sp;
-                }
-                sp += add;
-                __syncwarp();
-            } else {
-                if (lane < kFanout) s_items[warp][lane] = b;
-                __syncwarp();
-                unsigned mm = m;
-                const int64_t slot0 = (int64_t)(e >> 4) * kFanout;
-                while (mm) {
-                    const int j = __ffs(mm) - 1;
-                    mm &= mm - 1;
-                    const vs_box ib = s_items[warp][j];
-                    const int slot = (int)(slot0 + j);
+            double x0 = active ? x : INFINITY, x1 = active ? x : -INFINITY;
+            double y0 = active ? y : INFINITY, y1 = active ? y : -INFINITY;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                x0 = fmin(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+                x1 = fmax(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+                y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+                y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+            }
+            int sp = 0;
+            const vs_box root = s_nodes[a.level_off[top] - stage_base];
+            if (box_overlaps(root, x0, y0, x1, y1)) {
+                if (top == 0) {
+                    // a single polygon: the root is the item
                     bool want = false;
-                    if (active && box_has(ib, x, y)) {
+                    if (active && box_has(root, x, y)) {
                         ++n_cand;
-                        int loc = 0;
-                        if (a.accept_mask)
-                            loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot);
-                        if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
+                        const int loc = a.accept_mask ? geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off,
+                                                                                   a.geom_off, 0) : 0;
+                        if (loc == LOC_UNDECIDED) defer(a.defer, row, 0);
                         else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                     }
-                    wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                    wemit_sync(out, a.sink, want, row, a.item_geom[0]);
+                } else {
+                    if (lane == 0) s_stack[warp][0] = top;  // node 0 of the top level
+                    sp = 1;
                 }
-                __syncwarp();
             }
+            __syncwarp();
+            while (sp > 0) {
+                --sp;
+                const int e = s_stack[warp][sp];
+                __syncwarp();
+                const int cl = (e & 15) - 1;
+                const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
+                const bool in_range = lane < kFanout && c < a.level_size[cl];
+                vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
+                if (in_range)
+                    b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
+                const bool hit = in_range && box_overlaps(b, x0, y0, x1, y1);
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (cl > 0) {
+                    if (hit) {
+                        const int pos = sp + __popc(m & lt);
+                        if (pos < kStack) s_stack[warp][pos] = (int)(c << 4) | cl;
+                    }
+                    int add = __popc(m);
+                    if (sp + add > kStack) {
+                        if (lane == 0) atomicOr(&a.counters[4], 1ull);  // cannot happen for < 2^31 items
+                        add = kStack - sp;
+                    }
+                    sp += add;
+                    __syncwarp();
+                } else {
+                    if (lane < kFanout) s_items[warp][lane] = b;
+                    __syncwarp();
+                    unsigned mm = m;
+                    const int64_t slot0 = (int64_t)(e >> 4) * kFanout;
+                    while (mm) {
+                        const int j = __ffs(mm) - 1;
+                        mm &= mm - 1;
+                        const vs_box ib = s_items[warp][j];
+                        const int slot = (int)(slot0 + j);
+                        bool want = false;
+                        if (active && box_has(ib, x, y)) {
+                            ++n_cand;
+                            int loc = 0;
+                            if (a.accept_mask)
+                                loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot);
+                            if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
+                            else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
+                        }
+                        wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                    }
+                    __syncwarp();
+                }
+            }
+            wflush(out, a.sink, false);
         }
-        wflush(out, a.sink, false);
     }
     wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
@@ -358,7 +366,7 @@ int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
     VS_TRY(q.order.alloc((size_t)n, s));
     VS_TRY(q.n_valid.alloc(1, s));
     VS_CUDA_TRY(cudaMemsetAsync(q.n_valid.p, 0, sizeof(uint32_t), s));
-    point_sort_key_kernel<<<grid_for(n, 256, 16), 256, 0, s>>>(*pts, idx->frame, q.keys.p, q.order.p, q.n_valid.p);
+    point_sort_key_kernel<<<resident_grid(point_sort_key_kernel, n, 256), 256, 0, s>>>(*pts, idx->frame, q.keys.p, q.order.p, q.n_valid.p);
     VS_LAUNCHED("point_sort_key", s);
     // Sorting by the top 24 key bits (a level-12 Hilbert cell) already makes
     // a warp's 32 points spatially coherent; the low byte is left unsorted.
@@ -398,17 +406,23 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.defer = dsink;
     a.counters = ctx->d_counters;
     if (brute) {
-        join_brute_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, 0, ctx->stream>>>(a);
+        phase_mark(ctx, 1);
+        phase_mark(ctx, 2);
+        join_brute_kernel<<<resident_grid(join_brute_kernel, pts->n, kJoinThreads), kJoinThreads, 0, ctx->stream>>>(a);
         VS_LAUNCHED("join_brute", ctx->stream);
         return VS_OK;
     }
     QueryOrder q;
     VS_TRY(prepare_queries(ctx, idx, pts, q));
+    phase_mark(ctx, 1);
+    phase_mark(ctx, 2);
     a.order = q.order.p;
     a.n_sorted = q.n_valid.p;
+    a.work = &ctx->d_counters[kWorkCounter];
     const size_t smem = (size_t)a.staged * sizeof(vs_box);
     VS_CUDA_TRY(cudaFuncSetAttribute(join_rtree_packet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    join_rtree_packet_kernel<<<grid_for(pts->n, kJoinThreads, 8), kJoinThreads, smem, ctx->stream>>>(a);
+    join_rtree_packet_kernel<<<resident_grid(join_rtree_packet_kernel, pts->n, kJoinThreads, smem), kJoinThreads, smem,
+                               ctx->stream>>>(a);
     VS_LAUNCHED("join_rtree_packet", ctx->stream);
     return VS_OK;
 }
@@ -429,14 +443,15 @@ int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_point
     a.count = dsink.counter;
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.counters = ctx->d_counters;
-    resolve_deferred_kernel<<<kNumSMs * 4, kJoinThreads, 0, ctx->stream>>>(a);
+    resolve_deferred_kernel<<<resident_grid(resolve_deferred_kernel, (int64_t)1 << 30, kJoinThreads), kJoinThreads, 0,
+                              ctx->stream>>>(a);
     VS_LAUNCHED("resolve_deferred", ctx->stream);
     return VS_OK;
 }
 
 int launch_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, uint8_t* d_out) {
     if (pts->n == 0) return VS_OK;
-    locate_aligned_kernel<<<grid_for(pts->n, 256, 16), 256, 0, ctx->stream>>>(*pts, *polys, d_out, ctx->d_counters);
+    locate_aligned_kernel<<<resident_grid(locate_aligned_kernel, pts->n, 256), 256, 0, ctx->stream>>>(*pts, *polys, d_out, ctx->d_counters);
     VS_LAUNCHED("locate_aligned", ctx->stream);
     return VS_OK;
 }

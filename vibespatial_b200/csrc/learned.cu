@@ -204,7 +204,7 @@ __global__ void pack_slots_kernel(int64_t M, const double2* __restrict__ origin,
         r.oy = origin[s].y;
         r.box = box32[s];
         r.err = err32[s];
-        r.geom = item_geom[s];
+        r.slot = (int32_t)s;
         const int32_t p0 = geom_off[s], p1 = geom_off[s + 1];
         r.c0 = -1;
         r.c1 = -1;
@@ -214,6 +214,13 @@ __global__ void pack_slots_kernel(int64_t M, const double2* __restrict__ origin,
         }
         out[s] = r;
     }
+}
+
+// One record per (cell, polygon) entry, in cell order.
+__global__ void entry_recs_kernel(int64_t E, const uint32_t* __restrict__ entries,
+                                  const SlotRecord* __restrict__ slots, SlotRecord* __restrict__ out) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = slots[entries[e]];
 }
 
 __global__ void pack_leaves_kernel(int nl, const double2* __restrict__ ab, const int2* __restrict__ err,
@@ -432,11 +439,30 @@ __global__ void rmi_window_stats_kernel(const uint32_t* __restrict__ leaf_of, in
 // ----------------------------------------------------------------- query ---
 // One grouped point: a full 32-byte sector, so the scatter writes whole
 // sectors (no read-modify-write of partially written ones).
-struct __align__(32) GroupedPoint {
+// A matched query point as the map pass leaves it: coordinates, row, cell
+// index and its rank among the cell's points.
+struct __align__(32) StagedPoint {
     double x, y;
     int32_t row;
     int32_t cell;
-    int64_t pad;
+    uint32_t rank;
+    int32_t pad;
+};
+
+// The map pass appends matched points to kStripes regions of the staging
+// array, region s taking the packets p with p % kStripes == s, so each
+// region's append counter sees 1/kStripes of the atomics and a region never
+// holds more than 32 * ceil(packets / kStripes) points.
+constexpr int kStripes = 2048;
+
+// A query point in cell order, with its cell's candidate range
+// [lo, lo + len) of the per-entry records.
+struct __align__(32) GroupedPoint {
+    double x, y;
+    int32_t row;
+    uint32_t lo;
+    uint32_t len;
+    int32_t pad;
 };
 
 struct LearnedArgs {
@@ -455,7 +481,7 @@ struct LearnedArgs {
     const uint32_t* entries;
     int64_t n_cells;
     const RmiLeaf* leaves;
-    const SlotRecord* slots;
+    const SlotRecord* recs;          // [n_entries] per-entry slot records
     const vs_box* boxes;       // FP64 slot boxes (R-tree level 0)
     const double2* origin;
     const float4* box32;
@@ -471,10 +497,13 @@ struct LearnedArgs {
     DeferSink defer;
     unsigned long long* counters;
     // grouping scratch (per join)
-    int2* point_cell;          // [n] (cell index or -1, rank within the cell)
+    StagedPoint* staged;       // [kStripes * stripe_cap] matched points, striped
+    uint32_t* stripe_count;    // [kStripes] points appended to each region
+    int64_t stripe_cap;        // points one region can hold
     uint32_t* cell_count;      // [n_cells] counts, then (after the scan) start offsets
     GroupedPoint* grouped;     // [n_grouped] points grouped by cell
     const uint32_t* n_grouped;
+    unsigned long long* work;  // refine work queue (grouped points handed out)
 };
 
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
@@ -579,7 +608,8 @@ __device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, do
 }
 
 // Pass 1 (map), points in input order: each point's cell and its rank among
-// the cell's points (warp-aggregated atomics on the per-cell counts).
+// the cell's points (warp-aggregated atomics on the per-cell counts); the
+// matched points are appended to the staging regions.
 __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LearnedArgs a) {
     __shared__ uint16_t s_lut[kHilbertLutSize];
     hilbert_lut_init(s_lut);
@@ -595,41 +625,94 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LearnedA
     for (int64_t b0 = gw * 32; b0 < a.n; b0 += nw * 32) {
         const int64_t i = b0 + lane;
         int c = -1;
+        double x = 0.0, y = 0.0;
         if (i < a.n) {
-            const double x = a.px[i], y = a.py[i];
+            x = a.px[i];
+            y = a.py[i];
             if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1)
                 c = learned_lookup(a, x, y, lox, loy, sx, sy, s_lut, n_wide);
         }
+        const unsigned lt = (1u << lane) - 1u;
         const unsigned peers = __match_any_sync(0xffffffffu, c);
         const int leader = __ffs(peers) - 1;
         uint32_t base = 0;
         if (c >= 0 && lane == leader) base = atomicAdd(&a.cell_count[c], (uint32_t)__popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (i < a.n) a.point_cell[i] = make_int2(c, (int)(base + __popc(peers & ((1u << lane) - 1u))));
+        // append the matched points of this packet to its stripe region
+        const unsigned mm = __ballot_sync(0xffffffffu, c >= 0);
+        if (mm) {
+            const int64_t stripe = (b0 >> 5) % kStripes;
+            uint32_t sb = 0;
+            if (lane == 0) sb = atomicAdd(&a.stripe_count[stripe], (uint32_t)__popc(mm));
+            sb = __shfl_sync(0xffffffffu, sb, 0);
+            if (c >= 0) {
+                StagedPoint p;
+                p.x = x;
+                p.y = y;
+                p.row = (int32_t)i;
+                p.cell = c;
+                p.rank = base + __popc(peers & lt);
+                p.pad = 0;
+                a.staged[stripe * a.stripe_cap + sb + __popc(mm & lt)] = p;
+            }
+        }
     }
     add_counter(a.counters, 6, n_wide);
 }
 
-// Pass 2 (scatter): after the exclusive scan of the counts, each matched
-// point writes one aligned 32-byte record at start[cell] + rank.  Points in
-// empty cells are dropped here.
+// Pass 2 (scatter): after the exclusive scan of the counts, every staged
+// point writes one aligned 32-byte record at start[cell] + rank, carrying its
+// cell's candidate range.  A block walks whole stripe regions (coalesced
+// reads, every lane busy); each thread keeps kScatterUnroll records in flight.
+#ifndef VS_SCATTER_UNROLL
+#define VS_SCATTER_UNROLL 2
+#endif
+constexpr int kScatterUnroll = VS_SCATTER_UNROLL;
+
 __global__ void __launch_bounds__(kThreads) learned_scatter_kernel(const LearnedArgs a) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int2 cr = a.point_cell[i];
-        if (cr.x >= 0) {
-            GroupedPoint g;
-            g.x = a.px[i];
-            g.y = a.py[i];
-            g.row = (int32_t)i;
-            g.cell = cr.x;
-            a.grouped[a.cell_count[cr.x] + (uint32_t)cr.y] = g;
+    for (int stripe = blockIdx.x; stripe < kStripes; stripe += gridDim.x) {
+        const uint32_t cnt = a.stripe_count[stripe];
+        const StagedPoint* src = a.staged + (int64_t)stripe * a.stripe_cap;
+        for (uint32_t k0 = threadIdx.x; k0 < cnt; k0 += blockDim.x * kScatterUnroll) {
+            StagedPoint p[kScatterUnroll];
+#pragma unroll
+            for (int u = 0; u < kScatterUnroll; ++u) {
+                const uint32_t k = k0 + u * blockDim.x;
+                if (k < cnt) p[u] = src[k];
+            }
+            GroupedPoint g[kScatterUnroll];
+            uint32_t pos[kScatterUnroll];
+#pragma unroll
+            for (int u = 0; u < kScatterUnroll; ++u) {
+                const uint32_t k = k0 + u * blockDim.x;
+                if (k < cnt) {
+                    const int c = p[u].cell;
+                    g[u].x = p[u].x;
+                    g[u].y = p[u].y;
+                    g[u].row = p[u].row;
+                    g[u].lo = a.cell_start[c];
+                    g[u].len = a.cell_start[c + 1] - g[u].lo;
+                    g[u].pad = 0;
+                    pos[u] = a.cell_count[c] + p[u].rank;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kScatterUnroll; ++u)
+                if (k0 + u * blockDim.x < cnt) a.grouped[pos[u]] = g[u];
         }
     }
 }
 
 // Pass 3 (join): a warp takes 32 consecutive grouped points, which share a
 // cell (and so a polygon list: broadcast reads) except at cell boundaries.
-__global__ void __launch_bounds__(kThreads, 5) learned_join_kernel(const LearnedArgs a) {
+#ifndef VS_JOIN_MIN_BLOCKS
+#define VS_JOIN_MIN_BLOCKS 5
+#endif
+#ifndef VS_JOIN_GRAB
+#define VS_JOIN_GRAB 32
+#endif
+constexpr int64_t kJoinGrab = VS_JOIN_GRAB;  // grouped points per work-queue grab (multiple of 32)
+__global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_join_kernel(const LearnedArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
     __shared__ unsigned s_cnt[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -637,65 +720,64 @@ __global__ void __launch_bounds__(kThreads, 5) learned_join_kernel(const Learned
     __syncwarp();
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
     const int64_t n = (int64_t)*a.n_grouped;
-    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long n_cand = 0;
     unsigned n32 = 0, n64 = 0;
-    for (int64_t base = gw * 32; base < n; base += nw * 32) {
-        const int64_t j = base + lane;
-        GroupedPoint g{0.0, 0.0, 0, 0, 0};
-        uint32_t lo = 0, hi = 0;
-        if (j < n) {
-            g = a.grouped[j];
-            lo = a.cell_start[g.cell];
-            hi = a.cell_start[g.cell + 1];
-        }
-        const double x = g.x, y = g.y;
-        // Candidate loop with one trip count for the whole warp (the longest
-        // list among its lanes; in grouped order the lanes mostly share one).
-        uint32_t len = hi - lo, maxlen = len;
+    for (;;) {
+        const int64_t b0 = warp_grab(a.work, kJoinGrab);
+        if (b0 >= n) break;
+        const int64_t e0 = b0 + kJoinGrab < n ? b0 + kJoinGrab : n;
+        for (int64_t base = b0; base < e0; base += 32) {
+            const int64_t j = base + lane;
+            GroupedPoint g{0.0, 0.0, 0, 0, 0, 0};
+            if (j < e0) g = a.grouped[j];
+            const double x = g.x, y = g.y;
+            const uint32_t lo = g.lo, len = g.len;
+            // Candidate loop with one trip count for the whole warp (the longest
+            // list among its lanes; in grouped order the lanes mostly share one).
+            uint32_t maxlen = len;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
-            maxlen = t > maxlen ? t : maxlen;
-        }
-        for (uint32_t k = 0; k < maxlen; ++k) {
-            bool want = false;
-            int32_t right = 0;
-            if (k < len) {
-                const int slot = (int)a.entries[lo + k];
-                const SlotRecord r = a.slots[slot];
-                const float qx = __double2float_rn(x - r.ox), qy = __double2float_rn(y - r.oy);
-                const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-                // FP32 box filter (rounded outward: never rejects a point of the box)
-                if (!(__fadd_ru(qx, dp) < r.box.x || __fsub_rd(qx, dp) > r.box.z || __fadd_ru(qy, dp) < r.box.y ||
-                      __fsub_rd(qy, dp) > r.box.w)) {
-                    bool cand = true;
-                    int loc = 0;
-                    if (a.accept_mask) {
-                        // The exact location rejects points outside the box by itself.
-                        const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
-                        loc = r.c0 >= 0 ? ring_location_split(x, y, qx, qy, t, a.xy32, a.xy, r.c0, r.c1, n32, n64)
-                                        : geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
-                    } else {
-                        // Box candidates only: decide the box exactly in FP64.
-                        const vs_box bb = a.boxes[slot];
-                        cand = x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy;
-                    }
-                    if (cand) {
-                        ++n_cand;
-                        if (loc == LOC_UNDECIDED) {
-                            defer(a.defer, g.row, slot);
-                        } else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) {
-                            want = true;
-                            right = r.geom;
+            for (int o = 16; o > 0; o >>= 1) {
+                const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
+                maxlen = t > maxlen ? t : maxlen;
+            }
+            for (uint32_t k = 0; k < maxlen; ++k) {
+                bool want = false;
+                int32_t right = 0;
+                if (k < len) {
+                    const SlotRecord r = a.recs[lo + k];
+                    const int slot = r.slot;
+                    const float qx = __double2float_rn(x - r.ox), qy = __double2float_rn(y - r.oy);
+                    const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
+                    // FP32 box filter (rounded outward: never rejects a point of the box)
+                    if (!(__fadd_ru(qx, dp) < r.box.x || __fsub_rd(qx, dp) > r.box.z || __fadd_ru(qy, dp) < r.box.y ||
+                          __fsub_rd(qy, dp) > r.box.w)) {
+                        bool cand = true;
+                        int loc = 0;
+                        if (a.accept_mask) {
+                            // The exact location rejects points outside the box by itself.
+                            const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
+                            loc = r.c0 >= 0 ? ring_location_split(x, y, qx, qy, t, a.xy32, a.xy, r.c0, r.c1, n32, n64)
+                                            : geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
+                        } else {
+                            // Box candidates only: decide the box exactly in FP64.
+                            const vs_box bb = a.boxes[slot];
+                            cand = x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy;
+                        }
+                        if (cand) {
+                            ++n_cand;
+                            if (loc == LOC_UNDECIDED) {
+                                defer(a.defer, g.row, slot);
+                            } else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) {
+                                want = true;
+                                right = a.item_geom[slot];
+                            }
                         }
                     }
                 }
+                wemit_sync(out, a.sink, want, g.row, right);
             }
-            wemit_sync(out, a.sink, want, g.row, right);
+            wflush(out, a.sink, false);
         }
-        wflush(out, a.sink, false);
     }
     wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
@@ -839,7 +921,7 @@ void free_learned_index(vs_index* idx) {
     cudaFree(li.err32);
     cudaFree(li.xy32);
     cudaFree(li.leaves);
-    cudaFree(li.slots);
+    cudaFree(li.recs);
     li = LearnedIndex{};
 }
 
@@ -939,9 +1021,13 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     split_copy_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
                                                             idx->xy, li.origin, li.box32, li.err32, li.xy32);
     VS_CUDA_TRY(cudaGetLastError());
-    VS_TRY(dalloc(&li.slots, (size_t)M, bytes));
+    Scratch<SlotRecord> slots;
+    VS_TRY(slots.alloc((size_t)M, s));
+    VS_TRY(dalloc(&li.recs, (size_t)E, bytes));
     pack_slots_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, li.origin, li.box32, li.err32, idx->item_geom, idx->geom_off,
-                                                       idx->part_off, idx->ring_off, li.slots);
+                                                       idx->part_off, idx->ring_off, slots.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    entry_recs_kernel<<<grid_for(E, 256), 256, 0, s>>>((int64_t)E, li.entries, slots.p, li.recs);
     VS_CUDA_TRY(cudaGetLastError());
     VS_CUDA_TRY(cudaStreamSynchronize(s));
     idx->has_learned = true;
@@ -953,14 +1039,18 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     const LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
     const int64_t n = pts->n;
-    Scratch<int2> point_cell;
-    Scratch<uint32_t> cell_count, n_grouped;
+    const int64_t packets = (n + 31) / 32;
+    const int64_t stripe_cap = 32 * ((packets + kStripes - 1) / kStripes);
+    Scratch<StagedPoint> staged;
+    Scratch<uint32_t> cell_count, n_grouped, stripe_count;
     Scratch<GroupedPoint> grouped;
-    VS_TRY(point_cell.alloc((size_t)n, s));
+    VS_TRY(staged.alloc((size_t)(kStripes * stripe_cap), s));
     VS_TRY(grouped.alloc((size_t)n, s));
     VS_TRY(cell_count.alloc((size_t)li.n_cells, s));
     VS_TRY(n_grouped.alloc(1, s));
+    VS_TRY(stripe_count.alloc((size_t)kStripes, s));
     VS_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, (size_t)li.n_cells * sizeof(uint32_t), s));
+    VS_CUDA_TRY(cudaMemsetAsync(stripe_count.p, 0, (size_t)kStripes * sizeof(uint32_t), s));
     LearnedArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
@@ -977,7 +1067,7 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.entries = li.entries;
     a.n_cells = li.n_cells;
     a.leaves = li.leaves;
-    a.slots = li.slots;
+    a.recs = li.recs;
     a.boxes = idx->nodes;
     a.origin = li.origin;
     a.box32 = li.box32;
@@ -992,17 +1082,28 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.defer = dsink;
     a.counters = ctx->d_counters;
-    a.point_cell = point_cell.p;
+    a.staged = staged.p;
+    a.stripe_count = stripe_count.p;
+    a.stripe_cap = stripe_cap;
     a.cell_count = cell_count.p;
     a.grouped = grouped.p;
     a.n_grouped = n_grouped.p;
-    const int grid = grid_for(n, kThreads, 8);
-    learned_map_kernel<<<grid, kThreads, 0, s>>>(a);
+    a.work = &ctx->d_counters[kWorkCounter];
+#ifndef VS_LEARNED_BLOCKS_PER_SM
+#define VS_LEARNED_BLOCKS_PER_SM 8  // map and scatter blocks per SM (0: one resident wave)
+#endif
+    auto grid = [&](auto kernel, int64_t items) {
+        return VS_LEARNED_BLOCKS_PER_SM > 0 ? grid_for(items, kThreads, VS_LEARNED_BLOCKS_PER_SM)
+                                            : resident_grid(kernel, items, kThreads);
+    };
+    learned_map_kernel<<<grid(learned_map_kernel, n), kThreads, 0, s>>>(a);
     VS_LAUNCHED("learned_map", s);
     VS_TRY(exclusive_scan_u32(cell_count.p, cell_count.p, li.n_cells, n_grouped.p, s));
-    learned_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
+    phase_mark(ctx, 1);
+    learned_scatter_kernel<<<kStripes, kThreads, 0, s>>>(a);
     VS_LAUNCHED("learned_scatter", s);
-    learned_join_kernel<<<grid, kThreads, 0, s>>>(a);
+    phase_mark(ctx, 2);
+    learned_join_kernel<<<resident_grid(learned_join_kernel, n, kThreads), kThreads, 0, s>>>(a);
     VS_LAUNCHED("learned_join", s);
     return VS_OK;
 }

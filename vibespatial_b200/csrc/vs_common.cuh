@@ -19,6 +19,8 @@ int check_polygons(const vs_polygons* p);
 // Pinned host words of a context (read-back of the device counters and of
 // per-call extras).
 constexpr int kHostCounters = 16;
+constexpr int kDevCounters = 16;
+constexpr int kWorkCounter = 8;
 
 #define VS_CUDA_TRY(expr)                                                        \
     do {                                                                         \
@@ -74,6 +76,22 @@ inline int grid_for(int64_t n, int block, int per_sm = 8) {
     return (int)(need < cap ? need : cap);
 }
 
+// Grid for a grid-stride kernel: at most one full wave of resident blocks
+// (blocks per SM from the occupancy calculator x SMs), so no partial second
+// wave runs on a fraction of the SMs.
+template <class Kernel>
+int resident_grid(Kernel kernel, int64_t n_items, int block, size_t smem = 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    int64_t need = (n_items + block - 1) / block;
+    const int64_t cap = (int64_t)kNumSMs * per_sm;
+    if (need < 1) need = 1;
+    return (int)(need < cap ? need : cap);
+}
+
 // Order-preserving map from double to int64 so atomicMin/atomicMax on
 // long long order doubles correctly (NaN excluded by the callers).
 __device__ __forceinline__ long long dbl_to_ordered(double v) {
@@ -113,12 +131,22 @@ struct vs_context {
     vs::Arena arena;
     // Pinned host words (kHostCounters) used to read back counts.
     unsigned long long* h_counter;
-    // Device counters: [0] pair count, [1] exact-fallback count,
-    // [2] fp32-filter decided edges, [3] edges sent past the fp32 filter,
-    // [4] error flags, [5] candidate (bbox) count, [6] wide learned-index
-    // windows, [7] deferred pairs.
+    // Device counters (kDevCounters, zeroed at the start of every join):
+    // [0] pair count, [1] exact-fallback count, [2] fp32-filter decided
+    // edges, [3] edges sent past the fp32 filter, [4] error flags,
+    // [5] candidate (bbox) count, [6] wide learned-index windows,
+    // [7] deferred pairs, [8] work queue of the refine kernel.
     unsigned long long* d_counters;
     // Pairs deferred to the exact pass (grown on demand).
     int2* defer_buf;
     unsigned long long defer_cap;
+    // Phase boundaries of one join (vs_join_stats.phase_ms): marks 0..4
+    // around locate / group / refine / exact; recorded only while phase_on.
+    cudaEvent_t phase_ev[5];
+    bool phase_on;
 };
+
+// Record phase boundary k of the current join on the context stream.
+inline void phase_mark(vs_context* ctx, int k) {
+    if (ctx->phase_on) cudaEventRecord(ctx->phase_ev[k], ctx->stream);
+}
