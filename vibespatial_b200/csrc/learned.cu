@@ -665,7 +665,7 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LearnedA
 // cell's candidate range.  A block walks whole stripe regions (coalesced
 // reads, every lane busy); each thread keeps kScatterUnroll records in flight.
 #ifndef VS_SCATTER_UNROLL
-#define VS_SCATTER_UNROLL 2
+#define VS_SCATTER_UNROLL 4
 #endif
 constexpr int kScatterUnroll = VS_SCATTER_UNROLL;
 
@@ -779,6 +779,113 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_join_ker
             wflush(out, a.sink, false);
         }
     }
+    wflush(out, a.sink, true);
+    add_counter(a.counters, 5, n_cand);
+    add_counter(a.counters, 2, n32);
+    add_counter(a.counters, 3, n64);
+}
+
+// Pass 3 with candidate compaction (predicates with a location test): the
+// warp walks its grouped points' candidate lists, and every (point,
+// candidate) pair that passes the FP32 box filter is appended to a warp-local
+// queue in shared memory.  Each time 32 pairs are queued, every lane refines
+// one of them.  So the ring walks, which dominate, run with all lanes busy
+// instead of only the lanes whose point lies in the current candidate's box.
+// Neighbouring queue entries mostly share a polygon, so vertex reads stay
+// broadcasts.
+struct QueuedPair {
+    double x, y;
+    int32_t row;
+    uint32_t rec;  // index into the per-entry records
+};
+constexpr int kQueue = 64;  // >= 31 left over + 32 appended in one step
+
+__device__ __forceinline__ void refine_queued(const LearnedArgs& a, const WarpOut& out, const QueuedPair* q, int nq,
+                                              int lane, unsigned& n32, unsigned& n64) {
+    bool want = false;
+    int32_t row = 0, right = 0;
+    if (lane < nq) {
+        const QueuedPair jb = q[lane];
+        row = jb.row;
+        const SlotRecord r = a.recs[jb.rec];
+        const float qx = __double2float_rn(jb.x - r.ox), qy = __double2float_rn(jb.y - r.oy);
+        const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
+        const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
+        const int loc = r.c0 >= 0 ? ring_location_split(jb.x, jb.y, qx, qy, t, a.xy32, a.xy, r.c0, r.c1, n32, n64)
+                                  : geometry_location_split(jb.x, jb.y, qx, qy, t, a, r.slot, n32, n64);
+        if (loc == LOC_UNDECIDED) {
+            defer(a.defer, jb.row, r.slot);
+        } else if ((a.accept_mask >> loc) & 1) {
+            want = true;
+            right = a.item_geom[r.slot];
+        }
+    }
+    wemit_sync(out, a.sink, want, row, right);
+}
+
+__global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_kernel(const LearnedArgs a) {
+    __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
+    __shared__ unsigned s_cnt[kThreads / 32];
+    __shared__ QueuedPair s_q[kThreads / 32][kQueue];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncwarp();
+    const WarpOut out{s_buf[warp], &s_cnt[warp]};
+    QueuedPair* q = s_q[warp];
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t n = (int64_t)*a.n_grouped;
+    unsigned long long n_cand = 0;
+    unsigned n32 = 0, n64 = 0;
+    int nq = 0;  // warp-uniform queue length
+    for (;;) {
+        const int64_t b0 = warp_grab(a.work, kJoinGrab);
+        if (b0 >= n) break;
+        const int64_t e0 = b0 + kJoinGrab < n ? b0 + kJoinGrab : n;
+        for (int64_t base = b0; base < e0; base += 32) {
+            const int64_t j = base + lane;
+            GroupedPoint g{0.0, 0.0, 0, 0, 0, 0};
+            if (j < e0) g = a.grouped[j];
+            uint32_t maxlen = g.len;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
+                maxlen = t > maxlen ? t : maxlen;
+            }
+            for (uint32_t k = 0; k < maxlen; ++k) {
+                bool inbox = false;
+                if (k < g.len) {
+                    const SlotRecord* rp = a.recs + g.lo + k;
+                    const double2 o = *reinterpret_cast<const double2*>(&rp->ox);
+                    const float4 bx = rp->box;
+                    const float qx = __double2float_rn(g.x - o.x), qy = __double2float_rn(g.y - o.y);
+                    const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
+                    // FP32 box filter (rounded outward: never rejects a point of the box)
+                    inbox = !(__fadd_ru(qx, dp) < bx.x || __fsub_rd(qx, dp) > bx.z || __fadd_ru(qy, dp) < bx.y ||
+                              __fsub_rd(qy, dp) > bx.w);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, inbox);
+                if (inbox) {
+                    QueuedPair& e = q[nq + __popc(m & lt)];
+                    e.x = g.x;
+                    e.y = g.y;
+                    e.row = g.row;
+                    e.rec = g.lo + k;
+                    ++n_cand;
+                }
+                nq += __popc(m);
+                __syncwarp();
+                if (nq >= 32) {
+                    refine_queued(a, out, q, 32, lane, n32, n64);
+                    __syncwarp();
+                    if (lane < nq - 32) q[lane] = q[32 + lane];
+                    nq -= 32;
+                    __syncwarp();
+                }
+            }
+            wflush(out, a.sink, false);
+        }
+    }
+    if (nq > 0) refine_queued(a, out, q, nq, lane, n32, n64);
     wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 2, n32);
@@ -1103,8 +1210,16 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     learned_scatter_kernel<<<kStripes, kThreads, 0, s>>>(a);
     VS_LAUNCHED("learned_scatter", s);
     phase_mark(ctx, 2);
-    learned_join_kernel<<<resident_grid(learned_join_kernel, n, kThreads), kThreads, 0, s>>>(a);
-    VS_LAUNCHED("learned_join", s);
+#ifndef VS_REFINE_QUEUE
+#define VS_REFINE_QUEUE 1
+#endif
+    if (VS_REFINE_QUEUE && accept_mask) {
+        learned_refine_kernel<<<resident_grid(learned_refine_kernel, n, kThreads), kThreads, 0, s>>>(a);
+        VS_LAUNCHED("learned_refine", s);
+    } else {
+        learned_join_kernel<<<resident_grid(learned_join_kernel, n, kThreads), kThreads, 0, s>>>(a);
+        VS_LAUNCHED("learned_join", s);
+    }
     return VS_OK;
 }
 
