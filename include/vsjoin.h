@@ -200,10 +200,11 @@ int vs_hilbert_keys(vs_context* ctx, const double* d_x, const double* d_y, int64
 typedef struct vs_batch_plan vs_batch_plan;
 
 typedef struct vs_batch_options {
-    int32_t blocks_per_sm;    /* join kernel blocks per SM, 1..8 (0 = 4) */
-    int32_t packets_per_grab; /* 32-point packets a warp takes per work-counter grab (0 = 4) */
-    int32_t sort_levels;      /* Hilbert levels the points of a job are sorted by (0 = 8) */
-    int32_t reserved;
+    int32_t blocks_per_sm;    /* R-tree: join kernel blocks per SM, 1..8 (0 = 4) */
+    int32_t packets_per_grab; /* R-tree: 32-point packets a warp takes per work-counter grab (0 = 4) */
+    int32_t sort_levels;      /* R-tree: Hilbert levels the points of a job are sorted by (0 = 8) */
+    int32_t method;           /* VS_METHOD_RTREE (0) or VS_METHOD_LEARNED: every index with polygons
+                                 must then have its learned part (VS_E_ARG otherwise) */
 } vs_batch_options;
 
 /* At most 4096 jobs and 2^31-1 points in total. */

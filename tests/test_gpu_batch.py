@@ -16,7 +16,7 @@ def _jobs(seed=7, n_jobs=12):
 
 
 class _Batch:
-    def __init__(self, abi, ctx, jobs, pvalid=None, options=None, empty_index_jobs=()):
+    def __init__(self, abi, ctx, jobs, pvalid=None, options=None, empty_index_jobs=(), learned=False):
         self.jobs = jobs
         self.px = np.concatenate([w.px for w in jobs])
         self.py = np.concatenate([w.py for w in jobs])
@@ -30,7 +30,9 @@ class _Batch:
                 bufs["valid"] = to_dev(np.zeros(len(w.polys.geom_off) - 1, np.uint8))
                 P.d_valid = bufs["valid"].data_ptr()
             self._keep.append(bufs)
-            self.indexes.append(abi.DeviceIndex(ctx, P))
+            self.indexes.append(abi.DeviceIndex(ctx, P, learned=learned))
+        if learned:
+            options = dict(options or {}, method=abi.METHOD_LEARNED)
         self.plan = abi.BatchPlan(ctx, self.indexes, self.pts, self.job_start, options=options)
 
     def split(self, left, right):
@@ -184,3 +186,60 @@ def test_autotuned_options_round_trip(vsabi, ctx, batch, tmp_path):
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x[0], y[0])
         np.testing.assert_array_equal(x[1], y[1])
+
+
+# ---- learned method: the same batches through the learned cell indexes ----
+
+@pytest.fixture(scope="module")
+def lbatch(vsabi, ctx):
+    return _Batch(vsabi, ctx, _jobs(), learned=True)
+
+
+@pytest.mark.parametrize("predicate", ["within", "intersects", "touches", None])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_learned_batch_matches_oracle(lbatch, oracle, predicate, use_graph):
+    left, right, _ = _run(lbatch, predicate, use_graph=use_graph)
+    assert len(left) == len(set(zip(left.tolist(), right.tolist())))
+    for j, (l, r) in enumerate(lbatch.split(left, right)):
+        w = lbatch.jobs[j]
+        el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), predicate)
+        np.testing.assert_array_equal(l, el)
+        np.testing.assert_array_equal(r, er)
+
+
+def test_learned_batch_single_job_equals_vs_join(vsabi, ctx):
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.zipf_join(seed=9, n_points=400_000, n_polys=8_000)
+    b = _Batch(vsabi, ctx, [w], learned=True)
+    left, right, _ = _run(b, "within")
+    (l, r), = b.split(left, right)
+    pts, _k = upload_points(vsabi, w.px, w.py)
+    gl, gr, _ = b.indexes[0].join(pts, PRED_CODES["within"], vsabi.METHOD_LEARNED, sort=True)
+    np.testing.assert_array_equal(l, gl.cpu().numpy())
+    np.testing.assert_array_equal(r, gr.cpu().numpy())
+
+
+def test_learned_batch_nulls_empty_jobs(vsabi, ctx, oracle):
+    from vibespatial_b200.testing import synthetic as syn
+
+    jobs = _jobs(seed=4, n_jobs=5)
+    jobs.insert(1, syn.star_join(seed=98, n_points=0, n_polys=10))
+    n = sum(w.n_points for w in jobs)
+    pvalid = (np.random.default_rng(2).random(n) > 0.2).astype(np.uint8)
+    b = _Batch(vsabi, ctx, jobs, pvalid=pvalid, empty_index_jobs=(3,), learned=True)
+    left, right, _ = _run(b, "intersects")
+    for j, (l, r) in enumerate(b.split(left, right)):
+        if j == 3:
+            assert len(l) == 0
+            continue
+        w = jobs[j]
+        pv = pvalid[b.job_start[j]:b.job_start[j + 1]]
+        el, er = oracle.join(w.px, w.py, pv, oracle_polys(oracle, w.polys), "intersects")
+        np.testing.assert_array_equal(l, el)
+        np.testing.assert_array_equal(r, er)
+
+
+def test_learned_batch_needs_learned_indexes(vsabi, ctx, batch):
+    with pytest.raises(ValueError):
+        vsabi.BatchPlan(ctx, batch.indexes, batch.pts, batch.job_start, options={"method": vsabi.METHOD_LEARNED})

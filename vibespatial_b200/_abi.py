@@ -82,10 +82,10 @@ class JoinStats(ctypes.Structure):
 
 class BatchOptions(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_int32), ("packets_per_grab", ctypes.c_int32),
-                ("sort_levels", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("sort_levels", ctypes.c_int32), ("method", ctypes.c_int32)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class IndexInfo(ctypes.Structure):

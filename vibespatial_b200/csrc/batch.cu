@@ -30,6 +30,7 @@
 #include "hilbert.cuh"
 #include "index.cuh"
 #include "join.cuh"
+#include "learned.cuh"
 #include "primitives.cuh"
 
 namespace vs {
@@ -327,6 +328,13 @@ struct vs_batch_plan {
     int32_t* g_right = nullptr;
     int64_t g_cap = -1;
     long long g_kernels = 0;  // kernels in the captured graph
+    // learned method: per-job query descriptors and the pipeline's scratch
+    bool learned = false;
+    vs::LearnedJob* d_ljobs = nullptr;
+    vs::LearnedJob h_single{};  // the descriptor when the batch has one job
+    int64_t n_cells = 0;        // batch-wide learned cells
+    void* lscratch = nullptr;
+    vs::LearnedScratch lsc{};
 };
 
 namespace vs {
@@ -346,6 +354,8 @@ void free_plan(vs_batch_plan* p) {
     cudaFree(p->defer);
     cudaFree(p->d_work);
     cudaFree(p->d_n_valid);
+    cudaFree(p->d_ljobs);
+    cudaFree(p->lscratch);
 }
 
 BatchArgs plan_args(vs_batch_plan* p, int mask, int32_t* left, int32_t* right, int64_t capacity) {
@@ -376,6 +386,26 @@ int enqueue_batch(vs_batch_plan* p, cudaStream_t s, int mask, int32_t* left, int
     const BatchArgs a = plan_args(p, mask, left, right, capacity);
     VS_CUDA_TRY(cudaMemsetAsync(p->ctx->d_counters, 0, kDevCounters * sizeof(unsigned long long), s));
     VS_CUDA_TRY(cudaMemsetAsync(p->d_work, 0, 2 * sizeof(unsigned long long), s));
+    if (p->learned) {
+        LearnedQuery q{};
+        q.px = p->pts.d_x;
+        q.py = p->pts.d_y;
+        q.pvalid = p->pts.d_valid;
+        q.n = p->n_points;
+        q.jobs = p->d_ljobs;
+        q.n_jobs = p->n_jobs;
+        q.job_start = p->d_job_start;
+        q.n_cells = p->n_cells;
+        q.accept_mask = mask;
+        VS_TRY(enqueue_learned(s, nullptr, q, p->n_jobs == 1 ? &p->h_single : nullptr, p->lsc, a.sink, a.defer,
+                               a.counters, &p->d_work[0]));
+        if (mask) {
+            batch_resolve_kernel<<<resident_grid(batch_resolve_kernel, (int64_t)1 << 30, kBThreads), kBThreads, 0,
+                                   s>>>(a);
+            VS_LAUNCHED("batch_resolve", s);
+        }
+        return VS_OK;
+    }
     VS_CUDA_TRY(cudaMemsetAsync(p->d_n_valid, 0, sizeof(uint32_t), s));
     const size_t smem = (size_t)(p->n_jobs + 1) * sizeof(int64_t);
     batch_key_kernel<<<resident_grid(batch_key_kernel, p->n_points, 256, smem), 256, smem, s>>>(a, p->n_points);
@@ -502,6 +532,39 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
         t.levels = ix->levels;
         t.n_geoms = ix->levels > 0 ? ix->n_geoms : 0;
     }
+    p->learned = p->opts.method == VS_METHOD_LEARNED;
+    if (p->opts.method != VS_METHOD_RTREE && !p->learned) {
+        set_error("batch method %d: use VS_METHOD_RTREE or VS_METHOD_LEARNED", p->opts.method);
+        delete p;
+        return VS_E_ARG;
+    }
+    std::vector<LearnedJob> ljobs;
+    if (p->learned) {
+        ljobs.resize(n_jobs);
+        int64_t base = 0;
+        for (int j = 0; j < n_jobs; ++j) {
+            const vs_index* ix = indexes[j];
+            LearnedJob& d = ljobs[j];
+            memset(&d, 0, sizeof(d));
+            const bool has_polys = ix->n_geoms > 0 && ix->h_frame[0] <= ix->h_frame[2];
+            if (ix->has_learned) {
+                d = ix->learned.h_desc;
+                d.cell_base = (uint32_t)base;
+                base += ix->learned.n_cells;
+            } else if (has_polys) {
+                set_error("job %d: index was built without its learned part", j);
+                delete p;
+                return VS_E_ARG;
+            }
+        }
+        if (base >= 0x7fffffffLL) {
+            set_error("batch has %lld learned cells (at most 2^31-1)", (long long)base);
+            delete p;
+            return VS_E_ARG;
+        }
+        p->n_cells = base;
+        p->h_single = ljobs[0];
+    }
     p->defer_cap = (unsigned long long)(N / 16 + (1 << 16));
     const size_t nn = (size_t)(N > 0 ? N : 1);
     if (cudaMalloc((void**)&p->d_jobs, sizeof(JobTree) * n_jobs) != cudaSuccess ||
@@ -510,7 +573,9 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
         cudaMalloc((void**)&p->order, sizeof(uint32_t) * nn) != cudaSuccess ||
         cudaMalloc((void**)&p->defer, sizeof(int2) * p->defer_cap) != cudaSuccess ||
         cudaMalloc((void**)&p->d_work, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc((void**)&p->d_n_valid, sizeof(uint32_t)) != cudaSuccess) {
+        cudaMalloc((void**)&p->d_n_valid, sizeof(uint32_t)) != cudaSuccess ||
+        (p->learned && (cudaMalloc((void**)&p->d_ljobs, sizeof(LearnedJob) * n_jobs) != cudaSuccess ||
+                        cudaMalloc(&p->lscratch, learned_scratch_bytes(N, p->n_cells)) != cudaSuccess))) {
         cudaGetLastError();
         set_error("batch plan allocation failed (%lld points)", (long long)N);
         free_plan(p);
@@ -531,6 +596,10 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
     cudaError_t e = cudaMemcpyAsync(p->d_jobs, jobs.data(), sizeof(JobTree) * n_jobs, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(p->d_job_start, h_job_start, sizeof(int64_t) * (n_jobs + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && p->learned) {
+        e = cudaMemcpyAsync(p->d_ljobs, ljobs.data(), sizeof(LearnedJob) * n_jobs, cudaMemcpyHostToDevice, s);
+        learned_scratch_carve(p->lscratch, N, p->n_cells, p->lsc);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_error("batch plan upload failed: %s", cudaGetErrorString(e));

@@ -50,6 +50,34 @@ struct RmiModel {
     int32_t n_keys;
 };
 
+// One learned index as the query kernels see it (device memory, or
+// the kernel parameters for a single join).  A batch of
+// joins passes an array of these; job j's cells are numbered from
+// cell_base in the batch-wide cell numbering.
+struct LearnedJob {
+    // frame and quantisation scales, computed on the device exactly as the
+    // build computed them
+    double lox, loy, hix, hiy, sx, sy;
+    int32_t L;
+    int32_t occ_shift;   // cell key >> occ_shift = occupancy bit
+    int32_t root_shift;  // cell key >> root_shift = root-table index
+    uint32_t cell_base;
+    int64_t n_cells;
+    const uint32_t* occ;
+    const uint16_t* root_table;
+    const RmiLeaf* leaves;
+    const uint32_t* cell_keys;
+    const uint32_t* cell_start;
+    const SlotRecord* recs;  // [n_entries] per-entry slot records, cell order
+    const float2* xy32;
+    const double2* xy;
+    const int32_t* item_geom;
+    const int32_t* geom_off;
+    const int32_t* part_off;
+    const int32_t* ring_off;
+    const vs_box* boxes;     // FP64 slot boxes (R-tree level 0)
+};
+
 struct LearnedIndex {
     int32_t level = 0;               // grid level L (cells of frame / 2^L per axis)
     int32_t occ_level = 0;           // occupancy bitmap level (<= L)
@@ -73,6 +101,8 @@ struct LearnedIndex {
     RmiLeaf* leaves = nullptr;       // [n_leaves] the two above packed for queries
     int32_t n_leaves = 0;
     SlotRecord* recs = nullptr;      // [n_entries] record of each entry's slot, cell order
+    LearnedJob* desc = nullptr;      // device: this index as the query kernels see it
+    LearnedJob h_desc{};             // host copy of *desc
     // FP32 tile-relative copies used by the split-precision filter
     double2* origin = nullptr;       // [n_geoms] slot origin (box centre, FP64)
     float4* box32 = nullptr;         // [n_geoms] slot box relative to the origin, rounded outward

@@ -15,23 +15,7 @@
 //   5. FP32 copies of every polygon relative to its own origin (box centre),
 //      with a per-polygon bound on the rounding error, for the split filter
 //
-// Query, three passes over the points (a counting sort keyed by the learned
-// index's own positions, so no general sort is needed):
-//   map      input order: level-L cell key -> occupancy bit -> root table ->
-//            leaf model -> binary search inside the leaf's error window ->
-//            cell index (or none); warp-aggregated atomics on the per-cell
-//            counts return each point's rank within its cell
-//   scatter  after an exclusive scan of the counts, each matched point
-//            writes one aligned 32-byte record (x, y, row, cell) at
-//            start[cell] + rank; points in empty cells drop out
-//   join     a warp takes 32 consecutive records, which share a polygon list
-//            except at cell boundaries, so the lanes read each polygon's data
-//            together (broadcast); each candidate is box-filtered in FP32
-//            (rounded outward) and refined with the FP32 crossing test on
-//            tile-relative coordinates; only edges whose FP32 decision lies
-//            within the rounding-error bound are re-decided in FP64, and a
-//            pair the FP64 filter cannot certify is deferred to the exact
-//            pass.
+// The query passes over this index live in learned_query.cu.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -46,6 +30,7 @@
 #include "hilbert.cuh"
 #include "index.cuh"
 #include "join.cuh"
+#include "learned.cuh"
 #include "primitives.cuh"
 #include "rmi.cuh"
 
@@ -436,460 +421,17 @@ __global__ void rmi_window_stats_kernel(const uint32_t* __restrict__ leaf_of, in
     }
 }
 
-// ----------------------------------------------------------------- query ---
-// One grouped point: a full 32-byte sector, so the scatter writes whole
-// sectors (no read-modify-write of partially written ones).
-// A matched query point as the map pass leaves it: coordinates, row, cell
-// index and its rank among the cell's points.
-struct __align__(32) StagedPoint {
-    double x, y;
-    int32_t row;
-    int32_t cell;
-    uint32_t rank;
-    int32_t pad;
-};
-
-// The map pass appends matched points to kStripes regions of the staging
-// array, region s taking the packets p with p % kStripes == s, so each
-// region's append counter sees 1/kStripes of the atomics and a region never
-// holds more than 32 * ceil(packets / kStripes) points.
-constexpr int kStripes = 2048;
-
-// A query point in cell order, with its cell's candidate range
-// [lo, lo + len) of the per-entry records.
-struct __align__(32) GroupedPoint {
-    double x, y;
-    int32_t row;
-    uint32_t lo;
-    uint32_t len;
-    int32_t pad;
-};
-
-struct LearnedArgs {
-    const double* px;
-    const double* py;
-    const uint8_t* pvalid;
-    int64_t n;
-    const double* frame;
-    int L;
-    int occ_shift;             // cell key >> occ_shift = occupancy bit
-    int root_shift;            // cell key >> root_shift = root-table index
-    const uint32_t* occ;
-    const uint16_t* root_table;
-    const uint32_t* cell_keys;
-    const uint32_t* cell_start;
-    const uint32_t* entries;
-    int64_t n_cells;
-    const RmiLeaf* leaves;
-    const SlotRecord* recs;          // [n_entries] per-entry slot records
-    const vs_box* boxes;       // FP64 slot boxes (R-tree level 0)
-    const double2* origin;
-    const float4* box32;
-    const float* err32;
-    const float2* xy32;
-    const double2* xy;
-    const int32_t* item_geom;
-    const int32_t* geom_off;
-    const int32_t* part_off;
-    const int32_t* ring_off;
-    int accept_mask;
-    PairSink sink;
-    DeferSink defer;
-    unsigned long long* counters;
-    // grouping scratch (per join)
-    StagedPoint* staged;       // [kStripes * stripe_cap] matched points, striped
-    uint32_t* stripe_count;    // [kStripes] points appended to each region
-    int64_t stripe_cap;        // points one region can hold
-    uint32_t* cell_count;      // [n_cells] counts, then (after the scan) start offsets
-    GroupedPoint* grouped;     // [n_grouped] points grouped by cell
-    const uint32_t* n_grouped;
-    unsigned long long* work;  // refine work queue (grouped points handed out)
-};
-
-// One edge in FP32 on tile-relative coordinates.  Returns false when some
-// decision the exact walk needs lies within the rounding-error bound `t`
-// (the caller then re-decides the edge in FP64); otherwise applies the same
-// decision the exact walk would (the point cannot be on this edge).
-__device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, float by, float px, float py, float t,
-                                               bool& inside) {
-    const float A2 = __fsub_rn(ay, py), B2 = __fsub_rn(by, py);
-    if (fabsf(A2) <= t || fabsf(B2) <= t) return false;
-    const bool sA = A2 > 0.f, sB = B2 > 0.f;
-    if (sA == sB) return true;  // py strictly outside the edge's y-range
-    const float A1 = __fsub_rn(ax, px), B1 = __fsub_rn(bx, px);
-    if (A1 > t && B1 > t) {  // edge strictly right of the point: the +x ray crosses it
-        inside = !inside;
-        return true;
-    }
-    if (A1 < -t && B1 < -t) return true;  // strictly left
-    const float l = __fmul_rn(A1, B2), r = __fmul_rn(A2, B1);
-    const float det = __fsub_rn(l, r);
-    const float m = fmaxf(fmaxf(fabsf(A1), fabsf(A2)), fmaxf(fabsf(B1), fabsf(B2)));
-    const float e = __fmaf_ru(m, 6.0e-8f, t);
-    const float S = __fadd_ru(__fadd_ru(fabsf(A1), fabsf(A2)), __fadd_ru(fabsf(B1), fabsf(B2)));
-    float bound = __fmaf_ru(3.6e-7f, __fadd_ru(fabsf(l), fabsf(r)), __fmaf_ru(S, e, __fmul_ru(2.0f, __fmul_ru(e, e))));
-    bound = __fmaf_ru(bound, 1.01f, 1e-30f);
-    if (det > bound) {
-        if (sB) inside = !inside;  // o > 0 and, since the edge crosses, by > ay <=> sB
-        return true;
-    }
-    if (det < -bound) {
-        if (!sB) inside = !inside;
-        return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ int ring_location_split(double px, double py, float qx, float qy, float t,
-                                                   const float2* __restrict__ xy32, const double2* __restrict__ xy,
-                                                   int start, int end, unsigned& n32, unsigned& n64) {
-    if (end - start < 2) return LOC_OUTSIDE;
-    bool inside = false;
-    float2 a = xy32[end - 1];
-    int ia = end - 1;
-    for (int i = start; i < end; ++i) {
-        const float2 b = xy32[i];
-        if (edge_step_fp32(a.x, a.y, b.x, b.y, qx, qy, t, inside)) {
-            ++n32;
-        } else {
-            ++n64;
-            const double2 A = xy[ia], B = xy[i];
-            const int r = edge_step_filtered(A.x, A.y, B.x, B.y, px, py, inside);
-            if (r == 1) return LOC_BOUNDARY;
-            if (r == 2) return LOC_UNDECIDED;
-        }
-        a = b;
-        ia = i;
-    }
-    return inside ? LOC_INTERIOR : LOC_OUTSIDE;
-}
-
-__device__ __forceinline__ int geometry_location_split(double px, double py, float qx, float qy, float t,
-                                                       const LearnedArgs& a, int g, unsigned& n32, unsigned& n64) {
-    const int p0 = a.geom_off[g], p1 = a.geom_off[g + 1];
-    for (int part = p0; part < p1; ++part) {
-        bool inside = false;
-        const int r0 = a.part_off[part], r1 = a.part_off[part + 1];
-        for (int ring = r0; ring < r1; ++ring) {
-            const int k = ring_location_split(px, py, qx, qy, t, a.xy32, a.xy, a.ring_off[ring], a.ring_off[ring + 1],
-                                              n32, n64);
-            if (k == LOC_BOUNDARY || k == LOC_UNDECIDED) return k;
-            if (k == LOC_INTERIOR) inside = !inside;
-        }
-        if (inside) return LOC_INTERIOR;
-    }
-    return LOC_OUTSIDE;
-}
-
-// Exact lookup of a point's cell in the learned index: level-L cell key ->
-// occupancy bit -> root table -> leaf model -> binary search inside the
-// leaf's error window.  Returns the cell's index, or -1 when no stored cell
-// matches (no polygon box overlaps the point's cell).
-__device__ __forceinline__ int learned_lookup(const LearnedArgs& a, double x, double y, double lox, double loy,
-                                              double sx, double sy, const uint16_t* lut,
-                                              unsigned long long& n_wide) {
-    const uint32_t cell = hilbert_key_lut(quantize(x, lox, sx), quantize(y, loy, sy), a.L, lut);
-    const uint32_t ob = cell >> a.occ_shift;
-    if (!((a.occ[ob >> 5] >> (ob & 31)) & 1u)) return -1;
-    const RmiLeaf lf = a.leaves[a.root_table[cell >> a.root_shift]];
-    if (lf.lo > lf.hi) return -1;  // no stored key routes to this leaf
-    const long long pred = rmi_predict(make_double2(lf.a, lf.b), cell);
-    long long l0 = pred + lf.lo, h0 = pred + lf.hi + 1;  // search [l0, h0)
-    l0 = l0 < 0 ? 0 : l0;
-    h0 = h0 > a.n_cells ? a.n_cells : h0;
-    if (h0 - l0 > 256) ++n_wide;
-    const long long h1 = h0;
-    while (l0 < h0) {
-        const long long mid = (l0 + h0) >> 1;
-        if (a.cell_keys[mid] < cell) l0 = mid + 1;
-        else h0 = mid;
-    }
-    return (l0 < h1 && a.cell_keys[l0] == cell) ? (int)l0 : -1;
-}
-
-// Pass 1 (map), points in input order: each point's cell and its rank among
-// the cell's points (warp-aggregated atomics on the per-cell counts); the
-// matched points are appended to the staging regions.
-__global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LearnedArgs a) {
-    __shared__ uint16_t s_lut[kHilbertLutSize];
-    hilbert_lut_init(s_lut);
-    __syncthreads();
+// Frame fields of the query descriptor, computed exactly as the build
+// quantised (frame_q), so query-side cell keys match the registered ones.
+__global__ void learned_desc_kernel(const double* __restrict__ fr, LearnedJob* __restrict__ d) {
     double lox, loy, sx, sy;
-    frame_q(a.frame, lox, loy, sx, sy);
-    const double fx1 = a.frame[2], fy1 = a.frame[3];
-    unsigned long long n_wide = 0;
-    const int lane = threadIdx.x & 31;
-    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    // Warp-uniform loop: the whole warp reaches the match and shuffle together.
-    for (int64_t b0 = gw * 32; b0 < a.n; b0 += nw * 32) {
-        const int64_t i = b0 + lane;
-        int c = -1;
-        double x = 0.0, y = 0.0;
-        if (i < a.n) {
-            x = a.px[i];
-            y = a.py[i];
-            if ((a.pvalid == nullptr || a.pvalid[i]) && x >= lox && x <= fx1 && y >= loy && y <= fy1)
-                c = learned_lookup(a, x, y, lox, loy, sx, sy, s_lut, n_wide);
-        }
-        const unsigned lt = (1u << lane) - 1u;
-        const unsigned peers = __match_any_sync(0xffffffffu, c);
-        const int leader = __ffs(peers) - 1;
-        uint32_t base = 0;
-        if (c >= 0 && lane == leader) base = atomicAdd(&a.cell_count[c], (uint32_t)__popc(peers));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        // append the matched points of this packet to its stripe region
-        const unsigned mm = __ballot_sync(0xffffffffu, c >= 0);
-        if (mm) {
-            const int64_t stripe = (b0 >> 5) % kStripes;
-            uint32_t sb = 0;
-            if (lane == 0) sb = atomicAdd(&a.stripe_count[stripe], (uint32_t)__popc(mm));
-            sb = __shfl_sync(0xffffffffu, sb, 0);
-            if (c >= 0) {
-                StagedPoint p;
-                p.x = x;
-                p.y = y;
-                p.row = (int32_t)i;
-                p.cell = c;
-                p.rank = base + __popc(peers & lt);
-                p.pad = 0;
-                a.staged[stripe * a.stripe_cap + sb + __popc(mm & lt)] = p;
-            }
-        }
-    }
-    add_counter(a.counters, 6, n_wide);
-}
-
-// Pass 2 (scatter): after the exclusive scan of the counts, every staged
-// point writes one aligned 32-byte record at start[cell] + rank, carrying its
-// cell's candidate range.  A block walks whole stripe regions (coalesced
-// reads, every lane busy); each thread keeps kScatterUnroll records in flight.
-#ifndef VS_SCATTER_UNROLL
-#define VS_SCATTER_UNROLL 4
-#endif
-constexpr int kScatterUnroll = VS_SCATTER_UNROLL;
-
-__global__ void __launch_bounds__(kThreads) learned_scatter_kernel(const LearnedArgs a) {
-    for (int stripe = blockIdx.x; stripe < kStripes; stripe += gridDim.x) {
-        const uint32_t cnt = a.stripe_count[stripe];
-        const StagedPoint* src = a.staged + (int64_t)stripe * a.stripe_cap;
-        for (uint32_t k0 = threadIdx.x; k0 < cnt; k0 += blockDim.x * kScatterUnroll) {
-            StagedPoint p[kScatterUnroll];
-#pragma unroll
-            for (int u = 0; u < kScatterUnroll; ++u) {
-                const uint32_t k = k0 + u * blockDim.x;
-                if (k < cnt) p[u] = src[k];
-            }
-            GroupedPoint g[kScatterUnroll];
-            uint32_t pos[kScatterUnroll];
-#pragma unroll
-            for (int u = 0; u < kScatterUnroll; ++u) {
-                const uint32_t k = k0 + u * blockDim.x;
-                if (k < cnt) {
-                    const int c = p[u].cell;
-                    g[u].x = p[u].x;
-                    g[u].y = p[u].y;
-                    g[u].row = p[u].row;
-                    g[u].lo = a.cell_start[c];
-                    g[u].len = a.cell_start[c + 1] - g[u].lo;
-                    g[u].pad = 0;
-                    pos[u] = a.cell_count[c] + p[u].rank;
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kScatterUnroll; ++u)
-                if (k0 + u * blockDim.x < cnt) a.grouped[pos[u]] = g[u];
-        }
-    }
-}
-
-// Pass 3 (join): a warp takes 32 consecutive grouped points, which share a
-// cell (and so a polygon list: broadcast reads) except at cell boundaries.
-#ifndef VS_JOIN_MIN_BLOCKS
-#define VS_JOIN_MIN_BLOCKS 5
-#endif
-#ifndef VS_JOIN_GRAB
-#define VS_JOIN_GRAB 32
-#endif
-constexpr int64_t kJoinGrab = VS_JOIN_GRAB;  // grouped points per work-queue grab (multiple of 32)
-__global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_join_kernel(const LearnedArgs a) {
-    __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
-    __shared__ unsigned s_cnt[kThreads / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) s_cnt[warp] = 0;
-    __syncwarp();
-    const WarpOut out{s_buf[warp], &s_cnt[warp]};
-    const int64_t n = (int64_t)*a.n_grouped;
-    unsigned long long n_cand = 0;
-    unsigned n32 = 0, n64 = 0;
-    for (;;) {
-        const int64_t b0 = warp_grab(a.work, kJoinGrab);
-        if (b0 >= n) break;
-        const int64_t e0 = b0 + kJoinGrab < n ? b0 + kJoinGrab : n;
-        for (int64_t base = b0; base < e0; base += 32) {
-            const int64_t j = base + lane;
-            GroupedPoint g{0.0, 0.0, 0, 0, 0, 0};
-            if (j < e0) g = a.grouped[j];
-            const double x = g.x, y = g.y;
-            const uint32_t lo = g.lo, len = g.len;
-            // Candidate loop with one trip count for the whole warp (the longest
-            // list among its lanes; in grouped order the lanes mostly share one).
-            uint32_t maxlen = len;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
-                maxlen = t > maxlen ? t : maxlen;
-            }
-            for (uint32_t k = 0; k < maxlen; ++k) {
-                bool want = false;
-                int32_t right = 0;
-                if (k < len) {
-                    const SlotRecord r = a.recs[lo + k];
-                    const int slot = r.slot;
-                    const float qx = __double2float_rn(x - r.ox), qy = __double2float_rn(y - r.oy);
-                    const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-                    // FP32 box filter (rounded outward: never rejects a point of the box)
-                    if (!(__fadd_ru(qx, dp) < r.box.x || __fsub_rd(qx, dp) > r.box.z || __fadd_ru(qy, dp) < r.box.y ||
-                          __fsub_rd(qy, dp) > r.box.w)) {
-                        bool cand = true;
-                        int loc = 0;
-                        if (a.accept_mask) {
-                            // The exact location rejects points outside the box by itself.
-                            const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
-                            loc = r.c0 >= 0 ? ring_location_split(x, y, qx, qy, t, a.xy32, a.xy, r.c0, r.c1, n32, n64)
-                                            : geometry_location_split(x, y, qx, qy, t, a, slot, n32, n64);
-                        } else {
-                            // Box candidates only: decide the box exactly in FP64.
-                            const vs_box bb = a.boxes[slot];
-                            cand = x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy;
-                        }
-                        if (cand) {
-                            ++n_cand;
-                            if (loc == LOC_UNDECIDED) {
-                                defer(a.defer, g.row, slot);
-                            } else if (!a.accept_mask || ((a.accept_mask >> loc) & 1)) {
-                                want = true;
-                                right = a.item_geom[slot];
-                            }
-                        }
-                    }
-                }
-                wemit_sync(out, a.sink, want, g.row, right);
-            }
-            wflush(out, a.sink, false);
-        }
-    }
-    wflush(out, a.sink, true);
-    add_counter(a.counters, 5, n_cand);
-    add_counter(a.counters, 2, n32);
-    add_counter(a.counters, 3, n64);
-}
-
-// Pass 3 with candidate compaction (predicates with a location test): the
-// warp walks its grouped points' candidate lists, and every (point,
-// candidate) pair that passes the FP32 box filter is appended to a warp-local
-// queue in shared memory.  Each time 32 pairs are queued, every lane refines
-// one of them.  So the ring walks, which dominate, run with all lanes busy
-// instead of only the lanes whose point lies in the current candidate's box.
-// Neighbouring queue entries mostly share a polygon, so vertex reads stay
-// broadcasts.
-struct QueuedPair {
-    double x, y;
-    int32_t row;
-    uint32_t rec;  // index into the per-entry records
-};
-constexpr int kQueue = 64;  // >= 31 left over + 32 appended in one step
-
-__device__ __forceinline__ void refine_queued(const LearnedArgs& a, const WarpOut& out, const QueuedPair* q, int nq,
-                                              int lane, unsigned& n32, unsigned& n64) {
-    bool want = false;
-    int32_t row = 0, right = 0;
-    if (lane < nq) {
-        const QueuedPair jb = q[lane];
-        row = jb.row;
-        const SlotRecord r = a.recs[jb.rec];
-        const float qx = __double2float_rn(jb.x - r.ox), qy = __double2float_rn(jb.y - r.oy);
-        const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-        const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
-        const int loc = r.c0 >= 0 ? ring_location_split(jb.x, jb.y, qx, qy, t, a.xy32, a.xy, r.c0, r.c1, n32, n64)
-                                  : geometry_location_split(jb.x, jb.y, qx, qy, t, a, r.slot, n32, n64);
-        if (loc == LOC_UNDECIDED) {
-            defer(a.defer, jb.row, r.slot);
-        } else if ((a.accept_mask >> loc) & 1) {
-            want = true;
-            right = a.item_geom[r.slot];
-        }
-    }
-    wemit_sync(out, a.sink, want, row, right);
-}
-
-__global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_kernel(const LearnedArgs a) {
-    __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
-    __shared__ unsigned s_cnt[kThreads / 32];
-    __shared__ QueuedPair s_q[kThreads / 32][kQueue];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) s_cnt[warp] = 0;
-    __syncwarp();
-    const WarpOut out{s_buf[warp], &s_cnt[warp]};
-    QueuedPair* q = s_q[warp];
-    const unsigned lt = (1u << lane) - 1u;
-    const int64_t n = (int64_t)*a.n_grouped;
-    unsigned long long n_cand = 0;
-    unsigned n32 = 0, n64 = 0;
-    int nq = 0;  // warp-uniform queue length
-    for (;;) {
-        const int64_t b0 = warp_grab(a.work, kJoinGrab);
-        if (b0 >= n) break;
-        const int64_t e0 = b0 + kJoinGrab < n ? b0 + kJoinGrab : n;
-        for (int64_t base = b0; base < e0; base += 32) {
-            const int64_t j = base + lane;
-            GroupedPoint g{0.0, 0.0, 0, 0, 0, 0};
-            if (j < e0) g = a.grouped[j];
-            uint32_t maxlen = g.len;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
-                maxlen = t > maxlen ? t : maxlen;
-            }
-            for (uint32_t k = 0; k < maxlen; ++k) {
-                bool inbox = false;
-                if (k < g.len) {
-                    const SlotRecord* rp = a.recs + g.lo + k;
-                    const double2 o = *reinterpret_cast<const double2*>(&rp->ox);
-                    const float4 bx = rp->box;
-                    const float qx = __double2float_rn(g.x - o.x), qy = __double2float_rn(g.y - o.y);
-                    const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-                    // FP32 box filter (rounded outward: never rejects a point of the box)
-                    inbox = !(__fadd_ru(qx, dp) < bx.x || __fsub_rd(qx, dp) > bx.z || __fadd_ru(qy, dp) < bx.y ||
-                              __fsub_rd(qy, dp) > bx.w);
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, inbox);
-                if (inbox) {
-                    QueuedPair& e = q[nq + __popc(m & lt)];
-                    e.x = g.x;
-                    e.y = g.y;
-                    e.row = g.row;
-                    e.rec = g.lo + k;
-                    ++n_cand;
-                }
-                nq += __popc(m);
-                __syncwarp();
-                if (nq >= 32) {
-                    refine_queued(a, out, q, 32, lane, n32, n64);
-                    __syncwarp();
-                    if (lane < nq - 32) q[lane] = q[32 + lane];
-                    nq -= 32;
-                    __syncwarp();
-                }
-            }
-            wflush(out, a.sink, false);
-        }
-    }
-    if (nq > 0) refine_queued(a, out, q, nq, lane, n32, n64);
-    wflush(out, a.sink, true);
-    add_counter(a.counters, 5, n_cand);
-    add_counter(a.counters, 2, n32);
-    add_counter(a.counters, 3, n64);
+    frame_q(fr, lox, loy, sx, sy);
+    d->lox = lox;
+    d->loy = loy;
+    d->hix = fr[2];
+    d->hiy = fr[3];
+    d->sx = sx;
+    d->sy = sy;
 }
 
 template <class T>
@@ -1029,6 +571,7 @@ void free_learned_index(vs_index* idx) {
     cudaFree(li.xy32);
     cudaFree(li.leaves);
     cudaFree(li.recs);
+    cudaFree(li.desc);
     li = LearnedIndex{};
 }
 
@@ -1136,90 +679,33 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_CUDA_TRY(cudaGetLastError());
     entry_recs_kernel<<<grid_for(E, 256), 256, 0, s>>>((int64_t)E, li.entries, slots.p, li.recs);
     VS_CUDA_TRY(cudaGetLastError());
+    // 7. the query descriptor (one job, cells numbered from 0)
+    LearnedJob d{};
+    d.L = L;
+    d.occ_shift = 2 * (L - li.occ_level);
+    d.root_shift = 2 * (L - li.root_level);
+    d.cell_base = 0;
+    d.n_cells = li.n_cells;
+    d.occ = li.occ;
+    d.root_table = li.root_table;
+    d.leaves = li.leaves;
+    d.cell_keys = li.cell_keys;
+    d.cell_start = li.cell_start;
+    d.recs = li.recs;
+    d.xy32 = li.xy32;
+    d.xy = idx->xy;
+    d.item_geom = idx->item_geom;
+    d.geom_off = idx->geom_off;
+    d.part_off = idx->part_off;
+    d.ring_off = idx->ring_off;
+    d.boxes = idx->nodes;
+    VS_TRY(dalloc(&li.desc, 1, bytes));
+    VS_CUDA_TRY(cudaMemcpyAsync(li.desc, &d, sizeof(d), cudaMemcpyHostToDevice, s));
+    learned_desc_kernel<<<1, 1, 0, s>>>(idx->frame, li.desc);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_CUDA_TRY(cudaMemcpyAsync(&li.h_desc, li.desc, sizeof(LearnedJob), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
     idx->has_learned = true;
-    return VS_OK;
-}
-
-int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, int32_t* d_left,
-                        int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
-    const LearnedIndex& li = idx->learned;
-    cudaStream_t s = ctx->stream;
-    const int64_t n = pts->n;
-    const int64_t packets = (n + 31) / 32;
-    const int64_t stripe_cap = 32 * ((packets + kStripes - 1) / kStripes);
-    Scratch<StagedPoint> staged;
-    Scratch<uint32_t> cell_count, n_grouped, stripe_count;
-    Scratch<GroupedPoint> grouped;
-    VS_TRY(staged.alloc((size_t)(kStripes * stripe_cap), s));
-    VS_TRY(grouped.alloc((size_t)n, s));
-    VS_TRY(cell_count.alloc((size_t)li.n_cells, s));
-    VS_TRY(n_grouped.alloc(1, s));
-    VS_TRY(stripe_count.alloc((size_t)kStripes, s));
-    VS_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, (size_t)li.n_cells * sizeof(uint32_t), s));
-    VS_CUDA_TRY(cudaMemsetAsync(stripe_count.p, 0, (size_t)kStripes * sizeof(uint32_t), s));
-    LearnedArgs a{};
-    a.px = pts->d_x;
-    a.py = pts->d_y;
-    a.pvalid = pts->d_valid;
-    a.n = n;
-    a.frame = idx->frame;
-    a.L = li.level;
-    a.occ_shift = 2 * (li.level - li.occ_level);
-    a.root_shift = 2 * (li.level - li.root_level);
-    a.occ = li.occ;
-    a.root_table = li.root_table;
-    a.cell_keys = li.cell_keys;
-    a.cell_start = li.cell_start;
-    a.entries = li.entries;
-    a.n_cells = li.n_cells;
-    a.leaves = li.leaves;
-    a.recs = li.recs;
-    a.boxes = idx->nodes;
-    a.origin = li.origin;
-    a.box32 = li.box32;
-    a.err32 = li.err32;
-    a.xy32 = li.xy32;
-    a.xy = idx->xy;
-    a.item_geom = idx->item_geom;
-    a.geom_off = idx->geom_off;
-    a.part_off = idx->part_off;
-    a.ring_off = idx->ring_off;
-    a.accept_mask = accept_mask;
-    a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
-    a.defer = dsink;
-    a.counters = ctx->d_counters;
-    a.staged = staged.p;
-    a.stripe_count = stripe_count.p;
-    a.stripe_cap = stripe_cap;
-    a.cell_count = cell_count.p;
-    a.grouped = grouped.p;
-    a.n_grouped = n_grouped.p;
-    a.work = &ctx->d_counters[kWorkCounter];
-#ifndef VS_LEARNED_BLOCKS_PER_SM
-#define VS_LEARNED_BLOCKS_PER_SM 8  // map and scatter blocks per SM (0: one resident wave)
-#endif
-    auto grid = [&](auto kernel, int64_t items) {
-        return VS_LEARNED_BLOCKS_PER_SM > 0 ? grid_for(items, kThreads, VS_LEARNED_BLOCKS_PER_SM)
-                                            : resident_grid(kernel, items, kThreads);
-    };
-    learned_map_kernel<<<grid(learned_map_kernel, n), kThreads, 0, s>>>(a);
-    VS_LAUNCHED("learned_map", s);
-    VS_TRY(exclusive_scan_u32(cell_count.p, cell_count.p, li.n_cells, n_grouped.p, s));
-    phase_mark(ctx, 1);
-    learned_scatter_kernel<<<kStripes, kThreads, 0, s>>>(a);
-    VS_LAUNCHED("learned_scatter", s);
-    phase_mark(ctx, 2);
-#ifndef VS_REFINE_QUEUE
-#define VS_REFINE_QUEUE 1
-#endif
-    if (VS_REFINE_QUEUE && accept_mask) {
-        learned_refine_kernel<<<resident_grid(learned_refine_kernel, n, kThreads), kThreads, 0, s>>>(a);
-        VS_LAUNCHED("learned_refine", s);
-    } else {
-        learned_join_kernel<<<resident_grid(learned_join_kernel, n, kThreads), kThreads, 0, s>>>(a);
-        VS_LAUNCHED("learned_join", s);
-    }
     return VS_OK;
 }
 
