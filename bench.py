@@ -281,7 +281,8 @@ def run_ours(args, rank, world, local_rank):
     d_poly = {k: torch.from_numpy(np.ascontiguousarray(getattr(pol, k))).to(dev)
               for k in ("x", "y", "ring_off", "part_off", "geom_off")}
     P = _abi.make_polygons(d_poly["x"], d_poly["y"], d_poly["ring_off"], d_poly["part_off"], d_poly["geom_off"])
-    method = _abi.METHOD_LEARNED if args.method == "learned" else _abi.METHOD_RTREE
+    method = _abi.METHOD_RTREE if args.method == "rtree" else _abi.METHOD_LEARNED
+    batched = args.method == "learned-batched"
     pred = {"within": _abi.PRED_WITHIN, "intersects": _abi.PRED_INTERSECTS}[args.predicate]
     t0 = time.perf_counter()
     index = _abi.DeviceIndex(ctx, P, learned=(method == _abi.METHOD_LEARNED))
@@ -291,6 +292,15 @@ def run_ours(args, rank, world, local_rank):
     dx = torch.from_numpy(w.px).to(dev)
     dy = torch.from_numpy(w.py).to(dev)
     pts = _abi.make_points(dx, dy)
+    # learned + batched: the join as a one-job batch plan (the persistent
+    # learned pipeline replayed from a CUDA graph)
+    plan = _abi.BatchPlan(ctx, [index], pts, [0, N], options={"method": _abi.METHOD_LEARNED}) if batched else None
+
+    def join(lft, rgt):
+        if plan is not None:
+            return plan.run_into(pred, lft, rgt, use_graph=True)
+        return index.join_into(pts, pred, method, lft, rgt)
+
     # size the pair buffers once (exact count from a first join)
     cap = max(1024, N)
     left = torch.empty(cap, dtype=torch.int32, device=dev)
@@ -302,6 +312,7 @@ def run_ours(args, rank, world, local_rank):
         left = torch.empty(cap, dtype=torch.int32, device=dev)
         right = torch.empty(cap, dtype=torch.int32, device=dev)
         n_pairs, stats = index.join_into(pts, pred, method, left, right)
+    assert join(left, right)[0] == n_pairs
     # plain R-tree on the same GPU, for the learned-vs-plain ratio
     plain = None
     if method == _abi.METHOD_LEARNED:
@@ -309,7 +320,7 @@ def run_ours(args, rank, world, local_rank):
         assert n_plain == n_pairs, (n_plain, n_pairs)
 
     for _ in range(args.warmup):
-        index.join_into(pts, pred, method, left, right)
+        join(left, right)
     if dist:
         tdist.barrier()
     torch.cuda.synchronize()
@@ -322,7 +333,7 @@ def run_ours(args, rank, world, local_rank):
             torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
         for k in range(args.steps):
             ev[k][0].record(stream)
-            n_k, st = index.join_into(pts, pred, method, left, right)
+            n_k, st = join(left, right)
             ev[k][1].record(stream)
             kernel_ms.append(st["kernel_ms"])
             phases.append(st["phase_ms"])
@@ -341,22 +352,27 @@ def run_ours(args, rank, world, local_rank):
                 pph.append(stp["phase_ms"])
             plain = float(np.median(pm))
             plain_phases = [float(v) for v in np.median(np.array(pph), axis=0)]
-        # e2e through the C-ABI with host buffers: H2D points, join, D2H pairs
+        if batched:
+            # per-phase device times of the same learned pipeline, launched
+            # directly (a graph replay records no phase marks)
+            dph = []
+            for _ in range(max(3, args.steps // 2)):
+                dph.append(index.join_into(pts, pred, _abi.METHOD_LEARNED, left, right)[1]["phase_ms"])
+            phases = dph
+        # e2e through the C-ABI with host buffers: H2D of the points into the
+        # buffers the join reads, the join, D2H of the pairs
         hx = torch.from_numpy(w.px).pin_memory()
         hy = torch.from_numpy(w.py).pin_memory()
         hl = torch.empty(cap, dtype=torch.int32).pin_memory()
         hr = torch.empty(cap, dtype=torch.int32).pin_memory()
-        ex = torch.empty_like(dx)
-        ey = torch.empty_like(dy)
-        epts = _abi.make_points(ex, ey)
         e2e_ms = []
         for k in range(max(3, args.steps)):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             with torch.cuda.stream(stream):
                 a.record(stream)
-                ex.copy_(hx, non_blocking=True)
-                ey.copy_(hy, non_blocking=True)
-                n_e, _ = index.join_into(epts, pred, method, left, right)
+                dx.copy_(hx, non_blocking=True)
+                dy.copy_(hy, non_blocking=True)
+                n_e, _ = join(left, right)
                 assert n_e == n_pairs, (n_e, n_pairs)
                 hl[:n_e].copy_(left[:n_e], non_blocking=True)
                 hr[:n_e].copy_(right[:n_e], non_blocking=True)
@@ -432,6 +448,8 @@ def run_batched(args, rank, world, local_rank):
     if dist:
         import torch.distributed as tdist
     jobs = make_batched(rank, args.scale)
+    learned = args.method != "rtree"
+    bmethod = _abi.METHOD_LEARNED if learned else _abi.METHOD_RTREE
     ctx = _abi.Context(dev)
     stream = ctx.torch_stream
     pred = {"within": _abi.PRED_WITHIN, "intersects": _abi.PRED_INTERSECTS}[args.predicate]
@@ -440,7 +458,8 @@ def run_batched(args, rank, world, local_rank):
     for w in jobs:
         d = {k: torch.from_numpy(np.ascontiguousarray(getattr(w.polys, k))).to(dev)
              for k in ("x", "y", "ring_off", "part_off", "geom_off")}
-        ix = _abi.DeviceIndex(ctx, _abi.make_polygons(d["x"], d["y"], d["ring_off"], d["part_off"], d["geom_off"]))
+        ix = _abi.DeviceIndex(ctx, _abi.make_polygons(d["x"], d["y"], d["ring_off"], d["part_off"], d["geom_off"]),
+                              learned=learned)
         indexes.append(ix)
         build_ms += ix.info()["build_ms"]
         n_polys += len(w.polys)
@@ -453,7 +472,7 @@ def run_batched(args, rank, world, local_rank):
     dy = torch.from_numpy(py).to(dev)
     pts = _abi.make_points(dx, dy)
     # exact pair count from a first direct run, then buffers of that size
-    probe = _abi.BatchPlan(ctx, indexes, pts, job_start)
+    probe = _abi.BatchPlan(ctx, indexes, pts, job_start, options={"method": bmethod})
     probe_l, _, _ = probe.run(pred, use_graph=False)
     n_pairs = int(probe_l.numel())
     del probe_l
@@ -464,7 +483,9 @@ def run_batched(args, rank, world, local_rank):
     name, sms = autotune.device_identity(dev)
     key = autotune.cache_key(name, sms, autotune.shape_class(len(jobs), N, n_polys), pred)
     tune_s = None
-    if args.autotune:
+    if learned:
+        opts, opts_src = {}, "learned pipeline (no R-tree launch shape)"
+    elif args.autotune:
         t1 = time.perf_counter()
         opts = autotune.tuned_options(ctx, indexes, pts, job_start, pred, n_polys, left=left, right=right,
                                       use_cache=False)
@@ -474,7 +495,7 @@ def run_batched(args, rank, world, local_rank):
         opts = autotune.lookup(key)
         opts_src = "cache" if opts else "defaults"
         opts = opts or dict(autotune.DEFAULTS)
-    plan = _abi.BatchPlan(ctx, indexes, pts, job_start, options=opts)
+    plan = _abi.BatchPlan(ctx, indexes, pts, job_start, options=dict(opts, method=bmethod))
     for _ in range(args.warmup):
         n_w, _ = plan.run_into(pred, left, right, use_graph=True)
         assert n_w == n_pairs, (n_w, n_pairs)
@@ -497,6 +518,19 @@ def run_batched(args, rank, world, local_rank):
         if args.profile:
             torch.cuda.profiler.stop()
         step_ms = [a.elapsed_time(b) for a, b in ev]
+        # the R-tree batch on the same jobs, for the learned-vs-plain ratio
+        rtree_batch_ms = None
+        if learned:
+            rplan = _abi.BatchPlan(ctx, indexes, pts, job_start,
+                                   options=dict(autotune.lookup(key) or autotune.DEFAULTS, method=_abi.METHOD_RTREE))
+            rms = []
+            for k in range(3 + max(3, args.steps // 2)):
+                n_r, st_r = rplan.run_into(pred, left, right, use_graph=True)
+                assert n_r == n_pairs, (n_r, n_pairs)
+                if k >= 3:
+                    rms.append(st_r["kernel_ms"])
+            rplan.close()
+            rtree_batch_ms = float(np.median(rms))
         # the same jobs one vs_join call at a time (how a caller without the
         # batch API runs them), after the timed region
         loop_ms = []
@@ -506,7 +540,7 @@ def run_batched(args, rank, world, local_rank):
             a_ev.record(stream)
             off = 0
             for ix, (pv, _a) in zip(indexes, views):
-                n_j, _ = ix.join_into(pv, pred, _abi.METHOD_RTREE, left[off:], right[off:])
+                n_j, _ = ix.join_into(pv, pred, bmethod, left[off:], right[off:])
                 off += n_j
             b_ev.record(stream)
             torch.cuda.synchronize()
@@ -547,7 +581,7 @@ def run_batched(args, rank, world, local_rank):
     B = sum(algorithmic_bytes(w, 0) for w in jobs) + 8 * n_pairs
     achieved = B / (kmed / 1e3) / 1e9
     traffic = None
-    prof = ROOT / "profiles" / "traffic_batched_rtree.json"
+    prof = ROOT / "profiles" / f"traffic_batched_{'learned' if learned else 'rtree'}.json"
     if prof.exists():
         try:
             traffic = json.loads(prof.read_text()).get("traffic_bytes_per_launch")
@@ -565,7 +599,8 @@ def run_batched(args, rank, world, local_rank):
         "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate, "method": "rtree, batched",
+        "config": {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate,
+                   "method": ("learned" if learned else "rtree") + ", batched",
                    "n_jobs": len(jobs), "n_points_per_gpu": N, "n_polygons": n_polys, "n_pairs": n_pairs,
                    "parallelism": f"jobs replicated per GPU ({world} GPU(s)), independent",
                    "l2": "inputs (1.1 GB of points) larger than L2; no flush",
@@ -582,6 +617,9 @@ def run_batched(args, rank, world, local_rank):
         "per_job_loop_ms": loop_med,
         "batched_vs_loop": loop_med / kmed,
     }
+    if rtree_batch_ms is not None:
+        line["plain_rtree_batched_ms"] = rtree_batch_ms
+        line["learned_vs_plain"] = rtree_batch_ms / kmed
     line["clocks"] = clk.summary()
     print(json.dumps(line), flush=True)
 
@@ -594,7 +632,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOAD_DESC), default="zipf")
     ap.add_argument("--predicate", choices=["within", "intersects"], default="within")
-    ap.add_argument("--method", choices=["learned", "rtree"], default="learned")
+    ap.add_argument("--method", choices=["learned-batched", "learned", "rtree"], default="learned-batched",
+                    help="learned-batched: the learned pipeline as a batch plan replayed from a CUDA graph; "
+                         "learned: vs_join with the learned index; rtree: the plain R-tree traversal")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-sample", type=int, default=4_000_000)

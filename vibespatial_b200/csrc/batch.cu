@@ -661,7 +661,10 @@ int vs_batch_run(vs_batch_plan* p, int32_t predicate, int32_t* d_left, int32_t* 
     *n_pairs = (int64_t)h[0];
     if (stats) {
         stats->exact_fallbacks = (int64_t)h[1];
+        stats->fp32_edges = (int64_t)h[2];
+        stats->fp64_edges = (int64_t)h[3];
         stats->candidates = (int64_t)h[5];
+        stats->rmi_fallbacks = (int64_t)h[6];
         stats->kernel_ms = ms;
         stats->kernel_launches = launches;
     }

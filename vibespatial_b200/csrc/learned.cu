@@ -641,7 +641,10 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     const uint32_t Eu = (uint32_t)E;
     VS_CUDA_TRY(cudaMemcpyAsync(li.cell_start + nc, &Eu, sizeof(Eu), cudaMemcpyHostToDevice, s));
     // 4. occupancy bitmap
-    li.occ_level = std::min(L, 11);
+#ifndef VS_OCC_MAX_LEVEL
+#define VS_OCC_MAX_LEVEL 12
+#endif
+    li.occ_level = std::min(L, VS_OCC_MAX_LEVEL);
     const int64_t occ_bits = 1ll << (2 * li.occ_level);
     VS_TRY(dalloc(&li.occ, (size_t)((occ_bits + 31) / 32), bytes));
     VS_CUDA_TRY(cudaMemsetAsync(li.occ, 0, (size_t)((occ_bits + 31) / 32) * sizeof(uint32_t), s));

@@ -100,6 +100,9 @@ __device__ __forceinline__ const LearnedJob& job_desc(const LqArgs& a, int job) 
 }
 
 // ------------------------------------------------------- split refine ---
+#ifndef VS_RING_PREFETCH
+#define VS_RING_PREFETCH 0
+#endif
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
 // decision the exact walk needs lies within the rounding-error bound `t`
 // (the caller then re-decides the edge in FP64); otherwise applies the same
@@ -141,8 +144,16 @@ __device__ __forceinline__ int ring_location_split(double px, double py, float q
     bool inside = false;
     float2 a = xy32[end - 1];
     int ia = end - 1;
+#if VS_RING_PREFETCH
+    float2 nb = xy32[start];
+#endif
     for (int i = start; i < end; ++i) {
+#if VS_RING_PREFETCH
+        const float2 b = nb;
+        if (i + 1 < end) nb = xy32[i + 1];  // next vertex in flight while this edge is decided
+#else
         const float2 b = xy32[i];
+#endif
         if (edge_step_fp32(a.x, a.y, b.x, b.y, qx, qy, t, inside)) {
             ++n32;
         } else {
@@ -288,8 +299,11 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LqArgs a
 #endif
 constexpr int kScatterUnroll = VS_SCATTER_UNROLL;
 
+#ifndef VS_SCATTER_MIN_BLOCKS
+#define VS_SCATTER_MIN_BLOCKS 1
+#endif
 template <bool kMulti>
-__global__ void __launch_bounds__(kThreads) learned_scatter_kernel(const LqArgs a) {
+__global__ void __launch_bounds__(kThreads, VS_SCATTER_MIN_BLOCKS) learned_scatter_kernel(const LqArgs a) {
     for (int stripe = blockIdx.x; stripe < kStripes; stripe += gridDim.x) {
         const uint32_t cnt = a.stripe_count[stripe];
         const StagedPoint* src = a.staged + (int64_t)stripe * a.stripe_cap;
