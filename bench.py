@@ -144,22 +144,23 @@ def algorithmic_bytes(w, n_pairs: int) -> int:
 
 
 def cpu_sample_rate(w, predicate: str, threads: int, target_s: float = 10.0):
-    """Oracle (all host threads) on a bounded prefix of the same points; points/sec."""
+    """Oracle (all host threads) on consecutive 2M-point chunks of the same
+    points until ~target_s of work; points/sec."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     O.build()
     P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
-    n = min(w.n_points, 200_000)
-    t0 = time.perf_counter()
-    O.join(w.px[:n], w.py[:n], None, P, predicate, threads)
-    dt = time.perf_counter() - t0
-    # grow the sample towards ~target_s of work (bounded by the workload)
-    n2 = int(min(w.n_points, max(n, n * target_s / max(dt, 1e-3) * 0.5)))
-    t0 = time.perf_counter()
-    O.join(w.px[:n2], w.py[:n2], None, P, predicate, threads)
-    dt2 = time.perf_counter() - t0
-    return n2 / dt2, n2, dt2
+    chunk = min(w.n_points, 2_000_000)
+    n, dt, start = 0, 0.0, 0
+    while dt < target_s and n < w.n_points:
+        stop = min(start + chunk, w.n_points)
+        t0 = time.perf_counter()
+        O.join(w.px[start:stop], w.py[start:stop], None, P, predicate, threads)
+        dt += time.perf_counter() - t0
+        n += stop - start
+        start = stop
+    return n / dt, n, dt
 
 
 def cpu_sample_batched(jobs, predicate: str, threads: int, target_s: float = 10.0):
