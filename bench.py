@@ -353,6 +353,12 @@ def run_ours(args, rank, world, local_rank):
                 pph.append(stp["phase_ms"])
             plain = float(np.median(pm))
             plain_phases = [float(v) for v in np.median(np.array(pph), axis=0)]
+            # the plain traversal with leaf blocks by bulk copies (TMA)
+            pb = []
+            for _ in range(max(3, args.steps // 2)):
+                _, stb = index.join_into(pts, pred, _abi.METHOD_RTREE, left, right, flags=_abi.JOIN_BULK_LEAVES)
+                pb.append(stb["kernel_ms"])
+            plain_bulk = float(np.median(pb))
         if batched:
             # per-phase device times of the same learned pipeline, launched
             # directly (a graph replay records no phase marks)
@@ -431,6 +437,7 @@ def run_ours(args, rank, world, local_rank):
     }
     if plain is not None:
         line["plain_rtree_ms"] = plain
+        line["plain_rtree_bulk_leaves_ms"] = plain_bulk
         line["plain_phases_ms"] = dict(zip(PHASES, plain_phases))
         line["learned_vs_plain"] = plain / kmed
     line["clocks"] = clk.summary()

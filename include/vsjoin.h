@@ -64,7 +64,9 @@ enum vs_method {
 };
 
 /* Join flags. */
-#define VS_JOIN_SORT 1u /* return pairs sorted by (left, right) */
+#define VS_JOIN_SORT 1u        /* return pairs sorted by (left, right) */
+#define VS_JOIN_BULK_LEAVES 2u /* R-tree method: load leaf blocks with bulk copies (TMA, cp.async.bulk) into
+                                  shared memory instead of lane loads (same pairs; measured ~2% slower) */
 
 typedef struct vs_context vs_context;
 typedef struct vs_index vs_index;

@@ -243,3 +243,19 @@ def test_learned_batch_nulls_empty_jobs(vsabi, ctx, oracle):
 def test_learned_batch_needs_learned_indexes(vsabi, ctx, batch):
     with pytest.raises(ValueError):
         vsabi.BatchPlan(ctx, batch.indexes, batch.pts, batch.job_start, options={"method": vsabi.METHOD_LEARNED})
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_batch_deferred_buffer_grows(vsabi, ctx, oracle, learned):
+    """On-edge points defer more pairs than the plan's first buffer holds: the plan grows it and reruns."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.degenerate_join(seed=6, n_points=1_000_000, n_polys=10_000)
+    b = _Batch(vsabi, ctx, [w], learned=learned)
+    for use_graph in (True, True, False):
+        left, right, stats = _run(b, "intersects", use_graph=use_graph)
+        (l, r), = b.split(left, right)
+        el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), "intersects")
+        np.testing.assert_array_equal(l, el)
+        np.testing.assert_array_equal(r, er)
+        assert stats["exact_fallbacks"] > 0

@@ -66,6 +66,23 @@ def test_degenerate_join_reduced(vsabi, ctx, oracle, predicate, method):
         assert stats["fp64_edges"] > 0  # near-boundary edges leave the FP32 filter
 
 
+@pytest.mark.parametrize("workload", ["star", "zipf", "degenerate"])
+def test_rtree_bulk_leaf_copies(vsabi, ctx, oracle, workload):
+    """The plain traversal with leaf blocks loaded by bulk copies (TMA) gives the oracle's pairs."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = {"star": lambda: syn.star_join(seed=0),
+         "zipf": lambda: syn.zipf_join(seed=3, n_points=2_000_000, n_polys=100_000),
+         "degenerate": lambda: syn.degenerate_join(seed=5, n_points=200_000, n_polys=3_000)}[workload]()
+    for predicate in ("within", "intersects"):
+        el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), predicate)
+        pts, _k1 = upload_points(vsabi, w.px, w.py)
+        P, _k2 = upload_polys(vsabi, w.polys)
+        index = vsabi.DeviceIndex(ctx, P)
+        gl, gr, _ = index.join(pts, PRED_CODES[predicate], vsabi.METHOD_RTREE, flags=vsabi.JOIN_BULK_LEAVES)
+        assert_same_pairs(gl.cpu().numpy(), gr.cpu().numpy(), el, er)
+
+
 def test_learned_index_is_judged_by_rtree(vsabi, ctx):
     """Learned lookups and plain traversal give the same pair set (the R-tree is the judge)."""
     from vibespatial_b200.testing import synthetic as syn

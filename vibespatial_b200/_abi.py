@@ -19,6 +19,7 @@ VS_OK, VS_E_ARG, VS_E_OOM, VS_E_CAPACITY, VS_E_CUDA, VS_E_TIMEOUT, VS_E_STATE = 
 PRED_BBOX, PRED_INTERSECTS, PRED_WITHIN, PRED_COVERED_BY, PRED_TOUCHES = range(5)
 METHOD_RTREE, METHOD_LEARNED, METHOD_BRUTE = range(3)
 JOIN_SORT = 1
+JOIN_BULK_LEAVES = 2
 
 # Every function the header declares; tests check the library exports them.
 EXPORTED = (
@@ -258,7 +259,8 @@ class DeviceIndex:
         except Exception:
             pass
 
-    def join_into(self, pts: Points, predicate: int, method: int, left, right, *, sort: bool = False):
+    def join_into(self, pts: Points, predicate: int, method: int, left, right, *, sort: bool = False,
+                  flags: int = 0):
         """One vs_join call into caller buffers; returns (n_pairs, stats dict).
 
         Raises CapacityError (with .required) if the buffers are too small.
@@ -267,13 +269,13 @@ class DeviceIndex:
         st = JoinStats()
         cap = 0 if left is None else int(left.numel())
         status = load().vs_join(self.ctx.handle, self.handle, ctypes.byref(pts), int(predicate), int(method),
-                                JOIN_SORT if sort else 0, _ptr(left), _ptr(right), cap, ctypes.byref(n),
-                                ctypes.byref(st))
+                                (JOIN_SORT if sort else 0) | int(flags), _ptr(left), _ptr(right), cap,
+                                ctypes.byref(n), ctypes.byref(st))
         check(status, required=int(n.value))
         return int(n.value), st.as_dict()
 
     def join(self, pts: Points, predicate: int, method: int = METHOD_RTREE, *, sort: bool = True,
-             capacity: int | None = None):
+             capacity: int | None = None, flags: int = 0):
         """Join into freshly allocated int32 device tensors, growing them once if needed."""
         import torch
 
@@ -283,7 +285,7 @@ class DeviceIndex:
             left = torch.empty(cap, dtype=torch.int32, device=dev)
             right = torch.empty(cap, dtype=torch.int32, device=dev)
             try:
-                n, stats = self.join_into(pts, predicate, method, left, right, sort=sort)
+                n, stats = self.join_into(pts, predicate, method, left, right, sort=sort, flags=flags)
                 return left[:n], right[:n], stats
             except CapacityError as e:
                 cap = max(e.required, 1)

@@ -309,7 +309,8 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
         if (method == VS_METHOD_LEARNED)
             st = launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity, ds);
         else
-            st = launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, d_left, d_right, capacity, ds);
+            st = launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, (flags & VS_JOIN_BULK_LEAVES) != 0,
+                                   d_left, d_right, capacity, ds);
         phase_mark(ctx, 3);
         if (st == VS_OK && mask) st = launch_resolve_deferred(ctx, idx, pts, mask, d_left, d_right, capacity, ds);
         phase_mark(ctx, 4);
@@ -338,6 +339,10 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
         stats->kernel_ms = ev.ms();
         stats->kernel_launches = g_launches - launches0;
         for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&stats->phase_ms[k], ctx->phase_ev[k], ctx->phase_ev[k + 1]);
+    }
+    if (c[4] & 2) {
+        set_error("a bounded device wait (bulk copy) gave up; the join's result is incomplete");
+        return VS_E_TIMEOUT;
     }
     if (c[4] != 0) {
         set_error("device-side consistency check failed (flags 0x%llx)", (unsigned long long)c[4]);

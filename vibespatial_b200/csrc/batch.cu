@@ -629,32 +629,53 @@ int vs_batch_run(vs_batch_plan* p, int32_t predicate, int32_t* d_left, int32_t* 
     VS_TRY(use_device(ctx->device));
     if (p->n_points == 0) return VS_OK;
     cudaStream_t s = ctx->stream;
-    long long launches = g_launches;
-    if (use_graph) {
-        if (!p->graph || p->g_pred != predicate || p->g_left != d_left || p->g_right != d_right ||
-            p->g_cap != capacity)
-            VS_TRY(capture_graph(p, predicate, mask, d_left, d_right, capacity));
-        VS_CUDA_TRY(cudaEventRecord(p->ev_in, s));
-        VS_CUDA_TRY(cudaStreamWaitEvent(p->gstream, p->ev_in, 0));
-        VS_CUDA_TRY(cudaEventRecord(p->t0, p->gstream));
-        VS_CUDA_TRY(cudaGraphLaunch(p->graph, p->gstream));
-        VS_CUDA_TRY(cudaEventRecord(p->t1, p->gstream));
-        VS_CUDA_TRY(cudaEventRecord(p->ev_out, p->gstream));
-        VS_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_out, 0));
-        launches = p->g_kernels;
-    } else {
-        VS_CUDA_TRY(cudaEventRecord(p->t0, s));
-        VS_TRY(enqueue_batch(p, s, mask, d_left, d_right, capacity));
-        VS_CUDA_TRY(cudaEventRecord(p->t1, s));
-        launches = g_launches - launches;
-    }
-    unsigned long long* h = ctx->h_counter;  // pinned, 10 slots: counters then the plan's two
-    VS_CUDA_TRY(cudaMemcpyAsync(h, ctx->d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    VS_CUDA_TRY(cudaMemcpyAsync(h + 8, p->d_work, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    const cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        set_error("batched join failed: %s", cudaGetErrorString(e));
-        return VS_E_CUDA;
+    unsigned long long* h = ctx->h_counter;  // pinned: the context counters, then the plan's two
+    long long launches = 0;
+    // Pairs the filters cannot certify go to the plan's deferred buffer; if
+    // more were deferred than it holds, it grows to fit and the batch runs
+    // once more (the graph is captured again for the new buffer).
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        launches = g_launches;
+        if (use_graph) {
+            if (!p->graph || p->g_pred != predicate || p->g_left != d_left || p->g_right != d_right ||
+                p->g_cap != capacity)
+                VS_TRY(capture_graph(p, predicate, mask, d_left, d_right, capacity));
+            VS_CUDA_TRY(cudaEventRecord(p->ev_in, s));
+            VS_CUDA_TRY(cudaStreamWaitEvent(p->gstream, p->ev_in, 0));
+            VS_CUDA_TRY(cudaEventRecord(p->t0, p->gstream));
+            VS_CUDA_TRY(cudaGraphLaunch(p->graph, p->gstream));
+            VS_CUDA_TRY(cudaEventRecord(p->t1, p->gstream));
+            VS_CUDA_TRY(cudaEventRecord(p->ev_out, p->gstream));
+            VS_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_out, 0));
+            launches = p->g_kernels;
+        } else {
+            VS_CUDA_TRY(cudaEventRecord(p->t0, s));
+            VS_TRY(enqueue_batch(p, s, mask, d_left, d_right, capacity));
+            VS_CUDA_TRY(cudaEventRecord(p->t1, s));
+            launches = g_launches - launches;
+        }
+        VS_CUDA_TRY(cudaMemcpyAsync(h, ctx->d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        VS_CUDA_TRY(cudaMemcpyAsync(h + 8, p->d_work, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            set_error("batched join failed: %s", cudaGetErrorString(e));
+            return VS_E_CUDA;
+        }
+        if (h[9] <= p->defer_cap || attempt == 1) break;
+        const unsigned long long want = h[9] + h[9] / 8 + (1 << 16);
+        int2* grown = nullptr;
+        if (cudaMalloc((void**)&grown, sizeof(int2) * want) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc of the deferred-pair buffer (%llu pairs) failed", want);
+            return VS_E_OOM;
+        }
+        cudaFree(p->defer);
+        p->defer = grown;
+        p->defer_cap = want;
+        if (p->graph) {
+            cudaGraphExecDestroy(p->graph);
+            p->graph = nullptr;
+        }
     }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, p->t0, p->t1);
@@ -668,12 +689,16 @@ int vs_batch_run(vs_batch_plan* p, int32_t predicate, int32_t* d_left, int32_t* 
         stats->kernel_ms = ms;
         stats->kernel_launches = launches;
     }
+    if (h[4] & 2) {
+        set_error("a bounded device wait (bulk copy) gave up; the batch's result is incomplete");
+        return VS_E_TIMEOUT;
+    }
     if (h[4]) {
         set_error("device-side consistency check failed (flags 0x%llx)", h[4]);
         return VS_E_STATE;
     }
     if (h[9] > p->defer_cap) {
-        set_error("deferred-pair buffer of the batch plan overflowed (%llu > %llu pairs)", h[9], p->defer_cap);
+        set_error("deferred-pair buffer of the batch plan did not converge (%llu > %llu pairs)", h[9], p->defer_cap);
         return VS_E_STATE;
     }
     if ((int64_t)h[0] > capacity) {

@@ -30,6 +30,7 @@
 #include "index.cuh"
 #include "join.cuh"
 #include "primitives.cuh"
+#include "tma.cuh"
 
 namespace vs {
 namespace {
@@ -110,16 +111,25 @@ __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ fr
     }
 }
 
+// kBulk: leaf blocks (up to 16 FP64 boxes, 512 B) arrive by one bulk copy
+// (TMA, cp.async.bulk) into the warp's item buffer instead of lane loads
+// (VS_JOIN_BULK_LEAVES).
+template <bool kBulk>
 __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const RtreeArgs a) {
     extern __shared__ vs_box s_nodes[];
     __shared__ int2 s_buf[kWarps][kWarpBuf];
     __shared__ unsigned s_cnt[kWarps];
     __shared__ int s_stack[kWarps][kStack];
     __shared__ vs_box s_items[kWarps][kFanout];
+    __shared__ uint64_t s_bar[kWarps];
     const int64_t stage_base = a.level_off[a.stage_level];
     for (int k = threadIdx.x; k < a.staged; k += blockDim.x) s_nodes[k] = a.nodes[stage_base + k];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) s_cnt[warp] = 0;
+    if (lane == 0) {
+        s_cnt[warp] = 0;
+        mbar_init(&s_bar[warp]);
+    }
+    uint32_t phase = 0;
     __syncthreads();
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
     const unsigned lt = (1u << lane) - 1u;
@@ -177,8 +187,26 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
                 const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
                 const bool in_range = lane < kFanout && c < a.level_size[cl];
                 vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
-                if (in_range)
+                const bool bulk = kBulk && cl == 0 && cl < a.stage_level;  // warp-uniform
+                if (bulk) {
+                    // The leaf block (up to 16 boxes, 32 B each, 512-B aligned) arrives in the
+                    // warp's item buffer by one bulk copy; the lanes then read their box from it.
+                    const int64_t first = (int64_t)(e >> 4) * kFanout;
+                    const int64_t left = a.level_size[0] - first;
+                    const uint32_t bytes = (uint32_t)((left < kFanout ? left : kFanout) * sizeof(vs_box));
+                    if (lane == 0) bulk_load(s_items[warp], a.nodes + first, bytes, &s_bar[warp]);
+                    const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&s_bar[warp], phase));
+                    if (!ok) {
+                        // record the timeout, give the copy one more bounded wait, stop this warp
+                        if (lane == 0) atomicOr(&a.counters[4], 2ull);
+                        mbar_wait_bounded(&s_bar[warp], phase);
+                        return;
+                    }
+                    phase ^= 1u;
+                    if (in_range) b = s_items[warp][lane];
+                } else if (in_range) {
                     b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
+                }
                 const bool hit = in_range && box_overlaps(b, x0, y0, x1, y1);
                 const unsigned m = __ballot_sync(0xffffffffu, hit);
                 if (cl > 0) {
@@ -194,7 +222,7 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
                     sp += add;
                     __syncwarp();
                 } else {
-                    if (lane < kFanout) s_items[warp][lane] = b;
+                    if (!bulk && lane < kFanout) s_items[warp][lane] = b;
                     __syncwarp();
                     unsigned mm = m;
                     const int64_t slot0 = (int64_t)(e >> 4) * kFanout;
@@ -375,7 +403,7 @@ int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
 }
 
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
-                      int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
+                      bool bulk_leaves, int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
     RtreeArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
@@ -420,9 +448,9 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.n_sorted = q.n_valid.p;
     a.work = &ctx->d_counters[kWorkCounter];
     const size_t smem = (size_t)a.staged * sizeof(vs_box);
-    VS_CUDA_TRY(cudaFuncSetAttribute(join_rtree_packet_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    join_rtree_packet_kernel<<<resident_grid(join_rtree_packet_kernel, pts->n, kJoinThreads, smem), kJoinThreads, smem,
-                               ctx->stream>>>(a);
+    auto* kernel = bulk_leaves ? join_rtree_packet_kernel<true> : join_rtree_packet_kernel<false>;
+    VS_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kernel<<<resident_grid(kernel, pts->n, kJoinThreads, smem), kJoinThreads, smem, ctx->stream>>>(a);
     VS_LAUNCHED("join_rtree_packet", ctx->stream);
     return VS_OK;
 }

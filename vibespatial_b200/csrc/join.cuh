@@ -16,7 +16,7 @@ struct QueryOrder {
 int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q);
 int accept_mask_for(int predicate, int* mask);
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
-                      int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
+                      bool bulk_leaves, int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
                         int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
 // Exact pass over the pairs the filtered kernels deferred (count read on device).
