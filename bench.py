@@ -286,7 +286,7 @@ def run_ours(args, rank, world, local_rank):
     batched = args.method == "learned-batched"
     pred = {"within": _abi.PRED_WITHIN, "intersects": _abi.PRED_INTERSECTS}[args.predicate]
     t0 = time.perf_counter()
-    index = _abi.DeviceIndex(ctx, P, learned=(method == _abi.METHOD_LEARNED))
+    index = _abi.DeviceIndex(ctx, P, learned=(method == _abi.METHOD_LEARNED), ring_bin_min_vertices=args.ring_bin_min)
     build_wall = time.perf_counter() - t0
     info = index.info()
     del d_poly
@@ -467,7 +467,7 @@ def run_batched(args, rank, world, local_rank):
         d = {k: torch.from_numpy(np.ascontiguousarray(getattr(w.polys, k))).to(dev)
              for k in ("x", "y", "ring_off", "part_off", "geom_off")}
         ix = _abi.DeviceIndex(ctx, _abi.make_polygons(d["x"], d["y"], d["ring_off"], d["part_off"], d["geom_off"]),
-                              learned=learned)
+                              learned=learned, ring_bin_min_vertices=args.ring_bin_min)
         indexes.append(ix)
         build_ms += ix.info()["build_ms"]
         n_polys += len(w.polys)
@@ -647,6 +647,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-sample", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ring-bin-min", type=int, default=0,
+                    help="rings with at least this many vertices get y-bins (0: library default, <0: none)")
     ap.add_argument("--autotune", action="store_true",
                     help="batched workload: search the launch shape now instead of using the cache/defaults")
     ap.add_argument("--profile", action="store_true",

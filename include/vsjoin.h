@@ -96,6 +96,8 @@ typedef struct vs_index_options {
     int32_t cell_level;  /* learned index grid level (0 = choose automatically) */
     int32_t rmi_leaves;  /* learned index leaf models (0 = 4096) */
     int32_t rmi_train_steps; /* 0 = default */
+    int32_t ring_bin_min_vertices; /* rings with at least this many vertices get 8 y-bins of edges, so a
+                                      point's ring walk visits only the edges of its bin (0 = 16, < 0 = none) */
 } vs_index_options;
 
 typedef struct vs_join_stats {
@@ -124,6 +126,8 @@ typedef struct vs_index_info {
     float rmi_train_ms;
     float rmi_mean_window;    /* mean learned-index search window (entries) */
     int32_t rmi_max_window;
+    int64_t n_binned_rings;   /* rings with y-bins */
+    int64_t n_bin_edges;      /* (bin, edge) entries */
 } vs_index_info;
 
 /* ---------------------------------------------------------------------- */

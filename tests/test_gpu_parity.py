@@ -83,6 +83,27 @@ def test_rtree_bulk_leaf_copies(vsabi, ctx, oracle, workload):
         assert_same_pairs(gl.cpu().numpy(), gr.cpu().numpy(), el, er)
 
 
+@pytest.mark.parametrize("bin_min", [4, -1])
+@pytest.mark.parametrize("workload", ["star", "degenerate"])
+def test_ring_bins(vsabi, ctx, oracle, workload, bin_min):
+    """Walking only a point's y-bin of edges (bins on every ring of >= 4 vertices) or every edge (no bins)
+    gives the oracle's pairs for every method, on boundary and 1-ulp points too."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = (syn.star_join(seed=2, n_points=100_000, n_polys=2_000) if workload == "star"
+         else syn.degenerate_join(seed=8, n_points=200_000, n_polys=3_000))
+    pts, _k1 = upload_points(vsabi, w.px, w.py)
+    P, _k2 = upload_polys(vsabi, w.polys)
+    index = vsabi.DeviceIndex(ctx, P, learned=True, ring_bin_min_vertices=bin_min)
+    info = index.info()
+    assert (info["n_binned_rings"] > 0) == (bin_min > 0)
+    for predicate in ("within", "intersects", "touches"):
+        el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), predicate)
+        for method in (vsabi.METHOD_RTREE, vsabi.METHOD_LEARNED, vsabi.METHOD_BRUTE):
+            gl, gr, _ = index.join(pts, PRED_CODES[predicate], method)
+            assert_same_pairs(gl.cpu().numpy(), gr.cpu().numpy(), el, er)
+
+
 def test_learned_index_is_judged_by_rtree(vsabi, ctx):
     """Learned lookups and plain traversal give the same pair set (the R-tree is the judge)."""
     from vibespatial_b200.testing import synthetic as syn

@@ -63,7 +63,8 @@ class Points(ctypes.Structure):
 
 class IndexOptions(ctypes.Structure):
     _fields_ = [("method_mask", ctypes.c_int32), ("cell_level", ctypes.c_int32),
-                ("rmi_leaves", ctypes.c_int32), ("rmi_train_steps", ctypes.c_int32)]
+                ("rmi_leaves", ctypes.c_int32), ("rmi_train_steps", ctypes.c_int32),
+                ("ring_bin_min_vertices", ctypes.c_int32)]
 
 
 class JoinStats(ctypes.Structure):
@@ -96,6 +97,7 @@ class IndexInfo(ctypes.Structure):
         ("n_cell_entries", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
         ("build_ms", ctypes.c_float), ("rmi_train_ms", ctypes.c_float),
         ("rmi_mean_window", ctypes.c_float), ("rmi_max_window", ctypes.c_int32),
+        ("n_binned_rings", ctypes.c_int64), ("n_bin_edges", ctypes.c_int64),
     ]
 
     def as_dict(self):
@@ -235,9 +237,10 @@ class DeviceIndex:
     """Owned handle of a built index (vs_index*)."""
 
     def __init__(self, ctx: Context, polys: Polygons, *, learned: bool = False, cell_level: int = 0,
-                 rmi_leaves: int = 0, rmi_train_steps: int = 0):
+                 rmi_leaves: int = 0, rmi_train_steps: int = 0, ring_bin_min_vertices: int = 0):
         self.ctx = ctx
-        opts = IndexOptions(1 | (2 if learned else 0), int(cell_level), int(rmi_leaves), int(rmi_train_steps))
+        opts = IndexOptions(1 | (2 if learned else 0), int(cell_level), int(rmi_leaves), int(rmi_train_steps),
+                            int(ring_bin_min_vertices))
         h = ctypes.c_void_p()
         check(load().vs_index_build(ctx.handle, ctypes.byref(polys), ctypes.byref(opts), ctypes.byref(h)))
         self.handle = h

@@ -213,6 +213,7 @@ int vs_index_build(vs_context* ctx, const vs_polygons* polys, const vs_index_opt
     EventPair ev;
     cudaEventRecord(ev.a, ctx->stream);
     int st = build_rtree(ctx, polys, idx);
+    if (st == VS_OK) st = build_ring_bins(ctx, idx, opts ? opts->ring_bin_min_vertices : 0);
     if (st == VS_OK && opts && (opts->method_mask & 2)) st = build_learned_index(ctx, idx, opts);
     if (st != VS_OK) {
         cudaStreamSynchronize(ctx->stream);
@@ -250,6 +251,8 @@ int vs_index_info_get(const vs_index* idx, vs_index_info* info) {
     info->rmi_train_ms = idx->learned.rmi_train_ms;
     info->rmi_mean_window = idx->learned.mean_window;
     info->rmi_max_window = idx->learned.max_window;
+    info->n_binned_rings = idx->n_binned_rings;
+    info->n_bin_edges = idx->n_bin_edges;
     return VS_OK;
 }
 

@@ -53,6 +53,7 @@ struct JobTree {
     double frame[4];
     int32_t levels;
     int32_t n_geoms;
+    RingIndex rings;
 };
 
 struct BatchArgs {
@@ -192,7 +193,8 @@ __global__ void __launch_bounds__(kBThreads) batch_join_kernel(const BatchArgs a
                         if (mine && box_has_b(root, x, y)) {
                             ++n_cand;
                             const int loc = a.accept_mask ? geometry_location_filtered(x, y, t.xy, t.ring_off,
-                                                                                       t.part_off, t.geom_off, 0)
+                                                                                       t.part_off, t.geom_off, 0,
+                                                                                       t.rings)
                                                           : 0;
                             if (loc == LOC_UNDECIDED) defer(a.defer, row, 0);
                             else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(kBThreads) batch_join_kernel(const BatchArgs a
                                 int loc = 0;
                                 if (a.accept_mask)
                                     loc = geometry_location_filtered(x, y, t.xy, t.ring_off, t.part_off, t.geom_off,
-                                                                     slot);
+                                                                     slot, t.rings);
                                 if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
                                 else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                             }
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(kBThreads) batch_resolve_kernel(const BatchArg
             pr = a.defer.buf[k];
             const JobTree& t = a.jobs[job_of(a.job_start, a.n_jobs, pr.x)];
             const int loc = geometry_location(a.px[pr.x], a.py[pr.x], t.xy, t.ring_off, t.part_off, t.geom_off, pr.y,
-                                              n_exact);
+                                              t.rings, n_exact);
             want = (a.accept_mask >> loc) & 1;
             right = want ? t.item_geom[pr.y] : 0;
         }
@@ -333,6 +335,7 @@ struct vs_batch_plan {
     vs::LearnedJob* d_ljobs = nullptr;
     vs::LearnedJob h_single{};  // the descriptor when the batch has one job
     int64_t n_cells = 0;        // batch-wide learned cells
+    bool has_ring_bins = false; // some job's index has binned rings long enough for the split walk
     void* lscratch = nullptr;
     vs::LearnedScratch lsc{};
 };
@@ -397,6 +400,7 @@ int enqueue_batch(vs_batch_plan* p, cudaStream_t s, int mask, int32_t* left, int
         q.job_start = p->d_job_start;
         q.n_cells = p->n_cells;
         q.accept_mask = mask;
+        q.has_ring_bins = p->has_ring_bins;
         VS_TRY(enqueue_learned(s, nullptr, q, p->n_jobs == 1 ? &p->h_single : nullptr, p->lsc, a.sink, a.defer,
                                a.counters, &p->d_work[0]));
         if (mask) {
@@ -531,6 +535,8 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
         for (int k = 0; k < 4; ++k) t.frame[k] = ix->h_frame[k];
         t.levels = ix->levels;
         t.n_geoms = ix->levels > 0 ? ix->n_geoms : 0;
+        t.rings = ix->ring_index();
+        p->has_ring_bins = p->has_ring_bins || ix->n_split_binned_rings > 0;
     }
     p->learned = p->opts.method == VS_METHOD_LEARNED;
     if (p->opts.method != VS_METHOD_RTREE && !p->learned) {

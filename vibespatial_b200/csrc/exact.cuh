@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ringbins.cuh"
+
 namespace vs {
 
 enum : int { LOC_OUTSIDE = 0, LOC_BOUNDARY = 1, LOC_INTERIOR = 2 };
@@ -171,31 +173,64 @@ __device__ __forceinline__ int edge_step_filtered(double ax, double ay, double b
     return 0;
 }
 
-__device__ __forceinline__ int ring_location_filtered(double px, double py, const double2* __restrict__ xy, int start,
-                                                      int end) {
-    if (end - start < 2) return LOC_OUTSIDE;
-    bool inside = false;
+// Walk only the edges of the point's y-bin when the ring has bins; `Step`
+// decides one edge (a -> b) and returns 0 to go on, or a nonzero code that
+// ends the walk and is returned.
+template <class Step>
+__device__ __forceinline__ int ring_walk(double py, const double2* __restrict__ xy, int start, int end, int ring,
+                                         const RingIndex& ri, bool& inside, Step step) {
+    const int rb = ri.ring_bin ? ri.ring_bin[ring] : -1;
+    if (rb >= 0) {
+        const RingBins& b = ri.bins[rb];
+        const int k = ring_bin_of(py, b.y0, b.scale);
+        const uint32_t e1 = b.off[k + 1];
+        int last = -2;  // an edge that continues the previous one reuses its end vertex
+        double2 lb = make_double2(0.0, 0.0);
+        for (uint32_t e = b.off[k]; e < e1; ++e) {
+            const int i = start + ri.edges[e];
+            const int ia = i == start ? end - 1 : i - 1;
+            const double2 A = ia == last ? lb : xy[ia], B = xy[i];
+            const int r = step(A, B, inside);
+            if (r) return r;
+            last = i;
+            lb = B;
+        }
+        return 0;
+    }
     double2 a = xy[end - 1];
     for (int i = start; i < end; ++i) {
         const double2 b = xy[i];
-        const int r = edge_step_filtered(a.x, a.y, b.x, b.y, px, py, inside);
-        if (r == 1) return LOC_BOUNDARY;
-        if (r == 2) return LOC_UNDECIDED;
+        const int r = step(a, b, inside);
+        if (r) return r;
         a = b;
     }
+    return 0;
+}
+
+__device__ __forceinline__ int ring_location_filtered(double px, double py, const double2* __restrict__ xy, int start,
+                                                      int end, int ring, const RingIndex& ri) {
+    if (end - start < 2) return LOC_OUTSIDE;
+    bool inside = false;
+    // step codes: 1 on the edge, 2 undecided by the filter
+    const int r = ring_walk(py, xy, start, end, ring, ri, inside, [&](const double2& A, const double2& B, bool& in) {
+        return edge_step_filtered(A.x, A.y, B.x, B.y, px, py, in);
+    });
+    if (r == 1) return LOC_BOUNDARY;
+    if (r == 2) return LOC_UNDECIDED;
     return inside ? LOC_INTERIOR : LOC_OUTSIDE;
 }
 
 __device__ __forceinline__ int geometry_location_filtered(double px, double py, const double2* __restrict__ xy,
                                                           const int32_t* __restrict__ ring_off,
                                                           const int32_t* __restrict__ part_off,
-                                                          const int32_t* __restrict__ geom_off, int g) {
+                                                          const int32_t* __restrict__ geom_off, int g,
+                                                          const RingIndex& ri) {
     const int p0 = geom_off[g], p1 = geom_off[g + 1];
     for (int part = p0; part < p1; ++part) {
         bool inside = false;
         const int r0 = part_off[part], r1 = part_off[part + 1];
         for (int ring = r0; ring < r1; ++ring) {
-            const int k = ring_location_filtered(px, py, xy, ring_off[ring], ring_off[ring + 1]);
+            const int k = ring_location_filtered(px, py, xy, ring_off[ring], ring_off[ring + 1], ring, ri);
             if (k == LOC_BOUNDARY || k == LOC_UNDECIDED) return k;
             if (k == LOC_INTERIOR) inside = !inside;
         }
@@ -207,15 +242,13 @@ __device__ __forceinline__ int geometry_location_filtered(double px, double py, 
 // Ring walk over interleaved vertices xy[start, end); the edge (end-1 -> start)
 // closes the ring exactly as in the reference's (i, j = i - 1) loop.
 __device__ __forceinline__ int ring_location(double px, double py, const double2* __restrict__ xy,
-                                             int start, int end, unsigned& n_exact) {
+                                             int start, int end, int ring, const RingIndex& ri, unsigned& n_exact) {
     if (end - start < 2) return LOC_OUTSIDE;
     bool inside = false;
-    double2 a = xy[end - 1];
-    for (int i = start; i < end; ++i) {
-        const double2 b = xy[i];
-        if (edge_step_exact(a.x, a.y, b.x, b.y, px, py, inside, n_exact)) return LOC_BOUNDARY;
-        a = b;
-    }
+    const int r = ring_walk(py, xy, start, end, ring, ri, inside, [&](const double2& A, const double2& B, bool& in) {
+        return edge_step_exact(A.x, A.y, B.x, B.y, px, py, in, n_exact) ? 1 : 0;
+    });
+    if (r) return LOC_BOUNDARY;
     return inside ? LOC_INTERIOR : LOC_OUTSIDE;
 }
 
@@ -241,13 +274,13 @@ __device__ __forceinline__ int geometry_location(double px, double py, const dou
                                                  const int32_t* __restrict__ ring_off,
                                                  const int32_t* __restrict__ part_off,
                                                  const int32_t* __restrict__ geom_off, int g,
-                                                 unsigned& n_exact) {
+                                                 const RingIndex& ri, unsigned& n_exact) {
     const int p0 = geom_off[g], p1 = geom_off[g + 1];
     for (int part = p0; part < p1; ++part) {
         bool inside = false;
         const int r0 = part_off[part], r1 = part_off[part + 1];
         for (int ring = r0; ring < r1; ++ring) {
-            const int k = ring_location(px, py, xy, ring_off[ring], ring_off[ring + 1], n_exact);
+            const int k = ring_location(px, py, xy, ring_off[ring], ring_off[ring + 1], ring, ri, n_exact);
             if (k == LOC_BOUNDARY) return LOC_BOUNDARY;
             if (k == LOC_INTERIOR) inside = !inside;
         }

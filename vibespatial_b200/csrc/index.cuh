@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ringbins.cuh"
 #include "vs_common.cuh"
 
 namespace vs {
@@ -76,6 +77,7 @@ struct LearnedJob {
     const int32_t* part_off;
     const int32_t* ring_off;
     const vs_box* boxes;     // FP64 slot boxes (R-tree level 0)
+    RingIndex rings;         // y-bins of the index's long rings
 };
 
 struct LearnedIndex {
@@ -131,6 +133,19 @@ struct vs_index {
     int32_t* ring_off = nullptr;
     double2* xy = nullptr;
     double* frame = nullptr;      // device [4]: minx, miny, maxx, maxy of valid boxes
+    // y-bins of the rings with many vertices (ringbins.cuh)
+    int32_t* ring_bin = nullptr;        // [n_rings] -1 or index into ring_bins
+    vs::RingBins* ring_bins = nullptr;  // [n_binned_rings]
+    uint16_t* bin_edges = nullptr;      // [n_bin_edges]
+    int64_t n_binned_rings = 0, n_bin_edges = 0;
+    int64_t n_split_binned_rings = 0;   // binned rings of >= kSplitBinMinVertices vertices
+    vs::RingIndex ring_index() const {
+        vs::RingIndex ri;
+        ri.ring_bin = ring_bin;
+        ri.bins = ring_bins;
+        ri.edges = bin_edges;
+        return ri;
+    }
     double h_frame[4] = {0, 0, 0, 0};
     bool has_learned = false;
     vs::LearnedIndex learned;

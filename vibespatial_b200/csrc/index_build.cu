@@ -215,6 +215,97 @@ int dalloc(T** p, size_t n, int64_t& bytes) {
     return VS_OK;
 }
 
+
+// ------------------------------------------------------------ ring bins ---
+// Pass 1, one thread per ring: is it binned (enough vertices, finite y,
+// positive height), its (y0, scale), and how many (bin, edge) entries it
+// needs (an edge is listed in every bin its closed y-range meets).
+__global__ void ring_bin_size_kernel(int64_t n_rings, const int32_t* __restrict__ ring_off,
+                                     const double2* __restrict__ xy, int min_vertices,
+                                     uint32_t* __restrict__ entries, uint32_t* __restrict__ binned,
+                                     double2* __restrict__ yinfo, unsigned long long* __restrict__ n_long) {
+    unsigned long long long_rings = 0;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rings;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int s0 = ring_off[r], s1 = ring_off[r + 1], nv = s1 - s0;
+        uint32_t cnt = 0, flag = 0;
+        double y0 = 0.0, sc = 0.0;
+        if (nv >= min_vertices && nv <= 65535) {
+            double lo = INFINITY, hi = -INFINITY;
+            bool finite = true;
+            for (int i = s0; i < s1; ++i) {
+                const double y = xy[i].y;
+                finite = finite && isfinite(y);
+                lo = fmin(lo, y);
+                hi = fmax(hi, y);
+            }
+            if (finite && hi > lo) {
+                sc = __ddiv_rn((double)kRingBins, __dsub_rn(hi, lo));
+                if (isfinite(sc) && sc > 0.0) {
+                    flag = 1;
+                    y0 = lo;
+                    long_rings += nv >= kSplitBinMinVertices ? 1 : 0;
+                    for (int e = 0; e < nv; ++e) {
+                        const double a = xy[e == 0 ? s1 - 1 : s0 + e - 1].y, b = xy[s0 + e].y;
+                        cnt += (uint32_t)(ring_bin_of(fmax(a, b), y0, sc) - ring_bin_of(fmin(a, b), y0, sc) + 1);
+                    }
+                }
+            }
+        }
+        entries[r] = cnt;
+        binned[r] = flag;
+        yinfo[r] = make_double2(y0, sc);
+    }
+    if (long_rings) atomicAdd(n_long, long_rings);
+}
+
+// Pass 2, one thread per binned ring: bin offsets, then the edge lists in
+// ring order within each bin.
+__global__ void ring_bin_fill_kernel(int64_t n_rings, const int32_t* __restrict__ ring_off,
+                                     const double2* __restrict__ xy, const uint32_t* __restrict__ entry_off,
+                                     const uint32_t* __restrict__ bin_idx, const uint32_t* __restrict__ binned,
+                                     const double2* __restrict__ yinfo, int32_t* __restrict__ ring_bin,
+                                     RingBins* __restrict__ bins, uint16_t* __restrict__ edges) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rings;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        if (!binned[r]) {
+            ring_bin[r] = -1;
+            continue;
+        }
+        const int s0 = ring_off[r], s1 = ring_off[r + 1], nv = s1 - s0;
+        const double y0 = yinfo[r].x, sc = yinfo[r].y;
+        uint32_t cnt[kRingBins];
+#pragma unroll
+        for (int k = 0; k < kRingBins; ++k) cnt[k] = 0;
+        for (int e = 0; e < nv; ++e) {
+            const double a = xy[e == 0 ? s1 - 1 : s0 + e - 1].y, b = xy[s0 + e].y;
+            const int k0 = ring_bin_of(fmin(a, b), y0, sc), k1 = ring_bin_of(fmax(a, b), y0, sc);
+            for (int k = k0; k <= k1; ++k) ++cnt[k];
+        }
+        RingBins rb;
+        rb.y0 = y0;
+        rb.scale = sc;
+        uint32_t o = entry_off[r];
+        for (int k = 0; k < kRingBins; ++k) {
+            rb.off[k] = o;
+            o += cnt[k];
+        }
+        rb.off[kRingBins] = o;
+        rb.pad[0] = rb.pad[1] = rb.pad[2] = 0;
+        const uint32_t b_i = bin_idx[r];
+        bins[b_i] = rb;
+        ring_bin[r] = (int32_t)b_i;
+        uint32_t cur[kRingBins];
+#pragma unroll
+        for (int k = 0; k < kRingBins; ++k) cur[k] = rb.off[k];
+        for (int e = 0; e < nv; ++e) {
+            const double a = xy[e == 0 ? s1 - 1 : s0 + e - 1].y, b = xy[s0 + e].y;
+            const int k0 = ring_bin_of(fmin(a, b), y0, sc), k1 = ring_bin_of(fmax(a, b), y0, sc);
+            for (int k = k0; k <= k1; ++k) edges[cur[k]++] = (uint16_t)e;
+        }
+    }
+}
+
 }  // namespace
 
 int hilbert_point_keys(const double* x, const double* y, int64_t n, double minx, double miny, double maxx,
@@ -234,6 +325,9 @@ void free_index_memory(vs_index* idx) {
     cudaFree(idx->ring_off);
     cudaFree(idx->xy);
     cudaFree(idx->frame);
+    cudaFree(idx->ring_bin);
+    cudaFree(idx->ring_bins);
+    cudaFree(idx->bin_edges);
     free_learned_index(idx);
 }
 
@@ -320,6 +414,49 @@ int build_rtree(vs_context* ctx, const vs_polygons* P, vs_index* idx) {
     }
     VS_CUDA_TRY(cudaMemcpyAsync(idx->h_frame, idx->frame, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
+    return VS_OK;
+}
+
+int build_ring_bins(vs_context* ctx, vs_index* idx, int min_vertices) {
+    if (min_vertices < 0 || idx->n_rings <= 0) return VS_OK;
+    if (idx->n_coords * kRingBins >= 0xffffffffLL) return VS_OK;  // entry offsets are 32-bit
+    if (min_vertices == 0) min_vertices = kRingBinMinVertices;
+    if (min_vertices < 3) min_vertices = 3;
+    cudaStream_t s = ctx->stream;
+    const int64_t R = idx->n_rings;
+    Scratch<uint32_t> entries, entry_off, binned, bin_idx, totals;
+    Scratch<double2> yinfo;
+    Scratch<unsigned long long> n_long;
+    VS_TRY(n_long.alloc(1, s));
+    VS_CUDA_TRY(cudaMemsetAsync(n_long.p, 0, sizeof(unsigned long long), s));
+    VS_TRY(entries.alloc((size_t)R, s));
+    VS_TRY(entry_off.alloc((size_t)R, s));
+    VS_TRY(binned.alloc((size_t)R, s));
+    VS_TRY(bin_idx.alloc((size_t)R, s));
+    VS_TRY(yinfo.alloc((size_t)R, s));
+    VS_TRY(totals.alloc(2, s));
+    ring_bin_size_kernel<<<grid_for(R, 256), 256, 0, s>>>(R, idx->ring_off, idx->xy, min_vertices, entries.p,
+                                                          binned.p, yinfo.p, n_long.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(exclusive_scan_u32(entries.p, entry_off.p, R, totals.p + 0, s));
+    VS_TRY(exclusive_scan_u32(binned.p, bin_idx.p, R, totals.p + 1, s));
+    uint32_t tot[2] = {0, 0};
+    unsigned long long h_long = 0;
+    VS_CUDA_TRY(cudaMemcpyAsync(tot, totals.p, sizeof(tot), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaMemcpyAsync(&h_long, n_long.p, sizeof(h_long), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (tot[1] == 0) return VS_OK;  // no ring qualifies
+    int64_t& bytes = idx->device_bytes;
+    VS_TRY(dalloc(&idx->ring_bin, (size_t)R, bytes));
+    VS_TRY(dalloc(&idx->ring_bins, (size_t)tot[1], bytes));
+    VS_TRY(dalloc(&idx->bin_edges, (size_t)tot[0], bytes));
+    ring_bin_fill_kernel<<<grid_for(R, 256), 256, 0, s>>>(R, idx->ring_off, idx->xy, entry_off.p, bin_idx.p, binned.p,
+                                                          yinfo.p, idx->ring_bin, idx->ring_bins, idx->bin_edges);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    idx->n_binned_rings = tot[1];
+    idx->n_bin_edges = tot[0];
+    idx->n_split_binned_rings = (int64_t)h_long;
     return VS_OK;
 }
 

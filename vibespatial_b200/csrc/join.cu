@@ -63,6 +63,7 @@ struct RtreeArgs {
     DeferSink defer;
     unsigned long long* counters;
     unsigned long long* work;  // traversal work queue (sorted points handed out)
+    RingIndex rings;           // y-bins of the long rings
 };
 
 #ifndef VS_RTREE_GRAB
@@ -114,8 +115,11 @@ __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ fr
 // kBulk: leaf blocks (up to 16 FP64 boxes, 512 B) arrive by one bulk copy
 // (TMA, cp.async.bulk) into the warp's item buffer instead of lane loads
 // (VS_JOIN_BULK_LEAVES).
-template <bool kBulk>
+// kBins: the index has y-binned rings (kernels without bins carry no binned
+// walk, which keeps their registers for the plain one).
+template <bool kBulk, bool kBins>
 __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const RtreeArgs a) {
+    const RingIndex rings = kBins ? a.rings : RingIndex{};
     extern __shared__ vs_box s_nodes[];
     __shared__ int2 s_buf[kWarps][kWarpBuf];
     __shared__ unsigned s_cnt[kWarps];
@@ -168,7 +172,7 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
                     if (active && box_has(root, x, y)) {
                         ++n_cand;
                         const int loc = a.accept_mask ? geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off,
-                                                                                   a.geom_off, 0) : 0;
+                                                                                   a.geom_off, 0, rings) : 0;
                         if (loc == LOC_UNDECIDED) defer(a.defer, row, 0);
                         else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                     }
@@ -236,7 +240,8 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
                             ++n_cand;
                             int loc = 0;
                             if (a.accept_mask)
-                                loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot);
+                                loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot,
+                                                                 rings);
                             if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
                             else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                         }
@@ -275,7 +280,7 @@ __global__ void __launch_bounds__(kJoinThreads) join_brute_kernel(const RtreeArg
                 ++n_cand;
                 int loc = 0;
                 if (a.accept_mask)
-                    loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, (int)c);
+                    loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, (int)c, a.rings);
                 if (loc == LOC_UNDECIDED) defer(a.defer, (int32_t)i, (int32_t)c);
                 else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
             }
@@ -303,6 +308,7 @@ struct ResolveArgs {
     const unsigned long long* count;
     PairSink sink;
     unsigned long long* counters;
+    RingIndex rings;
 };
 
 __global__ void __launch_bounds__(kJoinThreads) resolve_deferred_kernel(const ResolveArgs a) {
@@ -324,7 +330,7 @@ __global__ void __launch_bounds__(kJoinThreads) resolve_deferred_kernel(const Re
         if (k < n) {
             pr = a.pairs[k];
             const double x = a.px[pr.x], y = a.py[pr.x];
-            const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, pr.y, n_exact);
+            const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, pr.y, a.rings, n_exact);
             want = (a.accept_mask >> loc) & 1;
         }
         wemit_sync(out, a.sink, want, pr.x, want ? a.item_geom[pr.y] : 0);
@@ -433,6 +439,7 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.defer = dsink;
     a.counters = ctx->d_counters;
+    a.rings = idx->ring_index();
     if (brute) {
         phase_mark(ctx, 1);
         phase_mark(ctx, 2);
@@ -448,7 +455,9 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.n_sorted = q.n_valid.p;
     a.work = &ctx->d_counters[kWorkCounter];
     const size_t smem = (size_t)a.staged * sizeof(vs_box);
-    auto* kernel = bulk_leaves ? join_rtree_packet_kernel<true> : join_rtree_packet_kernel<false>;
+    const bool bins = idx->ring_bin != nullptr;
+    auto* kernel = bulk_leaves ? (bins ? join_rtree_packet_kernel<true, true> : join_rtree_packet_kernel<true, false>)
+                               : (bins ? join_rtree_packet_kernel<false, true> : join_rtree_packet_kernel<false, false>);
     VS_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kernel<<<resident_grid(kernel, pts->n, kJoinThreads, smem), kJoinThreads, smem, ctx->stream>>>(a);
     VS_LAUNCHED("join_rtree_packet", ctx->stream);
@@ -471,6 +480,7 @@ int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_point
     a.count = dsink.counter;
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.counters = ctx->d_counters;
+    a.rings = idx->ring_index();
     resolve_deferred_kernel<<<resident_grid(resolve_deferred_kernel, (int64_t)1 << 30, kJoinThreads), kJoinThreads, 0,
                               ctx->stream>>>(a);
     VS_LAUNCHED("resolve_deferred", ctx->stream);

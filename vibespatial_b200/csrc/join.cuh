@@ -26,6 +26,8 @@ int launch_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygo
 int sort_pairs(vs_context* ctx, int32_t* d_left, int32_t* d_right, int64_t n, uint64_t max_left,
                uint64_t max_right);
 int build_rtree(vs_context* ctx, const vs_polygons* P, vs_index* idx);
+// y-bins for rings of at least min_vertices vertices (0: the default, < 0: none).
+int build_ring_bins(vs_context* ctx, vs_index* idx, int min_vertices);
 void free_index_memory(vs_index* idx);
 int hilbert_point_keys(const double* x, const double* y, int64_t n, double minx, double miny, double maxx,
                        double maxy, uint64_t* keys, cudaStream_t s);

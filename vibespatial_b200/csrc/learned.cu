@@ -182,7 +182,8 @@ __global__ void split_copy_kernel(const vs_box* __restrict__ box, int64_t M, con
 __global__ void pack_slots_kernel(int64_t M, const double2* __restrict__ origin, const float4* __restrict__ box32,
                                   const float* __restrict__ err32, const int32_t* __restrict__ item_geom,
                                   const int32_t* __restrict__ geom_off, const int32_t* __restrict__ part_off,
-                                  const int32_t* __restrict__ ring_off, SlotRecord* __restrict__ out) {
+                                  const int32_t* __restrict__ ring_off, const int32_t* __restrict__ ring_bin,
+                                  SlotRecord* __restrict__ out) {
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M; s += (int64_t)gridDim.x * blockDim.x) {
         SlotRecord r;
         r.ox = origin[s].x;
@@ -193,9 +194,15 @@ __global__ void pack_slots_kernel(int64_t M, const double2* __restrict__ origin,
         const int32_t p0 = geom_off[s], p1 = geom_off[s + 1];
         r.c0 = -1;
         r.c1 = -1;
+        // single-ring polygons take the short path (c0 >= 0) unless the split
+        // walk would use the ring's y-bins
         if (p1 - p0 == 1 && part_off[p0 + 1] - part_off[p0] == 1) {
-            r.c0 = ring_off[part_off[p0]];
-            r.c1 = ring_off[part_off[p0] + 1];
+            const int ring = part_off[p0];
+            const int c0 = ring_off[ring], c1 = ring_off[ring + 1];
+            if (ring_bin == nullptr || ring_bin[ring] < 0 || c1 - c0 < kSplitBinMinVertices) {
+                r.c0 = c0;
+                r.c1 = c1;
+            }
         }
         out[s] = r;
     }
@@ -678,7 +685,7 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_TRY(slots.alloc((size_t)M, s));
     VS_TRY(dalloc(&li.recs, (size_t)E, bytes));
     pack_slots_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, li.origin, li.box32, li.err32, idx->item_geom, idx->geom_off,
-                                                       idx->part_off, idx->ring_off, slots.p);
+                                                       idx->part_off, idx->ring_off, idx->ring_bin, slots.p);
     VS_CUDA_TRY(cudaGetLastError());
     entry_recs_kernel<<<grid_for(E, 256), 256, 0, s>>>((int64_t)E, li.entries, slots.p, li.recs);
     VS_CUDA_TRY(cudaGetLastError());
@@ -702,6 +709,7 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     d.part_off = idx->part_off;
     d.ring_off = idx->ring_off;
     d.boxes = idx->nodes;
+    d.rings = idx->ring_index();
     VS_TRY(dalloc(&li.desc, 1, bytes));
     VS_CUDA_TRY(cudaMemcpyAsync(li.desc, &d, sizeof(d), cudaMemcpyHostToDevice, s));
     learned_desc_kernel<<<1, 1, 0, s>>>(idx->frame, li.desc);

@@ -35,6 +35,7 @@ struct LearnedQuery {
     const int64_t* job_start;
     int64_t n_cells;  // batch-wide cells
     int accept_mask;
+    bool has_ring_bins;  // some job's index has y-binned rings long enough for the split walk
 };
 
 // Enqueue map -> scan -> scatter -> refine on stream s (no host

@@ -100,9 +100,6 @@ __device__ __forceinline__ const LearnedJob& job_desc(const LqArgs& a, int job) 
 }
 
 // ------------------------------------------------------- split refine ---
-#ifndef VS_RING_PREFETCH
-#define VS_RING_PREFETCH 0
-#endif
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
 // decision the exact walk needs lies within the rounding-error bound `t`
 // (the caller then re-decides the edge in FP64); otherwise applies the same
@@ -137,6 +134,22 @@ __device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, flo
     return false;
 }
 
+// One edge (vertex ia -> vertex ib) of the split ring walk: FP32 first, the
+// FP64 filter when the FP32 bound is inconclusive.  0: go on, 1: on the
+// edge, 2: undecided by the FP64 filter too.
+__device__ __forceinline__ int split_edge(double px, double py, float qx, float qy, float t, float2 a, float2 b,
+                                          const double2* __restrict__ xy, int ia, int ib, bool& inside,
+                                          unsigned& n32, unsigned& n64) {
+    if (edge_step_fp32(a.x, a.y, b.x, b.y, qx, qy, t, inside)) {
+        ++n32;
+        return 0;
+    }
+    ++n64;
+    const double2 A = xy[ia], B = xy[ib];
+    return edge_step_filtered(A.x, A.y, B.x, B.y, px, py, inside);
+}
+
+// Split-precision location of a point in one ring, every edge.
 __device__ __forceinline__ int ring_location_split(double px, double py, float qx, float qy, float t,
                                                    const float2* __restrict__ xy32, const double2* __restrict__ xy,
                                                    int start, int end, unsigned& n32, unsigned& n64) {
@@ -144,31 +157,46 @@ __device__ __forceinline__ int ring_location_split(double px, double py, float q
     bool inside = false;
     float2 a = xy32[end - 1];
     int ia = end - 1;
-#if VS_RING_PREFETCH
-    float2 nb = xy32[start];
-#endif
     for (int i = start; i < end; ++i) {
-#if VS_RING_PREFETCH
-        const float2 b = nb;
-        if (i + 1 < end) nb = xy32[i + 1];  // next vertex in flight while this edge is decided
-#else
         const float2 b = xy32[i];
-#endif
-        if (edge_step_fp32(a.x, a.y, b.x, b.y, qx, qy, t, inside)) {
-            ++n32;
-        } else {
-            ++n64;
-            const double2 A = xy[ia], B = xy[i];
-            const int r = edge_step_filtered(A.x, A.y, B.x, B.y, px, py, inside);
-            if (r == 1) return LOC_BOUNDARY;
-            if (r == 2) return LOC_UNDECIDED;
-        }
+        const int r = split_edge(px, py, qx, qy, t, a, b, xy, ia, i, inside, n32, n64);
+        if (r == 1) return LOC_BOUNDARY;
+        if (r == 2) return LOC_UNDECIDED;
         a = b;
         ia = i;
     }
     return inside ? LOC_INTERIOR : LOC_OUTSIDE;
 }
 
+// The same for a ring with y-bins: only the edges of the point's bin, in ring
+// order; an edge that continues the previous one reuses its end vertex.
+__device__ __forceinline__ int ring_location_split_binned(double px, double py, float qx, float qy, float t,
+                                                          const float2* __restrict__ xy32,
+                                                          const double2* __restrict__ xy, int start, int end,
+                                                          const RingBins& bins, const uint16_t* __restrict__ edges,
+                                                          unsigned& n32, unsigned& n64) {
+    bool inside = false;
+    const int k = ring_bin_of(py, bins.y0, bins.scale);
+    const uint32_t e1 = bins.off[k + 1];
+    int last = -2;
+    float2 lb = make_float2(0.f, 0.f);
+    for (uint32_t e = bins.off[k]; e < e1; ++e) {
+        const int i = start + edges[e];
+        const int ia = i == start ? end - 1 : i - 1;
+        const float2 a = ia == last ? lb : xy32[ia];
+        const float2 b = xy32[i];
+        const int r = split_edge(px, py, qx, qy, t, a, b, xy, ia, i, inside, n32, n64);
+        if (r == 1) return LOC_BOUNDARY;
+        if (r == 2) return LOC_UNDECIDED;
+        last = i;
+        lb = b;
+    }
+    return inside ? LOC_INTERIOR : LOC_OUTSIDE;
+}
+
+// kBins: the index has y-binned rings (kernels without bins carry no binned
+// walk, which keeps their registers for the common short rings).
+template <bool kBins>
 __device__ __forceinline__ int geometry_location_split(double px, double py, float qx, float qy, float t,
                                                        const LearnedJob& J, int g, unsigned& n32, unsigned& n64) {
     const int p0 = J.geom_off[g], p1 = J.geom_off[g + 1];
@@ -176,8 +204,13 @@ __device__ __forceinline__ int geometry_location_split(double px, double py, flo
         bool inside = false;
         const int r0 = J.part_off[part], r1 = J.part_off[part + 1];
         for (int ring = r0; ring < r1; ++ring) {
-            const int k = ring_location_split(px, py, qx, qy, t, J.xy32, J.xy, J.ring_off[ring], J.ring_off[ring + 1],
-                                              n32, n64);
+            const int c0 = J.ring_off[ring], c1 = J.ring_off[ring + 1];
+            // the FP32 walk is cheap per edge, so bins pay off only on longer rings than for the FP64 walk
+            const int rb = (kBins && J.rings.ring_bin && c1 - c0 >= kSplitBinMinVertices) ? J.rings.ring_bin[ring] : -1;
+            const int k = rb >= 0
+                              ? ring_location_split_binned(px, py, qx, qy, t, J.xy32, J.xy, c0, c1, J.rings.bins[rb],
+                                                           J.rings.edges, n32, n64)
+                              : ring_location_split(px, py, qx, qy, t, J.xy32, J.xy, c0, c1, n32, n64);
             if (k == LOC_BOUNDARY || k == LOC_UNDECIDED) return k;
             if (k == LOC_INTERIOR) inside = !inside;
         }
@@ -411,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_bbox_ker
 }
 
 // Ring walks of up to 32 queued pairs, one per lane.
-template <bool kMulti>
+template <bool kMulti, bool kBins>
 __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& out, const QueuedPair* qp, int nq,
                                               int lane, unsigned& n32, unsigned& n64) {
     bool want = false;
@@ -425,7 +458,7 @@ __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& ou
         const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
         const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
         const int loc = r.c0 >= 0 ? ring_location_split(jb.x, jb.y, qx, qy, t, J.xy32, J.xy, r.c0, r.c1, n32, n64)
-                                  : geometry_location_split(jb.x, jb.y, qx, qy, t, J, r.slot, n32, n64);
+                                  : geometry_location_split<kBins>(jb.x, jb.y, qx, qy, t, J, r.slot, n32, n64);
         if (loc == LOC_UNDECIDED) {
             defer(a.defer, jb.row, r.slot);  // a batch's exact pass finds the job from the row
         } else if ((a.q.accept_mask >> loc) & 1) {
@@ -443,7 +476,7 @@ __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& ou
 // run with all lanes busy instead of only the lanes whose point lies in the
 // current candidate's box.  Neighbouring queue entries mostly share a
 // polygon, so vertex reads stay broadcasts.
-template <bool kMulti>
+template <bool kMulti, bool kBins>
 __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_kernel(const LqArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
     __shared__ unsigned s_cnt[kThreads / 32];
@@ -488,7 +521,7 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_k
                 nq += __popc(m);
                 __syncwarp();
                 if (nq >= 32) {
-                    refine_queued<kMulti>(a, out, qp, 32, lane, n32, n64);
+                    refine_queued<kMulti, kBins>(a, out, qp, 32, lane, n32, n64);
                     __syncwarp();
                     if (lane < nq - 32) qp[lane] = qp[32 + lane];
                     nq -= 32;
@@ -498,7 +531,7 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_k
             wflush(out, a.sink, false);
         }
     }
-    if (nq > 0) refine_queued<kMulti>(a, out, qp, nq, lane, n32, n64);
+    if (nq > 0) refine_queued<kMulti, kBins>(a, out, qp, nq, lane, n32, n64);
     wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 2, n32);
@@ -554,7 +587,8 @@ int launch_passes(cudaStream_t s, vs_context* ctx, const LqArgs& a) {
     VS_LAUNCHED("learned_scatter", s);
     if (ctx) phase_mark(ctx, 2);
     if (a.q.accept_mask) {
-        learned_refine_kernel<kMulti><<<resident_grid(learned_refine_kernel<kMulti>, n, kThreads), kThreads, 0, s>>>(a);
+        auto* kernel = a.q.has_ring_bins ? learned_refine_kernel<kMulti, true> : learned_refine_kernel<kMulti, false>;
+        kernel<<<resident_grid(kernel, n, kThreads), kThreads, 0, s>>>(a);
         VS_LAUNCHED("learned_refine", s);
     } else {
         learned_bbox_kernel<kMulti><<<resident_grid(learned_bbox_kernel<kMulti>, n, kThreads), kThreads, 0, s>>>(a);
@@ -606,6 +640,7 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     q.job_start = nullptr;
     q.n_cells = li.n_cells;
     q.accept_mask = accept_mask;
+    q.has_ring_bins = idx->n_split_binned_rings > 0;
     const PairSink sink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     return enqueue_learned(s, ctx, q, &li.h_desc, sc, sink, dsink, ctx->d_counters, &ctx->d_counters[kWorkCounter]);
 }
