@@ -79,6 +79,11 @@ static __device__ __noinline__ int orient2d_exact(double ax, double ay, double b
     int n = 0;
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) {
+        // a pair of products with a zero factor each adds nothing: skipping it
+        // leaves the expansion (and so the sign) unchanged.  When the four
+        // differences are exact (their tails are zero, as for lattice or
+        // nearby inputs) only k = 0 remains.
+        if ((la[k] == 0.0 || lb[k] == 0.0) && (ra[k] == 0.0 || rb[k] == 0.0)) continue;
         double p, q, t[4];
         two_product(la[k], lb[k], p, q);
         t[0] = q;
@@ -94,6 +99,7 @@ static __device__ __noinline__ int orient2d_exact(double ax, double ay, double b
             nxt = s;
         }
     }
+    if (n == 0) return 0;
     const double top = cur[n - 1];
     return (top > 0.0) - (top < 0.0);
 }
