@@ -227,6 +227,46 @@ int vs_batch_run(vs_batch_plan* plan, int32_t predicate, int32_t* d_left, int32_
 
 int vs_batch_plan_free(vs_batch_plan* plan);
 
+/* ---------------------------------------------------------------------- */
+/* WKB decode on the device (GeoParquet / GeoArrow WKB columns -> the
+ * columnar layout of the join's inputs).  Replaces the reference's Arrow WKB
+ * decode (decode_wkb_arrow_array_owned, src/vibespatial/io/wkb.py:5224) for
+ * Point, Polygon and MultiPolygon rows, either byte order, ISO or EWKB (Z, M
+ * and SRID are accepted; Z and M are dropped).  Two calls: the plan sizes the
+ * output (rows of other types count as unsupported, truncated or invalid
+ * bytes as malformed, and decode to null rows), the caller allocates, and the
+ * decode fills. */
+typedef struct vs_wkb_plan vs_wkb_plan;
+
+typedef struct vs_wkb_sizes {
+    int64_t n_rows;
+    int64_t n_points, n_polygons, n_multipolygons, n_null;
+    int64_t n_unsupported, n_malformed;
+    int64_t n_parts, n_rings, n_coords;
+} vs_wkb_sizes;
+
+/* Output buffers (device): per row tags (int8: -1 null, 0 Point, 2 Polygon,
+ * 5 MultiPolygon), px/py (the Point coordinates, NaN otherwise) and
+ * geom_off (n_rows + 1); part_off (n_parts + 1), ring_off (n_rings + 1),
+ * x/y (n_coords). */
+typedef struct vs_wkb_out {
+    int8_t* d_tags;
+    double* d_px;
+    double* d_py;
+    int32_t* d_geom_off;
+    int32_t* d_part_off;
+    int32_t* d_ring_off;
+    double* d_x;
+    double* d_y;
+} vs_wkb_out;
+
+/* d_offsets: n + 1 int64 byte offsets into d_wkb (Arrow binary layout);
+ * d_valid nullable.  The plan borrows the input buffers until it is freed. */
+int vs_wkb_plan_create(vs_context* ctx, const uint8_t* d_wkb, const int64_t* d_offsets,
+                       const uint8_t* d_valid, int64_t n, vs_wkb_plan** plan, vs_wkb_sizes* sizes);
+int vs_wkb_plan_decode(vs_wkb_plan* plan, const vs_wkb_out* out);
+int vs_wkb_plan_free(vs_wkb_plan* plan);
+
 /* Brute-force point x polygon join that allocates no device memory, for
  * callers that cannot allocate (a host that owns all device memory in a
  * fixed arena, a hard memory budget, a loop that cannot afford an

@@ -207,3 +207,38 @@ def test_sindex_query(backend):
     assert tree.sindex.query(q, predicate="contains").shape == (2, 0)
     with pytest.raises(NotImplementedError):
         tree.sindex.query(tree, predicate="intersects")
+
+
+def test_sindex_query_output_formats(backend):
+    tree = vs.GeometryArray.from_shapes([vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11)])
+    q = vs.GeometryArray.from_shapes([vs.Point(1, 1), vs.Point(4, 4), vs.Point(20, 20)])
+    dense = tree.sindex.query(q, predicate="intersects", output_format="dense")
+    assert dense.shape == (3, 3) and dense.dtype == bool
+    assert np.argwhere(dense).tolist() == [[0, 0], [0, 1], [1, 1]]  # (tree row, input row)
+    sparse = tree.sindex.query(q, predicate="intersects", output_format="sparse")
+    assert sparse.shape == (3, 3) and sparse.nnz == 3
+    np.testing.assert_array_equal(sparse.toarray(), dense)
+    # a scalar input: tree rows, a (len(tree),) mask, a 1-D sparse array
+    assert tree.sindex.query(vs.Point(4, 4), predicate="within").tolist() == [0, 1]
+    d1 = tree.sindex.query(vs.Point(4, 4), predicate="within", output_format="dense")
+    assert d1.tolist() == [True, True, False]
+    s1 = tree.sindex.query(vs.Point(4, 4), predicate="within", output_format="sparse")
+    assert s1.shape == (3,) and s1.nnz == 2
+    with pytest.raises(ValueError):
+        tree.sindex.query(q, output_format="bogus")
+    with pytest.raises(ValueError):
+        tree.sindex.query(q, output_format="dense", return_device=True)
+
+
+@pytest.mark.gpu
+def test_sindex_query_return_device(backend):
+    if backend != "gpu":
+        pytest.skip("device output needs the CUDA join")
+    tree = vs.GeometryArray.from_shapes([vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11)])
+    q = vs.GeometryArray.from_shapes([vs.Point(1, 1), vs.Point(4, 4), vs.Point(20, 20)])
+    rows, trees = tree.sindex.query(q, predicate="intersects", return_device=True)
+    assert rows.is_cuda and trees.is_cuda
+    assert rows.cpu().tolist() == [0, 1, 1] and trees.cpu().tolist() == [0, 0, 1]
+    # points as the tree: pairs swapped and re-sorted on the device
+    r2, t2 = q.sindex.query(tree, predicate="contains", return_device=True)
+    assert r2.cpu().tolist() == [0, 0, 1] and t2.cpu().tolist() == [0, 1, 1]

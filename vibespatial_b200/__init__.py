@@ -17,6 +17,7 @@ from .geometry import (
     box,
     points_from_xy,
 )
+from .io import from_wkb, geodataframe_from_arrow, geoseries_from_arrow, read_geoparquet
 from .query import SpatialIndex, query_spatial_index
 from .sjoin import sjoin
 
@@ -30,7 +31,11 @@ __all__ = [
     "Polygon",
     "SpatialIndex",
     "box",
+    "from_wkb",
+    "geodataframe_from_arrow",
+    "geoseries_from_arrow",
     "points_from_xy",
+    "read_geoparquet",
     "query_spatial_index",
     "sjoin",
 ]

@@ -27,6 +27,7 @@ EXPORTED = (
     "vs_context_synchronize", "vs_index_build", "vs_index_info_get", "vs_index_free",
     "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
+    "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free",
 )
 
 
@@ -90,6 +91,19 @@ class BatchOptions(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class WkbSizes(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("n_rows", "n_points", "n_polygons", "n_multipolygons", "n_null",
+                                               "n_unsupported", "n_malformed", "n_parts", "n_rings", "n_coords")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class WkbOut(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in ("d_tags", "d_px", "d_py", "d_geom_off", "d_part_off", "d_ring_off",
+                                                "d_x", "d_y")]
+
+
 class IndexInfo(ctypes.Structure):
     _fields_ = [
         ("n_geoms", ctypes.c_int32), ("fanout", ctypes.c_int32), ("levels", ctypes.c_int32),
@@ -146,6 +160,9 @@ def load(path: Path | str | None = None):
             "vs_batch_run": (ctypes.c_int, [vp, i32, vp, vp, i64, i32, ctypes.POINTER(i64),
                                             ctypes.POINTER(JoinStats)]),
             "vs_batch_plan_free": (ctypes.c_int, [vp]),
+            "vs_wkb_plan_create": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.POINTER(vp), ctypes.POINTER(WkbSizes)]),
+            "vs_wkb_plan_decode": (ctypes.c_int, [vp, ctypes.POINTER(WkbOut)]),
+            "vs_wkb_plan_free": (ctypes.c_int, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -358,6 +375,39 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+def wkb_decode(ctx: Context, data, offsets, valid=None):
+    """Decode WKB rows on the device (see vs_wkb_plan_create).
+
+    ``data``: uint8 CUDA tensor of the concatenated WKB values, ``offsets``:
+    int64 CUDA tensor of n + 1 byte offsets, ``valid``: optional uint8 CUDA
+    tensor.  Returns (sizes dict, dict of CUDA tensors tags, px, py,
+    geom_off, part_off, ring_off, x, y).
+    """
+    import torch
+
+    n = int(offsets.numel()) - 1
+    sizes = WkbSizes()
+    h = ctypes.c_void_p()
+    check(load().vs_wkb_plan_create(ctx.handle, _ptr(data), _ptr(offsets), _ptr(valid), n, ctypes.byref(h),
+                                    ctypes.byref(sizes)))
+    try:
+        dev = offsets.device
+        sz = sizes.as_dict()
+        out = dict(tags=torch.empty(n, dtype=torch.int8, device=dev),
+                   px=torch.empty(n, dtype=torch.float64, device=dev),
+                   py=torch.empty(n, dtype=torch.float64, device=dev),
+                   geom_off=torch.empty(n + 1, dtype=torch.int32, device=dev),
+                   part_off=torch.empty(sz["n_parts"] + 1, dtype=torch.int32, device=dev),
+                   ring_off=torch.empty(sz["n_rings"] + 1, dtype=torch.int32, device=dev),
+                   x=torch.empty(sz["n_coords"], dtype=torch.float64, device=dev),
+                   y=torch.empty(sz["n_coords"], dtype=torch.float64, device=dev))
+        o = WkbOut(*[_ptr(out[k]) for k in ("tags", "px", "py", "geom_off", "part_off", "ring_off", "x", "y")])
+        check(load().vs_wkb_plan_decode(h, ctypes.byref(o)))
+        return sz, out
+    finally:
+        load().vs_wkb_plan_free(h)
 
 
 def locate_aligned(ctx: Context, pts: Points, polys: Polygons, out) -> None:

@@ -72,17 +72,34 @@ def polygon_index(ga, learned: bool = True, device: int = 0) -> "_abi.DeviceInde
     return idx
 
 
-def join_pairs(points, polygons, predicate, *, method: str = "learned", device: int = 0):
-    """Sorted (point row, polygon row) pairs satisfying ``predicate`` (point on the left)."""
+def join_pairs(points, polygons, predicate, *, method: str = "learned", device: int = 0,
+               on_device: bool = False):
+    """Sorted (point row, polygon row) pairs satisfying ``predicate`` (point on the left).
+
+    Host intp arrays, or with ``on_device`` the int32 CUDA tensors the join
+    wrote (no device-to-host copy).
+    """
     code = PREDICATE_CODES[predicate]
     if len(points) == 0 or len(polygons) == 0:
+        if on_device:
+            torch = _torch()
+            e = torch.empty(0, dtype=torch.int32, device=device)
+            return e, e.clone()
         return np.empty(0, np.intp), np.empty(0, np.intp)
     learned = method == "learned"
     index = polygon_index(polygons, learned=learned, device=device)
     pts, _ = device_points(points, device)
     m = _abi.METHOD_LEARNED if learned else (_abi.METHOD_BRUTE if method == "brute" else _abi.METHOD_RTREE)
     left, right, _ = index.join(pts, code, m, sort=True)
+    if on_device:
+        return left, right
     return left.cpu().numpy().astype(np.intp), right.cpu().numpy().astype(np.intp)
+
+
+def sort_pairs_on_device(left, right, device: int = 0):
+    """Sort int32 device pairs by (left, right) in place (in-house radix sort)."""
+    _abi.sort_pairs(_abi.default_context(device), left, right)
+    return left, right
 
 
 def locate_aligned(points, polygons, device: int = 0) -> np.ndarray:

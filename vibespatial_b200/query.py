@@ -32,20 +32,54 @@ _TREE_POINTS = {None: None, "intersects": "intersects", "contains": "within", "c
 _pairs_backend = None
 
 
-def _pairs(points, polygons, predicate, method):
+def _pairs(points, polygons, predicate, method, on_device=False):
     if _pairs_backend is not None:
-        return _pairs_backend(points, polygons, predicate)
+        left, right = _pairs_backend(points, polygons, predicate)
+        if on_device:
+            import torch
+
+            return (torch.from_numpy(np.asarray(left, np.int32)).cuda(),
+                    torch.from_numpy(np.asarray(right, np.int32)).cuda())
+        return left, right
     from ._device import join_pairs
 
-    return join_pairs(points, polygons, predicate, method=method)
+    return join_pairs(points, polygons, predicate, method=method, on_device=on_device)
 
 
-def query_spatial_index(tree, geometry, *, predicate=None, sort=False, distance=None, method="learned"):
+def _query_device(tree, geometry, predicate, method):
+    """(geometry rows, tree rows) as int32 CUDA tensors sorted by (geometry row, tree row)."""
+    import torch
+
+    empty = (torch.empty(0, dtype=torch.int32, device="cuda"), torch.empty(0, dtype=torch.int32, device="cuda"))
+    if len(tree) == 0 or len(geometry) == 0:
+        return empty
+    if geometry.is_points() and tree.is_polygonal():
+        pred = _INPUT_POINTS[predicate]
+        return empty if pred == "empty" else _pairs(geometry, tree, pred, method, on_device=True)
+    if geometry.is_polygonal() and tree.is_points():
+        pred = _TREE_POINTS[predicate]
+        if pred == "empty":
+            return empty
+        pt, poly = _pairs(tree, geometry, pred, method, on_device=True)
+        if poly.numel():
+            from ._device import sort_pairs_on_device
+
+            poly, pt = sort_pairs_on_device(poly.contiguous(), pt.contiguous())
+        return poly, pt
+    raise NotImplementedError(
+        "vibespatial_b200 joins points with polygons/multipolygons only "
+        f"(tree families {sorted(tree.families())}, input families {sorted(geometry.families())})")
+
+
+def query_spatial_index(tree, geometry, *, predicate=None, sort=False, distance=None, method="learned",
+                        return_device=False):
     """(2, K) intp array of (geometry row, tree row) pairs satisfying ``predicate``.
 
     ``tree`` and ``geometry`` are GeometryArrays; one must hold points and the
     other polygons/multipolygons.  ``sort`` orders the pairs by (geometry row,
-    tree row) (the CUDA join always returns them sorted).
+    tree row) (the CUDA join always returns them sorted).  ``return_device``
+    returns the pairs as two int32 CUDA tensors that never leave the device
+    (the reference's DeviceSpatialJoinResult, src/vibespatial/spatial/query_types.py:176).
     """
     from .geometry import GeometryArray
 
@@ -55,6 +89,8 @@ def query_spatial_index(tree, geometry, *, predicate=None, sort=False, distance=
         raise NotImplementedError("the dwithin predicate is outside this point-in-polygon join")
     if not isinstance(tree, GeometryArray) or not isinstance(geometry, GeometryArray):
         raise TypeError("query_spatial_index expects GeometryArrays")
+    if return_device:
+        return _query_device(tree, geometry, predicate, method)
     empty = np.empty((2, 0), dtype=np.intp)
     if len(tree) == 0 or len(geometry) == 0:
         return empty
@@ -94,15 +130,54 @@ class SpatialIndex:
     def is_empty(self):
         return len(self.geometry) == 0
 
-    def query(self, geometry, predicate=None, sort=False, distance=None, method="learned"):
+    def query(self, geometry, predicate=None, sort=False, distance=None, output_format="indices",
+              return_device=False, method="learned"):
+        """Tree rows matching ``predicate(geometry, tree geometry)``.
+
+        ``output_format``: ``"indices"`` ((n,) tree rows for a scalar input,
+        (2, n) (input row, tree row) pairs for an array), ``"sparse"`` (a
+        boolean scipy.sparse COO array of shape (len(tree),) or
+        (len(tree), len(geometry))), or ``"dense"`` (the same as a numpy bool
+        array).  ``return_device=True`` (indices only) returns int32 CUDA
+        tensors: the tree rows for a scalar input, else (input rows, tree
+        rows), computed and kept on the device.  Mirrors sindex.query
+        (src/vibespatial/api/sindex.py:144, output formats :463-502).
+        """
         from .geometry import BaseGeometry, GeometryArray
 
-        if isinstance(geometry, BaseGeometry):
-            res = query_spatial_index(self.geometry, GeometryArray.from_shapes([geometry]), predicate=predicate,
-                                      sort=sort, distance=distance, method=method)
-            return res[1]
-        geometry = getattr(geometry, "values", geometry)
-        if not isinstance(geometry, GeometryArray):
-            geometry = GeometryArray.from_shapes(list(geometry))
-        return query_spatial_index(self.geometry, geometry, predicate=predicate, sort=sort, distance=distance,
-                                   method=method)
+        if output_format not in ("indices", "sparse", "dense"):
+            raise ValueError(f"Invalid output_format: '{output_format}'. Use one of 'indices', 'sparse', 'dense'.")
+        if return_device and output_format != "indices":
+            raise ValueError("return_device=True is only supported with output_format='indices'")
+        scalar = isinstance(geometry, BaseGeometry)
+        if scalar:
+            geometry = GeometryArray.from_shapes([geometry])
+        else:
+            geometry = getattr(geometry, "values", geometry)
+            if not isinstance(geometry, GeometryArray):
+                geometry = GeometryArray.from_shapes(list(geometry))
+        if return_device:
+            rows, tree_rows = query_spatial_index(self.geometry, geometry, predicate=predicate, sort=sort,
+                                                  distance=distance, method=method, return_device=True)
+            return tree_rows if scalar else (rows, tree_rows)
+        res = query_spatial_index(self.geometry, geometry, predicate=predicate, sort=sort, distance=distance,
+                                  method=method)
+        n_tree = len(self.geometry)
+        if output_format == "indices":
+            return res[1] if scalar else res
+        tree_rows, input_rows = res[1], res[0]
+        if output_format == "dense":
+            if scalar:
+                dense = np.zeros(n_tree, dtype=bool)
+                dense[tree_rows] = True
+            else:
+                dense = np.zeros((n_tree, len(geometry)), dtype=bool)
+                dense[tree_rows, input_rows] = True
+            return dense
+        import scipy.sparse
+
+        ones = np.ones(len(tree_rows), dtype=np.bool_)
+        if scalar:
+            return scipy.sparse.coo_array((ones, tree_rows.reshape(1, -1)), shape=(n_tree,), dtype=np.bool_)
+        return scipy.sparse.coo_array((ones, (tree_rows, input_rows)), shape=(n_tree, len(geometry)),
+                                      dtype=np.bool_)
