@@ -366,26 +366,22 @@ def run_ours(args, rank, world, local_rank):
             for _ in range(max(3, args.steps // 2)):
                 dph.append(index.join_into(pts, pred, _abi.METHOD_LEARNED, left, right)[1]["phase_ms"])
             phases = dph
-        # e2e through the C-ABI with host buffers: H2D of the points into the
-        # buffers the join reads, the join, D2H of the pairs
+        # e2e through the C-ABI with HOST buffers (vs_join_host): pinned host
+        # points in, pinned host pairs out, the chunked copies overlapping the join
         hx = torch.from_numpy(w.px).pin_memory()
         hy = torch.from_numpy(w.py).pin_memory()
         hl = torch.empty(cap, dtype=torch.int32).pin_memory()
         hr = torch.empty(cap, dtype=torch.int32).pin_memory()
         e2e_ms = []
-        for k in range(max(3, args.steps)):
+        for k in range(max(3, args.steps) + 1):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(stream):
-                a.record(stream)
-                dx.copy_(hx, non_blocking=True)
-                dy.copy_(hy, non_blocking=True)
-                n_e, _ = join(left, right)
-                assert n_e == n_pairs, (n_e, n_pairs)
-                hl[:n_e].copy_(left[:n_e], non_blocking=True)
-                hr[:n_e].copy_(right[:n_e], non_blocking=True)
-                b.record(stream)
+            a.record(stream)
+            n_e, _ = index.join_host(hx, hy, pred, method, hl, hr)
+            b.record(stream)
             torch.cuda.synchronize()
-            e2e_ms.append(a.elapsed_time(b))
+            assert n_e == n_pairs, (n_e, n_pairs)
+            if k:  # the first call warms the host pipeline
+                e2e_ms.append(a.elapsed_time(b))
     total_ms = float(sum(step_ms))
     if dist:
         t = torch.tensor([total_ms, float(np.median(e2e_ms))], device=dev, dtype=torch.float64)

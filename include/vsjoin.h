@@ -169,6 +169,19 @@ int vs_join(vs_context* ctx, const vs_index* index, const vs_points* pts, int32_
             int32_t method, uint32_t flags, int32_t* d_left, int32_t* d_right, int64_t capacity,
             int64_t* n_pairs, vs_join_stats* stats);
 
+/* vs_join on HOST buffers: h_x / h_y / h_valid (n points; pinned memory lets
+ * the copies run asynchronously) in, (left, right) pairs into h_left /
+ * h_right (capacity entries each) out.  The points are streamed in chunks
+ * so host-to-device copies, the join and device-to-host copies of the pairs
+ * overlap.  Same predicates, methods, VS_JOIN_SORT, VS_E_CAPACITY contract
+ * and stats as vs_join (stats->kernel_ms: the whole pipeline).  Replaces the
+ * reference's move_to H2D + device join + pair D2H round trip
+ * (src/vibespatial/spatial/query.py:124, query_spatial_index :247). */
+int vs_join_host(vs_context* ctx, const vs_index* index, const double* h_x, const double* h_y,
+                 const uint8_t* h_valid, int64_t n, int32_t predicate, int32_t method, uint32_t flags,
+                 int32_t* h_left, int32_t* h_right, int64_t capacity, int64_t* n_pairs,
+                 vs_join_stats* stats);
+
 /* Element-wise location of point row i in polygon row i (aligned arrays):
  * d_out[i] = 0 outside / 1 boundary / 2 interior / 255 null-or-empty.
  * Replaces the point-region fast path of GeometryArray.within/contains

@@ -270,3 +270,54 @@ def test_full_size_zipf_join(vsabi, ctx, oracle):
 
     w = syn.zipf_join(seed=3)
     _check(vsabi, ctx, oracle, w, "within", METHODS["learned"])
+
+
+@pytest.mark.parametrize("chunk", [None, 3_000_000])
+@pytest.mark.parametrize("method", ["rtree", "learned"])
+def test_join_host_pipeline(vsabi, ctx, oracle, method, chunk, monkeypatch):
+    """vs_join_host (chunked host->device->host pipeline) gives the oracle's pairs: one or several
+    chunks, a null mask, sorted and unsorted output, and the capacity error."""
+    import torch
+
+    from vibespatial_b200.testing import synthetic as syn
+
+    if chunk:
+        monkeypatch.setenv("VSJOIN_HOST_CHUNK", str(chunk))  # 3 chunks
+    w = syn.zipf_join(seed=12, n_points=9_000_000, n_polys=150_000)
+    rng = np.random.default_rng(1)
+    pvalid = (rng.random(w.n_points) > 0.05).astype(np.uint8)
+    P, _k = upload_polys(vsabi, w.polys)
+    index = vsabi.DeviceIndex(ctx, P, learned=True)
+    el, er = oracle.join(w.px, w.py, pvalid, oracle_polys(oracle, w.polys), "intersects")
+    hx = torch.from_numpy(w.px).pin_memory()
+    hy = torch.from_numpy(w.py).pin_memory()
+    hv = torch.from_numpy(pvalid).pin_memory()
+    cap = len(el) + 100
+    hl = torch.empty(cap, dtype=torch.int32).pin_memory()
+    hr = torch.empty(cap, dtype=torch.int32).pin_memory()
+    m = METHODS[method]
+    n, _ = index.join_host(hx, hy, PRED_CODES["intersects"], m, hl, hr, valid=hv, sort=True)
+    assert_same_pairs(hl[:n].numpy(), hr[:n].numpy(), el, er)
+    n2, _ = index.join_host(w.px, w.py, PRED_CODES["intersects"], m, hl.numpy(), hr.numpy(), valid=pvalid)
+    l2, r2 = hl[:n2].numpy(), hr[:n2].numpy()
+    o = np.lexsort((r2, l2))
+    assert_same_pairs(l2[o], r2[o], el, er)
+    with pytest.raises(vsabi.CapacityError) as ei:
+        index.join_host(hx, hy, PRED_CODES["intersects"], m, hl[:10], hr[:10], valid=hv)
+    assert ei.value.required == len(el)
+
+
+def test_join_host_grows_chunk_pair_buffer(vsabi, ctx, oracle):
+    """More pairs than points: the chunk's pair buffer grows and the chunk reruns."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.star_join(seed=13, n_points=300_000, n_polys=20_000)  # several box candidates per point
+    P, _k = upload_polys(vsabi, w.polys)
+    index = vsabi.DeviceIndex(ctx, P)
+    for predicate in (None, "intersects"):
+        el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), predicate)
+        hl = np.empty(len(el), np.int32)
+        hr = np.empty(len(el), np.int32)
+        n, _ = index.join_host(w.px, w.py, PRED_CODES[predicate], vsabi.METHOD_RTREE, hl, hr, sort=True)
+        assert n == len(el) > w.n_points  # more pairs than the first chunk buffer holds
+        assert_same_pairs(hl, hr, el, er)

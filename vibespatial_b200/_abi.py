@@ -27,7 +27,7 @@ EXPORTED = (
     "vs_context_synchronize", "vs_index_build", "vs_index_info_get", "vs_index_free",
     "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
-    "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free",
+    "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free", "vs_join_host",
 )
 
 
@@ -163,6 +163,8 @@ def load(path: Path | str | None = None):
             "vs_wkb_plan_create": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.POINTER(vp), ctypes.POINTER(WkbSizes)]),
             "vs_wkb_plan_decode": (ctypes.c_int, [vp, ctypes.POINTER(WkbOut)]),
             "vs_wkb_plan_free": (ctypes.c_int, [vp]),
+            "vs_join_host": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i32, i32, u32, vp, vp, i64, ctypes.POINTER(i64),
+                                            ctypes.POINTER(JoinStats)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -291,6 +293,30 @@ class DeviceIndex:
         status = load().vs_join(self.ctx.handle, self.handle, ctypes.byref(pts), int(predicate), int(method),
                                 (JOIN_SORT if sort else 0) | int(flags), _ptr(left), _ptr(right), cap,
                                 ctypes.byref(n), ctypes.byref(st))
+        check(status, required=int(n.value))
+        return int(n.value), st.as_dict()
+
+    def join_host(self, x, y, predicate: int, method: int, left, right, *, valid=None, sort: bool = False):
+        """vs_join_host: host (CPU) point buffers in, host pair buffers out; returns (n_pairs, stats).
+
+        x, y: float64 and valid: uint8 (or None) CPU tensors or numpy arrays;
+        left, right: int32 CPU tensors or numpy arrays (pinned tensors let the
+        copies overlap the join).  Raises CapacityError (with .required).
+        """
+        def ptr(a):
+            if a is None:
+                return None
+            return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+        def size(a):
+            return int(a.numel()) if hasattr(a, "numel") else int(a.size)
+
+        n = ctypes.c_int64(0)
+        st = JoinStats()
+        cap = 0 if left is None else size(left)
+        status = load().vs_join_host(self.ctx.handle, self.handle, ptr(x), ptr(y), ptr(valid), size(x),
+                                     int(predicate), int(method), JOIN_SORT if sort else 0, ptr(left), ptr(right),
+                                     cap, ctypes.byref(n), ctypes.byref(st))
         check(status, required=int(n.value))
         return int(n.value), st.as_dict()
 

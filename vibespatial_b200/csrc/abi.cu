@@ -70,8 +70,6 @@ int check_points(const vs_points* p) {
     return VS_OK;
 }
 
-namespace {
-
 int ensure_defer_capacity(vs_context* ctx, unsigned long long want) {
     if (ctx->defer_cap >= want) return VS_OK;
     if (ctx->defer_buf) {
@@ -89,6 +87,8 @@ int ensure_defer_capacity(vs_context* ctx, unsigned long long want) {
     ctx->defer_cap = want;
     return VS_OK;
 }
+
+namespace {
 
 struct EventPair {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -177,6 +177,7 @@ int vs_context_destroy(vs_context* ctx) {
     if (!ctx) return VS_OK;
     use_device(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    free_host_pipe(ctx);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->defer_buf);
     cudaFreeHost(ctx->h_counter);

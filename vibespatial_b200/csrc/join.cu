@@ -64,6 +64,7 @@ struct RtreeArgs {
     unsigned long long* counters;
     unsigned long long* work;  // traversal work queue (sorted points handed out)
     RingIndex rings;           // y-bins of the long rings
+    int64_t row_base;          // added to emitted / deferred rows (chunked joins)
 };
 
 #ifndef VS_RTREE_GRAB
@@ -149,10 +150,12 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
             const bool active = i < e0;
             double x = 0.0, y = 0.0;
             int32_t row = -1;
+            int32_t grow = -1;  // the row reported for the point
             if (active) {
                 row = (int32_t)a.order[i];
                 x = a.px[row];
                 y = a.py[row];
+                grow = (int32_t)(row + a.row_base);
             }
             double x0 = active ? x : INFINITY, x1 = active ? x : -INFINITY;
             double y0 = active ? y : INFINITY, y1 = active ? y : -INFINITY;
@@ -173,10 +176,10 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
                         ++n_cand;
                         const int loc = a.accept_mask ? geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off,
                                                                                    a.geom_off, 0, rings) : 0;
-                        if (loc == LOC_UNDECIDED) defer(a.defer, row, 0);
+                        if (loc == LOC_UNDECIDED) defer(a.defer, grow, 0);
                         else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                     }
-                    wemit_sync(out, a.sink, want, row, a.item_geom[0]);
+                    wemit_sync(out, a.sink, want, grow, a.item_geom[0]);
                 } else {
                     if (lane == 0) s_stack[warp][0] = top;  // node 0 of the top level
                     sp = 1;
@@ -242,10 +245,10 @@ __global__ void __launch_bounds__(kJoinThreads) join_rtree_packet_kernel(const R
                             if (a.accept_mask)
                                 loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot,
                                                                  rings);
-                            if (loc == LOC_UNDECIDED) defer(a.defer, row, slot);
+                            if (loc == LOC_UNDECIDED) defer(a.defer, grow, slot);
                             else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
                         }
-                        wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                        wemit_sync(out, a.sink, want, grow, a.item_geom[slot]);
                     }
                     __syncwarp();
                 }
@@ -281,10 +284,10 @@ __global__ void __launch_bounds__(kJoinThreads) join_brute_kernel(const RtreeArg
                 int loc = 0;
                 if (a.accept_mask)
                     loc = geometry_location_filtered(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, (int)c, a.rings);
-                if (loc == LOC_UNDECIDED) defer(a.defer, (int32_t)i, (int32_t)c);
+                if (loc == LOC_UNDECIDED) defer(a.defer, (int32_t)(i + a.row_base), (int32_t)c);
                 else want = !a.accept_mask || ((a.accept_mask >> loc) & 1);
             }
-            wemit_sync(out, a.sink, want, (int32_t)i, a.item_geom[c]);
+            wemit_sync(out, a.sink, want, (int32_t)(i + a.row_base), a.item_geom[c]);
         }
         wflush(out, a.sink, false);
     }
@@ -309,6 +312,7 @@ struct ResolveArgs {
     PairSink sink;
     unsigned long long* counters;
     RingIndex rings;
+    int64_t row_base;  // deferred rows are chunk rows + row_base
 };
 
 __global__ void __launch_bounds__(kJoinThreads) resolve_deferred_kernel(const ResolveArgs a) {
@@ -329,7 +333,7 @@ __global__ void __launch_bounds__(kJoinThreads) resolve_deferred_kernel(const Re
         int2 pr = make_int2(0, 0);
         if (k < n) {
             pr = a.pairs[k];
-            const double x = a.px[pr.x], y = a.py[pr.x];
+            const double x = a.px[pr.x - a.row_base], y = a.py[pr.x - a.row_base];
             const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, pr.y, a.rings, n_exact);
             want = (a.accept_mask >> loc) & 1;
         }
@@ -409,7 +413,8 @@ int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
 }
 
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
-                      bool bulk_leaves, int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
+                      bool bulk_leaves, int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink,
+                      int64_t row_base) {
     RtreeArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
@@ -440,6 +445,7 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
     a.defer = dsink;
     a.counters = ctx->d_counters;
     a.rings = idx->ring_index();
+    a.row_base = row_base;
     if (brute) {
         phase_mark(ctx, 1);
         phase_mark(ctx, 2);
@@ -465,7 +471,8 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
 }
 
 int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
-                            int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
+                            int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink,
+                            int64_t row_base) {
     ResolveArgs a{};
     a.px = pts->d_x;
     a.py = pts->d_y;
@@ -481,6 +488,7 @@ int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_point
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     a.counters = ctx->d_counters;
     a.rings = idx->ring_index();
+    a.row_base = row_base;
     resolve_deferred_kernel<<<resident_grid(resolve_deferred_kernel, (int64_t)1 << 30, kJoinThreads), kJoinThreads, 0,
                               ctx->stream>>>(a);
     VS_LAUNCHED("resolve_deferred", ctx->stream);

@@ -15,13 +15,22 @@ struct QueryOrder {
 };
 int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q);
 int accept_mask_for(int predicate, int* mask);
+// row_base is added to every emitted or deferred point row (a chunk of a
+// larger point array); the exact pass subtracts it to read the chunk's points.
 int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, bool brute,
-                      bool bulk_leaves, int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
+                      bool bulk_leaves, int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink,
+                      int64_t row_base = 0);
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
-                        int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
+                        int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink,
+                        int64_t row_base = 0);
 // Exact pass over the pairs the filtered kernels deferred (count read on device).
 int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
-                            int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink);
+                            int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink,
+                            int64_t row_base = 0);
+// Grow the context's deferred-pair buffer to at least `want` pairs.
+int ensure_defer_capacity(vs_context* ctx, unsigned long long want);
+// Release the context's vs_join_host pipeline (streams, events, buffers).
+void free_host_pipe(vs_context* ctx);
 int launch_locate_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, uint8_t* d_out);
 int sort_pairs(vs_context* ctx, int32_t* d_left, int32_t* d_right, int64_t n, uint64_t max_left,
                uint64_t max_right);

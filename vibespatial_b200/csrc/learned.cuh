@@ -36,6 +36,7 @@ struct LearnedQuery {
     int64_t n_cells;  // batch-wide cells
     int accept_mask;
     bool has_ring_bins;  // some job's index has y-binned rings long enough for the split walk
+    int64_t row_base;    // added to every emitted / deferred point row (chunked joins)
 };
 
 // Enqueue map -> scan -> scatter -> refine on stream s (no host

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LqArgs a
                 StagedPoint p;
                 p.x = x;
                 p.y = y;
-                p.row = (int32_t)i;
+                p.row = (int32_t)(i + q.row_base);
                 p.cell = c;
                 p.rank = base + __popc(peers & lt);
                 p.job = job;
@@ -623,7 +623,7 @@ int enqueue_learned(cudaStream_t s, vs_context* ctx, const LearnedQuery& q, cons
 }
 
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, int32_t* d_left,
-                        int32_t* d_right, int64_t capacity, const DeferSink& dsink) {
+                        int32_t* d_right, int64_t capacity, const DeferSink& dsink, int64_t row_base) {
     const LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
     Scratch<char> buf;
@@ -641,6 +641,7 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     q.n_cells = li.n_cells;
     q.accept_mask = accept_mask;
     q.has_ring_bins = idx->n_split_binned_rings > 0;
+    q.row_base = row_base;
     const PairSink sink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     return enqueue_learned(s, ctx, q, &li.h_desc, sc, sink, dsink, ctx->d_counters, &ctx->d_counters[kWorkCounter]);
 }

@@ -123,6 +123,10 @@ struct __align__(32) vs_box {
     double minx, miny, maxx, maxy;
 };
 
+namespace vs {
+struct HostPipe;
+}
+
 // Opaque handles of the C-ABI.
 struct vs_context {
     int device;
@@ -144,6 +148,8 @@ struct vs_context {
     // around locate / group / refine / exact; recorded only while phase_on.
     cudaEvent_t phase_ev[5];
     bool phase_on;
+    // Streams and double buffers of vs_join_host, kept between calls.
+    vs::HostPipe* host_pipe;
 };
 
 // Record phase boundary k of the current join on the context stream.
