@@ -138,6 +138,11 @@ int vs_version(void);
 /* Message of the last failing call on this thread ("" if none). */
 const char* vs_last_error(void);
 
+/* Kernels the library has launched from the calling thread so far; the
+ * difference across calls counts their launches (benchmark diagnostics; no
+ * counterpart in the reference). */
+long long vs_thread_kernel_launches(void);
+
 /* A context = one device + one stream + a scratch arena.  `stream` is a
  * cudaStream_t (NULL: the context creates its own non-blocking stream; pass
  * cudaStreamLegacy to run on the legacy default stream).  Not thread-safe: callers
@@ -245,10 +250,11 @@ int vs_batch_plan_free(vs_batch_plan* plan);
  * columnar layout of the join's inputs).  Replaces the reference's Arrow WKB
  * decode (decode_wkb_arrow_array_owned, src/vibespatial/io/wkb.py:5224) for
  * Point, Polygon and MultiPolygon rows, either byte order, ISO or EWKB (Z, M
- * and SRID are accepted; Z and M are dropped).  Two calls: the plan sizes the
- * output (rows of other types count as unsupported, truncated or invalid
- * bytes as malformed, and decode to null rows), the caller allocates, and the
- * decode fills. */
+ * and SRID are accepted; Z and M are dropped).  Two calls: the plan writes
+ * the per-row outputs and sizes the rest (rows of other types count as
+ * unsupported, truncated or invalid bytes as malformed, and decode to null
+ * rows), the caller allocates the part / ring / coordinate buffers, and the
+ * decode fills them. */
 typedef struct vs_wkb_plan vs_wkb_plan;
 
 typedef struct vs_wkb_sizes {
@@ -258,10 +264,11 @@ typedef struct vs_wkb_sizes {
     int64_t n_parts, n_rings, n_coords;
 } vs_wkb_sizes;
 
-/* Output buffers (device): per row tags (int8: -1 null, 0 Point, 2 Polygon,
- * 5 MultiPolygon), px/py (the Point coordinates, NaN otherwise) and
- * geom_off (n_rows + 1); part_off (n_parts + 1), ring_off (n_rings + 1),
- * x/y (n_coords). */
+/* Output buffers (device).  Per row, written by vs_wkb_plan_create: tags
+ * (int8: -1 null, 0 Point, 2 Polygon, 5 MultiPolygon), px/py (the Point
+ * coordinates, NaN otherwise) and geom_off (n_rows + 1).  Written by
+ * vs_wkb_plan_decode: part_off (n_parts + 1), ring_off (n_rings + 1), x/y
+ * (n_coords). */
 typedef struct vs_wkb_out {
     int8_t* d_tags;
     double* d_px;
@@ -274,9 +281,14 @@ typedef struct vs_wkb_out {
 } vs_wkb_out;
 
 /* d_offsets: n + 1 int64 byte offsets into d_wkb (Arrow binary layout);
- * d_valid nullable.  The plan borrows the input buffers until it is freed. */
+ * d_valid nullable.  `rows` gives the per-row outputs (its other fields are
+ * ignored); the plan borrows the inputs and the row outputs until it is
+ * freed.  Returns after one host synchronisation (the sizes). */
 int vs_wkb_plan_create(vs_context* ctx, const uint8_t* d_wkb, const int64_t* d_offsets,
-                       const uint8_t* d_valid, int64_t n, vs_wkb_plan** plan, vs_wkb_sizes* sizes);
+                       const uint8_t* d_valid, int64_t n, const vs_wkb_out* rows,
+                       vs_wkb_plan** plan, vs_wkb_sizes* sizes);
+/* Fills out->d_part_off, d_ring_off, d_x, d_y (the row fields are ignored);
+ * returns when the outputs are complete. */
 int vs_wkb_plan_decode(vs_wkb_plan* plan, const vs_wkb_out* out);
 int vs_wkb_plan_free(vs_wkb_plan* plan);
 

@@ -11,6 +11,10 @@ predicate, the reference's point location:
 * polygon/multipolygon -- src/vibespatial/predicates/point_relations_kernels.py:37-96
 * predicate mapping    -- src/vibespatial/predicates/point_relations.py:100-130
 
+``oracle/wkb.c`` restates the reference's staged WKB decode
+(src/vibespatial/io/wkb.py:3755-3781 header scan, :3954 and :4043 payload
+walks) as the checker of the device WKB decoder.
+
 Parity pins: ``tests/test_oracle_golden.py`` checks this oracle against the
 reference test-suite's known answers (NYBB boroughs, Natural Earth
 cities x countries, the point-in-polygon unit cases) and against exact
@@ -48,8 +52,8 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 def build(force: bool = False) -> Path:
     """Compile ``liboracle.so`` with the committed Makefile."""
-    src = _HERE / "exact_pip.c"
-    if force or not _LIB_PATH.exists() or _LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+    srcs = [_HERE / "exact_pip.c", _HERE / "wkb.c"]
+    if force or not _LIB_PATH.exists() or any(_LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(_HERE), "-s"], check=True)
     return _LIB_PATH
 
@@ -77,6 +81,13 @@ def lib():
         L.orc_max_threads.restype = ctypes.c_int
         L.orc_geometry_bounds.restype = None
         L.orc_geometry_bounds.argtypes = [_dp, _dp, _i32p, _i32p, _i32p, _u8p, ctypes.c_int64, _dp]
+        _i64p = ctypes.POINTER(ctypes.c_int64)
+        L.orc_wkb_count.restype = None
+        L.orc_wkb_count.argtypes = [_u8p, _i64p, _u8p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int8), _dp, _dp,
+                                    _i64p, _i64p, ctypes.c_int]
+        L.orc_wkb_fill.restype = None
+        L.orc_wkb_fill.argtypes = [_u8p, _i64p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int8), _i64p, _i32p, _i32p,
+                                   _i32p, _dp, _dp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -157,6 +168,43 @@ def join(px, py, pvalid, polys: Polygons, predicate="within", threads: int = 0):
     finally:
         L.orc_pairs_free(h)
     return left, right
+
+
+WKB_SIZE_KEYS = ("n_rows", "n_points", "n_polygons", "n_multipolygons", "n_null", "n_unsupported", "n_malformed",
+                 "n_parts", "n_rings", "n_coords")
+
+
+def wkb_decode(data, offsets, valid=None, threads: int = 0):
+    """Decode WKB rows (Arrow binary layout: bytes + n + 1 int64 offsets).
+
+    Returns (sizes dict, dict of numpy arrays tags, px, py, geom_off,
+    part_off, ring_off, x, y) -- the device decoder's layout.
+    """
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    if data.size == 0:
+        data = np.zeros(1, np.uint8)
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    valid = _u8(valid)
+    n = len(off) - 1
+    threads = int(threads) or nthreads_default()
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    i8p = ctypes.POINTER(ctypes.c_int8)
+    out = dict(tags=np.empty(n, np.int8), px=np.empty(n, np.float64), py=np.empty(n, np.float64))
+    counts = np.empty(max(3 * n, 1), np.int64)
+    sizes = np.zeros(10, np.int64)
+    L = lib()
+    L.orc_wkb_count(_p(data, _u8p), _p(off, i64p), _p(valid, _u8p), n, _p(out["tags"], i8p), _p(out["px"], _dp),
+                    _p(out["py"], _dp), _p(counts, i64p), _p(sizes, i64p), threads)
+    sz = dict(zip(WKB_SIZE_KEYS, (int(v) for v in sizes)))
+    out["geom_off"] = np.empty(n + 1, np.int32)
+    out["part_off"] = np.empty(sz["n_parts"] + 1, np.int32)
+    out["ring_off"] = np.empty(sz["n_rings"] + 1, np.int32)
+    out["x"] = np.empty(sz["n_coords"], np.float64)
+    out["y"] = np.empty(sz["n_coords"], np.float64)
+    L.orc_wkb_fill(_p(data, _u8p), _p(off, i64p), n, _p(out["tags"], i8p), _p(counts, i64p),
+                   _p(out["geom_off"], _i32p), _p(out["part_off"], _i32p), _p(out["ring_off"], _i32p),
+                   _p(out["x"], _dp), _p(out["y"], _dp), threads)
+    return sz, out
 
 
 def max_threads() -> int:

@@ -7,7 +7,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def header_symbols():
     text = (ROOT / "include" / "vsjoin.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(vs_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|const char\*)\s+(vs_\w+)\s*\(", text, re.M)))
 
 
 def test_library_builds_and_exports_header_symbols():

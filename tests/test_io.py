@@ -120,6 +120,105 @@ GOLDEN = [
 ]
 
 
+def test_oracle_wkb_golden_points(oracle):
+    data, off, valid = W.arrow_layout([bytes.fromhex(h) for h, _ in GOLDEN])
+    sz, out = oracle.wkb_decode(data, off, valid)
+    assert sz["n_points"] == len(GOLDEN) and sz["n_coords"] == 0
+    np.testing.assert_array_equal(np.c_[out["px"], out["py"]], np.array([xy for _, xy in GOLDEN]))
+
+
+def test_oracle_wkb_unsupported_and_malformed(oracle):
+    gc = bytes.fromhex("010700000000000000")  # tests/test_io_arrow.py:508 (GeometryCollection)
+    line = bytes.fromhex("01020000000100000000000000000008400000000000000840")  # test_array.py:167
+    truncated = W.polygon([_ring(0, 0, 1)])[:-5]
+    data, off, valid = W.arrow_layout([truncated, W.point(1, 2), gc, line, b"\x07", None, b""])
+    sz, out = oracle.wkb_decode(data, off, valid)
+    assert out["tags"].tolist() == [-1, 0, -1, -1, -1, -1, -1]
+    assert (sz["n_points"], sz["n_unsupported"], sz["n_malformed"], sz["n_null"]) == (1, 2, 2, 2)
+    assert sz["n_parts"] == sz["n_rings"] == sz["n_coords"] == 0
+
+
+@pytest.mark.parametrize("variant", ["little", "big", "iso_z", "ewkb_zm_srid", "mixed_order_parts"])
+def test_oracle_wkb_matches_from_shapes(oracle, variant):
+    """The CPU decoder against the host layout built from shape objects."""
+    shapes = _shapes() + [vs.Point(3.5, -1.25), None]
+    kw = {"little": dict(), "big": dict(little=False), "iso_z": dict(dims="xyz"),
+          "ewkb_zm_srid": dict(dims="xyzm", ewkb=True, srid=4326), "mixed_order_parts": dict(little=False)}[variant]
+    vals = []
+    for s in shapes:
+        if s is None:
+            vals.append(None)
+        elif isinstance(s, vs.Point):
+            vals.append(W.point(s.x, s.y, **kw))
+        elif isinstance(s, vs.MultiPolygon):
+            extra = {"part_little": [True, False]} if variant == "mixed_order_parts" else {}
+            vals.append(W.multipolygon([p.rings for p in s.polygons], **kw, **extra))
+        else:
+            vals.append(W.polygon([] if s.is_empty else s.rings, **kw))
+    sz, out = oracle.wkb_decode(*W.arrow_layout(vals))
+    ref = vs.GeometryArray.from_shapes(shapes)
+    np.testing.assert_array_equal(out["tags"], ref._tags)
+    for k in ("geom_off", "part_off", "ring_off", "x", "y"):
+        np.testing.assert_array_equal(out[k], getattr(ref, "_" + k))
+    np.testing.assert_array_equal(out["px"][out["tags"] == 0], ref._px[ref._tags == 0])
+
+
+def test_oracle_wkb_synthetic_polygons(oracle):
+    """The vectorised synthetic-column writer and the CPU decoder agree."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.degenerate_join(seed=5, n_points=1_000, n_polys=400)
+    sz, out = oracle.wkb_decode(*syn.wkb_polygons(w.polys))
+    assert sz["n_malformed"] == sz["n_unsupported"] == 0
+    for k in ("geom_off", "part_off", "ring_off", "x", "y"):
+        np.testing.assert_array_equal(out[k], getattr(w.polys, k))
+    data, off = syn.wkb_points(w.px, w.py)
+    sz, out = oracle.wkb_decode(data, off)
+    assert sz["n_points"] == w.n_points
+    np.testing.assert_array_equal(out["px"], w.px)
+    np.testing.assert_array_equal(out["py"], w.py)
+
+
+def _bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.int64) if a.dtype == np.float64 else a
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_wkb_fuzz_matches_oracle(ctx, vsabi, oracle, seed):
+    """Device decoder == CPU decoder, bit for bit, on seeded mixes of every
+    encoding, nulls, other types, truncated, corrupted and junk values."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    data, off, valid = W.arrow_layout(W.fuzz_values(rng, 30_000))
+    sz_o, out_o = oracle.wkb_decode(data, off, valid)
+    dev = torch.device("cuda", 0)
+    sz_d, out_d = vsabi.wkb_decode(ctx, torch.from_numpy(data).to(dev), torch.from_numpy(off).to(dev),
+                                   torch.from_numpy(valid).to(dev))
+    assert sz_d == sz_o
+    for k, v in out_o.items():
+        np.testing.assert_array_equal(_bits(out_d[k].cpu().numpy()), _bits(v), err_msg=k)
+
+
+@pytest.mark.gpu
+def test_wkb_synthetic_columns_match_oracle(ctx, vsabi, oracle):
+    """Large single-encoding columns (the ingest benchmark's layout)."""
+    import torch
+
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.zipf_join(seed=3, n_points=2_000_000, n_polys=100_000)
+    dev = torch.device("cuda", 0)
+    for data, off in (syn.wkb_polygons(w.polys), syn.wkb_points(w.px, w.py)):
+        sz_o, out_o = oracle.wkb_decode(data, off)
+        sz_d, out_d = vsabi.wkb_decode(ctx, torch.from_numpy(data).to(dev), torch.from_numpy(off).to(dev))
+        assert sz_d == sz_o
+        for k, v in out_o.items():
+            np.testing.assert_array_equal(_bits(out_d[k].cpu().numpy()), _bits(v), err_msg=k)
+
+
 @pytest.mark.gpu
 def test_wkb_golden_points():
     ga = vio.from_wkb([bytes.fromhex(h) for h, _ in GOLDEN])

@@ -28,6 +28,7 @@ EXPORTED = (
     "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
     "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free", "vs_join_host",
+    "vs_thread_kernel_launches",
 )
 
 
@@ -139,6 +140,7 @@ def load(path: Path | str | None = None):
         sig = {
             "vs_version": (ctypes.c_int, []),
             "vs_last_error": (ctypes.c_char_p, []),
+            "vs_thread_kernel_launches": (ctypes.c_longlong, []),
             "vs_context_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(vp)]),
             "vs_context_destroy": (ctypes.c_int, [vp]),
             "vs_context_synchronize": (ctypes.c_int, [vp]),
@@ -160,7 +162,8 @@ def load(path: Path | str | None = None):
             "vs_batch_run": (ctypes.c_int, [vp, i32, vp, vp, i64, i32, ctypes.POINTER(i64),
                                             ctypes.POINTER(JoinStats)]),
             "vs_batch_plan_free": (ctypes.c_int, [vp]),
-            "vs_wkb_plan_create": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.POINTER(vp), ctypes.POINTER(WkbSizes)]),
+            "vs_wkb_plan_create": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.POINTER(WkbOut), ctypes.POINTER(vp),
+                                                  ctypes.POINTER(WkbSizes)]),
             "vs_wkb_plan_decode": (ctypes.c_int, [vp, ctypes.POINTER(WkbOut)]),
             "vs_wkb_plan_free": (ctypes.c_int, [vp]),
             "vs_join_host": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i32, i32, u32, vp, vp, i64, ctypes.POINTER(i64),
@@ -414,18 +417,19 @@ def wkb_decode(ctx: Context, data, offsets, valid=None):
     import torch
 
     n = int(offsets.numel()) - 1
+    dev = offsets.device
+    out = dict(tags=torch.empty(n, dtype=torch.int8, device=dev),
+               px=torch.empty(n, dtype=torch.float64, device=dev),
+               py=torch.empty(n, dtype=torch.float64, device=dev),
+               geom_off=torch.empty(n + 1, dtype=torch.int32, device=dev))
+    rows = WkbOut(_ptr(out["tags"]), _ptr(out["px"]), _ptr(out["py"]), _ptr(out["geom_off"]), None, None, None, None)
     sizes = WkbSizes()
     h = ctypes.c_void_p()
-    check(load().vs_wkb_plan_create(ctx.handle, _ptr(data), _ptr(offsets), _ptr(valid), n, ctypes.byref(h),
-                                    ctypes.byref(sizes)))
+    check(load().vs_wkb_plan_create(ctx.handle, _ptr(data), _ptr(offsets), _ptr(valid), n, ctypes.byref(rows),
+                                    ctypes.byref(h), ctypes.byref(sizes)))
     try:
-        dev = offsets.device
         sz = sizes.as_dict()
-        out = dict(tags=torch.empty(n, dtype=torch.int8, device=dev),
-                   px=torch.empty(n, dtype=torch.float64, device=dev),
-                   py=torch.empty(n, dtype=torch.float64, device=dev),
-                   geom_off=torch.empty(n + 1, dtype=torch.int32, device=dev),
-                   part_off=torch.empty(sz["n_parts"] + 1, dtype=torch.int32, device=dev),
+        out.update(part_off=torch.empty(sz["n_parts"] + 1, dtype=torch.int32, device=dev),
                    ring_off=torch.empty(sz["n_rings"] + 1, dtype=torch.int32, device=dev),
                    x=torch.empty(sz["n_coords"], dtype=torch.float64, device=dev),
                    y=torch.empty(sz["n_coords"], dtype=torch.float64, device=dev))
@@ -434,6 +438,26 @@ def wkb_decode(ctx: Context, data, offsets, valid=None):
         return sz, out
     finally:
         load().vs_wkb_plan_free(h)
+
+
+def wkb_plan_sizes(ctx: Context, data, offsets, valid, rows) -> dict:
+    """Only the plan step of a WKB decode (the size pass): fills the row
+    outputs ``rows`` (dict of CUDA tensors tags, px, py, geom_off) and returns
+    the sizes; the plan is freed without decoding."""
+    n = int(offsets.numel()) - 1
+    o = WkbOut(_ptr(rows["tags"]), _ptr(rows["px"]), _ptr(rows["py"]), _ptr(rows["geom_off"]), None, None, None,
+               None)
+    sizes = WkbSizes()
+    h = ctypes.c_void_p()
+    check(load().vs_wkb_plan_create(ctx.handle, _ptr(data), _ptr(offsets), _ptr(valid), n, ctypes.byref(o),
+                                    ctypes.byref(h), ctypes.byref(sizes)))
+    load().vs_wkb_plan_free(h)
+    return sizes.as_dict()
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched from this thread so far."""
+    return int(load().vs_thread_kernel_launches())
 
 
 def locate_aligned(ctx: Context, pts: Points, polys: Polygons, out) -> None:

@@ -118,6 +118,8 @@ int vs_version(void) { return VSJOIN_ABI_VERSION; }
 
 const char* vs_last_error(void) { return g_err; }
 
+long long vs_thread_kernel_launches(void) { return g_launches; }
+
 int vs_context_create(int device, void* stream, vs_context** out) {
     if (!out) {
         set_error("out is NULL");

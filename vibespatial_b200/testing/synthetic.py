@@ -317,3 +317,73 @@ WORKLOADS = {
     "zipf": zipf_join,
     "degenerate": degenerate_join,
 }
+
+
+def wkb_points(x: np.ndarray, y: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Little-endian 2D WKB Points (21 bytes each), vectorised: (bytes uint8, offsets int64)."""
+    n = len(x)
+    rec = np.empty((n, 21), dtype=np.uint8)
+    rec[:, 0] = 1
+    rec[:, 1:5] = np.frombuffer(np.uint32(1).tobytes(), np.uint8)
+    rec[:, 5:13] = np.ascontiguousarray(x, dtype="<f8").view(np.uint8).reshape(n, 8)
+    rec[:, 13:21] = np.ascontiguousarray(y, dtype="<f8").view(np.uint8).reshape(n, 8)
+    return rec.reshape(-1), np.arange(n + 1, dtype=np.int64) * 21
+
+
+def wkb_polygons(p: PolygonSoA) -> tuple[np.ndarray, np.ndarray]:
+    """Little-endian 2D WKB of single-part polygons (MultiPolygon rows become MultiPolygons), vectorised."""
+    geom_off = np.asarray(p.geom_off, np.int64)
+    part_off = np.asarray(p.part_off, np.int64)
+    ring_off = np.asarray(p.ring_off, np.int64)
+    n = len(geom_off) - 1
+    nparts = np.diff(geom_off)
+    multi = nparts != 1
+    rings_per_part = np.diff(part_off)
+    pts_per_ring = np.diff(ring_off)
+    # bytes: row header 5 (+4 part count for multi); per part header 5 (multi only) + 4 ring count;
+    # per ring 4 + 16 * points
+    ring_bytes = 4 + 16 * pts_per_ring
+    part_bytes = 4 + np.add.reduceat(ring_bytes, part_off[:-1]) if len(ring_bytes) else np.zeros(0, np.int64)
+    part_bytes = np.where(rings_per_part > 0, part_bytes, 4)
+    part_row = np.repeat(np.arange(n), nparts)
+    part_hdr = np.where(multi[part_row], 5, 0)
+    row_bytes = 5 + 4 * multi + np.bincount(part_row, weights=part_bytes + part_hdr, minlength=n).astype(np.int64)
+    offsets = np.concatenate([[0], np.cumsum(row_bytes)])
+    out = np.zeros(offsets[-1], dtype=np.uint8)
+    u32 = lambda v: np.frombuffer(np.asarray(v, "<u4").tobytes(), np.uint8).reshape(-1, 4)  # noqa: E731
+
+    def put_u32(pos, vals):
+        b = u32(vals)
+        for k in range(4):
+            out[pos + k] = b[:, k]
+
+    out[offsets[:-1]] = 1
+    put_u32(offsets[:-1] + 1, np.where(multi, 6, 3))
+    put_u32(offsets[:-1][multi] + 5, nparts[multi])
+    # part starts
+    part_rank = np.arange(len(part_row)) - geom_off[part_row]
+    part_start_in_row = np.zeros(len(part_row), np.int64)
+    if len(part_row):
+        cum = np.cumsum(part_bytes + part_hdr) - (part_bytes + part_hdr)
+        part_start_in_row = cum - cum[geom_off[part_row]] if len(cum) else cum
+    part_pos = offsets[:-1][part_row] + 5 + 4 * multi[part_row] + part_start_in_row
+    mp = multi[part_row]
+    out[part_pos[mp]] = 1
+    put_u32(part_pos[mp] + 1, np.full(mp.sum(), 3))
+    ring_count_pos = part_pos + part_hdr
+    put_u32(ring_count_pos, rings_per_part)
+    # rings
+    ring_part = np.repeat(np.arange(len(rings_per_part)), rings_per_part)
+    cum_r = np.cumsum(ring_bytes) - ring_bytes
+    ring_start_in_part = cum_r - cum_r[part_off[ring_part]] if len(cum_r) else cum_r
+    ring_pos = ring_count_pos[ring_part] + 4 + ring_start_in_part
+    put_u32(ring_pos, pts_per_ring)
+    coord_ring = np.repeat(np.arange(len(pts_per_ring)), pts_per_ring)
+    k = np.arange(len(p.x)) - ring_off[coord_ring]
+    cpos = ring_pos[coord_ring] + 4 + 16 * k
+    xb = np.ascontiguousarray(p.x, "<f8").view(np.uint8).reshape(-1, 8)
+    yb = np.ascontiguousarray(p.y, "<f8").view(np.uint8).reshape(-1, 8)
+    for b in range(8):
+        out[cpos + b] = xb[:, b]
+        out[cpos + 8 + b] = yb[:, b]
+    return out, offsets
