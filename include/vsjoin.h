@@ -174,6 +174,34 @@ int vs_join(vs_context* ctx, const vs_index* index, const vs_points* pts, int32_
             int32_t method, uint32_t flags, int32_t* d_left, int32_t* d_right, int64_t capacity,
             int64_t* n_pairs, vs_join_stats* stats);
 
+/* Pairs within a distance: (point row, polygon row) with
+ * distance(point, polygon) <= d.  Replaces the reference's dwithin query
+ * (query_spatial_index with predicate 'dwithin', src/vibespatial/spatial/query.py:663-810:
+ * expanded-bounds candidates + _dwithin_refine_gpu, spatial/nearest.py:2855).
+ * distance(point, polygon) is 0 when the point is inside or on the polygon
+ * (exact location) and otherwise the smallest point-segment distance over all
+ * rings (comp.graphics.algorithms FAQ method, each operation rounded
+ * separately); a pair whose envelope distance exceeds d is rejected first.
+ * d is d_point_distance[point row] (device, n points), or
+ * d_geom_distance[polygon row] (device, polygon rows), or `distance` when
+ * both are NULL; negative or NaN distances match nothing.  Pairs, capacity,
+ * VS_JOIN_SORT and the VS_E_CAPACITY contract as for vs_join. */
+int vs_join_dwithin(vs_context* ctx, const vs_index* index, const vs_points* pts,
+                    const double* d_point_distance, const double* d_geom_distance, double distance,
+                    uint32_t flags, int32_t* d_left, int32_t* d_right, int64_t capacity,
+                    int64_t* n_pairs, vs_join_stats* stats);
+
+/* Nearest polygons of every point, all ties: for each valid point, every
+ * polygon at its minimum distance (same distance as vs_join_dwithin), if that
+ * minimum is <= max_distance (INFINITY: unbounded; negative: no pairs).
+ * Replaces sjoin_nearest's query (src/vibespatial/api/tools/sjoin.py
+ * sjoin_nearest -> query_nearest, src/vibespatial/spatial/nearest.py).
+ * d_distance (device, capacity entries, nullable) receives each pair's
+ * distance.  Pairs, capacity, VS_JOIN_SORT and VS_E_CAPACITY as for vs_join. */
+int vs_join_nearest(vs_context* ctx, const vs_index* index, const vs_points* pts, double max_distance,
+                    uint32_t flags, int32_t* d_left, int32_t* d_right, double* d_distance,
+                    int64_t capacity, int64_t* n_pairs, vs_join_stats* stats);
+
 /* vs_join on HOST buffers: h_x / h_y / h_valid (n points; pinned memory lets
  * the copies run asynchronously) in, (left, right) pairs into h_left /
  * h_right (capacity entries each) out.  The points are streamed in chunks

@@ -11,6 +11,10 @@ predicate, the reference's point location:
 * polygon/multipolygon -- src/vibespatial/predicates/point_relations_kernels.py:37-96
 * predicate mapping    -- src/vibespatial/predicates/point_relations.py:100-130
 
+``oracle/distance.c`` restates the distance joins (dwithin with the
+reference's distance <= threshold refine, src/vibespatial/spatial/nearest.py:2855
+and point_distance_kernels.py:238-310; nearest with all ties) by brute force.
+
 ``oracle/wkb.c`` restates the reference's staged WKB decode
 (src/vibespatial/io/wkb.py:3755-3781 header scan, :3954 and :4043 payload
 walks) as the checker of the device WKB decoder.
@@ -52,7 +56,7 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 def build(force: bool = False) -> Path:
     """Compile ``liboracle.so`` with the committed Makefile."""
-    srcs = [_HERE / "exact_pip.c", _HERE / "wkb.c"]
+    srcs = [_HERE / "exact_pip.c", _HERE / "wkb.c", _HERE / "distance.c"]
     if force or not _LIB_PATH.exists() or any(_LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(_HERE), "-s"], check=True)
     return _LIB_PATH
@@ -88,6 +92,21 @@ def lib():
         L.orc_wkb_fill.restype = None
         L.orc_wkb_fill.argtypes = [_u8p, _i64p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int8), _i64p, _i32p, _i32p,
                                    _i32p, _dp, _dp, ctypes.c_int]
+        L.orc_point_polygon_distance.restype = ctypes.c_double
+        L.orc_point_polygon_distance.argtypes = [ctypes.c_double, ctypes.c_double, _dp, _dp, _i32p, _i32p, _i32p,
+                                                 ctypes.c_int64]
+        L.orc_dwithin_join.restype = ctypes.c_void_p
+        L.orc_dwithin_join.argtypes = [_dp, _dp, _u8p, ctypes.c_int64, _dp, _dp, _i32p, _i32p, _i32p, _u8p,
+                                       ctypes.c_int64, _dp, _dp, ctypes.c_double, ctypes.c_int]
+        L.orc_nearest_join.restype = ctypes.c_void_p
+        L.orc_nearest_join.argtypes = [_dp, _dp, _u8p, ctypes.c_int64, _dp, _dp, _i32p, _i32p, _i32p, _u8p,
+                                       ctypes.c_int64, ctypes.c_double, ctypes.c_int]
+        L.orc_dpairs_count.restype = ctypes.c_int64
+        L.orc_dpairs_count.argtypes = [ctypes.c_void_p]
+        L.orc_dpairs_copy.restype = None
+        L.orc_dpairs_copy.argtypes = [ctypes.c_void_p, _i32p, _i32p, _dp]
+        L.orc_dpairs_free.restype = None
+        L.orc_dpairs_free.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -205,6 +224,46 @@ def wkb_decode(data, offsets, valid=None, threads: int = 0):
                    _p(out["geom_off"], _i32p), _p(out["part_off"], _i32p), _p(out["ring_off"], _i32p),
                    _p(out["x"], _dp), _p(out["y"], _dp), threads)
     return sz, out
+
+
+def _dpairs(h):
+    L = lib()
+    try:
+        n = L.orc_dpairs_count(h)
+        left = np.empty(n, dtype=np.int32)
+        right = np.empty(n, dtype=np.int32)
+        dist = np.empty(n, dtype=np.float64)
+        if n:
+            L.orc_dpairs_copy(h, _p(left, _i32p), _p(right, _i32p), _p(dist, _dp))
+    finally:
+        L.orc_dpairs_free(h)
+    return left, right, dist
+
+
+def point_polygon_distance(px: float, py: float, polys: Polygons, g: int) -> float:
+    return float(lib().orc_point_polygon_distance(float(px), float(py), *polys.args(), int(g)))
+
+
+def dwithin_join(px, py, pvalid, polys: Polygons, distance=0.0, *, point_distance=None, geom_distance=None,
+                 threads: int = 0):
+    """Sorted (point row, polygon row, distance) with distance <= the threshold
+    (per point, per polygon or the scalar ``distance``)."""
+    px, py, pvalid = _f64(px), _f64(py), _u8(pvalid)
+    dp = None if point_distance is None else _f64(point_distance)
+    dg = None if geom_distance is None else _f64(geom_distance)
+    h = lib().orc_dwithin_join(_p(px, _dp), _p(py, _dp), _p(pvalid, _u8p), len(px), *polys.args(),
+                               _p(polys.valid, _u8p), len(polys), _p(dp, _dp), _p(dg, _dp), float(distance),
+                               int(threads))
+    return _dpairs(h)
+
+
+def nearest_join(px, py, pvalid, polys: Polygons, max_distance=float("inf"), threads: int = 0):
+    """Sorted (point row, polygon row, distance): every polygon at each point's
+    minimum distance when that minimum is finite and <= max_distance."""
+    px, py, pvalid = _f64(px), _f64(py), _u8(pvalid)
+    h = lib().orc_nearest_join(_p(px, _dp), _p(py, _dp), _p(pvalid, _u8p), len(px), *polys.args(),
+                               _p(polys.valid, _u8p), len(polys), float(max_distance), int(threads))
+    return _dpairs(h)
 
 
 def max_threads() -> int:

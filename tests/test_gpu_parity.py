@@ -199,6 +199,25 @@ def test_edge_cases(vsabi, ctx, oracle, method):
     assert set(np.unique(gr)) <= {2, 4}
 
 
+@pytest.mark.parametrize("method", ["rtree", "learned", "brute"])
+def test_last_hilbert_cell_with_null_points(vsabi, ctx, oracle, method):
+    """Valid points in the frame's last Hilbert cell (the corner (maxx, miny))
+    sort before every null point even though the sort orders only the top key
+    bits; null points there never match."""
+    polys = S.soa([S.box(0, 0, 1000, 1000), S.box(990, 0, 1000, 10), S.box(0, 990, 10, 1000)])
+    rng = np.random.default_rng(3)
+    k = 4000
+    # half the points inside the last level-12 cell of the frame, interleaved with null points
+    px = np.concatenate([1000 - rng.uniform(0, 0.2, k), rng.uniform(0, 1000, k)])
+    py = np.concatenate([rng.uniform(0, 0.2, k), rng.uniform(0, 1000, k)])
+    pv = (np.arange(2 * k) % 3 != 0).astype(np.uint8)
+    P = oracle_polys(oracle, polys)
+    for predicate in ("intersects", "within"):
+        el, er = oracle.join(px, py, pv, P, predicate)
+        gl, gr, _ = gpu_join(vsabi, ctx, px, py, polys, predicate, METHODS[method], pv)
+        assert_same_pairs(gl, gr, el, er)
+
+
 def test_capacity_error_reports_required_size(vsabi, ctx, oracle):
     import torch
     from vibespatial_b200.testing import synthetic as syn

@@ -38,7 +38,25 @@ def backend(request, monkeypatch, oracle):
             P = oracle.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
             return oracle.locate_aligned(px, py, pv, P)
 
+        def dwithin(points, polygons, distance=0.0, point_distance=None, geom_distance=None):
+            px, py, pv = points.point_buffers()
+            pb = polygons.polygon_buffers()
+            P = oracle.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
+            left, right, _ = oracle.dwithin_join(px, py, pv, P, distance, point_distance=point_distance,
+                                                 geom_distance=geom_distance)
+            return left.astype(np.intp), right.astype(np.intp)
+
+        def nearest(points, polygons, max_distance=None):
+            px, py, pv = points.point_buffers()
+            pb = polygons.polygon_buffers()
+            P = oracle.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
+            md = float("inf") if max_distance is None else max_distance
+            left, right, dist = oracle.nearest_join(px, py, pv, P, md)
+            return left.astype(np.intp), right.astype(np.intp), dist
+
         monkeypatch.setattr(vs_query, "_pairs_backend", pairs)
+        monkeypatch.setattr(vs_query, "_dwithin_backend", dwithin)
+        monkeypatch.setattr(vs_query, "_nearest_backend", nearest)
         monkeypatch.setattr(vs_predicates, "_locate_backend", locate)
     return request.param
 
@@ -242,3 +260,100 @@ def test_sindex_query_return_device(backend):
     # points as the tree: pairs swapped and re-sorted on the device
     r2, t2 = q.sindex.query(tree, predicate="contains", return_device=True)
     assert r2.cpu().tolist() == [0, 0, 1] and t2.cpu().tolist() == [0, 1, 1]
+
+
+# ------------------------------------------------------------ distance joins
+
+def _distance_frames():
+    # unit squares; the second has a hole; points inside, on edges, in the hole and outside
+    polys = vs.GeoDataFrame({"geometry": [vs.box(0, 0, 1, 1),
+                                          vs.Polygon([(3, 0), (6, 0), (6, 3), (3, 3), (3, 0)],
+                                                     [[(4, 1), (4, 2), (5, 2), (5, 1), (4, 1)]]),
+                                          vs.box(10, 10, 11, 11)],
+                             "pid": [10, 11, 12]})
+    pts = vs.GeoDataFrame({"geometry": [vs.Point(0.5, 0.5), vs.Point(2, 0.5), vs.Point(4.5, 1.5), vs.Point(1, 1),
+                                        vs.Point(-3, -4), vs.Point(8, 8)],
+                           "qid": [0, 1, 2, 3, 4, 5]})
+    return pts, polys
+
+
+def test_sjoin_dwithin(backend):
+    pts, polys = _distance_frames()
+    res = vs.sjoin(pts, polys, predicate="dwithin", distance=1.0)
+    # (0.5,0.5) inside square 0; (2,0.5) is 1 from square 0 and 1 from polygon 1; (4.5,1.5) sits in the hole,
+    # 0.5 from the hole's edges; (1,1) on square 0's corner; (-3,-4) is 5 away; (8,8) is sqrt(8) from box 2
+    assert sorted(zip(res.index, res["index_right"])) == [(0, 0), (1, 0), (1, 1), (2, 1), (3, 0)]
+    res = vs.sjoin(pts, polys, predicate="dwithin", distance=5.0)
+    assert (4, 0) in set(zip(res.index, res["index_right"]))
+    # per-row distances (one per left row)
+    d = np.array([0.0, 0.5, 0.5, 0.0, 4.999999, 2.9])
+    res = vs.sjoin(pts, polys, predicate="dwithin", distance=d)
+    assert sorted(zip(res.index, res["index_right"])) == [(0, 0), (2, 1), (3, 0), (5, 2)]
+    # polygons on the left: one distance per polygon row
+    res = vs.sjoin(polys, pts, predicate="dwithin", distance=np.array([0.0, 0.5, 3.0]))
+    assert sorted(zip(res.index, res["index_right"])) == [(0, 0), (0, 3), (1, 2), (2, 5)]
+    with pytest.raises(ValueError):
+        vs.sjoin(pts, polys, predicate="dwithin")
+    with pytest.raises(ValueError):
+        vs.sjoin(pts, polys, predicate="dwithin", distance=np.ones(3))
+    with pytest.raises(ValueError):
+        vs.sjoin(pts, polys, predicate="intersects", distance=1.0)
+    # negative / NaN distances match nothing
+    assert vs.sjoin(pts, polys, predicate="dwithin", distance=-1.0).empty
+    assert vs.sjoin(pts, polys, predicate="dwithin", distance=np.full(6, np.nan)).empty
+    # sindex.query with dwithin
+    tree = polys.geometry.array
+    q = pts.geometry.array
+    r = tree.sindex.query(q, predicate="dwithin", distance=1.0)
+    assert r[0].tolist() == [0, 1, 1, 2, 3] and r[1].tolist() == [0, 0, 1, 1, 0]
+
+
+def test_sjoin_nearest(backend):
+    pts, polys = _distance_frames()
+    res = vs.sjoin_nearest(pts, polys, distance_col="dist")
+    # (2, 0.5) ties: 1.0 from square 0 and from polygon 1
+    got = sorted(zip(res.index, res["index_right"], res["dist"]))
+    assert got == [(0, 0, 0.0), (1, 0, 1.0), (1, 1, 1.0), (2, 1, 0.5), (3, 0, 0.0), (4, 0, 5.0),
+                   (5, 2, np.sqrt(8.0))]
+    assert list(res.columns) == ["geometry", "qid", "index_right", "pid", "dist"]
+    # max_distance: the far points drop out (inner) or keep NaN (left)
+    inner = vs.sjoin_nearest(pts, polys, max_distance=1.0, distance_col="dist")
+    assert sorted(set(inner.index)) == [0, 1, 2, 3]
+    left = vs.sjoin_nearest(pts, polys, how="left", max_distance=1.0, distance_col="dist")
+    # five matched rows (point 1 ties) + the two unmatched points
+    assert left.shape[0] == 7 and np.isnan(left.loc[4, "dist"]) and np.isnan(left.loc[5, "index_right"])
+    # how='right': the right frame's points get their nearest left polygons
+    right = vs.sjoin_nearest(polys, pts, how="right", distance_col="dist")
+    assert sorted(zip(right["index_left"], right.index)) == [(0, 0), (0, 1), (0, 3), (0, 4), (1, 1), (1, 2), (2, 5)]
+    assert list(right.columns) == ["index_left", "pid", "geometry", "qid", "dist"]
+    with pytest.raises(NotImplementedError):
+        vs.sjoin_nearest(polys, pts)
+    with pytest.raises(ValueError):
+        vs.sjoin_nearest(pts, polys, max_distance=-1)
+    # the method form
+    assert pts.sjoin_nearest(polys).shape == vs.sjoin_nearest(pts, polys).shape
+
+
+def test_sjoin_nearest_cities_countries(backend):
+    # tests/upstream/geopandas/tools/tests/test_sjoin.py:1355-1382: every city gets exactly one country,
+    # inner == left, and max_distance=1 keeps exactly the rows with dist < 1
+    w = dict(np.load(GOLDEN / "naturalearth_lowres.npz"))
+    c = dict(np.load(GOLDEN / "naturalearth_cities.npz"))
+    countries = vs.GeoDataFrame({"country": w["attr_name"]},
+                                geometry=GeometryArray.from_polygon_buffers(w["x"], w["y"], w["ring_off"],
+                                                                            w["part_off"], w["geom_off"],
+                                                                            geom_type=w["geom_type"]))
+    cities = vs.GeoDataFrame({"name": c["attr_name"]}, geometry=vs.points_from_xy(c["x"], c["y"]))
+    r1 = vs.sjoin_nearest(cities, countries, distance_col="dist")
+    assert r1.shape[0] == cities.shape[0]
+    r3 = vs.sjoin_nearest(cities, countries, distance_col="dist", how="left")
+    assert sorted(zip(r3.index, r3["index_right"])) == sorted(zip(r1.index, r1["index_right"]))
+    r4 = vs.sjoin_nearest(cities, countries, distance_col="dist", max_distance=1)
+    keep = r1[r1["dist"] < 1]
+    assert sorted(zip(r4.index, r4["index_right"])) == sorted(zip(keep.index, keep["index_right"]))
+    r5 = vs.sjoin_nearest(cities, countries, distance_col="dist", max_distance=1, how="left")
+    assert r5.shape[0] == cities.shape[0]
+    # cities inside their country are at distance 0 and agree with the within join
+    within = vs.sjoin(cities, countries, predicate="within")
+    zero = r1[r1["dist"] == 0]
+    assert set(zip(within.index, within["index_right"])) <= set(zip(zero.index, zero["index_right"]))

@@ -19,7 +19,7 @@ from .geometry import (
 )
 from .io import from_wkb, geodataframe_from_arrow, geoseries_from_arrow, read_geoparquet
 from .query import SpatialIndex, query_spatial_index
-from .sjoin import sjoin
+from .sjoin import sjoin, sjoin_nearest
 
 __all__ = [
     "GeoDataFrame",
@@ -38,4 +38,5 @@ __all__ = [
     "read_geoparquet",
     "query_spatial_index",
     "sjoin",
+    "sjoin_nearest",
 ]

@@ -28,7 +28,7 @@ EXPORTED = (
     "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
     "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free", "vs_join_host",
-    "vs_thread_kernel_launches",
+    "vs_thread_kernel_launches", "vs_join_dwithin", "vs_join_nearest",
 )
 
 
@@ -149,6 +149,10 @@ def load(path: Path | str | None = None):
             "vs_index_free": (ctypes.c_int, [vp]),
             "vs_join": (ctypes.c_int, [vp, vp, ctypes.POINTER(Points), i32, i32, u32, vp, vp, i64,
                                        ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
+            "vs_join_dwithin": (ctypes.c_int, [vp, vp, ctypes.POINTER(Points), vp, vp, ctypes.c_double, u32, vp, vp,
+                                               i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
+            "vs_join_nearest": (ctypes.c_int, [vp, vp, ctypes.POINTER(Points), ctypes.c_double, u32, vp, vp, vp,
+                                               i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
             "vs_locate_aligned": (ctypes.c_int, [vp, ctypes.POINTER(Points), ctypes.POINTER(Polygons), vp]),
             "vs_sort_pairs": (ctypes.c_int, [vp, vp, vp, i64]),
             "vs_radix_sort_pairs": (ctypes.c_int, [vp, vp, vp, i64, i32]),
@@ -322,6 +326,66 @@ class DeviceIndex:
                                      cap, ctypes.byref(n), ctypes.byref(st))
         check(status, required=int(n.value))
         return int(n.value), st.as_dict()
+
+    def dwithin_into(self, pts: Points, left, right, *, distance: float = 0.0, point_distance=None,
+                     geom_distance=None, sort: bool = False):
+        """vs_join_dwithin into caller buffers; returns (n_pairs, stats).
+
+        The distance is ``point_distance`` (float64 CUDA tensor, one per
+        point), ``geom_distance`` (one per polygon row) or the scalar
+        ``distance``.  Raises CapacityError (with .required).
+        """
+        n = ctypes.c_int64(0)
+        st = JoinStats()
+        cap = 0 if left is None else int(left.numel())
+        status = load().vs_join_dwithin(self.ctx.handle, self.handle, ctypes.byref(pts), _ptr(point_distance),
+                                        _ptr(geom_distance), float(distance), JOIN_SORT if sort else 0, _ptr(left),
+                                        _ptr(right), cap, ctypes.byref(n), ctypes.byref(st))
+        check(status, required=int(n.value))
+        return int(n.value), st.as_dict()
+
+    def nearest_into(self, pts: Points, left, right, distance=None, *, max_distance: float = float("inf"),
+                     sort: bool = False):
+        """vs_join_nearest into caller buffers (``distance``: float64 CUDA
+        tensor for the pair distances, or None); returns (n_pairs, stats)."""
+        n = ctypes.c_int64(0)
+        st = JoinStats()
+        cap = 0 if left is None else int(left.numel())
+        status = load().vs_join_nearest(self.ctx.handle, self.handle, ctypes.byref(pts), float(max_distance),
+                                        JOIN_SORT if sort else 0, _ptr(left), _ptr(right), _ptr(distance), cap,
+                                        ctypes.byref(n), ctypes.byref(st))
+        check(status, required=int(n.value))
+        return int(n.value), st.as_dict()
+
+    def _grow(self, pts: Points, run, capacity, with_distance=False):
+        import torch
+
+        dev = torch.device("cuda", self.ctx.device)
+        cap = int(capacity) if capacity is not None else max(1024, int(pts.n))
+        for _ in range(2):
+            left = torch.empty(cap, dtype=torch.int32, device=dev)
+            right = torch.empty(cap, dtype=torch.int32, device=dev)
+            dist = torch.empty(cap, dtype=torch.float64, device=dev) if with_distance else None
+            try:
+                n, stats = run(left, right, dist)
+                return left[:n], right[:n], (dist[:n] if dist is not None else None), stats
+            except CapacityError as e:
+                cap = max(e.required, 1)
+        raise RuntimeError("pair buffer sizing did not converge")
+
+    def dwithin(self, pts: Points, *, distance: float = 0.0, point_distance=None, geom_distance=None,
+                sort: bool = True, capacity: int | None = None):
+        """Pairs within the distance, into fresh int32 device tensors (left, right, stats)."""
+        left, right, _, st = self._grow(
+            pts, lambda l, r, d: self.dwithin_into(pts, l, r, distance=distance, point_distance=point_distance,
+                                                   geom_distance=geom_distance, sort=sort), capacity)
+        return left, right, st
+
+    def nearest(self, pts: Points, *, max_distance: float = float("inf"), sort: bool = True,
+                capacity: int | None = None):
+        """Nearest polygons (all ties): (left, right, distance, stats) device tensors."""
+        return self._grow(pts, lambda l, r, d: self.nearest_into(pts, l, r, d, max_distance=max_distance,
+                                                                 sort=sort), capacity, with_distance=True)
 
     def join(self, pts: Points, predicate: int, method: int = METHOD_RTREE, *, sort: bool = True,
              capacity: int | None = None, flags: int = 0):

@@ -114,3 +114,39 @@ def locate_aligned(points, polygons, device: int = 0) -> np.ndarray:
     out = torch.empty(n, dtype=torch.uint8, device=device)
     _abi.locate_aligned(ctx, pts, P, out)
     return out.cpu().numpy()
+
+
+def dwithin_pairs(points, polygons, *, distance=None, point_distance=None, geom_distance=None, method="learned",
+                  device: int = 0, on_device: bool = False):
+    """Sorted (point row, polygon row) pairs with distance(point, polygon) <= the
+    threshold: ``point_distance`` (one per point), ``geom_distance`` (one per
+    polygon) or the scalar ``distance``."""
+    if len(points) == 0 or len(polygons) == 0:
+        if on_device:
+            torch = _torch()
+            e = torch.empty(0, dtype=torch.int32, device=device)
+            return e, e.clone()
+        return np.empty(0, np.intp), np.empty(0, np.intp)
+    torch = _torch()
+    index = polygon_index(polygons, learned=method == "learned", device=device)
+    pts, _ = device_points(points, device)
+    pd_ = None if point_distance is None else _dev(np.asarray(point_distance, np.float64), torch, device)
+    gd_ = None if geom_distance is None else _dev(np.asarray(geom_distance, np.float64), torch, device)
+    left, right, _ = index.dwithin(pts, distance=0.0 if distance is None else float(distance), point_distance=pd_,
+                                   geom_distance=gd_, sort=True)
+    if on_device:
+        return left, right
+    return left.cpu().numpy().astype(np.intp), right.cpu().numpy().astype(np.intp)
+
+
+def nearest_pairs(points, polygons, *, max_distance=None, method="learned", device: int = 0):
+    """Sorted (point row, polygon row, distance): every polygon at each point's
+    minimum distance (within ``max_distance`` when given)."""
+    if len(points) == 0 or len(polygons) == 0:
+        return np.empty(0, np.intp), np.empty(0, np.intp), np.empty(0, np.float64)
+    index = polygon_index(polygons, learned=method == "learned", device=device)
+    pts, _ = device_points(points, device)
+    md = float("inf") if max_distance is None else float(max_distance)
+    left, right, dist, _ = index.nearest(pts, max_distance=md, sort=True)
+    return (left.cpu().numpy().astype(np.intp), right.cpu().numpy().astype(np.intp),
+            dist.cpu().numpy())

@@ -88,26 +88,6 @@ int ensure_defer_capacity(vs_context* ctx, unsigned long long want) {
     return VS_OK;
 }
 
-namespace {
-
-struct EventPair {
-    cudaEvent_t a = nullptr, b = nullptr;
-    EventPair() {
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
-    }
-    ~EventPair() {
-        if (a) cudaEventDestroy(a);
-        if (b) cudaEventDestroy(b);
-    }
-    float ms() {
-        float t = 0.f;
-        cudaEventElapsedTime(&t, a, b);
-        return t;
-    }
-};
-
-}  // namespace
 }  // namespace vs
 
 using namespace vs;

@@ -1,0 +1,577 @@
+// Distance joins of points against the polygon index: dwithin
+// (sjoin(predicate='dwithin'), sindex.query(..., predicate='dwithin')) and
+// nearest (sjoin_nearest).
+//
+// Reference behaviour replaced (src/vibespatial/...):
+//   spatial/query.py:663-810         dwithin: bbox candidates with the query
+//       bounds expanded by the distance, then _dwithin_refine_gpu
+//       (spatial/nearest.py:2855): a distance per candidate pair
+//       (spatial/point_distance_kernels.py:238-310), then distance <= threshold
+//   api/tools/sjoin.py sjoin_nearest -> spatial/nearest.py (query_nearest with
+//       all ties, max_distance, distances)
+//
+// Distance arithmetic.  distance(point, polygon) is 0 when the point is
+// inside or on the polygon (exact location, exact.cuh); otherwise it is the
+// minimum over every ring segment of the point-segment distance of the
+// comp.graphics.algorithms FAQ, the method GEOS's Distance::pointToSegment
+// uses:
+//   A == B            -> |p - A|
+//   r = ((p - A).(B - A)) / |B - A|^2;  r <= 0 -> |p - A|;  r >= 1 -> |p - B|
+//   otherwise         -> |s| * sqrt(|B - A|^2),
+//                        s = ((A.y - p.y)(B.x - A.x) - (A.x - p.x)(B.y - A.y)) / |B - A|^2
+// with |u| = sqrt(u.x^2 + u.y^2).  dwithin first applies the envelope
+// short-circuit (envelope distance > d -> false), then distance <= d.  Every
+// operation is rounded on its own (__dmul_rn, __dadd_rn, ...: no FMA
+// contraction), so an IEEE host evaluating the same expressions without
+// contraction gets the same bits.
+//
+// Candidates come from the packed Hilbert R-tree, walked by warp packets as
+// in the plain join (join.cu) with every point's box inflated by its search
+// radius (rounded outward, plus a relative 2^-30 margin, so no polygon within
+// the radius can be missed); the exact test above decides every candidate.
+//
+// Nearest (all ties): rounds of growing radius over the points still open.
+// A round computes each open point's minimum distance over the candidates
+// within the radius (no candidate of a point can be nearer than its minimum
+// unless it lies outside the radius, so a minimum <= radius is final), then
+// emits, for the points that closed, every candidate at exactly that
+// distance.  Radius: max_distance when given (one round), else a spacing
+// estimate of the polygon frame growing 4x a round, then unbounded.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "emit.cuh"
+#include "exact.cuh"
+#include "index.cuh"
+#include "join.cuh"
+#include "primitives.cuh"
+#include "vs_common.cuh"
+
+namespace vs {
+namespace {
+
+constexpr int kDistThreads = 256;
+constexpr int kDistWarps = kDistThreads / 32;
+constexpr int kDistStack = 112;
+constexpr int kDistMaxStaged = 273;
+constexpr int64_t kDistGrab = 32;
+constexpr int kNearestRounds = 8;  // growing rounds before the unbounded one
+
+enum : int { kDwithin = 0, kNearestMin = 1, kNearestEmit = 2 };
+
+__device__ __forceinline__ double point_point_distance(double px, double py, double ax, double ay) {
+    const double dx = __dsub_rn(px, ax), dy = __dsub_rn(py, ay);
+    return __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+}
+
+__device__ __forceinline__ double point_segment_distance(double px, double py, double ax, double ay, double bx,
+                                                         double by) {
+    if (ax == bx && ay == by) return point_point_distance(px, py, ax, ay);
+    const double ux = __dsub_rn(bx, ax), uy = __dsub_rn(by, ay);
+    const double len2 = __dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy));
+    const double r = __ddiv_rn(__dadd_rn(__dmul_rn(__dsub_rn(px, ax), ux), __dmul_rn(__dsub_rn(py, ay), uy)), len2);
+    if (r <= 0.0) return point_point_distance(px, py, ax, ay);
+    if (r >= 1.0) return point_point_distance(px, py, bx, by);
+    const double s =
+        __ddiv_rn(__dsub_rn(__dmul_rn(__dsub_rn(ay, py), ux), __dmul_rn(__dsub_rn(ax, px), uy)), len2);
+    return __dmul_rn(fabs(s), __dsqrt_rn(len2));
+}
+
+// Distance between the point and a polygon envelope (GEOS Envelope::distance
+// with the point's degenerate envelope).
+__device__ __forceinline__ double envelope_distance(const vs_box& b, double px, double py) {
+    double dx = 0.0, dy = 0.0;
+    if (px < b.minx) dx = __dsub_rn(b.minx, px);
+    else if (px > b.maxx) dx = __dsub_rn(px, b.maxx);
+    if (py < b.miny) dy = __dsub_rn(b.miny, py);
+    else if (py > b.maxy) dy = __dsub_rn(py, b.maxy);
+    if (dx == 0.0) return dy;
+    if (dy == 0.0) return dx;
+    return __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+}
+
+// Minimum segment distance over all rings of slot g; stops early once a
+// segment is within `stop` (the minimum's comparison with `stop` is then
+// already decided).
+__device__ double facet_distance(double px, double py, const double2* __restrict__ xy,
+                                 const int32_t* __restrict__ ring_off, const int32_t* __restrict__ part_off,
+                                 const int32_t* __restrict__ geom_off, int g, double stop) {
+    double best = INFINITY;
+    const int r0 = part_off[geom_off[g]], r1 = part_off[geom_off[g + 1]];
+    for (int ring = r0; ring < r1; ++ring) {
+        const int c0 = ring_off[ring], c1 = ring_off[ring + 1];
+        if (c1 - c0 < 2) continue;
+        double2 a = xy[c0];
+        for (int c = c0 + 1; c < c1; ++c) {
+            const double2 b = xy[c];
+            const double d = point_segment_distance(px, py, a.x, a.y, b.x, b.y);
+            best = d < best ? d : best;
+            if (best <= stop) return best;
+            a = b;
+        }
+    }
+    return best;
+}
+
+struct DistArgs {
+    const double* px;
+    const double* py;
+    const uint32_t* order;   // sorted position -> point row
+    const uint32_t* list;    // positions to visit (nullable: every position below *n_list)
+    const uint32_t* n_list;
+    const vs_box* nodes;
+    int64_t level_off[kMaxLevels];
+    int64_t level_size[kMaxLevels];
+    int levels;
+    int stage_level;
+    int staged;
+    const int32_t* item_geom;
+    const int32_t* geom_off;
+    const int32_t* part_off;
+    const int32_t* ring_off;
+    const double2* xy;
+    RingIndex rings;
+    const double* dist_pt;    // dwithin: per point row (nullable)
+    const double* dist_geom;  // dwithin: per polygon row (nullable)
+    double dist_scalar;       // dwithin: the distance, or the largest per-polygon one
+    double radius;            // nearest, min pass: this round's radius
+    double* best;             // nearest: per point row minimum distance
+    PairSink sink;
+    unsigned long long* counters;
+    unsigned long long* work;
+};
+
+// Search radius rounded outward with a relative margin: a polygon whose
+// computed distance is within q has its envelope within inflate(q).
+__device__ __forceinline__ double inflate(double q) {
+    return __dadd_ru(__dadd_ru(q, __dmul_ru(q, 0x1p-30)), 0x1p-1000);
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs a) {
+    extern __shared__ vs_box s_nodes[];
+    __shared__ int2 s_buf[kDistWarps][kWarpBuf];
+    __shared__ unsigned s_cnt[kDistWarps];
+    __shared__ int s_stack[kDistWarps][kDistStack];
+    __shared__ vs_box s_items[kDistWarps][kFanout];
+    const int64_t stage_base = a.level_off[a.stage_level];
+    for (int k = threadIdx.x; k < a.staged; k += blockDim.x) s_nodes[k] = a.nodes[stage_base + k];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncthreads();
+    const WarpOut out{s_buf[warp], &s_cnt[warp]};
+    const unsigned lt = (1u << lane) - 1u;
+    const int top = a.levels - 1;
+    const int64_t n = (int64_t)*a.n_list;
+    unsigned long long n_cand = 0;
+    unsigned n_exact = 0;
+    for (;;) {
+        const int64_t b0 = warp_grab(a.work, kDistGrab);
+        if (b0 >= n) break;
+        const int64_t i = b0 + lane;
+        bool active = i < n;
+        double x = 0.0, y = 0.0, q = 0.0;
+        int32_t row = -1;
+        if (active) {
+            const uint32_t pos = a.list ? a.list[i] : (uint32_t)i;
+            row = (int32_t)a.order[pos];
+            x = a.px[row];
+            y = a.py[row];
+            if (kMode == kDwithin) q = a.dist_pt ? a.dist_pt[row] : a.dist_scalar;
+            else if (kMode == kNearestMin) q = a.radius;
+            else q = a.best[row];
+            // a negative or NaN radius matches nothing; nearest emits only finite minima
+            active = q >= 0.0 && (kMode != kNearestEmit || q < INFINITY);
+        }
+        const double qi = active ? inflate(q) : 0.0;
+        const double lx0 = active ? __dsub_rd(x, qi) : INFINITY, lx1 = active ? __dadd_ru(x, qi) : -INFINITY;
+        const double ly0 = active ? __dsub_rd(y, qi) : INFINITY, ly1 = active ? __dadd_ru(y, qi) : -INFINITY;
+        double x0 = lx0, x1 = lx1, y0 = ly0, y1 = ly1;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            x0 = fmin(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+            x1 = fmax(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+            y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+            y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+        }
+        double my_best = INFINITY;  // nearest, min pass
+        int sp = 0;
+        if (__any_sync(0xffffffffu, active)) {
+            if (lane == 0) s_stack[warp][0] = top;
+            sp = 1;
+        }
+        __syncwarp();
+        while (sp > 0) {
+            --sp;
+            const int e = s_stack[warp][sp];
+            __syncwarp();
+            const int cl = e & 15;
+            const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
+            // the root level has one node; below it 16 children per node
+            const bool root = cl == top;
+            const bool in_range = root ? lane == 0 : (lane < kFanout && c < a.level_size[cl]);
+            const int64_t cc = root ? 0 : c;
+            vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
+            if (in_range)
+                b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + cc] : a.nodes[a.level_off[cl] + cc];
+            const bool hit = in_range && b.minx <= x1 && b.maxx >= x0 && b.miny <= y1 && b.maxy >= y0;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (cl > 0) {
+                // push the hit nodes' children blocks: node cc of level cl owns block cc of level cl - 1
+                if (hit) {
+                    const int pos = sp + __popc(m & lt);
+                    if (pos < kDistStack) s_stack[warp][pos] = (int)(cc << 4) | (cl - 1);
+                }
+                int add = __popc(m);
+                if (sp + add > kDistStack) {
+                    if (lane == 0) atomicOr(&a.counters[4], 1ull);
+                    add = kDistStack - sp;
+                }
+                sp += add;
+                __syncwarp();
+            } else {
+                if (lane < kFanout) s_items[warp][lane] = b;
+                __syncwarp();
+                unsigned mm = m;
+                const int64_t slot0 = root ? 0 : (int64_t)(e >> 4) * kFanout;
+                while (mm) {
+                    const int j = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    const vs_box ib = s_items[warp][j];
+                    const int slot = (int)(slot0 + j);
+                    bool want = false;
+                    if (active && ib.minx <= lx1 && ib.maxx >= lx0 && ib.miny <= ly1 && ib.maxy >= ly0) {
+                        ++n_cand;
+                        if (kMode == kDwithin) {
+                            const double d = a.dist_geom ? a.dist_geom[a.item_geom[slot]] : q;
+                            if (d >= 0.0 && !(envelope_distance(ib, x, y) > d)) {
+                                const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off,
+                                                                  slot, a.rings, n_exact);
+                                want = loc != LOC_OUTSIDE ||
+                                       facet_distance(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, d) <= d;
+                            }
+                        } else {
+                            const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot,
+                                                              a.rings, n_exact);
+                            const double d =
+                                loc != LOC_OUTSIDE
+                                    ? 0.0
+                                    : facet_distance(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, -1.0);
+                            if (kMode == kNearestMin) my_best = d < my_best ? d : my_best;
+                            else want = d == q;
+                        }
+                    }
+                    if (kMode != kNearestMin) wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                }
+                __syncwarp();
+            }
+        }
+        if (kMode == kNearestMin && active) a.best[row] = my_best;
+        if (kMode != kNearestMin) wflush(out, a.sink, false);
+    }
+    if (kMode != kNearestMin) wflush(out, a.sink, true);
+    add_counter(a.counters, 5, n_cand);
+    add_counter(a.counters, 1, n_exact);
+}
+
+// Open points of a nearest round: done (minimum within the radius and within
+// max_distance) or still open (another round follows).
+__global__ void nearest_classify_kernel(const uint32_t* __restrict__ list, int64_t m,
+                                        const uint32_t* __restrict__ order, const double* __restrict__ best,
+                                        double radius, double max_distance, bool last, uint32_t* __restrict__ done,
+                                        uint32_t* __restrict__ open) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t pos = list ? list[i] : (uint32_t)i;
+        const double b = best[order[pos]];
+        const bool closed = b <= radius;
+        done[i] = closed && b <= max_distance ? 1u : 0u;
+        open[i] = !closed && !last ? 1u : 0u;
+    }
+}
+
+// out[scan[i]] = position i of the list where flag[i] is set (flag == scan
+// difference), keeping the list's order.
+__global__ void compact_positions_kernel(const uint32_t* __restrict__ list, int64_t m,
+                                         const uint32_t* __restrict__ flag, const uint32_t* __restrict__ scan,
+                                         uint32_t* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        if (flag[i]) out[scan[i]] = list ? list[i] : (uint32_t)i;
+}
+
+__global__ void gather_pair_distance_kernel(const int32_t* __restrict__ left, int64_t n,
+                                            const double* __restrict__ best, double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = best[left[i]];
+}
+
+// Largest non-NaN value (as an order-preserving integer; all inputs >= 0 or
+// negative values that never match).
+__global__ void max_distance_kernel(const double* __restrict__ d, int64_t n, unsigned long long* __restrict__ out) {
+    long long m = dbl_to_ordered(-INFINITY);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = d[i];
+        if (v == v) {
+            const long long k = dbl_to_ordered(v);
+            m = k > m ? k : m;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const long long t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<long long*>(out), m);
+}
+
+DistArgs dist_args(vs_context* ctx, const vs_index* idx, const vs_points* pts, const QueryOrder& q, size_t* smem) {
+    DistArgs a{};
+    a.px = pts->d_x;
+    a.py = pts->d_y;
+    a.order = q.order.p;
+    a.nodes = idx->nodes;
+    for (int l = 0; l < kMaxLevels; ++l) {
+        a.level_off[l] = idx->level_off[l];
+        a.level_size[l] = idx->level_size[l];
+    }
+    a.levels = idx->levels;
+    int sl = idx->levels - 1;
+    int64_t staged = idx->level_size[sl];
+    while (sl > 0 && staged + idx->level_size[sl - 1] <= kDistMaxStaged) {
+        --sl;
+        staged += idx->level_size[sl];
+    }
+    a.stage_level = sl;
+    a.staged = (int)staged;
+    a.item_geom = idx->item_geom;
+    a.geom_off = idx->geom_off;
+    a.part_off = idx->part_off;
+    a.ring_off = idx->ring_off;
+    a.xy = idx->xy;
+    a.rings = idx->ring_index();
+    a.counters = ctx->d_counters;
+    a.work = &ctx->d_counters[kWorkCounter];
+    *smem = (size_t)a.staged * sizeof(vs_box);
+    return a;
+}
+
+template <int kMode>
+int launch_dist(vs_context* ctx, const DistArgs& a, size_t smem, int64_t n_items) {
+    cudaStream_t s = ctx->stream;
+    VS_CUDA_TRY(cudaMemsetAsync(&ctx->d_counters[kWorkCounter], 0, sizeof(unsigned long long), s));
+    auto* kernel = dist_join_kernel<kMode>;
+    VS_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kernel<<<resident_grid(kernel, n_items > 0 ? n_items : 1, kDistThreads, smem), kDistThreads, smem, s>>>(a);
+    VS_LAUNCHED(kMode == kDwithin ? "dist_join<dwithin>" : kMode == kNearestMin ? "dist_join<nearest_min>"
+                                                                                : "dist_join<nearest_emit>",
+                s);
+    return VS_OK;
+}
+
+int check_join_args(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t* d_left, int32_t* d_right,
+                    int64_t capacity, int64_t* n_pairs) {
+    if (!ctx || !idx || !n_pairs) {
+        set_error("ctx/index/n_pairs is NULL");
+        return VS_E_ARG;
+    }
+    *n_pairs = 0;
+    VS_TRY(check_points(pts));
+    if (capacity < 0 || (capacity > 0 && (!d_left || !d_right))) {
+        set_error("invalid pair buffers (capacity %lld)", (long long)capacity);
+        return VS_E_ARG;
+    }
+    if (idx->device != ctx->device) {
+        set_error("index lives on device %d, context on device %d", idx->device, ctx->device);
+        return VS_E_ARG;
+    }
+    if (pts->n > 0x7fffffffLL) {
+        set_error("%lld points: more than the 32-bit rows address", (long long)pts->n);
+        return VS_E_ARG;
+    }
+    return VS_OK;
+}
+
+// Counters after the passes: pair count, flags, capacity, stats.
+int finish_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, uint32_t flags, int32_t* d_left,
+                int32_t* d_right, int64_t capacity, int64_t* n_pairs, vs_join_stats* stats, EventPair& ev,
+                long long launches0) {
+    cudaStream_t s = ctx->stream;
+    cudaEventRecord(ev.b, s);
+    VS_CUDA_TRY(cudaMemcpyAsync(ctx->h_counter, ctx->d_counters, 8 * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    const unsigned long long* c = ctx->h_counter;
+    const int64_t n = (int64_t)c[0];
+    *n_pairs = n;
+    if (stats) {
+        stats->exact_fallbacks = (int64_t)c[1];
+        stats->candidates = (int64_t)c[5];
+        stats->kernel_ms = ev.ms();
+        stats->kernel_launches = g_launches - launches0;
+    }
+    if (c[4] != 0) {
+        set_error("device-side consistency check failed (flags 0x%llx)", (unsigned long long)c[4]);
+        return VS_E_STATE;
+    }
+    if (n > capacity) {
+        set_error("pair buffer holds %lld pairs, %lld required", (long long)capacity, (long long)n);
+        return VS_E_CAPACITY;
+    }
+    if ((flags & VS_JOIN_SORT) && n > 1) {
+        EventPair es;
+        cudaEventRecord(es.a, s);
+        VS_TRY(sort_pairs(ctx, d_left, d_right, n, (uint64_t)pts->n, (uint64_t)idx->n_geoms));
+        cudaEventRecord(es.b, s);
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (stats) {
+            stats->sort_ms = es.ms();
+            stats->kernel_launches = g_launches - launches0;
+        }
+    }
+    return VS_OK;
+}
+
+}  // namespace
+}  // namespace vs
+
+using namespace vs;
+
+extern "C" {
+
+int vs_join_dwithin(vs_context* ctx, const vs_index* idx, const vs_points* pts, const double* d_point_distance,
+                    const double* d_geom_distance, double distance, uint32_t flags, int32_t* d_left,
+                    int32_t* d_right, int64_t capacity, int64_t* n_pairs, vs_join_stats* stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    VS_TRY(check_join_args(ctx, idx, pts, d_left, d_right, capacity, n_pairs));
+    if (d_point_distance && d_geom_distance) {
+        set_error("give per-point or per-polygon distances, not both");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    if (pts->n == 0 || idx->n_geoms == 0 || !(idx->h_frame[0] <= idx->h_frame[2])) return VS_OK;
+    cudaStream_t s = ctx->stream;
+    const long long launches0 = g_launches;
+    if (d_geom_distance) {
+        // the candidate search uses the largest per-polygon distance
+        const unsigned long long init = (unsigned long long)host_dbl_to_ordered(-INFINITY);
+        VS_CUDA_TRY(cudaMemcpyAsync(&ctx->d_counters[9], &init, sizeof(init), cudaMemcpyHostToDevice, s));
+        max_distance_kernel<<<resident_grid(max_distance_kernel, idx->n_geoms, 256), 256, 0, s>>>(
+            d_geom_distance, idx->n_geoms, &ctx->d_counters[9]);
+        VS_LAUNCHED("max_distance", s);
+        unsigned long long m = 0;
+        VS_CUDA_TRY(cudaMemcpyAsync(&m, &ctx->d_counters[9], sizeof(m), cudaMemcpyDeviceToHost, s));
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+        long long k = (long long)m;
+        k = k >= 0 ? k : (k ^ 0x7fffffffffffffffLL);
+        memcpy(&distance, &k, sizeof(distance));
+    }
+    EventPair ev;
+    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, kDevCounters * sizeof(unsigned long long), s));
+    cudaEventRecord(ev.a, s);
+    QueryOrder q;
+    VS_TRY(prepare_queries(ctx, idx, pts, q, true));
+    size_t smem = 0;
+    DistArgs a = dist_args(ctx, idx, pts, q, &smem);
+    a.n_list = q.n_valid.p;
+    a.dist_pt = d_point_distance;
+    a.dist_geom = d_geom_distance;
+    a.dist_scalar = distance;
+    a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
+    VS_TRY(launch_dist<kDwithin>(ctx, a, smem, pts->n));
+    return finish_join(ctx, idx, pts, flags, d_left, d_right, capacity, n_pairs, stats, ev, launches0);
+}
+
+int vs_join_nearest(vs_context* ctx, const vs_index* idx, const vs_points* pts, double max_distance, uint32_t flags,
+                    int32_t* d_left, int32_t* d_right, double* d_distance, int64_t capacity, int64_t* n_pairs,
+                    vs_join_stats* stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    VS_TRY(check_join_args(ctx, idx, pts, d_left, d_right, capacity, n_pairs));
+    if (max_distance != max_distance) {
+        set_error("max_distance is NaN");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    if (pts->n == 0 || idx->n_geoms == 0 || !(idx->h_frame[0] <= idx->h_frame[2])) return VS_OK;
+    if (max_distance < 0.0) return VS_OK;
+    cudaStream_t s = ctx->stream;
+    const long long launches0 = g_launches;
+    EventPair ev;
+    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, kDevCounters * sizeof(unsigned long long), s));
+    cudaEventRecord(ev.a, s);
+    QueryOrder q;
+    VS_TRY(prepare_queries(ctx, idx, pts, q, true));
+    uint32_t n_open = 0;
+    VS_CUDA_TRY(cudaMemcpyAsync(&n_open, q.n_valid.p, sizeof(n_open), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    const int64_t n = pts->n;
+    Scratch<double> best;
+    Scratch<uint32_t> lists, flags_buf, scans, counts;
+    VS_TRY(best.alloc((size_t)n, s));
+    // two lists (open, next open) + a done list; flags and scans for two kinds
+    VS_TRY(lists.alloc(3 * (size_t)n, s));
+    VS_TRY(flags_buf.alloc(2 * (size_t)n, s));
+    VS_TRY(scans.alloc(2 * (size_t)n + 2, s));
+    VS_TRY(counts.alloc(4, s));
+    uint32_t* list_a = lists.p;
+    uint32_t* list_b = lists.p + n;
+    uint32_t* done = lists.p + 2 * n;
+    size_t smem = 0;
+    DistArgs a = dist_args(ctx, idx, pts, q, &smem);
+    a.best = best.p;
+    a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
+    const bool bounded = max_distance < INFINITY;
+    // first radius: the spacing of the polygons over their frame
+    const double w = idx->h_frame[2] - idx->h_frame[0], h = idx->h_frame[3] - idx->h_frame[1];
+    double radius = sqrt(fmax(w * h, fmax(w, h) * fmax(w, h) * 1e-6) / (double)idx->n_geoms);
+    if (!(radius > 0.0) || !(radius < INFINITY)) radius = 1.0;
+    if (bounded) radius = max_distance;
+    const uint32_t* open = nullptr;  // null: every sorted position below n_open
+    for (int round = 0; n_open > 0; ++round) {
+        const bool last = bounded || round == kNearestRounds;
+        if (round == kNearestRounds && !bounded) radius = INFINITY;
+        // minimum distance of every open point over its candidates
+        a.list = open;
+        a.n_list = counts.p;
+        VS_CUDA_TRY(cudaMemcpyAsync(counts.p, &n_open, sizeof(n_open), cudaMemcpyHostToDevice, s));
+        a.radius = radius;
+        VS_TRY(launch_dist<kNearestMin>(ctx, a, smem, n_open));
+        // split into done / still open, keeping the sorted order
+        uint32_t* f_done = flags_buf.p;
+        uint32_t* f_open = flags_buf.p + n;
+        nearest_classify_kernel<<<resident_grid(nearest_classify_kernel, n_open, 256), 256, 0, s>>>(
+            open, n_open, q.order.p, best.p, radius, bounded ? max_distance : INFINITY, last, f_done, f_open);
+        VS_LAUNCHED("nearest_classify", s);
+        VS_TRY(exclusive_scan_u32(f_done, scans.p, n_open, counts.p + 1, s));
+        VS_TRY(exclusive_scan_u32(f_open, scans.p + n, n_open, counts.p + 2, s));
+        uint32_t* next = open == list_a ? list_b : list_a;
+        compact_positions_kernel<<<resident_grid(compact_positions_kernel, n_open, 256), 256, 0, s>>>(
+            open, n_open, f_done, scans.p, done);
+        VS_LAUNCHED("compact_positions", s);
+        compact_positions_kernel<<<resident_grid(compact_positions_kernel, n_open, 256), 256, 0, s>>>(
+            open, n_open, f_open, scans.p + n, next);
+        VS_LAUNCHED("compact_positions", s);
+        // every candidate at exactly the minimum, for the points that closed
+        DistArgs e = a;
+        e.list = done;
+        e.n_list = counts.p + 1;
+        VS_TRY(launch_dist<kNearestEmit>(ctx, e, smem, n_open));
+        uint32_t tot[2] = {0, 0};
+        VS_CUDA_TRY(cudaMemcpyAsync(tot, counts.p + 1, sizeof(tot), cudaMemcpyDeviceToHost, s));
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+        n_open = tot[1];
+        open = next;
+        radius *= 4.0;
+    }
+    const int st = finish_join(ctx, idx, pts, flags, d_left, d_right, capacity, n_pairs, stats, ev, launches0);
+    if (st != VS_OK) return st;
+    if (d_distance && *n_pairs > 0) {
+        gather_pair_distance_kernel<<<resident_grid(gather_pair_distance_kernel, *n_pairs, 256), 256, 0, s>>>(
+            d_left, *n_pairs, best.p, d_distance);
+        VS_LAUNCHED("gather_pair_distance", s);
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return VS_OK;
+}
+
+}  // extern "C"

@@ -80,8 +80,10 @@ __device__ __forceinline__ bool box_overlaps(const vs_box& b, double x0, double 
     return b.minx <= x1 && b.maxx >= x0 && b.miny <= y1 && b.maxy >= y0;
 }
 
+// clamp: points outside the frame are keyed at the nearest frame position
+// and kept (distance joins); otherwise they get the sentinel key.
 __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ frame, uint32_t* __restrict__ keys,
-                                      uint32_t* __restrict__ idx, uint32_t* __restrict__ n_valid) {
+                                      uint32_t* __restrict__ idx, uint32_t* __restrict__ n_valid, bool clamp) {
     __shared__ uint16_t s_lut[kHilbertLutSize];
     hilbert_lut_init(s_lut);
     __syncthreads();
@@ -90,12 +92,18 @@ __global__ void point_sort_key_kernel(vs_points p, const double* __restrict__ fr
     const double sy = f3 > f1 ? 4294967295.0 / (f3 - f1) : 0.0;
     uint32_t cnt = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double x = p.d_x[i], y = p.d_y[i];
+        double x = p.d_x[i], y = p.d_y[i];
+        if (clamp && x == x && y == y) {
+            x = fmin(fmax(x, f0), f2);
+            y = fmin(fmax(y, f1), f3);
+        }
         const bool ok = (p.d_valid == nullptr || p.d_valid[i]) && x >= f0 && x <= f2 && y >= f1 && y <= f3;
         uint32_t k = 0xffffffffu;
         if (ok) {
+            // The sort orders the top 24 bits only: keep valid keys out of the
+            // sentinel's top-24 group, so every valid point sorts before it.
             k = hilbert_key_lut(quantize(x, f0, sx), quantize(y, f1, sy), 16, s_lut);
-            if (k == 0xffffffffu) k = 0xfffffffeu;  // keep the sentinel unique
+            if (k > 0xfffffeffu) k = 0xfffffeffu;
         }
         keys[i] = k;
         idx[i] = (uint32_t)i;
@@ -397,14 +405,15 @@ int accept_mask_for(int predicate, int* mask) {
     }
 }
 
-int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q) {
+int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q, bool clamp) {
     cudaStream_t s = ctx->stream;
     const int64_t n = pts->n;
     VS_TRY(q.keys.alloc((size_t)n, s));
     VS_TRY(q.order.alloc((size_t)n, s));
     VS_TRY(q.n_valid.alloc(1, s));
     VS_CUDA_TRY(cudaMemsetAsync(q.n_valid.p, 0, sizeof(uint32_t), s));
-    point_sort_key_kernel<<<resident_grid(point_sort_key_kernel, n, 256), 256, 0, s>>>(*pts, idx->frame, q.keys.p, q.order.p, q.n_valid.p);
+    point_sort_key_kernel<<<resident_grid(point_sort_key_kernel, n, 256), 256, 0, s>>>(*pts, idx->frame, q.keys.p, q.order.p, q.n_valid.p,
+                                                                                   clamp);
     VS_LAUNCHED("point_sort_key", s);
     // Sorting by the top 24 key bits (a level-12 Hilbert cell) already makes
     // a warp's 32 points spatially coherent; the low byte is left unsorted.

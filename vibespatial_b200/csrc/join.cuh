@@ -13,7 +13,9 @@ namespace vs {
 struct QueryOrder {
     Scratch<uint32_t> keys, order, n_valid;
 };
-int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q);
+// clamp: keep points outside the polygon frame (keyed at the frame's edge),
+// as distance joins need them; otherwise they are left out.
+int prepare_queries(vs_context* ctx, const vs_index* idx, const vs_points* pts, QueryOrder& q, bool clamp = false);
 int accept_mask_for(int predicate, int* mask);
 // row_base is added to every emitted or deferred point row (a chunk of a
 // larger point array); the exact pass subtracts it to read the chunk's points.

@@ -152,6 +152,28 @@ struct vs_context {
     vs::HostPipe* host_pipe;
 };
 
+namespace vs {
+// Two events bracketing device work on a stream; ms() after both completed.
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~EventPair() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    EventPair(const EventPair&) = delete;
+    EventPair& operator=(const EventPair&) = delete;
+    float ms() {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        return t;
+    }
+};
+}  // namespace vs
+
 // Record phase boundary k of the current join on the context stream.
 inline void phase_mark(vs_context* ctx, int k) {
     if (ctx->phase_on) cudaEventRecord(ctx->phase_ev[k], ctx->stream);

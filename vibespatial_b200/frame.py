@@ -202,6 +202,13 @@ class GeoDataFrame(pd.DataFrame):
 
         return sjoin(self, df, how=how, predicate=predicate, lsuffix=lsuffix, rsuffix=rsuffix, **kwargs)
 
+    def sjoin_nearest(self, right, how="inner", max_distance=None, lsuffix="left", rsuffix="right",
+                      distance_col=None, exclusive=False, **kwargs):
+        from .sjoin import sjoin_nearest
+
+        return sjoin_nearest(self, right, how=how, max_distance=max_distance, lsuffix=lsuffix, rsuffix=rsuffix,
+                             distance_col=distance_col, exclusive=exclusive, **kwargs)
+
 
 def _geodataframe_or_dataframe(*args, geometry_column=None, **kwargs):
     df = pd.DataFrame(*args, **kwargs)

@@ -27,9 +27,11 @@ _TREE_POINTS = {None: None, "intersects": "intersects", "contains": "within", "c
                 "covers": "covered_by", "touches": "touches", "within": "empty", "covered_by": "empty",
                 "overlaps": "empty", "crosses": "empty"}
 
-# Pair generator: the CUDA join.  Tests of the host logic substitute the CPU
-# oracle here; the package itself never does.
+# Pair generators: the CUDA joins.  Tests of the host logic substitute the
+# CPU oracle here; the package itself never does.
 _pairs_backend = None
+_dwithin_backend = None
+_nearest_backend = None
 
 
 def _pairs(points, polygons, predicate, method, on_device=False):
@@ -44,6 +46,67 @@ def _pairs(points, polygons, predicate, method, on_device=False):
     from ._device import join_pairs
 
     return join_pairs(points, polygons, predicate, method=method, on_device=on_device)
+
+
+def _dwithin(points, polygons, method, on_device=False, **dist):
+    """(point rows, polygon rows) within the distance (``distance``,
+    ``point_distance`` or ``geom_distance``)."""
+    if _dwithin_backend is not None:
+        left, right = _dwithin_backend(points, polygons, **dist)
+        if on_device:
+            import torch
+
+            return (torch.from_numpy(np.asarray(left, np.int32)).cuda(),
+                    torch.from_numpy(np.asarray(right, np.int32)).cuda())
+        return left, right
+    from ._device import dwithin_pairs
+
+    return dwithin_pairs(points, polygons, method=method, on_device=on_device, **dist)
+
+
+def nearest_pairs(points, polygons, *, max_distance=None, method="learned"):
+    """(point rows, polygon rows, distances): every polygon at each point's
+    minimum distance, within ``max_distance`` when given, sorted by (point,
+    polygon).  The query of sjoin_nearest (the reference's query_nearest with
+    all ties, src/vibespatial/spatial/nearest.py)."""
+    if _nearest_backend is not None:
+        return _nearest_backend(points, polygons, max_distance=max_distance)
+    from ._device import nearest_pairs as device_nearest
+
+    return device_nearest(points, polygons, max_distance=max_distance, method=method)
+
+
+def _distance_args(distance, n_geometry, geometry_is_points):
+    """Per-row or scalar threshold for the join: the geometry (input) side
+    owns the per-row values, whichever side holds the points."""
+    if distance is None:
+        raise ValueError("'distance' parameter is required for 'dwithin' predicate")
+    d = np.asarray(distance, dtype=np.float64)
+    if d.ndim == 0:
+        return {"distance": float(d)}
+    if d.shape != (n_geometry,):
+        raise ValueError("Could not broadcast distance array to the number of geometries: "
+                         f"{d.shape} vs ({n_geometry},)")
+    return {"point_distance": d} if geometry_is_points else {"geom_distance": d}
+
+
+def _query_dwithin(tree, geometry, distance, method, on_device):
+    if geometry.is_points() and tree.is_polygonal():
+        return _dwithin(geometry, tree, method, on_device, **_distance_args(distance, len(geometry), True))
+    if geometry.is_polygonal() and tree.is_points():
+        pt, poly = _dwithin(tree, geometry, method, on_device, **_distance_args(distance, len(geometry), False))
+        if on_device:
+            if poly.numel():
+                from ._device import sort_pairs_on_device
+
+                poly, pt = sort_pairs_on_device(poly.contiguous(), pt.contiguous())
+            return poly, pt
+        out = np.vstack([poly, pt]).astype(np.intp)
+        order = np.lexsort((out[1], out[0]))
+        return out[0][order], out[1][order]
+    raise NotImplementedError(
+        "vibespatial_b200 joins points with polygons/multipolygons only "
+        f"(tree families {sorted(tree.families())}, input families {sorted(geometry.families())})")
 
 
 def _query_device(tree, geometry, predicate, method):
@@ -85,10 +148,22 @@ def query_spatial_index(tree, geometry, *, predicate=None, sort=False, distance=
 
     if predicate not in VALID_PREDICATES:
         raise ValueError(f"Got predicate='{predicate}'; `predicate` must be one of {sorted(map(str, VALID_PREDICATES))}")
-    if predicate == "dwithin" or distance is not None:
-        raise NotImplementedError("the dwithin predicate is outside this point-in-polygon join")
+    if distance is not None and predicate != "dwithin":
+        raise ValueError("'distance' parameter is only supported in combination with 'dwithin' predicate")
     if not isinstance(tree, GeometryArray) or not isinstance(geometry, GeometryArray):
         raise TypeError("query_spatial_index expects GeometryArrays")
+    if predicate == "dwithin":
+        if distance is None:
+            raise ValueError("'distance' parameter is required for 'dwithin' predicate")
+        if len(tree) == 0 or len(geometry) == 0:
+            if return_device:
+                import torch
+
+                e = torch.empty(0, dtype=torch.int32, device="cuda")
+                return e, e.clone()
+            return np.empty((2, 0), dtype=np.intp)
+        left, right = _query_dwithin(tree, geometry, distance, method, return_device)
+        return (left, right) if return_device else np.vstack([left, right]).astype(np.intp)
     if return_device:
         return _query_device(tree, geometry, predicate, method)
     empty = np.empty((2, 0), dtype=np.intp)
@@ -118,7 +193,7 @@ def query_spatial_index(tree, geometry, *, predicate=None, sort=False, distance=
 class SpatialIndex:
     """``GeometryArray.sindex``: a reusable index over the array (the tree side)."""
 
-    valid_query_predicates = {p for p in VALID_PREDICATES if p != "dwithin"}
+    valid_query_predicates = set(VALID_PREDICATES)
 
     def __init__(self, geometry):
         self.geometry = geometry

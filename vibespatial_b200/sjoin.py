@@ -98,26 +98,33 @@ def _suffix_overlaps(left_cols, right_cols, lsuffix, rsuffix, lgeom, rgeom):
 
 
 def _adjust_indexers(l_idx, r_idx, n_left, n_right, how):
-    """Row indexers for each ``how`` (-1 = missing row), as GeoPandas builds them."""
+    """Row indexers for each ``how`` (-1 = missing row), as GeoPandas builds
+    them, and for every output row the pair it came from (-1 for an added
+    unmatched row)."""
+    src = np.arange(len(l_idx), dtype=np.intp)
     if how == "inner":
-        return l_idx, r_idx
+        return l_idx, r_idx, src
     if how == "outer":
         counts = np.bincount(l_idx, minlength=n_left) if len(l_idx) else np.zeros(n_left, np.intp)
         repeats = np.maximum(counts, 1)
         out_l = np.repeat(np.arange(n_left, dtype=np.intp), repeats)
         out_r = np.full(len(out_l), -1, dtype=np.intp)
+        out_src = np.full(len(out_l), -1, dtype=np.intp)
         if len(l_idx):
             starts = np.cumsum(repeats) - repeats
             rank = np.arange(len(l_idx)) - np.repeat(np.cumsum(counts) - counts, counts)
             out_r[starts[l_idx] + rank] = r_idx
+            out_src[starts[l_idx] + rank] = src
         matched_right = np.zeros(n_right, dtype=bool)
         matched_right[r_idx] = True
         missing = np.flatnonzero(~matched_right)
-        return (np.concatenate([out_l, np.full(len(missing), -1, np.intp)]),
-                np.concatenate([out_r, missing.astype(np.intp)]))
+        minus = np.full(len(missing), -1, np.intp)
+        return (np.concatenate([out_l, minus]), np.concatenate([out_r, missing.astype(np.intp)]),
+                np.concatenate([out_src, minus]))
     if how == "right":
         order = np.lexsort((l_idx, r_idx))
         l_idx, r_idx = r_idx[order], l_idx[order]  # swapped: the right side drives
+        src = src[order]
         n = n_right
     else:
         n = n_left
@@ -126,9 +133,10 @@ def _adjust_indexers(l_idx, r_idx, n_left, n_right, how):
     ins = np.searchsorted(l_idx, missing)
     l_idx = np.insert(l_idx, ins, missing)
     r_idx = np.insert(r_idx, ins, -1)
+    src = np.insert(src, ins, -1)
     if how == "right":
         l_idx, r_idx = r_idx, l_idx
-    return l_idx, r_idx
+    return l_idx, r_idx, src
 
 
 def _take_rows(df, rows):
@@ -151,7 +159,10 @@ def _take_rows(df, rows):
     return pd.concat(parts, axis=1)
 
 
-def _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attribute):
+def _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attribute, pair_values=None,
+                value_col=None):
+    """The joined frame; ``pair_values`` (one float per pair, e.g. distances)
+    becomes the last column ``value_col``, NaN on unmatched rows."""
     lgeom = left_df.geometry.name
     rgeom = right_df.geometry.name
     if on_attribute:
@@ -174,7 +185,7 @@ def _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attri
     lcols, rcols = _suffix_overlaps(list(left.columns), list(right.columns), lsuffix, rsuffix, lgeom, rgeom)
     left.columns, right.columns = pd.Index(lcols), pd.Index(rcols)
     left_index_cols, right_index_cols = lcols[:left_nlevels], rcols[:right_nlevels]
-    l_idx, r_idx = _adjust_indexers(l_idx, r_idx, len(left), len(right), how)
+    l_idx, r_idx, src = _adjust_indexers(l_idx, r_idx, len(left), len(right), how)
     lpart = _take_rows(left, l_idx)
     rpart = _take_rows(right, r_idx)
     joined = pd.concat([lpart, rpart], axis=1)
@@ -194,6 +205,10 @@ def _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attri
             np.where(pick, np.arange(len(lg)) + len(lg), np.arange(len(lg))))
         joined[lgeom] = pd.Series(merged, index=joined.index)
         geometry, crs = lgeom, left_df.crs
+    if value_col is not None:
+        vals = np.asarray(pair_values, dtype=np.float64)
+        col = np.where(src >= 0, vals[np.maximum(src, 0)] if len(vals) else np.nan, np.nan)
+        joined[value_col] = pd.Series(col, index=joined.index)
     return GeoDataFrame(joined, geometry=geometry, crs=crs)
 
 
@@ -215,3 +230,37 @@ def sjoin(left_df, right_df, how="inner", predicate="intersects", lsuffix="left"
     _basic_checks(left_df, right_df, how, lsuffix, rsuffix, on_attribute=on_attribute)
     l_idx, r_idx = _geom_predicate_query(left_df, right_df, predicate, distance, on_attribute, method)
     return _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attribute)
+
+
+def sjoin_nearest(left_df, right_df, how="inner", max_distance=None, lsuffix="left", rsuffix="right",
+                  distance_col=None, exclusive=False, **kwargs):
+    """Nearest-neighbour join of points with polygons/multipolygons.
+
+    Drop-in for the reference's ``sjoin_nearest``
+    (src/vibespatial/api/tools/sjoin.py:1398): every row of the matched side
+    (the left frame, or the right frame for ``how='right'``) gets every
+    geometry of the other frame at its minimum distance (all ties), within
+    ``max_distance`` when given; ``distance_col`` adds the distances.  The
+    matched side must hold points and the other side polygons (the GPU index
+    is built over the polygons).  ``exclusive`` drops equal geometries, which a
+    point and a polygon never are.
+    """
+    from .query import nearest_pairs
+
+    method = kwargs.pop("method", "learned")
+    if kwargs:
+        first = next(iter(kwargs.keys()))
+        raise TypeError(f"sjoin_nearest() got an unexpected keyword argument '{first}'")
+    _basic_checks(left_df, right_df, how, lsuffix, rsuffix)
+    if max_distance is not None and max_distance < 0:
+        raise ValueError("max_distance must be greater than or equal to 0")
+    query_df, tree_df = (right_df, left_df) if how == "right" else (left_df, right_df)
+    q_geom, t_geom = query_df.geometry.array, tree_df.geometry.array
+    if len(q_geom) and len(t_geom) and not (q_geom.is_points() and t_geom.is_polygonal()):
+        raise NotImplementedError(
+            "sjoin_nearest matches points to their nearest polygons/multipolygons: the "
+            + ("right" if how == "right" else "left") + " frame must hold points and the other one polygons")
+    q_rows, t_rows, dist = nearest_pairs(q_geom, t_geom, max_distance=max_distance, method=method)
+    l_idx, r_idx = (t_rows, q_rows) if how == "right" else (q_rows, t_rows)
+    return _frame_join(left_df, right_df, np.asarray(l_idx, np.intp), np.asarray(r_idx, np.intp), how, lsuffix,
+                       rsuffix, None, pair_values=dist, value_col=distance_col)
