@@ -133,6 +133,9 @@ WORKLOAD_DESC = {
     "degenerate": "degenerate_join: 20M points x 200k polygons with holes/multiparts, on-edge and 1-ulp points",
     "batched": "batched_jobs: 256 independent star joins, points logU[1k,2M] (69.6M total), polygons "
                "logU[10,50k] (1.38M total), one persistent launch replayed from a CUDA graph",
+    "dwithin": "dwithin: zipf_join's 50M FP64 points x 1M footprints, pairs within distance 0.25 (1.7x the median "
+               "footprint side)",
+    "nearest": "nearest (sjoin_nearest, all ties, unbounded): zipf_join's 50M FP64 points x 1M footprints",
     "wkb": "wkb ingest: the zipf_join inputs as little-endian 2D WKB columns (50M Points, 21 B each; 1M Polygons), "
            "decoded on the device into the join's columnar layout",
 }
@@ -412,6 +415,202 @@ def run_wkb(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+DWITHIN_DISTANCE = 0.25
+
+
+def cpu_distance_rate(w, kind: str, threads: int, target_s: float = 10.0):
+    """CPU oracle of the distance join (grid index, all host threads) over
+    consecutive 1M-point chunks until ~target_s; points/sec."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+    chunk = min(w.n_points, 1_000_000)
+    n, dt, start = 0, 0.0, 0
+    while dt < target_s and n < w.n_points:
+        stop = min(start + chunk, w.n_points)
+        t0 = time.perf_counter()
+        if kind == "dwithin":
+            O.dwithin_join(w.px[start:stop], w.py[start:stop], None, P, DWITHIN_DISTANCE, threads=threads)
+        else:
+            O.nearest_join(w.px[start:stop], w.py[start:stop], None, P, threads=threads)
+        dt += time.perf_counter() - t0
+        n += stop - start
+        start = stop
+    return n / dt, n, dt
+
+
+def run_reference_distance(args, world):
+    w = make_workload("zipf", 0, args.scale)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+    n = min(w.n_points, args.ref_sample // 4)
+
+    def step():
+        if args.workload == "dwithin":
+            O.dwithin_join(w.px[:n], w.py[:n], None, P, DWITHIN_DISTANCE, threads=threads)
+        else:
+            O.nearest_join(w.px[:n], w.py[:n], None, P, threads=threads)
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = n * len(times) / tot
+    line = {
+        "impl": "reference", "metric": "query points/sec", "value": value, "unit": "points/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "sample_points": n, "n_polygons": len(w.polys)},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
+                         "sample": f"first {n} of {w.n_points} points vs all {len(w.polys)} polygons, CPU oracle "
+                                   "(C + OpenMP, grid index, same distance arithmetic); Shapely/GEOS is not "
+                                   "installable here"},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_distance(args, rank, world, local_rank):
+    """dwithin / nearest over the zipf inputs through vs_join_dwithin / vs_join_nearest."""
+    import torch
+
+    from vibespatial_b200 import _abi
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    w = make_workload("zipf", rank, args.scale)
+    N = w.n_points
+    ctx = _abi.Context(dev)
+    stream = ctx.torch_stream
+    pol = w.polys
+    d_poly = {k: torch.from_numpy(np.ascontiguousarray(getattr(pol, k))).to(dev)
+              for k in ("x", "y", "ring_off", "part_off", "geom_off")}
+    P = _abi.make_polygons(d_poly["x"], d_poly["y"], d_poly["ring_off"], d_poly["part_off"], d_poly["geom_off"])
+    index = _abi.DeviceIndex(ctx, P, learned=False)
+    dx = torch.from_numpy(w.px).to(dev)
+    dy = torch.from_numpy(w.py).to(dev)
+    pts = _abi.make_points(dx, dy)
+    nearest = args.workload == "nearest"
+    cap = max(1024, 2 * N)
+
+    def alloc(c):
+        return (torch.empty(c, dtype=torch.int32, device=dev), torch.empty(c, dtype=torch.int32, device=dev),
+                torch.empty(c, dtype=torch.float64, device=dev) if nearest else None)
+
+    left, right, dists = alloc(cap)
+
+    def join(l, r, d):
+        if nearest:
+            return index.nearest_into(pts, l, r, d)
+        return index.dwithin_into(pts, l, r, distance=DWITHIN_DISTANCE)
+
+    try:
+        n_pairs, st = join(left, right, dists)
+    except _abi.CapacityError as e:
+        cap = e.required
+        left, right, dists = alloc(cap)
+        n_pairs, st = join(left, right, dists)
+    for _ in range(args.warmup):
+        join(left, right, dists)
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms, launches = [], 0
+    with ClockSampler(dev) as clk:
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            n_k, st = join(left, right, dists)
+            ev[k][1].record(stream)
+            kernel_ms.append(st["kernel_ms"])
+            launches += st["kernel_launches"]
+            assert n_k == n_pairs
+        torch.cuda.synchronize()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        # e2e: points from pinned host memory, pairs (and distances) back to pinned host memory
+        hx = torch.from_numpy(w.px).pin_memory()
+        hy = torch.from_numpy(w.py).pin_memory()
+        hl = torch.empty(n_pairs, dtype=torch.int32).pin_memory()
+        hr = torch.empty(n_pairs, dtype=torch.int32).pin_memory()
+        hd = torch.empty(n_pairs, dtype=torch.float64).pin_memory() if nearest else None
+        e2e_ms = []
+        for k in range(max(3, args.steps) + 1):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            dx.copy_(hx, non_blocking=True)
+            dy.copy_(hy, non_blocking=True)
+            n_e, _ = join(left, right, dists)
+            hl.copy_(left[:n_e], non_blocking=True)
+            hr.copy_(right[:n_e], non_blocking=True)
+            if nearest:
+                hd.copy_(dists[:n_e], non_blocking=True)
+            b.record(stream)
+            torch.cuda.synchronize()
+            if k:
+                e2e_ms.append(a.elapsed_time(b))
+    total_ms = float(sum(step_ms))
+    if dist:
+        t = torch.tensor([total_ms, float(np.median(e2e_ms))], device=dev, dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        total_ms, e2e_med = float(t[0]), float(t[1])
+    else:
+        e2e_med = float(np.median(e2e_ms))
+    value = world * N * args.steps / (total_ms / 1e3)
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    kmed = float(np.median(kernel_ms))
+    B = algorithmic_bytes(w, n_pairs) + (8 * n_pairs if nearest else 0)
+    achieved = B / (kmed / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / f"traffic_{args.workload}_rtree.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("traffic_bytes_per_launch")
+        except Exception:
+            traffic = None
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        threads = os.cpu_count() or 1
+        rate, n_s, dt = cpu_distance_rate(w, args.workload, threads, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "points/s", "cores": threads, "kind": "port",
+               "sample": f"first {n_s} of {N} points vs all {len(w.polys)} polygons ({dt:.1f} s), CPU oracle "
+                         "(C + OpenMP, grid index, same distance arithmetic); Shapely/GEOS is not installable here"}
+    line = {
+        "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "method": "rtree (distance walk)",
+                   "n_points_per_gpu": N, "n_polygons": len(w.polys), "n_pairs": n_pairs,
+                   "distance": None if nearest else DWITHIN_DISTANCE,
+                   "parallelism": f"points sharded over {world} GPU(s), index replicated",
+                   "l2": "inputs (800 MB of points) larger than L2; no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel_ms": kmed,
+                     "algorithmic_bytes_per_launch": B},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
+                "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int((16 if nearest else 8) * n_pairs)},
+        "gpu_launches": launches,
+        "join_stats": st,
+    }
+    line["clocks"] = clk.summary()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -420,6 +619,9 @@ def run_reference(args, rank, world):
         return
     if args.workload == "wkb":
         run_reference_wkb(args, world)
+        return
+    if args.workload in ("dwithin", "nearest"):
+        run_reference_distance(args, world)
         return
     w = make_workload(args.workload, 0, args.scale)
     threads = os.cpu_count() or 1
@@ -860,6 +1062,8 @@ def main():
             run_batched(args, rank, world, local_rank)
         elif args.workload == "wkb":
             run_wkb(args, rank, world, local_rank)
+        elif args.workload in ("dwithin", "nearest"):
+            run_distance(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

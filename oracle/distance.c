@@ -17,7 +17,9 @@
  * Compiled with -ffp-contract=off, every operation rounds on its own, the
  * same arithmetic as the device code.
  *
- * Brute force over all polygons per point (small test sizes only).
+ * Candidates come from a uniform grid over the polygon boxes (the square of
+ * the search radius around the point, the radius growing for nearest); the
+ * exact test decides every candidate.
  */
 #include <math.h>
 #include <stdint.h>
@@ -136,6 +138,90 @@ static int begin_threads(int nthreads) {
     return nt;
 }
 
+/* A uniform grid over the valid polygon boxes: cell -> polygons whose box
+ * overlaps it (CSR).  Coordinates outside the frame clamp to the border cells,
+ * so a query square overlapping a polygon's box always shares a cell with it. */
+typedef struct {
+    double x0, y0, sx, sy, cw, ch;
+    int64_t side;
+    int64_t *start;
+    int32_t *items;
+    int64_t nvalid;
+} grid_t;
+
+static int64_t cell_of(double v, double lo, double s, int64_t side) {
+    const double c = floor((v - lo) * s);
+    if (!(c >= 0.0)) return 0; /* also NaN and -inf */
+    if (c >= (double)side) return side - 1;
+    return (int64_t)c;
+}
+
+static void grid_build(grid_t *gr, const double *bounds, int64_t ngeoms) {
+    double tx0 = INFINITY, ty0 = INFINITY, tx1 = -INFINITY, ty1 = -INFINITY;
+    int64_t nvalid = 0;
+    for (int64_t g = 0; g < ngeoms; ++g) {
+        const double *b = &bounds[4 * g];
+        if (!(b[0] <= b[2])) continue;
+        nvalid++;
+        tx0 = fmin(tx0, b[0]); ty0 = fmin(ty0, b[1]);
+        tx1 = fmax(tx1, b[2]); ty1 = fmax(ty1, b[3]);
+    }
+    gr->nvalid = nvalid;
+    int64_t side = (int64_t)sqrt((double)(nvalid > 0 ? nvalid : 1)) + 1;
+    if (side > 2048) side = 2048;
+    const double w = (tx1 - tx0) > 0 ? (tx1 - tx0) : 1.0, h = (ty1 - ty0) > 0 ? (ty1 - ty0) : 1.0;
+    gr->x0 = nvalid ? tx0 : 0.0;
+    gr->y0 = nvalid ? ty0 : 0.0;
+    gr->side = side;
+    gr->sx = side / w;
+    gr->sy = side / h;
+    gr->cw = w / side;
+    gr->ch = h / side;
+    const int64_t ncell = side * side;
+    gr->start = (int64_t *)calloc((size_t)ncell + 1, sizeof(int64_t));
+    for (int pass = 0; pass < 2; ++pass) {
+        int64_t *fill = NULL;
+        if (pass == 1) {
+            for (int64_t c = 0; c < ncell; ++c) gr->start[c + 1] += gr->start[c];
+            gr->items = (int32_t *)malloc((size_t)(gr->start[ncell] > 0 ? gr->start[ncell] : 1) * sizeof(int32_t));
+            fill = (int64_t *)malloc((size_t)ncell * sizeof(int64_t));
+            memcpy(fill, gr->start, (size_t)ncell * sizeof(int64_t));
+        }
+        for (int64_t g = 0; g < ngeoms; ++g) {
+            const double *b = &bounds[4 * g];
+            if (!(b[0] <= b[2])) continue;
+            const int64_t cx0 = cell_of(b[0], gr->x0, gr->sx, side), cx1 = cell_of(b[2], gr->x0, gr->sx, side);
+            const int64_t cy0 = cell_of(b[1], gr->y0, gr->sy, side), cy1 = cell_of(b[3], gr->y0, gr->sy, side);
+            for (int64_t cy = cy0; cy <= cy1; ++cy)
+                for (int64_t cx = cx0; cx <= cx1; ++cx) {
+                    if (pass == 0) gr->start[cy * side + cx + 1]++;
+                    else gr->items[fill[cy * side + cx]++] = (int32_t)g;
+                }
+        }
+        free(fill);
+    }
+}
+
+static void grid_free(grid_t *gr) {
+    free(gr->start);
+    free(gr->items);
+}
+
+/* Cells overlapped by the square of half-width r around (x, y), widened by a
+ * relative margin (a polygon whose computed distance is within r is found). */
+static void grid_cover(const grid_t *gr, double x, double y, double r, int64_t *c) {
+    const double q = r + r * 0x1p-30 + 0x1p-1000;
+    c[0] = cell_of(x - q, gr->x0, gr->sx, gr->side);
+    c[1] = cell_of(x + q, gr->x0, gr->sx, gr->side);
+    c[2] = cell_of(y - q, gr->y0, gr->sy, gr->side);
+    c[3] = cell_of(y + q, gr->y0, gr->sy, gr->side);
+}
+
+static int cmp_i32(const void *a, const void *b) {
+    const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
 /* d: d_pt[point] if d_pt, else d_geom[polygon] if d_geom, else d_scalar. */
 orc_dpairs *orc_dwithin_join(const double *px, const double *py, const uint8_t *pvalid, int64_t npts, const double *x,
                              const double *y, const int32_t *ring_off, const int32_t *part_off,
@@ -143,8 +229,19 @@ orc_dpairs *orc_dwithin_join(const double *px, const double *py, const uint8_t *
                              const double *d_geom, double d_scalar, int nthreads) {
     double *bounds = (double *)malloc((size_t)(ngeoms > 0 ? ngeoms : 1) * 4 * sizeof(double));
     orc_geometry_bounds(x, y, ring_off, part_off, geom_off, gvalid, ngeoms, bounds);
+    grid_t gr;
+    grid_build(&gr, bounds, ngeoms);
+    double dmax = d_scalar;
+    if (d_geom) {
+        dmax = -INFINITY;
+        for (int64_t g = 0; g < ngeoms; ++g)
+            if (d_geom[g] == d_geom[g] && d_geom[g] > dmax) dmax = d_geom[g];
+    }
     const int nt = begin_threads(nthreads);
     dvec *per = (dvec *)calloc((size_t)nt, sizeof(dvec));
+    int64_t *stamp = (int64_t *)malloc((size_t)nt * (size_t)(ngeoms > 0 ? ngeoms : 1) * sizeof(int64_t));
+    for (int64_t k = 0; k < (int64_t)nt * (ngeoms > 0 ? ngeoms : 1); ++k) stamp[k] = -1;
+    int32_t *cand = (int32_t *)malloc((size_t)nt * (size_t)(ngeoms > 0 ? ngeoms : 1) * sizeof(int32_t));
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static)
 #endif
@@ -153,32 +250,59 @@ orc_dpairs *orc_dwithin_join(const double *px, const double *py, const uint8_t *
 #ifdef _OPENMP
         tid = omp_get_thread_num();
 #endif
-        if ((pvalid && !pvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
-        for (int64_t g = 0; g < ngeoms; ++g) {
+        if (gr.nvalid == 0 || (pvalid && !pvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
+        const double q = d_pt ? d_pt[i] : dmax;
+        if (!(q >= 0.0)) continue;
+        int64_t *st = stamp + (size_t)tid * (size_t)ngeoms;
+        int32_t *cd = cand + (size_t)tid * (size_t)ngeoms;
+        int64_t nc = 0, c[4];
+        grid_cover(&gr, px[i], py[i], q, c);
+        for (int64_t cy = c[2]; cy <= c[3]; ++cy)
+            for (int64_t cx = c[0]; cx <= c[1]; ++cx)
+                for (int64_t k = gr.start[cy * gr.side + cx]; k < gr.start[cy * gr.side + cx + 1]; ++k) {
+                    const int32_t g = gr.items[k];
+                    if (st[g] == i) continue;
+                    st[g] = i;
+                    cd[nc++] = g;
+                }
+        qsort(cd, (size_t)nc, sizeof(int32_t), cmp_i32);
+        for (int64_t k = 0; k < nc; ++k) {
+            const int32_t g = cd[k];
             const double *b = &bounds[4 * g];
-            if (!(b[0] <= b[2])) continue; /* null or empty polygon */
             const double d = d_pt ? d_pt[i] : (d_geom ? d_geom[g] : d_scalar);
             if (!(d >= 0.0)) continue;
             if (orc_envelope_distance(b, px[i], py[i]) > d) continue;
             const double dist = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, g);
-            if (dist <= d) dvec_push(&per[tid], (int32_t)i, (int32_t)g, dist);
+            if (dist <= d) dvec_push(&per[tid], (int32_t)i, g, dist);
         }
     }
+    free(cand);
+    free(stamp);
+    grid_free(&gr);
     free(bounds);
     return gather(per, nt);
 }
 
 /* Every polygon at each point's minimum distance, if that minimum is finite
- * and <= max_distance. */
+ * and <= max_distance.  Grid search over a growing square: the minimum over
+ * the polygons registered in the cells within r is final once it is <= r
+ * (or once the square covers the whole grid). */
 orc_dpairs *orc_nearest_join(const double *px, const double *py, const uint8_t *pvalid, int64_t npts, const double *x,
                              const double *y, const int32_t *ring_off, const int32_t *part_off,
                              const int32_t *geom_off, const uint8_t *gvalid, int64_t ngeoms, double max_distance,
                              int nthreads) {
     double *bounds = (double *)malloc((size_t)(ngeoms > 0 ? ngeoms : 1) * 4 * sizeof(double));
     orc_geometry_bounds(x, y, ring_off, part_off, geom_off, gvalid, ngeoms, bounds);
+    grid_t gr;
+    grid_build(&gr, bounds, ngeoms);
     const int nt = begin_threads(nthreads);
     dvec *per = (dvec *)calloc((size_t)nt, sizeof(dvec));
-    double *dist = (double *)malloc((size_t)nt * (size_t)(ngeoms > 0 ? ngeoms : 1) * sizeof(double));
+    const size_t m = (size_t)(ngeoms > 0 ? ngeoms : 1);
+    int64_t *stamp = (int64_t *)malloc((size_t)nt * m * sizeof(int64_t));
+    for (size_t k = 0; k < (size_t)nt * m; ++k) stamp[k] = -1;
+    double *dist = (double *)malloc((size_t)nt * m * sizeof(double));
+    int32_t *cand = (int32_t *)malloc((size_t)nt * m * sizeof(int32_t));
+    const double r0 = fmax(gr.cw, gr.ch);
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static)
 #endif
@@ -187,24 +311,38 @@ orc_dpairs *orc_nearest_join(const double *px, const double *py, const uint8_t *
 #ifdef _OPENMP
         tid = omp_get_thread_num();
 #endif
-        if ((pvalid && !pvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
-        double *dg = dist + (size_t)tid * (size_t)ngeoms;
+        if (gr.nvalid == 0 || (pvalid && !pvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
+        int64_t *st = stamp + (size_t)tid * m;
+        double *dg = dist + (size_t)tid * m;
+        int32_t *cd = cand + (size_t)tid * m;
+        int64_t nc = 0;
         double best = INFINITY;
-        for (int64_t g = 0; g < ngeoms; ++g) {
-            const double *b = &bounds[4 * g];
-            dg[g] = INFINITY;
-            if (!(b[0] <= b[2])) continue;
-            /* the envelope bounds the distance from below (a relative margin
-             * covers the rounding of both) */
-            if (orc_envelope_distance(b, px[i], py[i]) > best * (1.0 + 0x1p-40)) continue;
-            dg[g] = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, g);
-            if (dg[g] < best) best = dg[g];
+        /* polygons are added as the square grows; each keeps its distance */
+        for (double r = r0;; r *= 2.0) {
+            int64_t c[4];
+            grid_cover(&gr, px[i], py[i], r, c);
+            for (int64_t cy = c[2]; cy <= c[3]; ++cy)
+                for (int64_t cx = c[0]; cx <= c[1]; ++cx)
+                    for (int64_t k = gr.start[cy * gr.side + cx]; k < gr.start[cy * gr.side + cx + 1]; ++k) {
+                        const int32_t g = gr.items[k];
+                        if (st[g] == i) continue;
+                        st[g] = i;
+                        cd[nc++] = g;
+                        dg[g] = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, g);
+                        if (dg[g] < best) best = dg[g];
+                    }
+            const int all = c[0] == 0 && c[2] == 0 && c[1] == gr.side - 1 && c[3] == gr.side - 1;
+            if (best <= r || all || !(r < INFINITY)) break;
         }
         if (!(best < INFINITY) || !(best <= max_distance)) continue;
-        for (int64_t g = 0; g < ngeoms; ++g)
-            if (dg[g] == best) dvec_push(&per[tid], (int32_t)i, (int32_t)g, best);
+        qsort(cd, (size_t)nc, sizeof(int32_t), cmp_i32);
+        for (int64_t k = 0; k < nc; ++k)
+            if (dg[cd[k]] == best) dvec_push(&per[tid], (int32_t)i, cd[k], best);
     }
+    free(cand);
     free(dist);
+    free(stamp);
+    grid_free(&gr);
     free(bounds);
     return gather(per, nt);
 }

@@ -30,13 +30,15 @@
 // radius (rounded outward, plus a relative 2^-30 margin, so no polygon within
 // the radius can be missed); the exact test above decides every candidate.
 //
-// Nearest (all ties): rounds of growing radius over the points still open.
-// A round computes each open point's minimum distance over the candidates
-// within the radius (no candidate of a point can be nearer than its minimum
-// unless it lies outside the radius, so a minimum <= radius is final), then
-// emits, for the points that closed, every candidate at exactly that
-// distance.  Radius: max_distance when given (one round), else a spacing
-// estimate of the polygon frame growing 4x a round, then unbounded.
+// Nearest (all ties), two walks.  The first finds each point's minimum: a
+// greedy descent per point (at every level the child box nearest to the
+// point, then the nearest item box) gives an upper bound; the walk then
+// visits, nearest first, only what lies within each point's current minimum
+// (capped by max_distance) -- a polygon nearer than the minimum is always
+// inside that box -- and the packet's box shrinks as the minima drop.  The
+// second walk emits every polygon at exactly the minimum.
+// Candidates whose envelope is certainly farther than the bound are skipped
+// before the exact distance.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -57,7 +59,6 @@ constexpr int kDistWarps = kDistThreads / 32;
 constexpr int kDistStack = 112;
 constexpr int kDistMaxStaged = 273;
 constexpr int64_t kDistGrab = 32;
-constexpr int kNearestRounds = 8;  // growing rounds before the unbounded one
 
 enum : int { kDwithin = 0, kNearestMin = 1, kNearestEmit = 2 };
 
@@ -149,6 +150,45 @@ __device__ __forceinline__ double inflate(double q) {
     return __dadd_ru(__dadd_ru(q, __dmul_ru(q, 0x1p-30)), 0x1p-1000);
 }
 
+__device__ __forceinline__ vs_box load_node(const DistArgs& a, const vs_box* s_nodes, int64_t stage_base, int cl,
+                                            int64_t c) {
+    return cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
+}
+
+// Squared distance from (x, y) to a box (plain rounding: only steers the
+// greedy descent and the walk's order).
+__device__ __forceinline__ double box_dist2(const vs_box& b, double x, double y) {
+    const double dx = fmax(fmax(b.minx - x, x - b.maxx), 0.0);
+    const double dy = fmax(fmax(b.miny - y, y - b.maxy), 0.0);
+    return dx * dx + dy * dy;
+}
+
+// Descent key of the greedy bound: the box distance, plus the distance to
+// the box centre so that of several boxes containing the point the one
+// centred nearest to it wins.
+__device__ __forceinline__ double descent_key(const vs_box& b, double x, double y) {
+    const double cx = 0.5 * (b.minx + b.maxx) - x, cy = 0.5 * (b.miny + b.maxy) - y;
+    return box_dist2(b, x, y) + cx * cx + cy * cy;
+}
+
+// Exact point-polygon distance of slot g (0 inside or on the boundary).
+__device__ __forceinline__ double polygon_distance(const DistArgs& a, double x, double y, int g, unsigned& n_exact) {
+    const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, g, a.rings, n_exact);
+    return loc != LOC_OUTSIDE ? 0.0 : facet_distance(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, g, -1.0);
+}
+
+// Warp-packet R-tree walk of the distance joins.
+//   kDwithin      per lane radius d (per point / per polygon / scalar); emits
+//                 the pairs within it
+//   kNearestMin   per lane minimum distance: each lane's greedy descent
+//                 (level by level the child box nearest to its point, ties
+//                 broken by the box centre, then the nearest item box) gives
+//                 it an upper bound; the walk then
+//                 visits, nearest to the packet's centroid first, what lies
+//                 within each lane's current minimum (capped by max_distance
+//                 in a.radius), the packet's box shrinking as the minima
+//                 drop; writes best[row]
+//   kNearestEmit  radius best[row]; emits every polygon at exactly that distance
 template <int kMode>
 __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs a) {
     extern __shared__ vs_box s_nodes[];
@@ -180,23 +220,86 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
             x = a.px[row];
             y = a.py[row];
             if (kMode == kDwithin) q = a.dist_pt ? a.dist_pt[row] : a.dist_scalar;
-            else if (kMode == kNearestMin) q = a.radius;
+            else if (kMode == kNearestMin) q = a.radius;  // the cap (max_distance or INFINITY)
             else q = a.best[row];
             // a negative or NaN radius matches nothing; nearest emits only finite minima
             active = q >= 0.0 && (kMode != kNearestEmit || q < INFINITY);
         }
-        const double qi = active ? inflate(q) : 0.0;
-        const double lx0 = active ? __dsub_rd(x, qi) : INFINITY, lx1 = active ? __dadd_ru(x, qi) : -INFINITY;
-        const double ly0 = active ? __dsub_rd(y, qi) : INFINITY, ly1 = active ? __dadd_ru(y, qi) : -INFINITY;
-        double x0 = lx0, x1 = lx1, y0 = ly0, y1 = ly1;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            x0 = fmin(x0, __shfl_xor_sync(0xffffffffu, x0, o));
-            x1 = fmax(x1, __shfl_xor_sync(0xffffffffu, x1, o));
-            y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
-            y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
-        }
         double my_best = INFINITY;  // nearest, min pass
+        double cx = 0.0, cy = 0.0;  // nearest, min pass: the packet's centroid
+        if (kMode == kNearestMin && __any_sync(0xffffffffu, active)) {
+            // the packet's centroid orders the walk below
+            double sx = active ? x : 0.0, sy = active ? y : 0.0;
+            int cnt = active ? 1 : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sx += __shfl_xor_sync(0xffffffffu, sx, o);
+                sy += __shfl_xor_sync(0xffffffffu, sy, o);
+                cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            }
+            cx = sx / cnt;
+            cy = sy / cnt;
+            // every lane descends on its own: at each level the child box nearest to
+            // its point, then the exact distance to the nearest item box of the
+            // leaf block reached -- an upper bound of the lane's minimum
+            if (active) {
+                int64_t node = 0;
+                bool ok = true;
+                for (int cl = top - 1; cl >= 1 && ok; --cl) {
+                    const int64_t first = node * kFanout;
+                    const int64_t last = first + kFanout < a.level_size[cl] ? first + kFanout : a.level_size[cl];
+                    double bd = INFINITY;
+                    int64_t bc = -1;
+                    for (int64_t c = first; c < last; ++c) {
+                        const vs_box b = load_node(a, s_nodes, stage_base, cl, c);
+                        if (!(b.minx <= b.maxx)) continue;
+                        const double d = descent_key(b, x, y);
+                        if (d < bd) {
+                            bd = d;
+                            bc = c;
+                        }
+                    }
+                    ok = bc >= 0;
+                    node = bc;
+                }
+                if (ok) {
+                    const int64_t first = top == 0 ? 0 : node * kFanout;
+                    const int64_t last = top == 0 ? 1 : (first + kFanout < a.level_size[0] ? first + kFanout
+                                                                                          : a.level_size[0]);
+                    double bd = INFINITY;
+                    int64_t bi = -1;
+                    for (int64_t c = first; c < last; ++c) {
+                        const vs_box b = a.nodes[a.level_off[0] + c];
+                        if (!(b.minx <= b.maxx)) continue;
+                        const double d = descent_key(b, x, y);
+                        if (d < bd) {
+                            bd = d;
+                            bi = c;
+                        }
+                    }
+                    if (bi >= 0) my_best = polygon_distance(a, x, y, (int)bi, n_exact);
+                }
+            }
+        }
+        // per lane search box and the packet's union box
+        double lx0, lx1, ly0, ly1, x0, x1, y0, y1;
+        auto boxes = [&]() {
+            const double r = kMode == kNearestMin ? fmin(my_best, q) : q;
+            const double qi = active ? inflate(r) : 0.0;
+            lx0 = active ? __dsub_rd(x, qi) : INFINITY;
+            lx1 = active ? __dadd_ru(x, qi) : -INFINITY;
+            ly0 = active ? __dsub_rd(y, qi) : INFINITY;
+            ly1 = active ? __dadd_ru(y, qi) : -INFINITY;
+            x0 = lx0, x1 = lx1, y0 = ly0, y1 = ly1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                x0 = fmin(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+                x1 = fmax(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+                y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+                y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+            }
+        };
+        boxes();
         int sp = 0;
         if (__any_sync(0xffffffffu, active)) {
             if (lane == 0) s_stack[warp][0] = top;
@@ -214,14 +317,26 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
             const bool in_range = root ? lane == 0 : (lane < kFanout && c < a.level_size[cl]);
             const int64_t cc = root ? 0 : c;
             vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
-            if (in_range)
-                b = cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + cc] : a.nodes[a.level_off[cl] + cc];
+            if (in_range) b = load_node(a, s_nodes, stage_base, cl, cc);
             const bool hit = in_range && b.minx <= x1 && b.maxx >= x0 && b.miny <= y1 && b.maxy >= y0;
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             if (cl > 0) {
                 // push the hit nodes' children blocks: node cc of level cl owns block cc of level cl - 1
+                int rank = __popc(m & lt);
+                if (kMode == kNearestMin) {
+                    // nearest to the packet's centroid on top of the stack: the first
+                    // leaves reached shrink the minima, and the boxes with them
+                    const double key = hit ? box_dist2(b, cx, cy) : INFINITY;
+                    int closer = 0;
+#pragma unroll
+                    for (int j = 0; j < kFanout; ++j) {
+                        const double kj = __shfl_sync(0xffffffffu, key, j);
+                        closer += ((m >> j) & 1u) && (kj < key || (kj == key && j < lane)) ? 1 : 0;
+                    }
+                    rank = __popc(m) - 1 - closer;
+                }
                 if (hit) {
-                    const int pos = sp + __popc(m & lt);
+                    const int pos = sp + rank;
                     if (pos < kDistStack) s_stack[warp][pos] = (int)(cc << 4) | (cl - 1);
                 }
                 int add = __popc(m);
@@ -253,51 +368,29 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
                                        facet_distance(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, d) <= d;
                             }
                         } else {
-                            const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot,
-                                                              a.rings, n_exact);
-                            const double d =
-                                loc != LOC_OUTSIDE
-                                    ? 0.0
-                                    : facet_distance(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, -1.0);
-                            if (kMode == kNearestMin) my_best = d < my_best ? d : my_best;
-                            else want = d == q;
+                            // a polygon whose envelope is farther than the bound (with a
+                            // margin above the rounding of both distances) can neither
+                            // lower the minimum nor tie it
+                            const double bound = kMode == kNearestMin ? my_best : q;
+                            if (!(envelope_distance(ib, x, y) > bound * (1.0 + 0x1p-40))) {
+                                const double d = polygon_distance(a, x, y, slot, n_exact);
+                                if (kMode == kNearestMin) my_best = d < my_best ? d : my_best;
+                                else want = d == q;
+                            }
                         }
                     }
                     if (kMode != kNearestMin) wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
                 }
                 __syncwarp();
+                if (kMode == kNearestMin) boxes();  // the minima only shrink: so does the packet's box
             }
         }
-        if (kMode == kNearestMin && active) a.best[row] = my_best;
+        if (kMode == kNearestMin && active) a.best[row] = my_best <= q ? my_best : INFINITY;
         if (kMode != kNearestMin) wflush(out, a.sink, false);
     }
     if (kMode != kNearestMin) wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 1, n_exact);
-}
-
-// Open points of a nearest round: done (minimum within the radius and within
-// max_distance) or still open (another round follows).
-__global__ void nearest_classify_kernel(const uint32_t* __restrict__ list, int64_t m,
-                                        const uint32_t* __restrict__ order, const double* __restrict__ best,
-                                        double radius, double max_distance, bool last, uint32_t* __restrict__ done,
-                                        uint32_t* __restrict__ open) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t pos = list ? list[i] : (uint32_t)i;
-        const double b = best[order[pos]];
-        const bool closed = b <= radius;
-        done[i] = closed && b <= max_distance ? 1u : 0u;
-        open[i] = !closed && !last ? 1u : 0u;
-    }
-}
-
-// out[scan[i]] = position i of the list where flag[i] is set (flag == scan
-// difference), keeping the list's order.
-__global__ void compact_positions_kernel(const uint32_t* __restrict__ list, int64_t m,
-                                         const uint32_t* __restrict__ flag, const uint32_t* __restrict__ scan,
-                                         uint32_t* __restrict__ out) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
-        if (flag[i]) out[scan[i]] = list ? list[i] : (uint32_t)i;
 }
 
 __global__ void gather_pair_distance_kernel(const int32_t* __restrict__ left, int64_t n,
@@ -501,68 +594,17 @@ int vs_join_nearest(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
     cudaEventRecord(ev.a, s);
     QueryOrder q;
     VS_TRY(prepare_queries(ctx, idx, pts, q, true));
-    uint32_t n_open = 0;
-    VS_CUDA_TRY(cudaMemcpyAsync(&n_open, q.n_valid.p, sizeof(n_open), cudaMemcpyDeviceToHost, s));
-    VS_CUDA_TRY(cudaStreamSynchronize(s));
-    const int64_t n = pts->n;
     Scratch<double> best;
-    Scratch<uint32_t> lists, flags_buf, scans, counts;
-    VS_TRY(best.alloc((size_t)n, s));
-    // two lists (open, next open) + a done list; flags and scans for two kinds
-    VS_TRY(lists.alloc(3 * (size_t)n, s));
-    VS_TRY(flags_buf.alloc(2 * (size_t)n, s));
-    VS_TRY(scans.alloc(2 * (size_t)n + 2, s));
-    VS_TRY(counts.alloc(4, s));
-    uint32_t* list_a = lists.p;
-    uint32_t* list_b = lists.p + n;
-    uint32_t* done = lists.p + 2 * n;
+    VS_TRY(best.alloc((size_t)pts->n, s));
     size_t smem = 0;
     DistArgs a = dist_args(ctx, idx, pts, q, &smem);
+    a.n_list = q.n_valid.p;
     a.best = best.p;
+    a.radius = max_distance;  // the search cap
     a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
-    const bool bounded = max_distance < INFINITY;
-    // first radius: the spacing of the polygons over their frame
-    const double w = idx->h_frame[2] - idx->h_frame[0], h = idx->h_frame[3] - idx->h_frame[1];
-    double radius = sqrt(fmax(w * h, fmax(w, h) * fmax(w, h) * 1e-6) / (double)idx->n_geoms);
-    if (!(radius > 0.0) || !(radius < INFINITY)) radius = 1.0;
-    if (bounded) radius = max_distance;
-    const uint32_t* open = nullptr;  // null: every sorted position below n_open
-    for (int round = 0; n_open > 0; ++round) {
-        const bool last = bounded || round == kNearestRounds;
-        if (round == kNearestRounds && !bounded) radius = INFINITY;
-        // minimum distance of every open point over its candidates
-        a.list = open;
-        a.n_list = counts.p;
-        VS_CUDA_TRY(cudaMemcpyAsync(counts.p, &n_open, sizeof(n_open), cudaMemcpyHostToDevice, s));
-        a.radius = radius;
-        VS_TRY(launch_dist<kNearestMin>(ctx, a, smem, n_open));
-        // split into done / still open, keeping the sorted order
-        uint32_t* f_done = flags_buf.p;
-        uint32_t* f_open = flags_buf.p + n;
-        nearest_classify_kernel<<<resident_grid(nearest_classify_kernel, n_open, 256), 256, 0, s>>>(
-            open, n_open, q.order.p, best.p, radius, bounded ? max_distance : INFINITY, last, f_done, f_open);
-        VS_LAUNCHED("nearest_classify", s);
-        VS_TRY(exclusive_scan_u32(f_done, scans.p, n_open, counts.p + 1, s));
-        VS_TRY(exclusive_scan_u32(f_open, scans.p + n, n_open, counts.p + 2, s));
-        uint32_t* next = open == list_a ? list_b : list_a;
-        compact_positions_kernel<<<resident_grid(compact_positions_kernel, n_open, 256), 256, 0, s>>>(
-            open, n_open, f_done, scans.p, done);
-        VS_LAUNCHED("compact_positions", s);
-        compact_positions_kernel<<<resident_grid(compact_positions_kernel, n_open, 256), 256, 0, s>>>(
-            open, n_open, f_open, scans.p + n, next);
-        VS_LAUNCHED("compact_positions", s);
-        // every candidate at exactly the minimum, for the points that closed
-        DistArgs e = a;
-        e.list = done;
-        e.n_list = counts.p + 1;
-        VS_TRY(launch_dist<kNearestEmit>(ctx, e, smem, n_open));
-        uint32_t tot[2] = {0, 0};
-        VS_CUDA_TRY(cudaMemcpyAsync(tot, counts.p + 1, sizeof(tot), cudaMemcpyDeviceToHost, s));
-        VS_CUDA_TRY(cudaStreamSynchronize(s));
-        n_open = tot[1];
-        open = next;
-        radius *= 4.0;
-    }
+    // each point's minimum distance, then every polygon at exactly that distance
+    VS_TRY(launch_dist<kNearestMin>(ctx, a, smem, pts->n));
+    VS_TRY(launch_dist<kNearestEmit>(ctx, a, smem, pts->n));
     const int st = finish_join(ctx, idx, pts, flags, d_left, d_right, capacity, n_pairs, stats, ev, launches0);
     if (st != VS_OK) return st;
     if (d_distance && *n_pairs > 0) {
