@@ -136,6 +136,8 @@ WORKLOAD_DESC = {
     "dwithin": "dwithin: zipf_join's 50M FP64 points x 1M footprints, pairs within distance 0.25 (1.7x the median "
                "footprint side)",
     "nearest": "nearest (sjoin_nearest, all ties, unbounded): zipf_join's 50M FP64 points x 1M footprints",
+    "export": "join export: zipf_join's within pairs (50M points x 1M footprints) to how='left' row indexers "
+              "(50M+ rows) after an on_attribute filter (codes row % 7 on both sides)",
     "wkb": "wkb ingest: the zipf_join inputs as little-endian 2D WKB columns (50M Points, 21 B each; 1M Polygons), "
            "decoded on the device into the join's columnar layout",
 }
@@ -611,6 +613,153 @@ def run_distance(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def _export_inputs(w, pairs_l, pairs_r):
+    n_left, n_right = w.n_points, len(w.polys.geom_off) - 1
+    return n_left, n_right, (np.arange(n_left, dtype=np.int64) % 7), (np.arange(n_right, dtype=np.int64) % 7)
+
+
+def run_reference_export(args, world):
+    """The host export (numpy restatement of the reference's _adjust_join_indexers
+    and attribute filter) on the same pairs, made by the CPU oracle."""
+    import importlib
+
+    sj = importlib.import_module("vibespatial_b200.sjoin")
+    w = make_workload("zipf", 0, args.scale)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+    hl, hr = O.join(w.px, w.py, None, P, "within", os.cpu_count() or 1)
+    n_left, n_right, lc, rc = _export_inputs(w, hl, hr)
+    for _ in range(args.warmup):
+        out = sj._join_indexers(hl, hr, n_left, n_right, "left", (lc, rc))
+    n_rows = len(out[0])
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sj._join_indexers(hl, hr, n_left, n_right, "left", (lc, rc))
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = n_rows * len(times) / tot
+    line = {
+        "impl": "reference", "metric": "join export rows/sec", "value": value, "unit": "rows/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC["export"], "n_pairs": int(len(hl)), "n_rows": n_rows},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": 1, "kind": "port",
+                         "sample": "the whole export each step: numpy restatement of the reference's host "
+                                   "_adjust_join_indexers + attribute filter"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_export(args, rank, world, local_rank):
+    """Join export (vs_join_export) of the zipf within pairs: how='left' + on_attribute codes."""
+    import importlib
+
+    import torch
+
+    from vibespatial_b200 import _abi
+
+    sj = importlib.import_module("vibespatial_b200.sjoin")
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    w = make_workload("zipf", rank, args.scale)
+    ctx = _abi.Context(dev)
+    stream = ctx.torch_stream
+    pol = w.polys
+    d_poly = {k: torch.from_numpy(np.ascontiguousarray(getattr(pol, k))).to(dev)
+              for k in ("x", "y", "ring_off", "part_off", "geom_off")}
+    P = _abi.make_polygons(d_poly["x"], d_poly["y"], d_poly["ring_off"], d_poly["part_off"], d_poly["geom_off"])
+    index = _abi.DeviceIndex(ctx, P, learned=True)
+    dx, dy = torch.from_numpy(w.px).to(dev), torch.from_numpy(w.py).to(dev)
+    pts = _abi.make_points(dx, dy)
+    left, right, _ = index.join(pts, _abi.PRED_WITHIN, _abi.METHOD_LEARNED, sort=True)
+    n_left, n_right, lc_h, rc_h = _export_inputs(w, left, right)
+    lc, rc = torch.from_numpy(lc_h).to(dev), torch.from_numpy(rc_h).to(dev)
+
+    def step():
+        return _abi.join_export(ctx, left, right, n_left, n_right, "left", lc, rc)
+
+    out = step()
+    n_rows = int(out[0].numel())
+    # the device rows equal the host export of the same pairs
+    hl, hr = left.cpu().numpy(), right.cpu().numpy()
+    el, er, es = sj._join_indexers(hl, hr, n_left, n_right, "left", (lc_h, rc_h))
+    assert np.array_equal(out[0].cpu().numpy(), el) and np.array_equal(out[1].cpu().numpy(), er)
+    assert np.array_equal(out[2].cpu().numpy(), es)
+    del out
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = _abi.kernel_launches()
+    with ClockSampler(dev) as clk:
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        launches = _abi.kernel_launches() - launches0
+        # e2e: pairs and codes from pinned host memory, the three indexers back to pinned host memory
+        h_l, h_r = torch.from_numpy(hl).pin_memory(), torch.from_numpy(hr).pin_memory()
+        h_lc, h_rc = torch.from_numpy(lc_h).pin_memory(), torch.from_numpy(rc_h).pin_memory()
+        o = [torch.empty(n_rows, dtype=torch.int64).pin_memory() for _ in range(3)]
+        e2e_ms = []
+        for k in range(max(3, args.steps) + 1):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            dl, dr = h_l.to(dev, non_blocking=True), h_r.to(dev, non_blocking=True)
+            dlc, drc = h_lc.to(dev, non_blocking=True), h_rc.to(dev, non_blocking=True)
+            res = _abi.join_export(ctx, dl, dr, n_left, n_right, "left", dlc, drc)
+            for t, d in zip(o, res):
+                t.copy_(d, non_blocking=True)
+            b.record(stream)
+            torch.cuda.synchronize()
+            if k:
+                e2e_ms.append(a.elapsed_time(b))
+    total_ms = float(sum(step_ms))
+    value = n_rows * args.steps / (total_ms / 1e3)
+    e2e_med = float(np.median(e2e_ms))
+    peak, peak_kind = _peaks()
+    n_pairs = int(left.numel())
+    # algorithmic bytes: pairs (8) + their two codes (16) read, kept pairs re-read, output rows (24) written,
+    # per-left-row counts (4 + 4 read) -- the minimum of a filter-then-expand export
+    B = 8 * n_pairs + 16 * n_pairs + 24 * n_rows + 8 * n_left
+    kmed = float(np.median(step_ms))
+    achieved = B / (kmed / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < min(args.cpu_seconds, 10.0) or reps == 0:
+            sj._join_indexers(hl, hr, n_left, n_right, "left", (lc_h, rc_h))
+            reps += 1
+        dt = time.perf_counter() - t0
+        cpu = {"value": n_rows * reps / dt, "unit": "rows/s", "cores": 1, "kind": "port",
+               "sample": f"the whole export, {reps} time(s) ({dt:.1f} s): numpy restatement of the reference's "
+                         "host _adjust_join_indexers + attribute filter"}
+    line = {
+        "metric": "join export rows/sec", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC["export"], "n_pairs": n_pairs, "n_left": n_left, "n_right": n_right,
+                   "n_rows": n_rows, "how": "left", "l2": "inputs (~0.6 GB) larger than L2; no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "kernel_ms": kmed, "algorithmic_bytes_per_launch": B},
+        "cpu_baseline": cpu,
+        "e2e": {"value": n_rows / (e2e_med / 1e3), "unit": "rows/s",
+                "h2d_bytes_per_step": int(8 * n_pairs + 8 * (n_left + n_right)),
+                "d2h_bytes_per_step": int(24 * n_rows)},
+        "gpu_launches": launches,
+    }
+    line["clocks"] = clk.summary()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -622,6 +771,9 @@ def run_reference(args, rank, world):
         return
     if args.workload in ("dwithin", "nearest"):
         run_reference_distance(args, world)
+        return
+    if args.workload == "export":
+        run_reference_export(args, world)
         return
     w = make_workload(args.workload, 0, args.scale)
     threads = os.cpu_count() or 1
@@ -1064,6 +1216,8 @@ def main():
             run_wkb(args, rank, world, local_rank)
         elif args.workload in ("dwithin", "nearest"):
             run_distance(args, rank, world, local_rank)
+        elif args.workload == "export":
+            run_export(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

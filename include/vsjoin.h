@@ -202,6 +202,26 @@ int vs_join_nearest(vs_context* ctx, const vs_index* index, const vs_points* pts
                     uint32_t flags, int32_t* d_left, int32_t* d_right, double* d_distance,
                     int64_t capacity, int64_t* n_pairs, vs_join_stats* stats);
 
+/* Join export: the row indexers of a relation join.  Replaces the
+ * reference's export (_adjust_join_indexers, src/vibespatial/api/_native_results.py:395-470)
+ * and its shared-attribute filter (src/vibespatial/api/tools/sjoin.py:826-888).
+ * Pairs (n_pairs, sorted by (left, right), as the joins return them) are
+ * first filtered by d_left_code[left] == d_right_code[right] when codes are
+ * given (int64 per row, equal values equal codes, < 0 = missing, never
+ * equal).  Output rows (int64, -1 = no row on that side):
+ *   VS_HOW_INNER  the kept pairs
+ *   VS_HOW_LEFT   every left row in order: its pairs, or (row, -1)
+ *   VS_HOW_RIGHT  every right row in order: its pairs (by left row), or (-1, row)
+ *   VS_HOW_OUTER  as LEFT, then (-1, row) for every right row without a pair
+ * d_out_src (nullable) receives each output row's input pair position (-1
+ * for an added row).  *n_out = the number of rows; VS_E_CAPACITY (buffers
+ * untouched) when it exceeds capacity.  Up to 2^31 - 1 pairs and rows a side. */
+enum { VS_HOW_INNER = 0, VS_HOW_LEFT = 1, VS_HOW_RIGHT = 2, VS_HOW_OUTER = 3 };
+int vs_join_export(vs_context* ctx, const int32_t* d_left, const int32_t* d_right, int64_t n_pairs,
+                   int64_t n_left, int64_t n_right, int32_t how, const int64_t* d_left_code,
+                   const int64_t* d_right_code, int64_t* d_out_left, int64_t* d_out_right,
+                   int64_t* d_out_src, int64_t capacity, int64_t* n_out);
+
 /* vs_join on HOST buffers: h_x / h_y / h_valid (n points; pinned memory lets
  * the copies run asynchronously) in, (left, right) pairs into h_left /
  * h_right (capacity entries each) out.  The points are streamed in chunks

@@ -357,3 +357,24 @@ def test_sjoin_nearest_cities_countries(backend):
     within = vs.sjoin(cities, countries, predicate="within")
     zero = r1[r1["dist"] == 0]
     assert set(zip(within.index, within["index_right"])) <= set(zip(zero.index, zero["index_right"]))
+
+
+def test_attribute_codes_and_host_export():
+    import importlib
+
+    vs_sjoin = importlib.import_module("vibespatial_b200.sjoin")
+
+    left = pd.DataFrame({"a": [1, 2, np.nan, 2, 3], "b": ["x", "y", "x", None, "y"]})
+    right = pd.DataFrame({"a": [2, 1, 3, np.nan], "b": ["y", "x", "x", "x"]})
+    lc, rc = vs_sjoin._attribute_codes(left, right, ["a"])
+    # missing values never match; equal values share a code
+    assert lc[2] == -1 and rc[3] == -1 and lc[1] == lc[3] == rc[0] and lc[0] == rc[1]
+    lc2, rc2 = vs_sjoin._attribute_codes(left, right, ["a", "b"])
+    assert lc2[3] == -1  # b missing
+    assert lc2[1] == rc2[0] and lc2[0] == rc2[1] and lc2[4] != rc2[2]
+    l = np.array([0, 0, 1, 3, 4, 4], np.intp)
+    r = np.array([0, 1, 0, 0, 2, 3], np.intp)
+    out_l, out_r, src = vs_sjoin._join_indexers(l, r, 5, 4, "left", (lc2, rc2))
+    # kept pairs: (0,1) [x,1 == x,1], (1,0) [y,2 == y,2]; rows 2, 3, 4 unmatched
+    assert out_l.tolist() == [0, 1, 2, 3, 4] and out_r.tolist() == [1, 0, -1, -1, -1]
+    assert src.tolist() == [1, 2, -1, -1, -1]

@@ -28,7 +28,7 @@ EXPORTED = (
     "vs_join", "vs_locate_aligned", "vs_sort_pairs", "vs_radix_sort_pairs", "vs_hilbert_keys",
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
     "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free", "vs_join_host",
-    "vs_thread_kernel_launches", "vs_join_dwithin", "vs_join_nearest",
+    "vs_thread_kernel_launches", "vs_join_dwithin", "vs_join_nearest", "vs_join_export",
 )
 
 
@@ -153,6 +153,8 @@ def load(path: Path | str | None = None):
                                                i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
             "vs_join_nearest": (ctypes.c_int, [vp, vp, ctypes.POINTER(Points), ctypes.c_double, u32, vp, vp, vp,
                                                i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
+            "vs_join_export": (ctypes.c_int, [vp, vp, vp, i64, i64, i64, i32, vp, vp, vp, vp, vp, i64,
+                                              ctypes.POINTER(i64)]),
             "vs_locate_aligned": (ctypes.c_int, [vp, ctypes.POINTER(Points), ctypes.POINTER(Polygons), vp]),
             "vs_sort_pairs": (ctypes.c_int, [vp, vp, vp, i64]),
             "vs_radix_sort_pairs": (ctypes.c_int, [vp, vp, vp, i64, i32]),
@@ -502,6 +504,33 @@ def wkb_decode(ctx: Context, data, offsets, valid=None):
         return sz, out
     finally:
         load().vs_wkb_plan_free(h)
+
+
+HOW_CODES = {"inner": 0, "left": 1, "right": 2, "outer": 3}
+
+
+def join_export(ctx: Context, left, right, n_left: int, n_right: int, how: str, left_code=None, right_code=None):
+    """vs_join_export: (left rows, right rows, source pair) int64 CUDA tensors
+    of the join's output rows (-1 = no row on that side / an added row).
+
+    ``left``/``right``: int32 CUDA tensors of pairs sorted by (left, right);
+    ``left_code``/``right_code``: optional int64 CUDA tensors of attribute
+    codes per row (pairs kept where equal; negative codes never match).
+    """
+    import torch
+
+    dev = left.device
+    n = int(left.numel())
+    cap = n + int(n_left) + int(n_right)
+    out_l = torch.empty(max(cap, 1), dtype=torch.int64, device=dev)
+    out_r = torch.empty(max(cap, 1), dtype=torch.int64, device=dev)
+    out_s = torch.empty(max(cap, 1), dtype=torch.int64, device=dev)
+    m = ctypes.c_int64(0)
+    check(load().vs_join_export(ctx.handle, _ptr(left), _ptr(right), n, int(n_left), int(n_right), HOW_CODES[how],
+                                _ptr(left_code), _ptr(right_code), _ptr(out_l), _ptr(out_r), _ptr(out_s), cap,
+                                ctypes.byref(m)), required=int(m.value))
+    k = int(m.value)
+    return out_l[:k], out_r[:k], out_s[:k]
 
 
 def wkb_plan_sizes(ctx: Context, data, offsets, valid, rows) -> dict:

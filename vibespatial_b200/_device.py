@@ -150,3 +150,16 @@ def nearest_pairs(points, polygons, *, max_distance=None, method="learned", devi
     left, right, dist, _ = index.nearest(pts, max_distance=md, sort=True)
     return (left.cpu().numpy().astype(np.intp), right.cpu().numpy().astype(np.intp),
             dist.cpu().numpy())
+
+
+def export_indexers(left, right, n_left: int, n_right: int, how: str, left_code=None, right_code=None,
+                    device: int = 0):
+    """Join export on the device (vs_join_export): host intp arrays (left
+    rows, right rows, source pair) after the attribute filter and ``how``."""
+    torch = _torch()
+    ctx = _abi.default_context(device)
+    lc = None if left_code is None else _dev(np.asarray(left_code, np.int64), torch, device)
+    rc = None if right_code is None else _dev(np.asarray(right_code, np.int64), torch, device)
+    out_l, out_r, src = _abi.join_export(ctx, left.contiguous(), right.contiguous(), n_left, n_right, how, lc, rc)
+    return (out_l.cpu().numpy().astype(np.intp), out_r.cpu().numpy().astype(np.intp),
+            src.cpu().numpy().astype(np.intp))

@@ -56,22 +56,62 @@ def _basic_checks(left_df, right_df, how, lsuffix, rsuffix, on_attribute=None):
                 raise ValueError("Active geometry column cannot be used as an input for on_attribute parameter.")
 
 
-def _geom_predicate_query(left_df, right_df, predicate, distance, on_attribute, method):
-    """(left rows, right rows) satisfying predicate(left geometry, right geometry)."""
+def _geom_predicate_query(left_df, right_df, predicate, distance, method):
+    """(left rows, right rows) satisfying predicate(left geometry, right
+    geometry), sorted: int32 CUDA tensors from the CUDA join (they stay on the
+    device for the export), host arrays when a test substitutes the pair
+    source."""
+    from . import query as _q
+
     left_geom = left_df.geometry.array
     right_geom = right_df.geometry.array
+    on_device = _q._pairs_backend is None and _q._dwithin_backend is None
     # tree = right side, input = left side (the reference's STRtree orientation)
     pairs = query_spatial_index(right_geom, left_geom, predicate=predicate, sort=True, distance=distance,
-                                method=method)
-    l_idx, r_idx = pairs[0], pairs[1]
-    if on_attribute and len(l_idx):
-        keep = np.ones(len(l_idx), dtype=bool)
-        for attr in on_attribute:
-            lv = left_df[attr].to_numpy()[l_idx]
-            rv = right_df[attr].to_numpy()[r_idx]
-            keep &= np.asarray(lv == rv, dtype=bool)
+                                method=method, return_device=on_device)
+    return pairs[0], pairs[1]
+
+
+def _attribute_codes(left_df, right_df, on_attribute):
+    """int64 codes per row of each frame: equal on_attribute values, equal
+    codes; a missing value anywhere gives -1 (never equal, as in pandas)."""
+    nl = len(left_df)
+    combined = None
+    for attr in on_attribute:
+        vals = pd.concat([pd.Series(left_df[attr].to_numpy()), pd.Series(right_df[attr].to_numpy())],
+                         ignore_index=True)
+        codes, uniq = pd.factorize(vals, use_na_sentinel=True)
+        codes = codes.astype(np.int64)
+        if combined is None:
+            combined = codes
+        else:
+            miss = (combined < 0) | (codes < 0)
+            mixed, _ = pd.factorize(combined * (len(uniq) + 1) + codes)
+            combined = np.where(miss, -1, mixed.astype(np.int64))
+    return combined[:nl], combined[nl:]
+
+
+def _join_indexers(l_idx, r_idx, n_left, n_right, how, codes=None):
+    """Output row indexers (-1 = missing) and each output row's source pair
+    (-1 = an added row), after the on_attribute filter.  Device pairs go
+    through vs_join_export; host pairs through the same steps in numpy."""
+    if not isinstance(l_idx, np.ndarray):
+        from ._device import export_indexers
+
+        lc, rc = codes if codes is not None else (None, None)
+        return export_indexers(l_idx, r_idx, n_left, n_right, how, lc, rc)
+    l_idx = np.asarray(l_idx, np.intp)
+    r_idx = np.asarray(r_idx, np.intp)
+    kept = None
+    if codes is not None and len(l_idx):
+        lc, rc = codes
+        keep = (lc[l_idx] >= 0) & (lc[l_idx] == rc[r_idx])
+        kept = np.flatnonzero(keep)
         l_idx, r_idx = l_idx[keep], r_idx[keep]
-    return l_idx, r_idx
+    l_out, r_out, src = _adjust_indexers(l_idx, r_idx, n_left, n_right, how)
+    if kept is not None:
+        src = np.where(src >= 0, kept[np.maximum(src, 0)] if len(kept) else -1, -1)
+    return l_out, r_out, src
 
 
 def _reset_index_with_suffix(df, suffix, other):
@@ -161,10 +201,12 @@ def _take_rows(df, rows):
 
 def _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attribute, pair_values=None,
                 value_col=None):
-    """The joined frame; ``pair_values`` (one float per pair, e.g. distances)
-    becomes the last column ``value_col``, NaN on unmatched rows."""
+    """The joined frame of the (left rows, right rows) pairs; ``pair_values``
+    (one float per pair, e.g. distances) becomes the last column
+    ``value_col``, NaN on unmatched rows."""
     lgeom = left_df.geometry.name
     rgeom = right_df.geometry.name
+    codes = _attribute_codes(left_df, right_df, on_attribute) if on_attribute else None
     if on_attribute:
         right_df = right_df.drop(columns=on_attribute)
     left = pd.DataFrame(left_df)
@@ -185,7 +227,7 @@ def _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attri
     lcols, rcols = _suffix_overlaps(list(left.columns), list(right.columns), lsuffix, rsuffix, lgeom, rgeom)
     left.columns, right.columns = pd.Index(lcols), pd.Index(rcols)
     left_index_cols, right_index_cols = lcols[:left_nlevels], rcols[:right_nlevels]
-    l_idx, r_idx, src = _adjust_indexers(l_idx, r_idx, len(left), len(right), how)
+    l_idx, r_idx, src = _join_indexers(l_idx, r_idx, len(left), len(right), how, codes)
     lpart = _take_rows(left, l_idx)
     rpart = _take_rows(right, r_idx)
     joined = pd.concat([lpart, rpart], axis=1)
@@ -228,7 +270,7 @@ def sjoin(left_df, right_df, how="inner", predicate="intersects", lsuffix="left"
         raise TypeError(f"sjoin() got an unexpected keyword argument '{first}'")
     on_attribute = _maybe_make_list(on_attribute)
     _basic_checks(left_df, right_df, how, lsuffix, rsuffix, on_attribute=on_attribute)
-    l_idx, r_idx = _geom_predicate_query(left_df, right_df, predicate, distance, on_attribute, method)
+    l_idx, r_idx = _geom_predicate_query(left_df, right_df, predicate, distance, method)
     return _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attribute)
 
 
