@@ -202,6 +202,17 @@ int vs_join_nearest(vs_context* ctx, const vs_index* index, const vs_points* pts
                     uint32_t flags, int32_t* d_left, int32_t* d_right, double* d_distance,
                     int64_t capacity, int64_t* n_pairs, vs_join_stats* stats);
 
+/* Element-wise distance of aligned rows: row i of the points against row i
+ * of the polygons (polys->n_geoms == pts->n).  d_distance[i] = the same
+ * point-polygon distance as vs_join_dwithin, d_envelope_distance[i]
+ * (nullable) = the distance to the polygon's envelope; both NaN for null or
+ * NaN points, null polygons and polygons without vertices.  Replaces the
+ * element-wise distance / dwithin of point x polygon rows
+ * (src/vibespatial/spatial/point_distance_kernels.py:238-310 via
+ * GeometryArray.distance / dwithin); dwithin(i) = !(envelope > d) && distance <= d. */
+int vs_distance_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, double* d_distance,
+                        double* d_envelope_distance);
+
 /* Join export: the row indexers of a relation join.  Replaces the
  * reference's export (_adjust_join_indexers, src/vibespatial/api/_native_results.py:395-470)
  * and its shared-attribute filter (src/vibespatial/api/tools/sjoin.py:826-888).

@@ -363,3 +363,25 @@ void orc_dpairs_free(orc_dpairs *p) {
     free(p->dist);
     free(p);
 }
+
+/* Row-wise: point i against polygon i (NaN for null / NaN / empty rows). */
+void orc_distance_aligned(const double *px, const double *py, const uint8_t *pvalid, int64_t n, const double *x,
+                          const double *y, const int32_t *ring_off, const int32_t *part_off, const int32_t *geom_off,
+                          const uint8_t *gvalid, double *dist, double *env) {
+    double b[4];
+    for (int64_t i = 0; i < n; ++i) {
+        dist[i] = NAN;
+        env[i] = NAN;
+        if ((pvalid && !pvalid[i]) || (gvalid && !gvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
+        const int32_t r0 = part_off[geom_off[i]], r1 = part_off[geom_off[i + 1]];
+        const int32_t c0 = ring_off[r0], c1 = ring_off[r1];
+        if (c1 <= c0) continue;
+        b[0] = INFINITY; b[1] = INFINITY; b[2] = -INFINITY; b[3] = -INFINITY;
+        for (int32_t c = c0; c < c1; ++c) {
+            b[0] = fmin(b[0], x[c]); b[1] = fmin(b[1], y[c]);
+            b[2] = fmax(b[2], x[c]); b[3] = fmax(b[3], y[c]);
+        }
+        env[i] = orc_envelope_distance(b, px[i], py[i]);
+        dist[i] = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, i);
+    }
+}

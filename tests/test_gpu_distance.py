@@ -176,3 +176,31 @@ def test_distance_joins_empty_sides(ctx, vsabi):
     index2, pts2, keep2 = _device(vsabi, ctx, w, gvalid=np.zeros(10, bool))
     assert index2.dwithin(pts2, distance=1e9)[0].numel() == 0
     assert index2.nearest(pts2)[0].numel() == 0
+
+
+@pytest.mark.parametrize("name", ["star", "degenerate", "lattice"])
+def test_distance_aligned_matches_oracle(ctx, vsabi, oracle, name):
+    import torch
+
+    w = WORKLOADS[name]()
+    p = w.polys
+    m = len(p.geom_off) - 1
+    rng = np.random.default_rng(9)
+    idx = rng.choice(len(w.px), m, replace=len(w.px) < m)
+    px, py = w.px[idx].copy(), w.py[idx].copy()
+    px[::17] = np.nan
+    pvalid = (np.arange(m) % 13 != 0).astype(np.uint8)
+    gvalid = (np.arange(m) % 11 != 0).astype(np.uint8)
+    t = {k: torch.from_numpy(np.ascontiguousarray(getattr(p, k))).cuda()
+         for k in ("x", "y", "ring_off", "part_off", "geom_off")}
+    gv = torch.from_numpy(gvalid).cuda()
+    P = vsabi.make_polygons(t["x"], t["y"], t["ring_off"], t["part_off"], t["geom_off"], gv)
+    dx, dy, dv = (torch.from_numpy(a).cuda() for a in (px, py, pvalid))
+    pts = vsabi.make_points(dx, dy, dv)
+    dist = torch.empty(m, dtype=torch.float64, device="cuda")
+    env = torch.empty(m, dtype=torch.float64, device="cuda")
+    vsabi.distance_aligned(ctx, pts, P, dist, env)
+    ed, ee = oracle.distance_aligned(px, py, pvalid, _oracle_polys(oracle, w, gvalid))
+    np.testing.assert_array_equal(dist.cpu().numpy().view(np.int64), ed.view(np.int64))
+    np.testing.assert_array_equal(env.cpu().numpy().view(np.int64), ee.view(np.int64))
+    assert np.isnan(ed[::13]).all() and (ed[np.isfinite(ed)] >= 0).all()

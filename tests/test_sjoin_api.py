@@ -57,7 +57,14 @@ def backend(request, monkeypatch, oracle):
         monkeypatch.setattr(vs_query, "_pairs_backend", pairs)
         monkeypatch.setattr(vs_query, "_dwithin_backend", dwithin)
         monkeypatch.setattr(vs_query, "_nearest_backend", nearest)
+        def distances(points, polygons):
+            px, py, pv = points.point_buffers()
+            pb = polygons.polygon_buffers()
+            P = oracle.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
+            return oracle.distance_aligned(px, py, pv, P)
+
         monkeypatch.setattr(vs_predicates, "_locate_backend", locate)
+        monkeypatch.setattr(vs_predicates, "_distance_backend", distances)
     return request.param
 
 
@@ -378,3 +385,21 @@ def test_attribute_codes_and_host_export():
     # kept pairs: (0,1) [x,1 == x,1], (1,0) [y,2 == y,2]; rows 2, 3, 4 unmatched
     assert out_l.tolist() == [0, 1, 2, 3, 4] and out_r.tolist() == [1, 0, -1, -1, -1]
     assert src.tolist() == [1, 2, -1, -1, -1]
+
+
+def test_elementwise_distance_dwithin(backend):
+    pts, polys = _distance_frames()
+    p = pts.geometry.iloc[:3].reset_index(drop=True)
+    g = polys.geometry.reset_index(drop=True)
+    d = p.distance(g)
+    # row-aligned: (0.5,0.5) in square 0; (2,0.5) 1 from polygon 1's edge x = 3; (4.5,1.5) vs box 2
+    np.testing.assert_allclose(d.to_numpy(), [0.0, 1.0, np.hypot(5.5, 8.5)])
+    assert p.dwithin(g, 1.0).tolist() == [True, True, False]
+    assert p.dwithin(g, np.array([0.0, 0.5, 20.0])).tolist() == [True, False, True]
+    # polygons on the left, a scalar point on the right, nulls
+    assert g.distance(vs.Point(0.5, 0.5)).tolist()[0] == 0.0
+    pn = vs.GeoSeries([None, vs.Point(0.5, 0.5), vs.Point(np.nan, 1.0)])
+    dn = pn.distance(g)
+    # row 1 pairs (0.5, 0.5) with polygon 1, whose left edge is x = 3
+    assert np.isnan(dn[0]) and dn[1] == 2.5 and np.isnan(dn[2])
+    assert pn.dwithin(g, 100.0).tolist() == [False, True, False]

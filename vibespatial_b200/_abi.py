@@ -29,6 +29,7 @@ EXPORTED = (
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
     "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free", "vs_join_host",
     "vs_thread_kernel_launches", "vs_join_dwithin", "vs_join_nearest", "vs_join_export",
+    "vs_distance_aligned",
 )
 
 
@@ -153,6 +154,7 @@ def load(path: Path | str | None = None):
                                                i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
             "vs_join_nearest": (ctypes.c_int, [vp, vp, ctypes.POINTER(Points), ctypes.c_double, u32, vp, vp, vp,
                                                i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
+            "vs_distance_aligned": (ctypes.c_int, [vp, ctypes.POINTER(Points), ctypes.POINTER(Polygons), vp, vp]),
             "vs_join_export": (ctypes.c_int, [vp, vp, vp, i64, i64, i64, i32, vp, vp, vp, vp, vp, i64,
                                               ctypes.POINTER(i64)]),
             "vs_locate_aligned": (ctypes.c_int, [vp, ctypes.POINTER(Points), ctypes.POINTER(Polygons), vp]),
@@ -551,6 +553,10 @@ def wkb_plan_sizes(ctx: Context, data, offsets, valid, rows) -> dict:
 def kernel_launches() -> int:
     """Kernels the library has launched from this thread so far."""
     return int(load().vs_thread_kernel_launches())
+
+
+def distance_aligned(ctx: Context, pts: Points, polys: Polygons, dist, env=None) -> None:
+    check(load().vs_distance_aligned(ctx.handle, ctypes.byref(pts), ctypes.byref(polys), _ptr(dist), _ptr(env)))
 
 
 def locate_aligned(ctx: Context, pts: Points, polys: Polygons, out) -> None:

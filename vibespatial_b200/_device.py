@@ -163,3 +163,18 @@ def export_indexers(left, right, n_left: int, n_right: int, how: str, left_code=
     out_l, out_r, src = _abi.join_export(ctx, left.contiguous(), right.contiguous(), n_left, n_right, how, lc, rc)
     return (out_l.cpu().numpy().astype(np.intp), out_r.cpu().numpy().astype(np.intp),
             src.cpu().numpy().astype(np.intp))
+
+
+def distance_aligned(points, polygons, device: int = 0):
+    """Row-wise (distance, envelope distance) float64 arrays; NaN for null or empty rows."""
+    torch = _torch()
+    n = len(points)
+    if n == 0:
+        return np.empty(0, np.float64), np.empty(0, np.float64)
+    ctx = _abi.default_context(device)
+    pts, _ = device_points(points, device)
+    P, _ = device_polygons(polygons, device)
+    dist = torch.empty(n, dtype=torch.float64, device=device)
+    env = torch.empty(n, dtype=torch.float64, device=device)
+    _abi.distance_aligned(ctx, pts, P, dist, env)
+    return dist.cpu().numpy(), env.cpu().numpy()

@@ -393,6 +393,54 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
     add_counter(a.counters, 1, n_exact);
 }
 
+// Element-wise: row i of the points against row i of the polygons (SoA
+// inputs).  dist = the point-polygon distance, env = the envelope distance
+// (GEOS's dwithin short-circuit); NaN for null / NaN points, null polygons
+// and polygons without vertices.
+__global__ void distance_aligned_kernel(vs_points pts, vs_polygons polys, double* __restrict__ dist,
+                                        double* __restrict__ env, unsigned long long* counters) {
+    unsigned n_exact = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pts.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool pv = pts.d_valid == nullptr || pts.d_valid[i];
+        const bool gv = polys.d_valid == nullptr || polys.d_valid[i];
+        const double x = pts.d_x[i], y = pts.d_y[i];
+        double d = NAN, e = NAN;
+        if (pv && gv && !isnan(x) && !isnan(y)) {
+            const int g = (int)i;
+            const int r0 = polys.d_part_off[polys.d_geom_off[g]], r1 = polys.d_part_off[polys.d_geom_off[g + 1]];
+            const int c0 = polys.d_ring_off[r0], c1 = polys.d_ring_off[r1];
+            if (c1 > c0) {
+                vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
+                for (int c = c0; c < c1; ++c) {
+                    b.minx = fmin(b.minx, polys.d_x[c]);
+                    b.miny = fmin(b.miny, polys.d_y[c]);
+                    b.maxx = fmax(b.maxx, polys.d_x[c]);
+                    b.maxy = fmax(b.maxy, polys.d_y[c]);
+                }
+                e = envelope_distance(b, x, y);
+                const int loc = geometry_location_soa(x, y, polys.d_x, polys.d_y, polys.d_ring_off, polys.d_part_off,
+                                                      polys.d_geom_off, g, n_exact);
+                if (loc != LOC_OUTSIDE) {
+                    d = 0.0;
+                } else {
+                    d = INFINITY;
+                    for (int ring = r0; ring < r1; ++ring) {
+                        const int a0 = polys.d_ring_off[ring], a1 = polys.d_ring_off[ring + 1];
+                        for (int c = a0 + 1; c < a1; ++c) {
+                            const double s = point_segment_distance(x, y, polys.d_x[c - 1], polys.d_y[c - 1],
+                                                                    polys.d_x[c], polys.d_y[c]);
+                            d = s < d ? s : d;
+                        }
+                    }
+                }
+            }
+        }
+        dist[i] = d;
+        if (env) env[i] = e;
+    }
+    if (n_exact) atomicAdd(&counters[1], (unsigned long long)n_exact);
+}
+
 __global__ void gather_pair_distance_kernel(const int32_t* __restrict__ left, int64_t n,
                                             const double* __restrict__ best, double* __restrict__ out) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -613,6 +661,31 @@ int vs_join_nearest(vs_context* ctx, const vs_index* idx, const vs_points* pts, 
         VS_LAUNCHED("gather_pair_distance", s);
         VS_CUDA_TRY(cudaStreamSynchronize(s));
     }
+    return VS_OK;
+}
+
+int vs_distance_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons* polys, double* d_distance,
+                        double* d_envelope_distance) {
+    if (!ctx || !polys || !d_distance) {
+        set_error("ctx/polys/distance is NULL");
+        return VS_E_ARG;
+    }
+    VS_TRY(check_points(pts));
+    if (polys->n_geoms != pts->n) {
+        set_error("aligned rows: %lld points, %d polygons", (long long)pts->n, polys->n_geoms);
+        return VS_E_ARG;
+    }
+    if (pts->n > 0x7fffffffLL) {
+        set_error("%lld rows: more than the 32-bit rows address", (long long)pts->n);
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    if (pts->n == 0) return VS_OK;
+    cudaStream_t s = ctx->stream;
+    distance_aligned_kernel<<<resident_grid(distance_aligned_kernel, pts->n, 256), 256, 0, s>>>(
+        *pts, *polys, d_distance, d_envelope_distance, ctx->d_counters);
+    VS_LAUNCHED("distance_aligned", s);
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
     return VS_OK;
 }
 

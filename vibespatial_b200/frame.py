@@ -72,7 +72,7 @@ class GeoSeries(pd.Series):
     def sindex(self):
         return self.array.sindex
 
-    def _binary(self, other, op, align):
+    def _rowwise(self, other, fn, align):
         if isinstance(other, GeoSeries):
             if align is None or align:
                 this, other = self.align(other)
@@ -80,10 +80,21 @@ class GeoSeries(pd.Series):
                 index = this.index
             else:
                 this_arr, other_arr, index = self.array, other.array, self.index
-            return pd.Series(this_arr._binary(other_arr, op), index=index)
+            return pd.Series(fn(this_arr, other_arr), index=index)
         if isinstance(other, BaseGeometry):
-            return pd.Series(self.array._binary(other, op), index=self.index)
-        return pd.Series(self.array._binary(_to_geometry_array(other), op), index=self.index)
+            return pd.Series(fn(self.array, other), index=self.index)
+        return pd.Series(fn(self.array, _to_geometry_array(other)), index=self.index)
+
+    def _binary(self, other, op, align):
+        return self._rowwise(other, lambda a, b: a._binary(b, op), align)
+
+    def distance(self, other, align=None):
+        """Row-wise distance to ``other`` (point x polygon rows)."""
+        return self._rowwise(other, lambda a, b: a.distance(b), align)
+
+    def dwithin(self, other, distance, align=None):
+        """Row-wise ``distance(self, other) <= distance`` (point x polygon rows)."""
+        return self._rowwise(other, lambda a, b: a.dwithin(b, distance), align)
 
     def within(self, other, align=None):
         return self._binary(other, "within", align)

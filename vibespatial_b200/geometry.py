@@ -525,6 +525,16 @@ class GeometryArray(ExtensionArray):
     def touches(self, other):
         return self._binary(other, "touches")
 
+    def distance(self, other):
+        from .predicates import distance
+
+        return distance(self, other)
+
+    def dwithin(self, other, distance):
+        from .predicates import dwithin
+
+        return dwithin(self, other, distance)
+
     # -- spatial index ----------------------------------------------------------------
     @property
     def sindex(self):

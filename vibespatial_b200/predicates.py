@@ -44,9 +44,10 @@ _POINT_RIGHT = {
     "covered_by": (),
 }
 
-# Locator used for aligned rows: the CUDA kernel.  Tests of the host logic
-# substitute the CPU oracle here; the package itself never does.
+# Locator and distance of aligned rows: the CUDA kernels.  Tests of the host
+# logic substitute the CPU oracle here; the package itself never does.
 _locate_backend = None
+_distance_backend = None
 
 
 def _locate(points, polygons):
@@ -89,3 +90,46 @@ def binary_predicate(left, right, op: str) -> np.ndarray:
         return np.zeros(n, dtype=bool)
     loc = _locate(points, polys)
     return np.isin(loc, accepted)
+
+
+def _aligned_pair(left, right):
+    right = _broadcast(right, len(left))
+    if left.is_points() and right.is_polygonal():
+        return left, right
+    if left.is_polygonal() and right.is_points():
+        return right, left
+    raise NotImplementedError(
+        "vibespatial_b200 evaluates point x polygon distances only "
+        f"(left families {sorted(left.families())}, right {sorted(right.families())})")
+
+
+def _distances(points, polygons):
+    if _distance_backend is not None:
+        return _distance_backend(points, polygons)
+    from ._device import distance_aligned
+
+    return distance_aligned(points, polygons)
+
+
+def distance(left, right) -> np.ndarray:
+    """Row-wise point-polygon distance (0 inside or on the boundary; NaN for
+    null or empty rows), the distance of the reference's point-distance
+    kernels (src/vibespatial/spatial/point_distance_kernels.py:238-310)."""
+    n = len(left)
+    if n == 0:
+        return np.zeros(0, dtype=np.float64)
+    points, polys = _aligned_pair(left, right)
+    return _distances(points, polys)[0]
+
+
+def dwithin(left, right, d) -> np.ndarray:
+    """Row-wise distance(left, right) <= d, after the envelope short-circuit
+    (envelope distance > d -> False); NaN distances and thresholds are False."""
+    n = len(left)
+    if n == 0:
+        return np.zeros(0, dtype=bool)
+    d = np.broadcast_to(np.asarray(d, dtype=np.float64), (n,))
+    points, polys = _aligned_pair(left, right)
+    dist, env = _distances(points, polys)
+    with np.errstate(invalid="ignore"):
+        return ~(env > d) & (dist <= d)
