@@ -202,6 +202,21 @@ int vs_join_nearest(vs_context* ctx, const vs_index* index, const vs_points* pts
                     uint32_t flags, int32_t* d_left, int32_t* d_right, double* d_distance,
                     int64_t capacity, int64_t* n_pairs, vs_join_stats* stats);
 
+/* Nearest points of every polygon, all ties (sjoin_nearest with the polygons
+ * as the matched side): for each valid query polygon, every point at its
+ * minimum distance (the same point-polygon distance as vs_join_nearest), if
+ * that minimum is <= max_distance.  point_index is an index over the points
+ * built by vs_index_build with each point as a polygon of one ring of one
+ * vertex (geom_off = part_off = ring_off = 0, 1, ..., n; null or NaN points
+ * get no box).  Pairs: d_left = query polygon row, d_right = point row;
+ * d_distance (nullable) the pair distances.  Capacity, VS_JOIN_SORT and
+ * VS_E_CAPACITY as for vs_join.  Replaces the reference's sjoin_nearest query
+ * with the polygon frame as the query side (src/vibespatial/api/tools/sjoin.py:1398,
+ * src/vibespatial/spatial/nearest.py). */
+int vs_join_nearest_polygons(vs_context* ctx, const vs_index* point_index, const vs_polygons* queries,
+                             double max_distance, uint32_t flags, int32_t* d_left, int32_t* d_right,
+                             double* d_distance, int64_t capacity, int64_t* n_pairs, vs_join_stats* stats);
+
 /* Element-wise distance of aligned rows: row i of the points against row i
  * of the polygons (polys->n_geoms == pts->n).  d_distance[i] = the same
  * point-polygon distance as vs_join_dwithin, d_envelope_distance[i]

@@ -385,3 +385,45 @@ void orc_distance_aligned(const double *px, const double *py, const uint8_t *pva
         dist[i] = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, i);
     }
 }
+
+/* Every point at each polygon's minimum distance (pairs sorted by polygon
+ * row, then point row), if that minimum is finite and <= max_distance: the
+ * sjoin_nearest query with the polygons as the matched side.  Brute force
+ * over the points with the envelope lower bound (small test sizes). */
+orc_dpairs *orc_nearest_polygons_join(const double *px, const double *py, const uint8_t *pvalid, int64_t npts,
+                                      const double *x, const double *y, const int32_t *ring_off,
+                                      const int32_t *part_off, const int32_t *geom_off, const uint8_t *gvalid,
+                                      int64_t ngeoms, double max_distance, int nthreads) {
+    double *bounds = (double *)malloc((size_t)(ngeoms > 0 ? ngeoms : 1) * 4 * sizeof(double));
+    orc_geometry_bounds(x, y, ring_off, part_off, geom_off, gvalid, ngeoms, bounds);
+    const int nt = begin_threads(nthreads);
+    dvec *per = (dvec *)calloc((size_t)nt, sizeof(dvec));
+    const size_t m = (size_t)(npts > 0 ? npts : 1);
+    double *dist = (double *)malloc((size_t)nt * m * sizeof(double));
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t g = 0; g < ngeoms; ++g) {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        const double *b = &bounds[4 * g];
+        if (!(b[0] <= b[2])) continue;
+        double *dp = dist + (size_t)tid * m;
+        double best = INFINITY;
+        for (int64_t i = 0; i < npts; ++i) {
+            dp[i] = INFINITY;
+            if ((pvalid && !pvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
+            if (orc_envelope_distance(b, px[i], py[i]) > best * (1.0 + 0x1p-40)) continue;
+            dp[i] = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, g);
+            if (dp[i] < best) best = dp[i];
+        }
+        if (!(best < INFINITY) || !(best <= max_distance)) continue;
+        for (int64_t i = 0; i < npts; ++i)
+            if (dp[i] == best) dvec_push(&per[tid], (int32_t)g, (int32_t)i, best);
+    }
+    free(dist);
+    free(bounds);
+    return gather(per, nt);
+}

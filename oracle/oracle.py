@@ -104,6 +104,9 @@ def lib():
         L.orc_distance_aligned.restype = None
         L.orc_distance_aligned.argtypes = [_dp, _dp, _u8p, ctypes.c_int64, _dp, _dp, _i32p, _i32p, _i32p, _u8p, _dp,
                                            _dp]
+        L.orc_nearest_polygons_join.restype = ctypes.c_void_p
+        L.orc_nearest_polygons_join.argtypes = [_dp, _dp, _u8p, ctypes.c_int64, _dp, _dp, _i32p, _i32p, _i32p, _u8p,
+                                                ctypes.c_int64, ctypes.c_double, ctypes.c_int]
         L.orc_dpairs_count.restype = ctypes.c_int64
         L.orc_dpairs_count.argtypes = [ctypes.c_void_p]
         L.orc_dpairs_copy.restype = None
@@ -279,6 +282,15 @@ def distance_aligned(px, py, pvalid, polys: Polygons):
     lib().orc_distance_aligned(_p(px, _dp), _p(py, _dp), _p(pvalid, _u8p), n, *polys.args(), _p(polys.valid, _u8p),
                                _p(dist, _dp), _p(env, _dp))
     return dist, env
+
+
+def nearest_polygons_join(px, py, pvalid, polys: Polygons, max_distance=float("inf"), threads: int = 0):
+    """Sorted (polygon row, point row, distance): every point at each polygon's
+    minimum distance when that minimum is finite and <= max_distance."""
+    px, py, pvalid = _f64(px), _f64(py), _u8(pvalid)
+    h = lib().orc_nearest_polygons_join(_p(px, _dp), _p(py, _dp), _p(pvalid, _u8p), len(px), *polys.args(),
+                                        _p(polys.valid, _u8p), len(polys), float(max_distance), int(threads))
+    return _dpairs(h)
 
 
 def max_threads() -> int:

@@ -204,3 +204,30 @@ def test_distance_aligned_matches_oracle(ctx, vsabi, oracle, name):
     np.testing.assert_array_equal(dist.cpu().numpy().view(np.int64), ed.view(np.int64))
     np.testing.assert_array_equal(env.cpu().numpy().view(np.int64), ee.view(np.int64))
     assert np.isnan(ed[::13]).all() and (ed[np.isfinite(ed)] >= 0).all()
+
+
+@pytest.mark.parametrize("name", sorted(WORKLOADS))
+def test_nearest_polygons_matches_oracle(ctx, vsabi, oracle, name):
+    """The reverse query (nearest points of every polygon) against the oracle."""
+    import torch
+
+    rng = np.random.default_rng(10)
+    w = _with_outside_points(WORKLOADS[name](), rng)
+    n = len(w.px)
+    m = len(w.polys.geom_off) - 1
+    pvalid = (rng.random(n) > 0.05).astype(np.uint8)
+    gvalid = (rng.random(m) > 0.05).astype(np.uint8)
+    dx, dy, dv = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (w.px, w.py, pvalid))
+    pidx = vsabi.point_index(ctx, dx, dy, dv)
+    t = {k: torch.from_numpy(np.ascontiguousarray(getattr(w.polys, k))).cuda()
+         for k in ("x", "y", "ring_off", "part_off", "geom_off")}
+    gv = torch.from_numpy(gvalid).cuda()
+    P = vsabi.make_polygons(t["x"], t["y"], t["ring_off"], t["part_off"], t["geom_off"], gv)
+    OP = _oracle_polys(oracle, w, gvalid)
+    span = float(np.nanmax(w.polys.x) - np.nanmin(w.polys.x))
+    for md in (np.inf, 0.0, 0.01 * span):
+        el, er, ed = oracle.nearest_polygons_join(w.px, w.py, pvalid, OP, md)
+        gl, gr, gd, _ = vsabi.nearest_polygons(ctx, pidx, P, max_distance=md)
+        np.testing.assert_array_equal(gl.cpu().numpy(), el, err_msg=f"{name} max_distance={md}")
+        np.testing.assert_array_equal(gr.cpu().numpy(), er, err_msg=f"{name} max_distance={md}")
+        np.testing.assert_array_equal(gd.cpu().numpy().view(np.int64), ed.view(np.int64))

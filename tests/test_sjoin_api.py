@@ -56,7 +56,16 @@ def backend(request, monkeypatch, oracle):
 
         monkeypatch.setattr(vs_query, "_pairs_backend", pairs)
         monkeypatch.setattr(vs_query, "_dwithin_backend", dwithin)
+        def nearest_polygons(polygons, points, max_distance=None):
+            px, py, pv = points.point_buffers()
+            pb = polygons.polygon_buffers()
+            P = oracle.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
+            md = float("inf") if max_distance is None else max_distance
+            left, right, dist = oracle.nearest_polygons_join(px, py, pv, P, md)
+            return left.astype(np.intp), right.astype(np.intp), dist
+
         monkeypatch.setattr(vs_query, "_nearest_backend", nearest)
+        monkeypatch.setattr(vs_query, "_nearest_polygons_backend", nearest_polygons)
         def distances(points, polygons):
             px, py, pv = points.point_buffers()
             pb = polygons.polygon_buffers()
@@ -333,8 +342,15 @@ def test_sjoin_nearest(backend):
     right = vs.sjoin_nearest(polys, pts, how="right", distance_col="dist")
     assert sorted(zip(right["index_left"], right.index)) == [(0, 0), (0, 1), (0, 3), (0, 4), (1, 1), (1, 2), (2, 5)]
     assert list(right.columns) == ["index_left", "pid", "geometry", "qid", "dist"]
+    # polygons as the matched side: each polygon's nearest points (ties at 0 on square 0)
+    rev = vs.sjoin_nearest(polys, pts, distance_col="dist")
+    got = sorted(zip(rev.index, rev["index_right"], rev["dist"]))
+    assert got == [(0, 0, 0.0), (0, 3, 0.0), (1, 2, 0.5), (2, 5, np.sqrt(8.0))]
+    # and how='right' with the polygons on the right: the same query
+    rr = vs.sjoin_nearest(pts, polys, how="right", distance_col="dist")
+    assert sorted(zip(rr.index, rr["index_left"], rr["dist"])) == got
     with pytest.raises(NotImplementedError):
-        vs.sjoin_nearest(polys, pts)
+        vs.sjoin_nearest(pts, pts)
     with pytest.raises(ValueError):
         vs.sjoin_nearest(pts, polys, max_distance=-1)
     # the method form

@@ -29,7 +29,7 @@ EXPORTED = (
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
     "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free", "vs_join_host",
     "vs_thread_kernel_launches", "vs_join_dwithin", "vs_join_nearest", "vs_join_export",
-    "vs_distance_aligned",
+    "vs_distance_aligned", "vs_join_nearest_polygons",
 )
 
 
@@ -154,6 +154,8 @@ def load(path: Path | str | None = None):
                                                i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
             "vs_join_nearest": (ctypes.c_int, [vp, vp, ctypes.POINTER(Points), ctypes.c_double, u32, vp, vp, vp,
                                                i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
+            "vs_join_nearest_polygons": (ctypes.c_int, [vp, vp, ctypes.POINTER(Polygons), ctypes.c_double, u32, vp,
+                                                        vp, vp, i64, ctypes.POINTER(i64), ctypes.POINTER(JoinStats)]),
             "vs_distance_aligned": (ctypes.c_int, [vp, ctypes.POINTER(Points), ctypes.POINTER(Polygons), vp, vp]),
             "vs_join_export": (ctypes.c_int, [vp, vp, vp, i64, i64, i64, i32, vp, vp, vp, vp, vp, i64,
                                               ctypes.POINTER(i64)]),
@@ -509,6 +511,43 @@ def wkb_decode(ctx: Context, data, offsets, valid=None):
 
 
 HOW_CODES = {"inner": 0, "left": 1, "right": 2, "outer": 3}
+
+
+def point_index(ctx: Context, x, y, valid=None) -> "DeviceIndex":
+    """An index over points (float64 CUDA tensors) for vs_join_nearest_polygons:
+    each point a polygon of one ring of one vertex."""
+    import torch
+
+    n = int(x.numel())
+    offs = torch.arange(n + 1, dtype=torch.int32, device=x.device)
+    P = make_polygons(x, y, offs, offs, offs, valid)
+    return DeviceIndex(ctx, P, learned=False)
+
+
+def nearest_polygons(ctx: Context, point_index: "DeviceIndex", polys: Polygons, *, max_distance: float = float("inf"),
+                     sort: bool = True, capacity: int | None = None):
+    """vs_join_nearest_polygons: (polygon rows, point rows, distances, stats), CUDA tensors."""
+    import torch
+
+    dev = torch.device("cuda", ctx.device)
+    cap = int(capacity) if capacity is not None else max(1024, int(polys.n_geoms))
+    for _ in range(2):
+        left = torch.empty(cap, dtype=torch.int32, device=dev)
+        right = torch.empty(cap, dtype=torch.int32, device=dev)
+        dist = torch.empty(cap, dtype=torch.float64, device=dev)
+        n = ctypes.c_int64(0)
+        st = JoinStats()
+        status = load().vs_join_nearest_polygons(ctx.handle, point_index.handle, ctypes.byref(polys),
+                                                 float(max_distance), JOIN_SORT if sort else 0, _ptr(left),
+                                                 _ptr(right), _ptr(dist), cap, ctypes.byref(n), ctypes.byref(st))
+        try:
+            check(status, required=int(n.value))
+        except CapacityError as e:
+            cap = max(e.required, 1)
+            continue
+        k = int(n.value)
+        return left[:k], right[:k], dist[:k], st.as_dict()
+    raise RuntimeError("pair buffer sizing did not converge")
 
 
 def join_export(ctx: Context, left, right, n_left: int, n_right: int, how: str, left_code=None, right_code=None):

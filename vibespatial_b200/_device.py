@@ -178,3 +178,27 @@ def distance_aligned(points, polygons, device: int = 0):
     env = torch.empty(n, dtype=torch.float64, device=device)
     _abi.distance_aligned(ctx, pts, P, dist, env)
     return dist.cpu().numpy(), env.cpu().numpy()
+
+
+def point_index(points, device: int = 0) -> "_abi.DeviceIndex":
+    """The points' index for nearest-point queries, built once per array."""
+    key = ("pindex", device)
+    idx = points._cache.get(key)
+    if idx is None:
+        _torch()
+        pts, t = device_points(points, device)
+        idx = points._cache[key] = _abi.point_index(_abi.default_context(device), t["x"], t["y"], t["valid"])
+    return idx
+
+
+def nearest_polygon_pairs(polygons, points, *, max_distance=None, device: int = 0):
+    """Sorted (polygon row, point row, distance): every point at each polygon's
+    minimum distance (within ``max_distance`` when given)."""
+    if len(points) == 0 or len(polygons) == 0:
+        return np.empty(0, np.intp), np.empty(0, np.intp), np.empty(0, np.float64)
+    ctx = _abi.default_context(device)
+    pidx = point_index(points, device)
+    P, _ = device_polygons(polygons, device)
+    md = float("inf") if max_distance is None else float(max_distance)
+    left, right, dist, _ = _abi.nearest_polygons(ctx, pidx, P, max_distance=md)
+    return (left.cpu().numpy().astype(np.intp), right.cpu().numpy().astype(np.intp), dist.cpu().numpy())

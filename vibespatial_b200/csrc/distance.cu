@@ -46,6 +46,7 @@
 
 #include "emit.cuh"
 #include "exact.cuh"
+#include "hilbert.cuh"
 #include "index.cuh"
 #include "join.cuh"
 #include "primitives.cuh"
@@ -573,6 +574,276 @@ int finish_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, uint
     return VS_OK;
 }
 
+// ---------------------------------------------------------- reverse nearest
+// Nearest points of every polygon (all ties).  The tree is an index over the
+// points, each point a one-vertex polygon, so a level-0 box is the point
+// itself; the queries are the polygons, in the Hilbert order of their
+// envelope centres.  Same two walks as the point queries: a greedy bound, a
+// nearest-first walk that keeps each lane's minimum, then the ties.
+
+struct PolyArgs {
+    const double* x;  // query polygons, original rows
+    const double* y;
+    const int32_t* ring_off;
+    const int32_t* part_off;
+    const int32_t* geom_off;
+    const vs_box* qbox;         // envelopes (inverted for null / empty rows)
+    const uint32_t* order;      // query rows, valid ones first
+    const uint32_t* n_valid;
+    const vs_box* nodes;        // the point index
+    int64_t level_off[kMaxLevels];
+    int64_t level_size[kMaxLevels];
+    int levels;
+    int stage_level;
+    int staged;
+    const int32_t* item_geom;   // slot -> point row
+    double cap;                 // max_distance (INFINITY: unbounded)
+    double* best;               // per query row
+    PairSink sink;
+    unsigned long long* counters;
+    unsigned long long* work;
+};
+
+// Distance from a point to query polygon g (SoA, original row): 0 inside or
+// on it, else the smallest point-segment distance over its rings.
+__device__ double point_polygon_soa(const PolyArgs& a, double px, double py, int g, unsigned& n_exact) {
+    if (geometry_location_soa(px, py, a.x, a.y, a.ring_off, a.part_off, a.geom_off, g, n_exact) != LOC_OUTSIDE)
+        return 0.0;
+    double best = INFINITY;
+    const int r0 = a.part_off[a.geom_off[g]], r1 = a.part_off[a.geom_off[g + 1]];
+    for (int ring = r0; ring < r1; ++ring) {
+        const int c0 = a.ring_off[ring], c1 = a.ring_off[ring + 1];
+        for (int c = c0 + 1; c < c1; ++c) {
+            const double d = point_segment_distance(px, py, a.x[c - 1], a.y[c - 1], a.x[c], a.y[c]);
+            best = d < best ? d : best;
+        }
+    }
+    return best;
+}
+
+__device__ __forceinline__ vs_box load_pnode(const PolyArgs& a, const vs_box* s_nodes, int64_t stage_base, int cl,
+                                             int64_t c) {
+    return cl >= a.stage_level ? s_nodes[a.level_off[cl] - stage_base + c] : a.nodes[a.level_off[cl] + c];
+}
+
+// Query polygons: envelope, Hilbert key of its centre in the point frame
+// (clamped; null / empty rows get the all-ones key and are counted out).
+__global__ void poly_query_key_kernel(vs_polygons q, const double* __restrict__ frame, vs_box* __restrict__ qbox,
+                                      uint32_t* __restrict__ keys, uint32_t* __restrict__ order,
+                                      uint32_t* __restrict__ n_valid) {
+    const double f0 = frame[0], f1 = frame[1], f2 = frame[2], f3 = frame[3];
+    const double sx = f2 > f0 ? 4294967295.0 / (f2 - f0) : 0.0;
+    const double sy = f3 > f1 ? 4294967295.0 / (f3 - f1) : 0.0;
+    uint32_t cnt = 0;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < q.n_geoms; g += (int64_t)gridDim.x * blockDim.x) {
+        vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
+        if (q.d_valid == nullptr || q.d_valid[g]) {
+            const int c0 = q.d_ring_off[q.d_part_off[q.d_geom_off[g]]];
+            const int c1 = q.d_ring_off[q.d_part_off[q.d_geom_off[g + 1]]];
+            for (int c = c0; c < c1; ++c) {
+                b.minx = fmin(b.minx, q.d_x[c]);
+                b.miny = fmin(b.miny, q.d_y[c]);
+                b.maxx = fmax(b.maxx, q.d_x[c]);
+                b.maxy = fmax(b.maxy, q.d_y[c]);
+            }
+        }
+        qbox[g] = b;
+        const bool ok = b.minx <= b.maxx && b.miny <= b.maxy;
+        uint32_t k = 0xffffffffu;
+        if (ok) {
+            const double cx = fmin(fmax(0.5 * (b.minx + b.maxx), f0), f2);
+            const double cy = fmin(fmax(0.5 * (b.miny + b.maxy), f1), f3);
+            k = (uint32_t)hilbert_key(quantize(cx, f0, sx), quantize(cy, f1, sy), 16);
+            if (k == 0xffffffffu) k = 0xfffffffeu;
+        }
+        keys[g] = k;
+        order[g] = (uint32_t)g;
+        cnt += ok ? 1u : 0u;
+    }
+    cnt = (uint32_t)warp_sum(cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(n_valid, cnt);
+}
+
+template <bool kEmit>
+__global__ void __launch_bounds__(kDistThreads) poly_nearest_kernel(const PolyArgs a) {
+    extern __shared__ vs_box s_nodes[];
+    __shared__ int2 s_buf[kDistWarps][kWarpBuf];
+    __shared__ unsigned s_cnt[kDistWarps];
+    __shared__ int s_stack[kDistWarps][kDistStack];
+    __shared__ vs_box s_items[kDistWarps][kFanout];
+    const int64_t stage_base = a.level_off[a.stage_level];
+    for (int k = threadIdx.x; k < a.staged; k += blockDim.x) s_nodes[k] = a.nodes[stage_base + k];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_cnt[warp] = 0;
+    __syncthreads();
+    const WarpOut out{s_buf[warp], &s_cnt[warp]};
+    const unsigned lt = (1u << lane) - 1u;
+    const int top = a.levels - 1;
+    const int64_t n = (int64_t)*a.n_valid;
+    unsigned long long n_cand = 0;
+    unsigned n_exact = 0;
+    for (;;) {
+        const int64_t b0 = warp_grab(a.work, kDistGrab);
+        if (b0 >= n) break;
+        const int64_t i = b0 + lane;
+        bool active = i < n;
+        int32_t row = -1;
+        vs_box qb{INFINITY, INFINITY, -INFINITY, -INFINITY};
+        double q = 0.0;
+        if (active) {
+            row = (int32_t)a.order[i];
+            qb = a.qbox[row];
+            q = kEmit ? a.best[row] : a.cap;
+            active = q >= 0.0 && (!kEmit || q < INFINITY);
+        }
+        const double mx = 0.5 * (qb.minx + qb.maxx), my = 0.5 * (qb.miny + qb.maxy);
+        double my_best = INFINITY;
+        double sx = active ? mx : 0.0, sy = active ? my : 0.0;
+        int cnt = active ? 1 : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        }
+        const double cx = cnt ? sx / cnt : 0.0, cy = cnt ? sy / cnt : 0.0;
+        if (!kEmit && active) {
+            // greedy descent towards the envelope centre, then the nearest point of the block
+            int64_t node = 0;
+            bool ok = true;
+            for (int cl = top - 1; cl >= 1 && ok; --cl) {
+                const int64_t first = node * kFanout;
+                const int64_t last = first + kFanout < a.level_size[cl] ? first + kFanout : a.level_size[cl];
+                double bd = INFINITY;
+                int64_t bc = -1;
+                for (int64_t c = first; c < last; ++c) {
+                    const vs_box b = load_pnode(a, s_nodes, stage_base, cl, c);
+                    if (!(b.minx <= b.maxx)) continue;
+                    const double d = descent_key(b, mx, my);
+                    if (d < bd) {
+                        bd = d;
+                        bc = c;
+                    }
+                }
+                ok = bc >= 0;
+                node = bc;
+            }
+            if (ok) {
+                const int64_t first = top == 0 ? 0 : node * kFanout;
+                const int64_t last = top == 0 ? 1 : (first + kFanout < a.level_size[0] ? first + kFanout
+                                                                                      : a.level_size[0]);
+                double bd = INFINITY;
+                int64_t bi = -1;
+                for (int64_t c = first; c < last; ++c) {
+                    const vs_box b = a.nodes[a.level_off[0] + c];
+                    if (!(b.minx <= b.maxx)) continue;
+                    const double d = box_dist2(qb, b.minx, b.miny);
+                    if (d < bd) {
+                        bd = d;
+                        bi = c;
+                    }
+                }
+                if (bi >= 0) {
+                    const vs_box b = a.nodes[a.level_off[0] + bi];
+                    my_best = point_polygon_soa(a, b.minx, b.miny, row, n_exact);
+                }
+            }
+        }
+        double lx0, lx1, ly0, ly1, x0, x1, y0, y1;
+        auto boxes = [&]() {
+            const double r = kEmit ? q : fmin(my_best, q);
+            const double qi = active ? inflate(r) : 0.0;
+            lx0 = active ? __dsub_rd(qb.minx, qi) : INFINITY;
+            lx1 = active ? __dadd_ru(qb.maxx, qi) : -INFINITY;
+            ly0 = active ? __dsub_rd(qb.miny, qi) : INFINITY;
+            ly1 = active ? __dadd_ru(qb.maxy, qi) : -INFINITY;
+            x0 = lx0, x1 = lx1, y0 = ly0, y1 = ly1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                x0 = fmin(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+                x1 = fmax(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+                y0 = fmin(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+                y1 = fmax(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+            }
+        };
+        boxes();
+        int sp = 0;
+        if (__any_sync(0xffffffffu, active)) {
+            if (lane == 0) s_stack[warp][0] = top;
+            sp = 1;
+        }
+        __syncwarp();
+        while (sp > 0) {
+            --sp;
+            const int e = s_stack[warp][sp];
+            __syncwarp();
+            const int cl = e & 15;
+            const int64_t c = (int64_t)(e >> 4) * kFanout + (lane & 15);
+            const bool root = cl == top;
+            const bool in_range = root ? lane == 0 : (lane < kFanout && c < a.level_size[cl]);
+            const int64_t cc = root ? 0 : c;
+            vs_box b{INFINITY, INFINITY, -INFINITY, -INFINITY};
+            if (in_range) b = load_pnode(a, s_nodes, stage_base, cl, cc);
+            const bool hit = in_range && b.minx <= x1 && b.maxx >= x0 && b.miny <= y1 && b.maxy >= y0;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (cl > 0) {
+                int rank = __popc(m & lt);
+                if (!kEmit) {
+                    // nearest to the packet's centre on top of the stack
+                    const double key = hit ? box_dist2(b, cx, cy) : INFINITY;
+                    int closer = 0;
+#pragma unroll
+                    for (int j = 0; j < kFanout; ++j) {
+                        const double kj = __shfl_sync(0xffffffffu, key, j);
+                        closer += ((m >> j) & 1u) && (kj < key || (kj == key && j < lane)) ? 1 : 0;
+                    }
+                    rank = __popc(m) - 1 - closer;
+                }
+                if (hit) {
+                    const int pos = sp + rank;
+                    if (pos < kDistStack) s_stack[warp][pos] = (int)(cc << 4) | (cl - 1);
+                }
+                int add = __popc(m);
+                if (sp + add > kDistStack) {
+                    if (lane == 0) atomicOr(&a.counters[4], 1ull);
+                    add = kDistStack - sp;
+                }
+                sp += add;
+                __syncwarp();
+            } else {
+                if (lane < kFanout) s_items[warp][lane] = b;
+                __syncwarp();
+                unsigned mm = m;
+                const int64_t slot0 = root ? 0 : (int64_t)(e >> 4) * kFanout;
+                while (mm) {
+                    const int j = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    const vs_box ib = s_items[warp][j];  // a point: (x, y, x, y)
+                    const int slot = (int)(slot0 + j);
+                    bool want = false;
+                    if (active && ib.minx <= lx1 && ib.maxx >= lx0 && ib.miny <= ly1 && ib.maxy >= ly0) {
+                        ++n_cand;
+                        const double bound = kEmit ? q : my_best;
+                        if (!(envelope_distance(qb, ib.minx, ib.miny) > bound * (1.0 + 0x1p-40))) {
+                            const double d = point_polygon_soa(a, ib.minx, ib.miny, row, n_exact);
+                            if (kEmit) want = d == q;
+                            else my_best = d < my_best ? d : my_best;
+                        }
+                    }
+                    if (kEmit) wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                }
+                __syncwarp();
+                if (!kEmit) boxes();
+            }
+        }
+        if (!kEmit && active) a.best[row] = my_best <= q ? my_best : INFINITY;
+        if (kEmit) wflush(out, a.sink, false);
+    }
+    if (kEmit) wflush(out, a.sink, true);
+    add_counter(a.counters, 5, n_cand);
+    add_counter(a.counters, 1, n_exact);
+}
+
 }  // namespace
 }  // namespace vs
 
@@ -686,6 +957,107 @@ int vs_distance_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons
         *pts, *polys, d_distance, d_envelope_distance, ctx->d_counters);
     VS_LAUNCHED("distance_aligned", s);
     VS_CUDA_TRY(cudaStreamSynchronize(s));
+    return VS_OK;
+}
+
+int vs_join_nearest_polygons(vs_context* ctx, const vs_index* point_index, const vs_polygons* queries,
+                              double max_distance, uint32_t flags, int32_t* d_left, int32_t* d_right,
+                              double* d_distance, int64_t capacity, int64_t* n_pairs, vs_join_stats* stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!ctx || !point_index || !n_pairs) {
+        set_error("ctx/index/n_pairs is NULL");
+        return VS_E_ARG;
+    }
+    *n_pairs = 0;
+    VS_TRY(check_polygons(queries));
+    if (capacity < 0 || (capacity > 0 && (!d_left || !d_right))) {
+        set_error("invalid pair buffers (capacity %lld)", (long long)capacity);
+        return VS_E_ARG;
+    }
+    if (point_index->device != ctx->device) {
+        set_error("index lives on device %d, context on device %d", point_index->device, ctx->device);
+        return VS_E_ARG;
+    }
+    if (max_distance != max_distance) {
+        set_error("max_distance is NaN");
+        return VS_E_ARG;
+    }
+    VS_TRY(use_device(ctx->device));
+    const int64_t nq = queries->n_geoms;
+    if (nq == 0 || point_index->n_geoms == 0 || !(point_index->h_frame[0] <= point_index->h_frame[2]) ||
+        max_distance < 0.0)
+        return VS_OK;
+    cudaStream_t s = ctx->stream;
+    const long long launches0 = g_launches;
+    EventPair ev;
+    VS_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, kDevCounters * sizeof(unsigned long long), s));
+    cudaEventRecord(ev.a, s);
+    Scratch<vs_box> qbox;
+    Scratch<uint32_t> keys, order, n_valid;
+    Scratch<double> best;
+    VS_TRY(qbox.alloc((size_t)nq, s));
+    VS_TRY(keys.alloc((size_t)nq, s));
+    VS_TRY(order.alloc((size_t)nq, s));
+    VS_TRY(n_valid.alloc(1, s));
+    VS_TRY(best.alloc((size_t)nq, s));
+    VS_CUDA_TRY(cudaMemsetAsync(n_valid.p, 0, sizeof(uint32_t), s));
+    poly_query_key_kernel<<<resident_grid(poly_query_key_kernel, nq, 256), 256, 0, s>>>(
+        *queries, point_index->frame, qbox.p, keys.p, order.p, n_valid.p);
+    VS_LAUNCHED("poly_query_key", s);
+    VS_TRY(radix_sort_u32_u32(keys.p, order.p, nq, 32, s, 0));
+    PolyArgs a{};
+    a.x = queries->d_x;
+    a.y = queries->d_y;
+    a.ring_off = queries->d_ring_off;
+    a.part_off = queries->d_part_off;
+    a.geom_off = queries->d_geom_off;
+    a.qbox = qbox.p;
+    a.order = order.p;
+    a.n_valid = n_valid.p;
+    a.nodes = point_index->nodes;
+    for (int l = 0; l < kMaxLevels; ++l) {
+        a.level_off[l] = point_index->level_off[l];
+        a.level_size[l] = point_index->level_size[l];
+    }
+    a.levels = point_index->levels;
+    int sl = point_index->levels - 1;
+    int64_t staged = point_index->level_size[sl];
+    while (sl > 0 && staged + point_index->level_size[sl - 1] <= kDistMaxStaged) {
+        --sl;
+        staged += point_index->level_size[sl];
+    }
+    a.stage_level = sl;
+    a.staged = (int)staged;
+    a.item_geom = point_index->item_geom;
+    a.cap = max_distance;
+    a.best = best.p;
+    a.sink = PairSink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
+    a.counters = ctx->d_counters;
+    a.work = &ctx->d_counters[kWorkCounter];
+    const size_t smem = (size_t)a.staged * sizeof(vs_box);
+    // each polygon's minimum distance, then every point at exactly that distance
+    VS_CUDA_TRY(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
+    VS_CUDA_TRY(cudaFuncSetAttribute(poly_nearest_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    poly_nearest_kernel<false><<<resident_grid(poly_nearest_kernel<false>, nq, kDistThreads, smem), kDistThreads,
+                                 smem, s>>>(a);
+    VS_LAUNCHED("poly_nearest<min>", s);
+    VS_CUDA_TRY(cudaMemsetAsync(a.work, 0, sizeof(unsigned long long), s));
+    VS_CUDA_TRY(cudaFuncSetAttribute(poly_nearest_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    poly_nearest_kernel<true><<<resident_grid(poly_nearest_kernel<true>, nq, kDistThreads, smem), kDistThreads,
+                                smem, s>>>(a);
+    VS_LAUNCHED("poly_nearest<emit>", s);
+    vs_points qp{};
+    qp.n = nq;  // the pair sort keys left rows by the query count
+    const int st = finish_join(ctx, point_index, &qp, flags, d_left, d_right, capacity, n_pairs, stats, ev, launches0);
+    if (st != VS_OK) return st;
+    if (d_distance && *n_pairs > 0) {
+        gather_pair_distance_kernel<<<resident_grid(gather_pair_distance_kernel, *n_pairs, 256), 256, 0, s>>>(
+            d_left, *n_pairs, best.p, d_distance);
+        VS_LAUNCHED("gather_pair_distance", s);
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
+    }
     return VS_OK;
 }
 

@@ -32,6 +32,7 @@ _TREE_POINTS = {None: None, "intersects": "intersects", "contains": "within", "c
 _pairs_backend = None
 _dwithin_backend = None
 _nearest_backend = None
+_nearest_polygons_backend = None
 
 
 def _pairs(points, polygons, predicate, method, on_device=False):
@@ -74,6 +75,17 @@ def nearest_pairs(points, polygons, *, max_distance=None, method="learned"):
     from ._device import nearest_pairs as device_nearest
 
     return device_nearest(points, polygons, max_distance=max_distance, method=method)
+
+
+def nearest_polygon_pairs(polygons, points, *, max_distance=None):
+    """(polygon rows, point rows, distances): every point at each polygon's
+    minimum distance, within ``max_distance`` when given, sorted by (polygon,
+    point) -- the query of sjoin_nearest when the polygons are the matched side."""
+    if _nearest_polygons_backend is not None:
+        return _nearest_polygons_backend(polygons, points, max_distance=max_distance)
+    from ._device import nearest_polygon_pairs as device_nearest
+
+    return device_nearest(polygons, points, max_distance=max_distance)
 
 
 def _distance_args(distance, n_geometry, geometry_is_points):

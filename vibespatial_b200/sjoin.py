@@ -282,12 +282,13 @@ def sjoin_nearest(left_df, right_df, how="inner", max_distance=None, lsuffix="le
     (src/vibespatial/api/tools/sjoin.py:1398): every row of the matched side
     (the left frame, or the right frame for ``how='right'``) gets every
     geometry of the other frame at its minimum distance (all ties), within
-    ``max_distance`` when given; ``distance_col`` adds the distances.  The
-    matched side must hold points and the other side polygons (the GPU index
-    is built over the polygons).  ``exclusive`` drops equal geometries, which a
-    point and a polygon never are.
+    ``max_distance`` when given; ``distance_col`` adds the distances.  One
+    side must hold points and the other polygons: points matched to polygons
+    use the polygons' index, polygons matched to points an index over the
+    points.  ``exclusive`` drops equal geometries, which a point and a polygon
+    never are.
     """
-    from .query import nearest_pairs
+    from .query import nearest_pairs, nearest_polygon_pairs
 
     method = kwargs.pop("method", "learned")
     if kwargs:
@@ -298,11 +299,16 @@ def sjoin_nearest(left_df, right_df, how="inner", max_distance=None, lsuffix="le
         raise ValueError("max_distance must be greater than or equal to 0")
     query_df, tree_df = (right_df, left_df) if how == "right" else (left_df, right_df)
     q_geom, t_geom = query_df.geometry.array, tree_df.geometry.array
-    if len(q_geom) and len(t_geom) and not (q_geom.is_points() and t_geom.is_polygonal()):
+    if len(q_geom) and len(t_geom) and q_geom.is_points() and t_geom.is_polygonal():
+        q_rows, t_rows, dist = nearest_pairs(q_geom, t_geom, max_distance=max_distance, method=method)
+    elif len(q_geom) and len(t_geom) and q_geom.is_polygonal() and t_geom.is_points():
+        q_rows, t_rows, dist = nearest_polygon_pairs(q_geom, t_geom, max_distance=max_distance)
+    elif len(q_geom) == 0 or len(t_geom) == 0:
+        q_rows, t_rows, dist = np.empty(0, np.intp), np.empty(0, np.intp), np.empty(0, np.float64)
+    else:
         raise NotImplementedError(
-            "sjoin_nearest matches points to their nearest polygons/multipolygons: the "
-            + ("right" if how == "right" else "left") + " frame must hold points and the other one polygons")
-    q_rows, t_rows, dist = nearest_pairs(q_geom, t_geom, max_distance=max_distance, method=method)
+            "vibespatial_b200 joins points with polygons/multipolygons only "
+            f"(families {sorted(q_geom.families())} and {sorted(t_geom.families())})")
     l_idx, r_idx = (t_rows, q_rows) if how == "right" else (q_rows, t_rows)
     return _frame_join(left_df, right_df, np.asarray(l_idx, np.intp), np.asarray(r_idx, np.intp), how, lsuffix,
                        rsuffix, None, pair_values=dist, value_col=distance_col)
