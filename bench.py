@@ -136,6 +136,8 @@ WORKLOAD_DESC = {
     "dwithin": "dwithin: zipf_join's 50M FP64 points x 1M footprints, pairs within distance 0.25 (1.7x the median "
                "footprint side)",
     "nearest": "nearest (sjoin_nearest, all ties, unbounded): zipf_join's 50M FP64 points x 1M footprints",
+    "nearest_polygons": "nearest points of every polygon (sjoin_nearest with the polygons matched, all ties, "
+                        "unbounded): zipf_join's 1M footprints x 50M points",
     "export": "join export: zipf_join's within pairs (50M points x 1M footprints) to how='left' row indexers "
               "(50M+ rows) after an on_attribute filter (codes row % 7 on both sides)",
     "wkb": "wkb ingest: the zipf_join inputs as little-endian 2D WKB columns (50M Points, 21 B each; 1M Polygons), "
@@ -760,6 +762,84 @@ def run_export(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_nearest_polygons(args, rank, world, local_rank):
+    """Nearest points of every polygon through vs_join_nearest_polygons (index over the points)."""
+    import torch
+
+    from vibespatial_b200 import _abi
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    w = make_workload("zipf", rank, args.scale)
+    ctx = _abi.Context(dev)
+    stream = ctx.torch_stream
+    pol = w.polys
+    d_poly = {k: torch.from_numpy(np.ascontiguousarray(getattr(pol, k))).to(dev)
+              for k in ("x", "y", "ring_off", "part_off", "geom_off")}
+    P = _abi.make_polygons(d_poly["x"], d_poly["y"], d_poly["ring_off"], d_poly["part_off"], d_poly["geom_off"])
+    dx, dy = torch.from_numpy(w.px).to(dev), torch.from_numpy(w.py).to(dev)
+    t0 = time.perf_counter()
+    pidx = _abi.point_index(ctx, dx, dy)
+    build_wall = time.perf_counter() - t0
+    M = len(pol.geom_off) - 1
+    left, right, dist, st = _abi.nearest_polygons(ctx, pidx, P)
+    n_pairs = int(left.numel())
+    cap = max(n_pairs, 1)
+    for _ in range(args.warmup):
+        _abi.nearest_polygons(ctx, pidx, P, capacity=cap)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms, launches = [], 0
+    with ClockSampler(dev) as clk:
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            _, _, _, st = _abi.nearest_polygons(ctx, pidx, P, capacity=cap)
+            ev[k][1].record(stream)
+            kernel_ms.append(st["kernel_ms"])
+            launches += st["kernel_launches"]
+        torch.cuda.synchronize()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    value = M * args.steps / (total_ms / 1e3)
+    peak, peak_kind = _peaks()
+    kmed = float(np.median(kernel_ms))
+    B = algorithmic_bytes(w, n_pairs) + 8 * n_pairs
+    achieved = B / (kmed / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        O.build()
+        threads = os.cpu_count() or 1
+        k = 64
+        sub = {"x": pol.x, "y": pol.y, "ring_off": pol.ring_off, "part_off": pol.part_off,
+               "geom_off": pol.geom_off[:k + 1]}
+        SP = O.Polygons(sub["x"], sub["y"], sub["ring_off"], sub["part_off"], sub["geom_off"])
+        t0 = time.perf_counter()
+        O.nearest_polygons_join(w.px, w.py, None, SP, threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": k / dt, "unit": "polygons/s", "cores": threads, "kind": "port",
+               "sample": f"the first {k} of {M} polygons against all {w.n_points} points ({dt:.1f} s), CPU oracle "
+                         "(C + OpenMP, brute force over the points with the envelope bound)"}
+    line = {
+        "metric": "query polygons/sec", "value": value, "unit": "polygons/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC["nearest_polygons"], "n_polygons": M, "n_points": w.n_points,
+                   "n_pairs": n_pairs, "point_index_build_wall_s": build_wall,
+                   "l2": "inputs (800 MB of points, index 1.6 GB) larger than L2; no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "kernel_ms": kmed, "algorithmic_bytes_per_launch": B},
+        "cpu_baseline": cpu,
+        "e2e": None,
+        "gpu_launches": launches,
+        "join_stats": st,
+    }
+    line["clocks"] = clk.summary()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -774,6 +854,12 @@ def run_reference(args, rank, world):
         return
     if args.workload == "export":
         run_reference_export(args, world)
+        return
+    if args.workload == "nearest_polygons":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's polygon-side nearest query needs "
+                                                              "Shapely/GEOS (not installable here); the bench line "
+                                                              "times the CPU oracle on a sample as cpu_baseline"}),
+              flush=True)
         return
     w = make_workload(args.workload, 0, args.scale)
     threads = os.cpu_count() or 1
@@ -1218,6 +1304,8 @@ def main():
             run_distance(args, rank, world, local_rank)
         elif args.workload == "export":
             run_export(args, rank, world, local_rank)
+        elif args.workload == "nearest_polygons":
+            run_nearest_polygons(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

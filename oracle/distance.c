@@ -398,8 +398,6 @@ orc_dpairs *orc_nearest_polygons_join(const double *px, const double *py, const 
     orc_geometry_bounds(x, y, ring_off, part_off, geom_off, gvalid, ngeoms, bounds);
     const int nt = begin_threads(nthreads);
     dvec *per = (dvec *)calloc((size_t)nt, sizeof(dvec));
-    const size_t m = (size_t)(npts > 0 ? npts : 1);
-    double *dist = (double *)malloc((size_t)nt * m * sizeof(double));
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static)
 #endif
@@ -410,20 +408,22 @@ orc_dpairs *orc_nearest_polygons_join(const double *px, const double *py, const 
 #endif
         const double *b = &bounds[4 * g];
         if (!(b[0] <= b[2])) continue;
-        double *dp = dist + (size_t)tid * m;
+        /* the minimum, then (a second pass) every point at exactly it */
         double best = INFINITY;
         for (int64_t i = 0; i < npts; ++i) {
-            dp[i] = INFINITY;
             if ((pvalid && !pvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
             if (orc_envelope_distance(b, px[i], py[i]) > best * (1.0 + 0x1p-40)) continue;
-            dp[i] = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, g);
-            if (dp[i] < best) best = dp[i];
+            const double d = orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, g);
+            if (d < best) best = d;
         }
         if (!(best < INFINITY) || !(best <= max_distance)) continue;
-        for (int64_t i = 0; i < npts; ++i)
-            if (dp[i] == best) dvec_push(&per[tid], (int32_t)g, (int32_t)i, best);
+        for (int64_t i = 0; i < npts; ++i) {
+            if ((pvalid && !pvalid[i]) || isnan(px[i]) || isnan(py[i])) continue;
+            if (orc_envelope_distance(b, px[i], py[i]) > best * (1.0 + 0x1p-40)) continue;
+            if (orc_point_polygon_distance(px[i], py[i], x, y, ring_off, part_off, geom_off, g) == best)
+                dvec_push(&per[tid], (int32_t)g, (int32_t)i, best);
+        }
     }
-    free(dist);
     free(bounds);
     return gather(per, nt);
 }
