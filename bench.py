@@ -762,6 +762,40 @@ def run_export(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_nearest_polygons(args, world):
+    """The CPU oracle (brute force over the points with the envelope bound, all
+    host threads) on the first polygons of the same workload."""
+    w = make_workload("zipf", 0, args.scale)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.build()
+    pol = w.polys
+    k = 32
+    SP = O.Polygons(pol.x, pol.y, pol.ring_off, pol.part_off, pol.geom_off[:k + 1])
+    for _ in range(args.warmup):
+        O.nearest_polygons_join(w.px, w.py, None, SP, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.nearest_polygons_join(w.px, w.py, None, SP, threads=threads)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = k * len(times) / tot
+    line = {
+        "impl": "reference", "metric": "query polygons/sec", "value": value, "unit": "polygons/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC["nearest_polygons"], "sample_polygons": k, "n_points": w.n_points},
+        "cpu_baseline": {"value": value, "unit": "polygons/s", "cores": threads, "kind": "port",
+                         "sample": f"the first {k} polygons against all {w.n_points} points each step, CPU oracle "
+                                   "(C + OpenMP); Shapely/GEOS is not installable here"},
+        "e2e": {"value": value, "unit": "polygons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_nearest_polygons(args, rank, world, local_rank):
     """Nearest points of every polygon through vs_join_nearest_polygons (index over the points)."""
     import torch
@@ -856,10 +890,7 @@ def run_reference(args, rank, world):
         run_reference_export(args, world)
         return
     if args.workload == "nearest_polygons":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference's polygon-side nearest query needs "
-                                                              "Shapely/GEOS (not installable here); the bench line "
-                                                              "times the CPU oracle on a sample as cpu_baseline"}),
-              flush=True)
+        run_reference_nearest_polygons(args, world)
         return
     w = make_workload(args.workload, 0, args.scale)
     threads = os.cpu_count() or 1
