@@ -218,6 +218,31 @@ def test_last_hilbert_cell_with_null_points(vsabi, ctx, oracle, method):
         assert_same_pairs(gl, gr, el, er)
 
 
+def test_index_counts_skip_null_polygons(vsabi, ctx, oracle):
+    """Null polygons own no rings in the index's layout; later passes over
+    the layout (the ring y-bins, the learned index's FP32 vertices) cover only
+    the laid-out rings."""
+    from types import SimpleNamespace
+
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.star_join(seed=6, n_points=20_000, n_polys=400)  # 8-64 vertices: long rings get y-bins
+    m = len(w.polys.geom_off) - 1
+    gvalid = (np.arange(m) % 3 != 0).astype(np.uint8)
+    polys = SimpleNamespace(x=w.polys.x, y=w.polys.y, ring_off=w.polys.ring_off, part_off=w.polys.part_off,
+                            geom_off=w.polys.geom_off, valid=gvalid)
+    pts, keep1 = upload_points(vsabi, w.px, w.py, None)
+    P, keep2 = upload_polys(vsabi, polys)
+    index = vsabi.DeviceIndex(ctx, P, learned=True)
+    info = index.info()
+    n_valid_rings = int(gvalid.sum())  # one ring per star polygon
+    assert 0 < info["n_binned_rings"] <= n_valid_rings
+    el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, polys), "within")
+    for method in (0, 1):
+        gl, gr, _ = index.join(pts, PRED_CODES["within"], method, sort=True)
+        assert_same_pairs(gl.cpu().numpy(), gr.cpu().numpy(), el, er)
+
+
 def test_capacity_error_reports_required_size(vsabi, ctx, oracle):
     import torch
     from vibespatial_b200.testing import synthetic as syn

@@ -377,6 +377,7 @@ int build_rtree(vs_context* ctx, const vs_polygons* P, vs_index* idx) {
     VS_TRY(vals.alloc((size_t)M, s));
     VS_TRY(keys.alloc((size_t)M, s));
     VS_TRY(totals.alloc(4, s));
+    VS_CUDA_TRY(cudaMemsetAsync(totals.p, 0, 4 * sizeof(uint32_t), s));
 
     if (M > 0) {
         geom_bounds_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(*P, box.p, np.p, nr.p, nc.p);
@@ -413,7 +414,15 @@ int build_rtree(vs_context* ctx, const vs_polygons* P, vs_index* idx) {
         VS_CUDA_TRY(cudaMemcpyAsync(idx->nodes, &empty, sizeof(empty), cudaMemcpyHostToDevice, s));
     }
     VS_CUDA_TRY(cudaMemcpyAsync(idx->h_frame, idx->frame, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    uint32_t laid[3] = {0, 0, 0};
+    VS_CUDA_TRY(cudaMemcpyAsync(laid, totals.p, sizeof(laid), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
+    // Null polygons own no parts, rings or vertices in the slot layout: the
+    // index's counts are those laid out, which is what every later pass over
+    // part_off / ring_off / xy may read.
+    idx->n_parts = (int32_t)laid[0];
+    idx->n_rings = (int32_t)laid[1];
+    idx->n_coords = (int64_t)laid[2];
     return VS_OK;
 }
 
