@@ -419,3 +419,21 @@ def test_elementwise_distance_dwithin(backend):
     # row 1 pairs (0.5, 0.5) with polygon 1, whose left edge is x = 3
     assert np.isnan(dn[0]) and dn[1] == 2.5 and np.isnan(dn[2])
     assert pn.dwithin(g, 100.0).tolist() == [False, True, False]
+
+
+def test_sindex_nearest(backend):
+    pts, polys = _distance_frames()
+    tree = polys.geometry.array
+    q = pts.geometry.array
+    idx, dist = tree.sindex.nearest(q, return_distance=True)
+    assert idx[0].tolist() == [0, 1, 1, 2, 3, 4, 5] and idx[1].tolist() == [0, 0, 1, 1, 0, 0, 2]
+    np.testing.assert_allclose(dist, [0, 1, 1, 0.5, 0, 5, np.sqrt(8)])
+    one = tree.sindex.nearest(q, return_all=False)
+    assert one[0].tolist() == [0, 1, 2, 3, 4, 5] and one[1].tolist() == [0, 0, 1, 0, 0, 2]
+    assert tree.sindex.nearest(q, max_distance=0.6)[0].tolist() == [0, 2, 3]
+    assert tree.sindex.nearest(vs.Point(8, 8)).tolist() == [[0], [2]]
+    # polygons as the input, points as the tree
+    r = q.sindex.nearest(tree)
+    assert r[0].tolist() == [0, 0, 1, 2] and r[1].tolist() == [0, 3, 2, 5]
+    with pytest.raises(NotImplementedError):
+        tree.sindex.nearest(q, k=2)

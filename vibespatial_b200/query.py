@@ -268,3 +268,42 @@ class SpatialIndex:
             return scipy.sparse.coo_array((ones, tree_rows.reshape(1, -1)), shape=(n_tree,), dtype=np.bool_)
         return scipy.sparse.coo_array((ones, (tree_rows, input_rows)), shape=(n_tree, len(geometry)),
                                       dtype=np.bool_)
+
+    def nearest(self, geometry, return_all=True, max_distance=None, return_distance=False, exclusive=False, k=1):
+        """The nearest tree geometries of every input geometry (sindex.nearest,
+        src/vibespatial/api/sindex.py:2018): a (2, n) intp array of (input row,
+        tree row), plus the distances with ``return_distance``.  Ties are all
+        returned unless ``return_all=False`` (then the smallest tree row).
+        ``max_distance`` bounds the search.  Points against polygons either way
+        round; ``exclusive`` drops equal geometries, which a point and a
+        polygon never are; ``k`` must be 1."""
+        from .geometry import BaseGeometry, GeometryArray
+
+        if k != 1:
+            raise NotImplementedError("k-nearest (k > 1) is outside this point x polygon join")
+        if max_distance is not None and max_distance < 0:
+            raise ValueError("max_distance must be greater than or equal to 0")
+        if isinstance(geometry, BaseGeometry):
+            geometry = GeometryArray.from_shapes([geometry])
+        else:
+            geometry = getattr(geometry, "values", geometry)
+            if not isinstance(geometry, GeometryArray):
+                geometry = GeometryArray.from_shapes(list(geometry))
+        tree = self.geometry
+        if len(tree) == 0 or len(geometry) == 0:
+            rows, trows, dist = np.empty(0, np.intp), np.empty(0, np.intp), np.empty(0, np.float64)
+        elif geometry.is_points() and tree.is_polygonal():
+            rows, trows, dist = nearest_pairs(geometry, tree, max_distance=max_distance)
+        elif geometry.is_polygonal() and tree.is_points():
+            rows, trows, dist = nearest_polygon_pairs(geometry, tree, max_distance=max_distance)
+        else:
+            raise NotImplementedError(
+                "vibespatial_b200 joins points with polygons/multipolygons only "
+                f"(tree families {sorted(tree.families())}, input families {sorted(geometry.families())})")
+        rows, trows, dist = np.asarray(rows, np.intp), np.asarray(trows, np.intp), np.asarray(dist, np.float64)
+        if not return_all and len(rows):
+            first = np.concatenate([[True], rows[1:] != rows[:-1]])
+            rows, trows, dist = rows[first], trows[first], dist[first]
+        out = np.vstack([rows, trows])
+        return (out, dist) if return_distance else out
+
