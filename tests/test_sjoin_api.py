@@ -437,3 +437,19 @@ def test_sindex_nearest(backend):
     assert r[0].tolist() == [0, 0, 1, 2] and r[1].tolist() == [0, 3, 2, 5]
     with pytest.raises(NotImplementedError):
         tree.sindex.nearest(q, k=2)
+
+
+def test_sindex_reductions(backend):
+    tree = vs.GeometryArray.from_shapes([vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11)])
+    q = vs.GeoSeries([vs.Point(1, 1), vs.Point(4, 4), vs.Point(20, 20)], index=["a", "b", "c"])
+    anyhit = tree.sindex.query_any(q, predicate="intersects")
+    assert anyhit.tolist() == [True, True, False] and list(anyhit.index) == ["a", "b", "c"]
+    agg = tree.sindex.query_aggregate(q, {"n": "size", "w": (np.array([1.0, 10.0, 100.0]), "sum")},
+                                      predicate="intersects")
+    assert agg["n"].tolist() == [1, 2, 0] and agg["w"].tolist() == [1.0, 11.0, 0.0]
+    assert tree.sindex.size == 3
+    assert tree.sindex.intersection((4, 4)).tolist() == [0, 1]
+    with pytest.raises(NotImplementedError):
+        tree.sindex.intersection((0, 0, 1, 1))
+    with pytest.raises(ValueError):
+        tree.sindex.query_aggregate(q, {"n": "mean"})

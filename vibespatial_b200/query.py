@@ -217,6 +217,118 @@ class SpatialIndex:
     def is_empty(self):
         return len(self.geometry) == 0
 
+    @property
+    def size(self):
+        """Number of geometries in the index."""
+        return len(self.geometry)
+
+    def _input(self, geometry):
+        """(GeometryArray, output index) of a query input."""
+        import pandas as pd
+
+        from .geometry import BaseGeometry, GeometryArray
+
+        if isinstance(geometry, BaseGeometry):
+            return GeometryArray.from_shapes([geometry]), pd.RangeIndex(1)
+        index = getattr(geometry, "index", None)
+        arr = getattr(geometry, "values", geometry)
+        if not isinstance(arr, GeometryArray):
+            arr = GeometryArray.from_shapes(list(arr))
+        return arr, (index if index is not None else pd.RangeIndex(len(arr)))
+
+    def _pair_rows(self, arr, predicate, distance):
+        """(input rows, tree rows): CUDA tensors from the CUDA join, host
+        arrays when a test substitutes the pair source."""
+        on_device = _pairs_backend is None and _dwithin_backend is None
+        res = query_spatial_index(self.geometry, arr, predicate=predicate, distance=distance,
+                                  return_device=on_device)
+        return res[0], res[1]
+
+    def query_any(self, geometry, *, predicate=None, distance=None):
+        """Whether each input geometry has any match (a boolean Series over
+        the input's index), without exporting the pairs: the reference's
+        sindex.query_any (src/vibespatial/api/sindex.py:594)."""
+        import pandas as pd
+
+        arr, index = self._input(geometry)
+        rows, _ = self._pair_rows(arr, predicate, distance)
+        n = len(arr)
+        if isinstance(rows, np.ndarray):
+            hit = np.bincount(rows, minlength=n)[:n] > 0 if len(rows) else np.zeros(n, bool)
+        else:
+            import torch
+
+            hit = (torch.bincount(rows.long(), minlength=n)[:n] > 0).cpu().numpy() if rows.numel() else \
+                np.zeros(n, bool)
+        return pd.Series(hit, index=index)
+
+    def query_aggregate(self, geometry, aggregations, *, predicate=None, distance=None):
+        """Per input geometry, reductions over its matches without exporting
+        the pairs: ``{"name": "size"}`` counts them, ``{"name": (values,
+        "sum")}`` sums ``values`` (one number per tree geometry) over them;
+        empty groups give 0.  The reference's sindex.query_aggregate
+        (src/vibespatial/api/sindex.py:505)."""
+        import pandas as pd
+
+        arr, index = self._input(geometry)
+        n, m = len(arr), len(self.geometry)
+        specs = {}
+        for name, spec in dict(aggregations).items():
+            if isinstance(spec, str):
+                if spec != "size":
+                    raise ValueError(f"unsupported aggregation {spec!r} for {name!r}: use 'size' or (values, 'sum')")
+                specs[name] = None
+            else:
+                values, op = spec
+                if op != "sum":
+                    raise ValueError(f"unsupported aggregation {op!r} for {name!r}: use 'sum'")
+                v = np.asarray(getattr(values, "to_numpy", lambda: values)(), dtype=np.float64)
+                if v.shape != (m,):
+                    raise ValueError(f"values of {name!r} must have one entry per indexed geometry ({m})")
+                specs[name] = v
+        rows, trows = self._pair_rows(arr, predicate, distance)
+        out = {}
+        if isinstance(rows, np.ndarray):
+            for name, v in specs.items():
+                if v is None:
+                    out[name] = np.bincount(rows, minlength=n)[:n].astype(np.int64) if len(rows) else \
+                        np.zeros(n, np.int64)
+                else:
+                    out[name] = np.bincount(rows, weights=v[trows], minlength=n)[:n] if len(rows) else np.zeros(n)
+        else:
+            import torch
+
+            r = rows.long()
+            for name, v in specs.items():
+                if v is None:
+                    c = torch.bincount(r, minlength=n)[:n] if r.numel() else torch.zeros(n, dtype=torch.int64)
+                    out[name] = c.cpu().numpy().astype(np.int64)
+                else:
+                    acc = torch.zeros(n, dtype=torch.float64, device=r.device)
+                    if r.numel():
+                        dv = torch.from_numpy(v).to(r.device)
+                        acc.index_add_(0, r, dv[trows.long()])
+                    out[name] = acc.cpu().numpy()
+        return pd.DataFrame(out, index=index)
+
+    def intersection(self, coordinates):
+        """Compatibility form of query (rtree's Index.intersection): tree rows
+        whose box contains the point ``(x, y)``.  Rectangle bounds are not
+        supported by this point-query join."""
+        try:
+            coords = tuple(coordinates)
+        except TypeError as err:
+            raise TypeError("Invalid coordinates, must be iterable in format (minx, miny, maxx, maxy) (for bounds) "
+                            f"or (x, y) (for points). Got `coordinates` = {coordinates}.") from err
+        from .geometry import Point
+
+        if len(coords) == 2:
+            return self.query(Point(*coords), predicate=None)
+        if len(coords) == 4:
+            raise NotImplementedError("rectangle queries are outside this point x polygon join; query a point")
+        raise TypeError("Invalid coordinates, must be iterable in format (minx, miny, maxx, maxy) (for bounds) "
+                        f"or (x, y) (for points). Got `coordinates` = {coordinates}.")
+
     def query(self, geometry, predicate=None, sort=False, distance=None, output_format="indices",
               return_device=False, method="learned"):
         """Tree rows matching ``predicate(geometry, tree geometry)``.
