@@ -221,6 +221,11 @@ def test_elementwise_within_contains(backend):
     assert polys.contains(pts).tolist() == [False, False, False, True, False]
     assert polys.covers(pts).tolist() == [False, False, False, True, True]
     assert pts.touches(polys).tolist() == [False, False, False, False, True]
+    assert polys.contains_properly(pts).tolist() == [False, False, False, True, False]
+    assert not pts.crosses(polys).any() and not polys.overlaps(pts).any()
+    # disjoint: the empty pair is disjoint, missing rows are not, the boundary point intersects
+    assert pts.disjoint(polys).tolist() == [False, True, False, False, False]
+    assert polys.disjoint(vs.GeoSeries([vs.Point(3, 3)] * 5)).tolist() == [True, True, False, True, False]
     # scalar broadcast and index alignment
     s = vs.GeoSeries([vs.Point(1, 1), vs.Point(3, 3)], index=[10, 20])
     assert s.within(vs.box(0, 0, 2, 2)).tolist() == [True, False]

@@ -114,6 +114,18 @@ class GeoSeries(pd.Series):
     def touches(self, other, align=None):
         return self._binary(other, "touches", align)
 
+    def contains_properly(self, other, align=None):
+        return self._binary(other, "contains_properly", align)
+
+    def crosses(self, other, align=None):
+        return self._binary(other, "crosses", align)
+
+    def overlaps(self, other, align=None):
+        return self._binary(other, "overlaps", align)
+
+    def disjoint(self, other, align=None):
+        return self._binary(other, "disjoint", align)
+
 
 def _geoseries_or_series(*args, **kwargs):
     s = pd.Series(*args, **kwargs)

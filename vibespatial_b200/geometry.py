@@ -525,6 +525,18 @@ class GeometryArray(ExtensionArray):
     def touches(self, other):
         return self._binary(other, "touches")
 
+    def contains_properly(self, other):
+        return self._binary(other, "contains_properly")
+
+    def crosses(self, other):
+        return self._binary(other, "crosses")
+
+    def overlaps(self, other):
+        return self._binary(other, "overlaps")
+
+    def disjoint(self, other):
+        return self._binary(other, "disjoint")
+
     def distance(self, other):
         from .predicates import distance
 

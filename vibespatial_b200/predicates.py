@@ -14,6 +14,8 @@ covers             False                interior or boundary
 covered_by         interior / boundary  False
 intersects         interior / boundary  interior or boundary
 touches            boundary             boundary
+crosses, overlaps  False                False
+disjoint           exterior             exterior
 =================  ===================  ====================
 
 Null and empty rows are False (the reference's NullBehavior.FALSE,
@@ -33,6 +35,9 @@ _POINT_LEFT = {
     "contains": (),
     "contains_properly": (),
     "covers": (),
+    "crosses": (),
+    "overlaps": (),
+    "disjoint": (OUTSIDE,),
 }
 _POINT_RIGHT = {
     "contains": (INTERIOR,),
@@ -42,6 +47,9 @@ _POINT_RIGHT = {
     "touches": (BOUNDARY,),
     "within": (),
     "covered_by": (),
+    "crosses": (),
+    "overlaps": (),
+    "disjoint": (OUTSIDE,),
 }
 
 # Locator and distance of aligned rows: the CUDA kernels.  Tests of the host
@@ -89,7 +97,13 @@ def binary_predicate(left, right, op: str) -> np.ndarray:
     if not accepted:
         return np.zeros(n, dtype=bool)
     loc = _locate(points, polys)
-    return np.isin(loc, accepted)
+    res = np.isin(loc, accepted)
+    if op == "disjoint":
+        # an empty geometry is disjoint from any present geometry; a missing one from nothing
+        left_na, right_na = np.asarray(left.isna()), np.asarray(right.isna())
+        empty = (np.asarray(left.is_empty) & ~left_na) | (np.asarray(right.is_empty) & ~right_na)
+        res |= empty & ~left_na & ~right_na
+    return res
 
 
 def _aligned_pair(left, right):
