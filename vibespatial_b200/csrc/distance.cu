@@ -376,7 +376,9 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
                             // margin above the rounding of both distances) can neither
                             // lower the minimum nor tie it
                             const double bound = kMode == kNearestMin ? my_best : q;
-                            if (!(envelope_distance(ib, x, y) > bound * (1.0 + 0x1p-40))) {
+                            // (a minimum of 0 cannot drop further: the min walk skips the rest)
+                            if ((kMode != kNearestMin || my_best > 0.0) &&
+                                !(envelope_distance(ib, x, y) > bound * (1.0 + 0x1p-40))) {
                                 const double d = polygon_distance(a, x, y, slot, n_exact);
                                 if (kMode == kNearestMin) my_best = d < my_best ? d : my_best;
                                 else want = d == q;
@@ -827,7 +829,9 @@ __global__ void __launch_bounds__(kDistThreads) poly_nearest_kernel(const PolyAr
                     if (active && ib.minx <= lx1 && ib.maxx >= lx0 && ib.miny <= ly1 && ib.maxy >= ly0) {
                         ++n_cand;
                         const double bound = kEmit ? q : my_best;
-                        if (!(envelope_distance(qb, ib.minx, ib.miny) > bound * (1.0 + 0x1p-40))) {
+                        // (a minimum of 0 cannot drop further: the min walk skips the rest)
+                        if ((kEmit || my_best > 0.0) &&
+                            !(envelope_distance(qb, ib.minx, ib.miny) > bound * (1.0 + 0x1p-40))) {
                             const double d = point_polygon_soa(a, ib.minx, ib.miny, row, n_exact);
                             if (kEmit) want = d == q;
                             else my_best = d < my_best ? d : my_best;
