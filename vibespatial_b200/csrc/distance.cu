@@ -193,19 +193,46 @@ __device__ __noinline__ double polygon_distance(const DistArgs& a, double x, dou
 //                 in a.radius), the packet's box shrinking as the minima
 //                 drop; writes best[row]
 //   kNearestEmit  radius best[row]; emits every polygon at exactly that distance
+// A dwithin candidate that passed the envelope test, queued for the exact test.
+struct DwPair {
+    double x, y, d;
+    int32_t row, slot;
+};
+
 template <int kMode>
 __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs a) {
+    constexpr int kQ = kMode == kDwithin ? 64 : 1;
     extern __shared__ vs_box s_nodes[];
     __shared__ int2 s_buf[kDistWarps][kWarpBuf];
     __shared__ unsigned s_cnt[kDistWarps];
     __shared__ int s_stack[kDistWarps][kDistStack];
     __shared__ vs_box s_items[kDistWarps][kFanout];
+    __shared__ DwPair s_dq[kDistWarps][kQ];
     const int64_t stage_base = a.level_off[a.stage_level];
     for (int k = threadIdx.x; k < a.staged; k += blockDim.x) s_nodes[k] = a.nodes[stage_base + k];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) s_cnt[warp] = 0;
     __syncthreads();
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
+    // dwithin: candidates that passed the envelope test queue up here and are
+    // decided 32 at a time, one per lane, so the exact tests run with every
+    // lane busy whichever lanes' boxes the candidates fell in
+    DwPair* dq = s_dq[warp];
+    int nq = 0;  // warp-uniform
+    unsigned n_exact_q = 0;
+    auto drain = [&](int cnt) {
+        bool want = false;
+        int32_t prow = 0, pgeom = 0;
+        if (lane < cnt) {
+            const DwPair e = dq[lane];
+            want = geometry_location(e.x, e.y, a.xy, a.ring_off, a.part_off, a.geom_off, e.slot, a.rings,
+                                     n_exact_q) != LOC_OUTSIDE ||
+                   facet_distance(e.x, e.y, a.xy, a.ring_off, a.part_off, a.geom_off, e.slot, e.d) <= e.d;
+            prow = e.row;
+            pgeom = a.item_geom[e.slot];
+        }
+        wemit_sync(out, a.sink, want, prow, pgeom);
+    };
     const unsigned lt = (1u << lane) - 1u;
     const int top = a.levels - 1;
     const int64_t n = (int64_t)*a.n_list;
@@ -361,16 +388,13 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
                     const vs_box ib = s_items[warp][j];
                     const int slot = (int)(slot0 + j);
                     bool want = false;
+                    bool queue = false;
+                    double qd = 0.0;
                     if (active && ib.minx <= lx1 && ib.maxx >= lx0 && ib.miny <= ly1 && ib.maxy >= ly0) {
                         ++n_cand;
                         if (kMode == kDwithin) {
-                            const double d = a.dist_geom ? a.dist_geom[a.item_geom[slot]] : q;
-                            if (d >= 0.0 && !(envelope_distance(ib, x, y) > d)) {
-                                const int loc = geometry_location(x, y, a.xy, a.ring_off, a.part_off, a.geom_off,
-                                                                  slot, a.rings, n_exact);
-                                want = loc != LOC_OUTSIDE ||
-                                       facet_distance(x, y, a.xy, a.ring_off, a.part_off, a.geom_off, slot, d) <= d;
-                            }
+                            qd = a.dist_geom ? a.dist_geom[a.item_geom[slot]] : q;
+                            queue = qd >= 0.0 && !(envelope_distance(ib, x, y) > qd);
                         } else {
                             // a polygon whose envelope is farther than the bound (with a
                             // margin above the rounding of both distances) can neither
@@ -385,7 +409,21 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
                             }
                         }
                     }
-                    if (kMode != kNearestMin) wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                    if (kMode == kDwithin) {
+                        const unsigned qm = __ballot_sync(0xffffffffu, queue);
+                        if (queue) dq[nq + __popc(qm & lt)] = DwPair{x, y, qd, row, slot};
+                        nq += __popc(qm);
+                        __syncwarp();
+                        if (nq >= 32) {
+                            drain(32);
+                            __syncwarp();
+                            if (lane < nq - 32) dq[lane] = dq[32 + lane];
+                            nq -= 32;
+                            __syncwarp();
+                        }
+                    } else if (kMode == kNearestEmit) {
+                        wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                    }
                 }
                 __syncwarp();
                 if (kMode == kNearestMin) boxes();  // the minima only shrink: so does the packet's box
@@ -394,9 +432,13 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
         if (kMode == kNearestMin && active) a.best[row] = my_best <= q ? my_best : INFINITY;
         if (kMode != kNearestMin) wflush(out, a.sink, false);
     }
+    if (kMode == kDwithin && nq > 0) {
+        drain(nq);
+        __syncwarp();
+    }
     if (kMode != kNearestMin) wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
-    add_counter(a.counters, 1, n_exact);
+    add_counter(a.counters, 1, n_exact + n_exact_q);
 }
 
 // Element-wise: row i of the points against row i of the polygons (SoA
