@@ -201,7 +201,7 @@ struct DwPair {
 
 template <int kMode>
 __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs a) {
-    constexpr int kQ = kMode == kDwithin ? 64 : 1;
+    constexpr int kQ = kMode != kNearestMin ? 64 : 1;
     extern __shared__ vs_box s_nodes[];
     __shared__ int2 s_buf[kDistWarps][kWarpBuf];
     __shared__ unsigned s_cnt[kDistWarps];
@@ -214,9 +214,10 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
     if (lane == 0) s_cnt[warp] = 0;
     __syncthreads();
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
-    // dwithin: candidates that passed the envelope test queue up here and are
-    // decided 32 at a time, one per lane, so the exact tests run with every
-    // lane busy whichever lanes' boxes the candidates fell in
+    // dwithin and the tie walk: candidates that passed the envelope test queue
+    // up here and are decided 32 at a time, one per lane, so the exact tests
+    // run with every lane busy whichever lanes' boxes the candidates fell in
+    // (d is the radius, or the lane's minimum for the tie walk)
     DwPair* dq = s_dq[warp];
     int nq = 0;  // warp-uniform
     unsigned n_exact_q = 0;
@@ -225,9 +226,12 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
         int32_t prow = 0, pgeom = 0;
         if (lane < cnt) {
             const DwPair e = dq[lane];
-            want = geometry_location(e.x, e.y, a.xy, a.ring_off, a.part_off, a.geom_off, e.slot, a.rings,
-                                     n_exact_q) != LOC_OUTSIDE ||
-                   facet_distance(e.x, e.y, a.xy, a.ring_off, a.part_off, a.geom_off, e.slot, e.d) <= e.d;
+            if (kMode == kDwithin)
+                want = geometry_location(e.x, e.y, a.xy, a.ring_off, a.part_off, a.geom_off, e.slot, a.rings,
+                                         n_exact_q) != LOC_OUTSIDE ||
+                       facet_distance(e.x, e.y, a.xy, a.ring_off, a.part_off, a.geom_off, e.slot, e.d) <= e.d;
+            else
+                want = polygon_distance(a, e.x, e.y, e.slot, n_exact_q) == e.d;
             prow = e.row;
             pgeom = a.item_geom[e.slot];
         }
@@ -387,7 +391,6 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
                     mm &= mm - 1;
                     const vs_box ib = s_items[warp][j];
                     const int slot = (int)(slot0 + j);
-                    bool want = false;
                     bool queue = false;
                     double qd = 0.0;
                     if (active && ib.minx <= lx1 && ib.maxx >= lx0 && ib.miny <= ly1 && ib.maxy >= ly0) {
@@ -403,13 +406,17 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
                             // (a minimum of 0 cannot drop further: the min walk skips the rest)
                             if ((kMode != kNearestMin || my_best > 0.0) &&
                                 !(envelope_distance(ib, x, y) > bound * (1.0 + 0x1p-40))) {
-                                const double d = polygon_distance(a, x, y, slot, n_exact);
-                                if (kMode == kNearestMin) my_best = d < my_best ? d : my_best;
-                                else want = d == q;
+                                if (kMode == kNearestMin) {
+                                    const double d = polygon_distance(a, x, y, slot, n_exact);
+                                    my_best = d < my_best ? d : my_best;
+                                } else {
+                                    queue = true;
+                                    qd = q;
+                                }
                             }
                         }
                     }
-                    if (kMode == kDwithin) {
+                    if (kMode != kNearestMin) {
                         const unsigned qm = __ballot_sync(0xffffffffu, queue);
                         if (queue) dq[nq + __popc(qm & lt)] = DwPair{x, y, qd, row, slot};
                         nq += __popc(qm);
@@ -421,8 +428,6 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
                             nq -= 32;
                             __syncwarp();
                         }
-                    } else if (kMode == kNearestEmit) {
-                        wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
                     }
                 }
                 __syncwarp();
@@ -432,7 +437,7 @@ __global__ void __launch_bounds__(kDistThreads) dist_join_kernel(const DistArgs 
         if (kMode == kNearestMin && active) a.best[row] = my_best <= q ? my_best : INFINITY;
         if (kMode != kNearestMin) wflush(out, a.sink, false);
     }
-    if (kMode == kDwithin && nq > 0) {
+    if (kMode != kNearestMin && nq > 0) {
         drain(nq);
         __syncwarp();
     }
