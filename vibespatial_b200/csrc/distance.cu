@@ -718,11 +718,13 @@ __global__ void poly_query_key_kernel(vs_polygons q, const double* __restrict__ 
 
 template <bool kEmit>
 __global__ void __launch_bounds__(kDistThreads) poly_nearest_kernel(const PolyArgs a) {
+    constexpr int kQ = kEmit ? 64 : 1;
     extern __shared__ vs_box s_nodes[];
     __shared__ int2 s_buf[kDistWarps][kWarpBuf];
     __shared__ unsigned s_cnt[kDistWarps];
     __shared__ int s_stack[kDistWarps][kDistStack];
     __shared__ vs_box s_items[kDistWarps][kFanout];
+    __shared__ DwPair s_dq[kDistWarps][kQ];
     const int64_t stage_base = a.level_off[a.stage_level];
     for (int k = threadIdx.x; k < a.staged; k += blockDim.x) s_nodes[k] = a.nodes[stage_base + k];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -734,6 +736,21 @@ __global__ void __launch_bounds__(kDistThreads) poly_nearest_kernel(const PolyAr
     const int64_t n = (int64_t)*a.n_valid;
     unsigned long long n_cand = 0;
     unsigned n_exact = 0;
+    // tie walk: candidate points queue up here (point, the polygon's minimum,
+    // polygon row, point slot) and are decided 32 at a time, one per lane
+    DwPair* dq = s_dq[warp];
+    int nq = 0;  // warp-uniform
+    auto drain = [&](int cnt) {
+        bool want = false;
+        int32_t prow = 0, ppt = 0;
+        if (lane < cnt) {
+            const DwPair e = dq[lane];
+            want = point_polygon_soa(a, e.x, e.y, e.row, n_exact) == e.d;
+            prow = e.row;
+            ppt = a.item_geom[e.slot];
+        }
+        wemit_sync(out, a.sink, want, prow, ppt);
+    };
     for (;;) {
         const int64_t b0 = warp_grab(a.work, kDistGrab);
         if (b0 >= n) break;
@@ -872,19 +889,34 @@ __global__ void __launch_bounds__(kDistThreads) poly_nearest_kernel(const PolyAr
                     mm &= mm - 1;
                     const vs_box ib = s_items[warp][j];  // a point: (x, y, x, y)
                     const int slot = (int)(slot0 + j);
-                    bool want = false;
+                    bool queue = false;
                     if (active && ib.minx <= lx1 && ib.maxx >= lx0 && ib.miny <= ly1 && ib.maxy >= ly0) {
                         ++n_cand;
                         const double bound = kEmit ? q : my_best;
                         // (a minimum of 0 cannot drop further: the min walk skips the rest)
                         if ((kEmit || my_best > 0.0) &&
                             !(envelope_distance(qb, ib.minx, ib.miny) > bound * (1.0 + 0x1p-40))) {
-                            const double d = point_polygon_soa(a, ib.minx, ib.miny, row, n_exact);
-                            if (kEmit) want = d == q;
-                            else my_best = d < my_best ? d : my_best;
+                            if (kEmit) {
+                                queue = true;
+                            } else {
+                                const double d = point_polygon_soa(a, ib.minx, ib.miny, row, n_exact);
+                                my_best = d < my_best ? d : my_best;
+                            }
                         }
                     }
-                    if (kEmit) wemit_sync(out, a.sink, want, row, a.item_geom[slot]);
+                    if (kEmit) {
+                        const unsigned qm = __ballot_sync(0xffffffffu, queue);
+                        if (queue) dq[nq + __popc(qm & lt)] = DwPair{ib.minx, ib.miny, q, row, slot};
+                        nq += __popc(qm);
+                        __syncwarp();
+                        if (nq >= 32) {
+                            drain(32);
+                            __syncwarp();
+                            if (lane < nq - 32) dq[lane] = dq[32 + lane];
+                            nq -= 32;
+                            __syncwarp();
+                        }
+                    }
                 }
                 __syncwarp();
                 if (!kEmit) boxes();
@@ -892,6 +924,10 @@ __global__ void __launch_bounds__(kDistThreads) poly_nearest_kernel(const PolyAr
         }
         if (!kEmit && active) a.best[row] = my_best <= q ? my_best : INFINITY;
         if (kEmit) wflush(out, a.sink, false);
+    }
+    if (kEmit && nq > 0) {
+        drain(nq);
+        __syncwarp();
     }
     if (kEmit) wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
