@@ -27,7 +27,11 @@ def _codes(rng, n, k, miss=0.1):
 
 @pytest.mark.parametrize("how", ["inner", "left", "right", "outer"])
 @pytest.mark.parametrize("with_codes", [False, True])
-@pytest.mark.parametrize("sizes", [(1000, 300, 5000), (50_000, 20_000, 400_000), (7, 5, 0), (0, 9, 0), (5, 0, 0)])
+# sizes: (left rows, right rows, pairs drawn); the export writes tiles of 2048
+# driving rows, so the cases cross tile edges (4096, 2049 rows) and give
+# single driving rows thousands of pairs (3 right rows, 20k pairs)
+@pytest.mark.parametrize("sizes", [(1000, 300, 5000), (50_000, 20_000, 400_000), (7, 5, 0), (0, 9, 0), (5, 0, 0),
+                                   (3000, 3, 20_000), (4096, 2049, 30_000), (2049, 1, 2049)])
 def test_export_matches_host(ctx, vsabi, how, with_codes, sizes):
     import torch
 
@@ -56,3 +60,10 @@ def test_export_rejects_out_of_range_pairs(ctx, vsabi):
         vsabi.join_export(ctx, l, r, 3, 2, "left")
     with pytest.raises(ValueError):
         vsabi.join_export(ctx, l[:2], r[:2], 3, 2, "left", torch.zeros(3, dtype=torch.int64, device="cuda"))
+    # with codes on both sides the attribute filter checks the ranges
+    codes_l = torch.zeros(3, dtype=torch.int64, device="cuda")
+    codes_r = torch.zeros(2, dtype=torch.int64, device="cuda")
+    with pytest.raises(ValueError):
+        vsabi.join_export(ctx, l, r, 3, 2, "left", codes_l, codes_r)
+    with pytest.raises(ValueError):
+        vsabi.join_export(ctx, l[:2], r[:2] - 1, 3, 2, "inner", codes_l, codes_r)

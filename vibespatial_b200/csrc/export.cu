@@ -10,8 +10,10 @@
 //      ordered compaction of the pairs and their source positions
 //   2. how = right: the kept pairs re-sorted by (right, left) (radix sort)
 //   3. per driving row (left rows; right rows for how = right) its pair
-//      count, scans of count and max(count, 1): a row's pairs land at its
-//      output start, an unmatched row gets one row with -1 on the other side
+//      count; per tile of 2048 driving rows its pairs and unmatched rows,
+//      scanned: a tile's output is one contiguous range, which one block
+//      writes in order (a row's pairs, or one row with -1 on the other side
+//      when it has none)
 //   4. how = outer: right rows no pair reaches are appended in order
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -31,13 +33,21 @@ __global__ void export_check_kernel(const int32_t* __restrict__ l, const int32_t
     if (b) atomicAdd(bad, b);
 }
 
+// Keep flags of the attribute filter; pairs outside the row ranges are
+// counted (and not kept) as export_check_kernel counts them.
 __global__ void export_keep_kernel(const int32_t* __restrict__ l, const int32_t* __restrict__ r, int64_t n,
-                                   const int64_t* __restrict__ lc, const int64_t* __restrict__ rc,
-                                   uint32_t* __restrict__ keep) {
+                                   int64_t n_left, int64_t n_right, const int64_t* __restrict__ lc,
+                                   const int64_t* __restrict__ rc, uint32_t* __restrict__ keep,
+                                   uint32_t* __restrict__ bad) {
+    uint32_t b = 0;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t a = lc[l[k]];
-        keep[k] = a >= 0 && a == rc[r[k]] ? 1u : 0u;
+        const int32_t li = l[k], ri = r[k];
+        const bool ok = li >= 0 && li < n_left && ri >= 0 && ri < n_right;
+        b += ok ? 0u : 1u;
+        const int64_t a = ok ? lc[li] : -1;
+        keep[k] = a >= 0 && a == rc[ri] ? 1u : 0u;
     }
+    if (b) atomicAdd(bad, b);
 }
 
 __global__ void export_compact_kernel(const int32_t* __restrict__ l, const int32_t* __restrict__ r, int64_t n,
@@ -67,37 +77,102 @@ __global__ void export_count_kernel(const int32_t* __restrict__ drive, const uin
         atomicAdd(&cnt[drive[perm ? perm[k] : (uint32_t)k]], 1u);
 }
 
-__global__ void export_rows_kernel(const uint32_t* __restrict__ cnt, int64_t n, uint32_t* __restrict__ rows) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        rows[i] = cnt[i] > 0 ? cnt[i] : 1u;
-}
+constexpr int kTileThreads = 256;
+constexpr int kTileRows = 2048;
+constexpr int kRowsPerThread = kTileRows / kTileThreads;
 
-// Pair k (in driving order) goes to start[i] + (k - first[i]), i its driving row.
-__global__ void export_scatter_kernel(const int32_t* __restrict__ drive, const int32_t* __restrict__ other,
-                                      const uint32_t* __restrict__ perm, const uint32_t* __restrict__ src, int64_t n,
-                                      const uint32_t* __restrict__ first, const uint32_t* __restrict__ start,
-                                      int64_t* __restrict__ o_drive, int64_t* __restrict__ o_other,
-                                      int64_t* __restrict__ o_src) {
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t j = perm ? perm[k] : (uint32_t)k;
-        const int32_t i = drive[j];
-        const int64_t p = (int64_t)start[i] + (k - (int64_t)first[i]);
-        o_drive[p] = i;
-        o_other[p] = other[j];
-        if (o_src) o_src[p] = src ? (int64_t)src[j] : (int64_t)j;
+// A driving row's share of the output, packed: its pairs in the low word,
+// 1 in the high word when it has none (it then owns one unmatched row).
+// Neither word carries into the other: pairs and rows are below 2^31.
+__device__ __forceinline__ uint64_t row_pack(uint32_t c) { return (uint64_t)c | ((uint64_t)(c == 0u) << 32); }
+
+__global__ void __launch_bounds__(kTileThreads) export_tile_sum_kernel(const uint32_t* __restrict__ cnt, int64_t n,
+                                                                       uint64_t* __restrict__ tile_sum) {
+    __shared__ uint64_t s_w[kTileThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kTileRows;
+    uint64_t v = 0;
+    for (int k = threadIdx.x; k < kTileRows; k += kTileThreads)
+        if (base + k < n) v += row_pack(cnt[base + k]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t t = 0;
+#pragma unroll
+        for (int w = 0; w < kTileThreads / 32; ++w) t += s_w[w];
+        tile_sum[blockIdx.x] = t;
     }
 }
 
-__global__ void export_unmatched_kernel(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ start,
-                                        int64_t n, int64_t* __restrict__ o_drive, int64_t* __restrict__ o_other,
-                                        int64_t* __restrict__ o_src) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        if (cnt[i] == 0) {
-            const int64_t p = start[i];
-            o_drive[p] = i;
+// One block per tile of driving rows. The tile's output is the range that
+// starts at its scanned offset (pairs before it + unmatched rows before it);
+// row k of the tile owns [s_start[k], s_start[k + 1]) of it and its pairs
+// are [s_first[k], s_first[k + 1]) of the tile's pairs in driving order.
+// Output positions go to consecutive threads, so the stores are contiguous.
+__global__ void __launch_bounds__(kTileThreads) export_write_kernel(
+    const uint32_t* __restrict__ cnt, int64_t n, const uint64_t* __restrict__ tile_off,
+    const int32_t* __restrict__ other, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ src,
+    int64_t* __restrict__ o_drive, int64_t* __restrict__ o_other, int64_t* __restrict__ o_src) {
+    __shared__ uint32_t s_start[kTileRows + 1];
+    __shared__ uint32_t s_first[kTileRows + 1];
+    __shared__ uint64_t s_w[kTileThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t base = (int64_t)blockIdx.x * kTileRows;
+    const int64_t r0 = base + (int64_t)t * kRowsPerThread;
+    uint64_t v[kRowsPerThread];
+    uint64_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) {
+        v[k] = r0 + k < n ? row_pack(cnt[r0 + k]) : 0ull;  // rows past the end own nothing
+        sum += v[k];
+    }
+    uint64_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    uint64_t run = incl - sum;
+    for (int w = 0; w < warp; ++w) run += s_w[w];
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) {
+        s_first[t * kRowsPerThread + k] = (uint32_t)run;
+        s_start[t * kRowsPerThread + k] = (uint32_t)run + (uint32_t)(run >> 32);
+        run += v[k];
+    }
+    if (t == kTileThreads - 1) {
+        s_first[kTileRows] = (uint32_t)run;
+        s_start[kTileRows] = (uint32_t)run + (uint32_t)(run >> 32);
+    }
+    __syncthreads();
+    const uint64_t off = tile_off[blockIdx.x];
+    const int64_t pair_base = (int64_t)(uint32_t)off;
+    const int64_t out_base = pair_base + (int64_t)(off >> 32);
+    const uint32_t total = s_start[kTileRows];
+    for (uint32_t o = t; o < total; o += kTileThreads) {
+        // the row that owns o: s_start[lo] <= o < s_start[hi]
+        int lo = 0, hi = kTileRows;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_start[mid] <= o) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t f0 = s_first[lo];
+        const int64_t p = out_base + o;
+        o_drive[p] = base + lo;
+        if (s_first[lo + 1] == f0) {
             o_other[p] = -1;
             if (o_src) o_src[p] = -1;
+        } else {
+            const int64_t k = pair_base + f0 + (o - s_start[lo]);
+            const uint32_t j = perm ? perm[k] : (uint32_t)k;
+            o_other[p] = other[j];
+            if (o_src) o_src[p] = src ? (int64_t)src[j] : (int64_t)j;
         }
+    }
 }
 
 __global__ void export_mark_kernel(const int32_t* __restrict__ r, int64_t n, uint32_t* __restrict__ matched) {
@@ -182,32 +257,35 @@ int vs_join_export(vs_context* ctx, const int32_t* d_left, const int32_t* d_righ
     int64_t m = n_pairs;
     Scratch<uint32_t> keep, kpos, ksrc_buf;
     Scratch<int32_t> kl_buf, kr_buf;
-    uint32_t h_tot[2] = {0, 0};
     Scratch<uint32_t> totals;
     VS_TRY(totals.alloc(4, s));
     VS_CUDA_TRY(cudaMemsetAsync(totals.p, 0, 4 * sizeof(uint32_t), s));
-    if (n_pairs > 0) {
+    auto bad_pairs = [&](uint32_t bad) {
+        set_error("%u pairs name rows outside [0, %lld) x [0, %lld)", bad, (long long)n_left, (long long)n_right);
+        return VS_E_ARG;
+    };
+    if (n_pairs > 0 && !with_codes) {
         export_check_kernel<<<grid_of(export_check_kernel, n_pairs), 256, 0, s>>>(d_left, d_right, n_pairs, n_left,
                                                                                   n_right, totals.p + 3);
         VS_LAUNCHED("export_check", s);
         uint32_t bad = 0;
         VS_CUDA_TRY(cudaMemcpyAsync(&bad, totals.p + 3, sizeof(bad), cudaMemcpyDeviceToHost, s));
         VS_CUDA_TRY(cudaStreamSynchronize(s));
-        if (bad) {
-            set_error("%u pairs name rows outside [0, %lld) x [0, %lld)", bad, (long long)n_left, (long long)n_right);
-            return VS_E_ARG;
-        }
+        if (bad) return bad_pairs(bad);
     }
     if (with_codes && n_pairs > 0) {
         VS_TRY(keep.alloc((size_t)n_pairs, s));
         VS_TRY(kpos.alloc((size_t)n_pairs, s));
-        export_keep_kernel<<<grid_of(export_keep_kernel, n_pairs), 256, 0, s>>>(d_left, d_right, n_pairs, d_left_code,
-                                                                                d_right_code, keep.p);
+        // the filter checks the row ranges too (before it reads a code)
+        export_keep_kernel<<<grid_of(export_keep_kernel, n_pairs), 256, 0, s>>>(
+            d_left, d_right, n_pairs, n_left, n_right, d_left_code, d_right_code, keep.p, totals.p + 3);
         VS_LAUNCHED("export_keep", s);
         VS_TRY(exclusive_scan_u32(keep.p, kpos.p, n_pairs, totals.p, s));
-        VS_CUDA_TRY(cudaMemcpyAsync(h_tot, totals.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        uint32_t h4[4] = {0, 0, 0, 0};
+        VS_CUDA_TRY(cudaMemcpyAsync(h4, totals.p, sizeof(h4), cudaMemcpyDeviceToHost, s));
         VS_CUDA_TRY(cudaStreamSynchronize(s));
-        m = h_tot[0];
+        if (h4[3]) return bad_pairs(h4[3]);
+        m = h4[0];
         VS_TRY(kl_buf.alloc((size_t)m, s));
         VS_TRY(kr_buf.alloc((size_t)m, s));
         VS_TRY(ksrc_buf.alloc((size_t)m, s));
@@ -247,23 +325,25 @@ int vs_join_export(vs_context* ctx, const int32_t* d_left, const int32_t* d_righ
         VS_TRY(radix_sort_u64_u32(rkeys.p, perm.p, m, 64, s));
     }
     const uint32_t* p_perm = right && m > 1 ? perm.p : nullptr;
-    // 3. counts per driving row, output starts
+    // 3. counts per driving row, tile sums and their scan
     const size_t nd = (size_t)(n_drive > 0 ? n_drive : 1);
-    Scratch<uint32_t> cnt, first, rows, start;
+    const int64_t n_tiles = (n_drive + kTileRows - 1) / kTileRows;
+    Scratch<uint32_t> cnt;
+    Scratch<uint64_t> tile_sum, tile_off, body_total;
     VS_TRY(cnt.alloc(nd, s));
-    VS_TRY(first.alloc(nd, s));
-    VS_TRY(rows.alloc(nd, s));
-    VS_TRY(start.alloc(nd, s));
+    VS_TRY(tile_sum.alloc((size_t)(n_tiles > 0 ? n_tiles : 1), s));
+    VS_TRY(tile_off.alloc((size_t)(n_tiles > 0 ? n_tiles : 1), s));
+    VS_TRY(body_total.alloc(1, s));
     VS_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, nd * sizeof(uint32_t), s));
+    VS_CUDA_TRY(cudaMemsetAsync(body_total.p, 0, sizeof(uint64_t), s));
     if (m > 0) {
         export_count_kernel<<<grid_of(export_count_kernel, m), 256, 0, s>>>(drive, p_perm, m, cnt.p);
         VS_LAUNCHED("export_count", s);
     }
-    if (n_drive > 0) {
-        export_rows_kernel<<<grid_of(export_rows_kernel, n_drive), 256, 0, s>>>(cnt.p, n_drive, rows.p);
-        VS_LAUNCHED("export_rows", s);
-        VS_TRY(exclusive_scan_u32(cnt.p, first.p, n_drive, totals.p, s));
-        VS_TRY(exclusive_scan_u32(rows.p, start.p, n_drive, totals.p + 1, s));
+    if (n_tiles > 0) {
+        export_tile_sum_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(cnt.p, n_drive, tile_sum.p);
+        VS_LAUNCHED("export_tile_sum", s);
+        VS_TRY(exclusive_scan_u64(tile_sum.p, tile_off.p, n_tiles, body_total.p, s));
     }
     // 4. outer: right rows no pair reaches
     Scratch<uint32_t> missing, mpos;
@@ -280,11 +360,13 @@ int vs_join_export(vs_context* ctx, const int32_t* d_left, const int32_t* d_righ
         VS_LAUNCHED("export_flip", s);
         VS_TRY(exclusive_scan_u32(missing.p, mpos.p, n_right, totals.p + 2, s));
     }
-    uint32_t t3[3] = {0, 0, 0};
-    VS_CUDA_TRY(cudaMemcpyAsync(t3, totals.p, sizeof(t3), cudaMemcpyDeviceToHost, s));
+    uint64_t packed = 0;
+    uint32_t appended = 0;
+    VS_CUDA_TRY(cudaMemcpyAsync(&packed, body_total.p, sizeof(packed), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaMemcpyAsync(&appended, totals.p + 2, sizeof(appended), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
-    const int64_t body = n_drive > 0 ? (int64_t)t3[1] : 0;
-    const int64_t total = body + (how == VS_HOW_OUTER && n_right > 0 ? (int64_t)t3[2] : 0);
+    const int64_t body = (int64_t)(uint32_t)packed + (int64_t)(packed >> 32);
+    const int64_t total = body + (how == VS_HOW_OUTER && n_right > 0 ? (int64_t)appended : 0);
     *n_out = total;
     if (total > capacity) {
         set_error("output holds %lld rows, %lld required", (long long)capacity, (long long)total);
@@ -292,16 +374,10 @@ int vs_join_export(vs_context* ctx, const int32_t* d_left, const int32_t* d_righ
     }
     int64_t* o_drive = right ? d_out_right : d_out_left;
     int64_t* o_other = right ? d_out_left : d_out_right;
-    if (m > 0) {
-        export_scatter_kernel<<<grid_of(export_scatter_kernel, m), 256, 0, s>>>(
-            drive, other, p_perm, ksrc, m, first.p, start.p, o_drive, o_other, d_out_src);
-        VS_LAUNCHED("export_scatter", s);
-    }
-    if (n_drive > 0) {
-        export_unmatched_kernel<<<grid_of(export_unmatched_kernel, n_drive), 256, 0, s>>>(cnt.p, start.p, n_drive,
-                                                                                            o_drive, o_other,
-                                                                                            d_out_src);
-        VS_LAUNCHED("export_unmatched", s);
+    if (n_tiles > 0) {
+        export_write_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(cnt.p, n_drive, tile_off.p, other, p_perm,
+                                                                       ksrc, o_drive, o_other, d_out_src);
+        VS_LAUNCHED("export_write", s);
     }
     if (how == VS_HOW_OUTER && n_right > 0) {
         export_append_kernel<<<grid_of(export_append_kernel, n_right), 256, 0, s>>>(
