@@ -91,8 +91,18 @@ __global__ void __launch_bounds__(kTileThreads) export_tile_sum_kernel(const uin
     __shared__ uint64_t s_w[kTileThreads / 32];
     const int64_t base = (int64_t)blockIdx.x * kTileRows;
     uint64_t v = 0;
-    for (int k = threadIdx.x; k < kTileRows; k += kTileThreads)
-        if (base + k < n) v += row_pack(cnt[base + k]);
+    if (base + kTileRows <= n) {
+        // a full tile: 16-byte loads (cnt is allocation-aligned, tiles are 8 KB apart)
+        const uint4* c4 = reinterpret_cast<const uint4*>(cnt + base);
+#pragma unroll
+        for (int k = 0; k < kTileRows / (4 * kTileThreads); ++k) {
+            const uint4 w = c4[threadIdx.x + k * kTileThreads];
+            v += row_pack(w.x) + row_pack(w.y) + row_pack(w.z) + row_pack(w.w);
+        }
+    } else {
+        for (int k = threadIdx.x; k < kTileRows; k += kTileThreads)
+            if (base + k < n) v += row_pack(cnt[base + k]);
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
@@ -122,11 +132,21 @@ __global__ void __launch_bounds__(kTileThreads) export_write_kernel(
     const int64_t r0 = base + (int64_t)t * kRowsPerThread;
     uint64_t v[kRowsPerThread];
     uint64_t sum = 0;
+    static_assert(kRowsPerThread == 8, "two 16-byte loads per thread");
+    if (r0 + kRowsPerThread <= n) {
+        // both loads stay 16-byte aligned: r0 is a multiple of 8 rows
+        const uint4 w0 = *reinterpret_cast<const uint4*>(cnt + r0);
+        const uint4 w1 = *reinterpret_cast<const uint4*>(cnt + r0 + 4);
+        const uint32_t c[kRowsPerThread] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
 #pragma unroll
-    for (int k = 0; k < kRowsPerThread; ++k) {
-        v[k] = r0 + k < n ? row_pack(cnt[r0 + k]) : 0ull;  // rows past the end own nothing
-        sum += v[k];
+        for (int k = 0; k < kRowsPerThread; ++k) v[k] = row_pack(c[k]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kRowsPerThread; ++k)
+            v[k] = r0 + k < n ? row_pack(cnt[r0 + k]) : 0ull;  // rows past the end own nothing
     }
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) sum += v[k];
     uint64_t incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
