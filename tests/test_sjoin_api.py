@@ -458,3 +458,59 @@ def test_sindex_reductions(backend):
         tree.sindex.intersection((0, 0, 1, 1))
     with pytest.raises(ValueError):
         tree.sindex.query_aggregate(q, {"n": "mean"})
+    # validation of sindex._normalize_query_aggregations / _validate_query_aggregate_values
+    with pytest.raises(ValueError, match="non-empty mapping"):
+        tree.sindex.query_aggregate(q, {})
+    with pytest.raises(TypeError, match="column names must be strings"):
+        tree.sindex.query_aggregate(q, {1: "size"})
+    with pytest.raises(ValueError, match="align with indexed tree geometries"):
+        tree.sindex.query_aggregate(q, {"w": (np.array([1.0, 2.0]), "sum")})
+    with pytest.raises(ValueError, match="one-dimensional"):
+        tree.sindex.query_aggregate(q, {"w": (np.ones((3, 1)), "sum")})
+    with pytest.raises(TypeError, match="must be numeric"):
+        tree.sindex.query_aggregate(q, {"w": (np.array(["a", "b", "c"]), "sum")})
+
+
+def test_sindex_relation_flow(backend):
+    """query_relation, the semijoins, the antijoin, match counts, the pair
+    aggregate of two aligned indexes and nearest_relation agree with the
+    exported pairs of sindex.query / sindex.nearest."""
+    tree = vs.GeometryArray.from_shapes([vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11),
+                                         vs.box(30, 30, 31, 31)])
+    q = vs.GeoSeries([vs.Point(1, 1), vs.Point(4, 4), vs.Point(20, 20), vs.Point(10.5, 10.5), vs.Point(4.5, 3.5)])
+    rel = tree.sindex.query_relation(q, predicate="intersects")
+    exported = tree.sindex.query(q, predicate="intersects")
+    np.testing.assert_array_equal(rel.to_numpy(), exported)
+    assert len(rel) == exported.shape[1] and rel.sorted_by_left
+    assert rel.left_row_count == 5 and rel.right_row_count == 4
+    host = tree.sindex.query_relation(q, predicate="intersects", return_device=False)
+    assert not host.is_device
+    np.testing.assert_array_equal(host.to_numpy(), exported)
+
+    assert tree.sindex.query_left_semijoin(q, predicate="intersects").to_numpy().tolist() == [0, 1, 3, 4]
+    assert tree.sindex.query_left_antijoin(q, predicate="intersects").to_numpy().tolist() == [2]
+    assert tree.sindex.query_right_semijoin(q, predicate="intersects").to_numpy().tolist() == [0, 1, 2]
+    counts = tree.sindex.query_left_match_count_expression(q, predicate="intersects")
+    assert counts.to_numpy().tolist() == [1, 2, 0, 1, 2] and counts.source_row_count == 5
+    assert counts.compare_scalar_selection(">", 1).to_numpy().tolist() == [1, 4]
+    with pytest.raises(ValueError):
+        counts.compare_scalar_selection("~", 1)
+
+    # a second index aligned with the first: row 0 smaller, row 1 the same, rows 2-3 elsewhere
+    other = vs.GeometryArray.from_shapes([vs.box(0, 0, 2, 2), vs.box(3, 3, 6, 6), vs.box(50, 50, 51, 51),
+                                          vs.box(10, 10, 11, 11)])
+    agg = tree.sindex.query_pair_aggregate(other.sindex, q, predicate="intersects")
+    assert list(agg.columns) == ["left_count", "right_count", "shared_count"]
+    assert agg["left_count"].tolist() == [3, 2, 1, 0]
+    assert agg["right_count"].tolist() == [1, 2, 0, 1]
+    assert agg["shared_count"].tolist() == [1, 2, 0, 0]
+    with pytest.raises(TypeError):
+        tree.sindex.query_pair_aggregate(object(), q, predicate="intersects")
+    with pytest.raises(ValueError, match="equal size"):
+        tree.sindex.query_pair_aggregate(vs.GeometryArray.from_shapes([vs.box(0, 0, 1, 1)]).sindex, q)
+
+    near = tree.sindex.nearest_relation(q)
+    pairs, dist = tree.sindex.nearest(q, return_distance=True)
+    np.testing.assert_array_equal(near.to_numpy(), pairs)
+    np.testing.assert_array_equal(near.distances, dist)
+    assert near.predicate == "nearest"

@@ -268,24 +268,40 @@ class SpatialIndex:
         "sum")}`` sums ``values`` (one number per tree geometry) over them;
         empty groups give 0.  The reference's sindex.query_aggregate
         (src/vibespatial/api/sindex.py:505)."""
+        from collections.abc import Mapping
+
         import pandas as pd
 
         arr, index = self._input(geometry)
         n, m = len(arr), len(self.geometry)
+        # validation and messages of sindex._normalize_query_aggregations and
+        # _validate_query_aggregate_values (src/vibespatial/api/sindex.py:1280-1334)
+        if not isinstance(aggregations, Mapping) or not aggregations:
+            raise ValueError("aggregations must be a non-empty mapping")
         specs = {}
-        for name, spec in dict(aggregations).items():
-            if isinstance(spec, str):
-                if spec != "size":
-                    raise ValueError(f"unsupported aggregation {spec!r} for {name!r}: use 'size' or (values, 'sum')")
+        for name, spec in aggregations.items():
+            if not isinstance(name, str):
+                raise TypeError("query aggregate output column names must be strings")
+            if isinstance(spec, str) and spec == "size":
                 specs[name] = None
-            else:
-                values, op = spec
-                if op != "sum":
-                    raise ValueError(f"unsupported aggregation {op!r} for {name!r}: use 'sum'")
-                v = np.asarray(getattr(values, "to_numpy", lambda: values)(), dtype=np.float64)
-                if v.shape != (m,):
-                    raise ValueError(f"values of {name!r} must have one entry per indexed geometry ({m})")
-                specs[name] = v
+                continue
+            if not (isinstance(spec, tuple) and len(spec) == 2 and spec[1] == "sum"):
+                raise ValueError("query aggregate specifications must be 'size' or (values, 'sum')")
+            values = spec[0]
+            shape = getattr(values, "shape", None)
+            if shape is not None and len(shape) != 1:
+                raise ValueError("query aggregate values must be one-dimensional")
+            try:
+                count = len(values)
+            except TypeError as exc:
+                raise ValueError("query aggregate values must be one-dimensional and aligned with indexed tree "
+                                 "geometries") from exc
+            if count != m:
+                raise ValueError("query aggregate values must align with indexed tree geometries")
+            raw = np.asarray(getattr(values, "to_numpy", lambda: values)())
+            if not pd.api.types.is_numeric_dtype(raw.dtype):
+                raise TypeError("query aggregate sum values must be numeric")
+            specs[name] = raw.astype(np.float64)
         rows, trows = self._pair_rows(arr, predicate, distance)
         out = {}
         if isinstance(rows, np.ndarray):
@@ -310,6 +326,97 @@ class SpatialIndex:
                         acc.index_add_(0, r, dv[trows.long()])
                     out[name] = acc.cpu().numpy()
         return pd.DataFrame(out, index=index)
+
+    # -- row flow without exported pairs (the reference's private relation
+    # -- methods, src/vibespatial/api/sindex.py:1592-1760, 2381) ------------
+
+    def query_relation(self, geometry, *, predicate=None, sort=False, distance=None, return_device=True):
+        """The query's pairs as a :class:`~vibespatial_b200.relation.Relation`
+        (query rows on the left, indexed rows on the right, sorted by left):
+        sindex.query_relation (src/vibespatial/api/sindex.py:1592).  With
+        ``return_device`` (the default) the arrays are the join's CUDA tensors."""
+        from .relation import Relation
+
+        arr, _ = self._input(geometry)
+        if return_device:
+            rows, trows = self._pair_rows(arr, predicate, distance)
+        else:
+            res = query_spatial_index(self.geometry, arr, predicate=predicate, sort=sort, distance=distance)
+            rows, trows = res[0], res[1]
+        return Relation(rows, trows, predicate=predicate, left_row_count=len(arr),
+                        right_row_count=len(self.geometry), sorted_by_left=True)
+
+    def query_left_semijoin(self, geometry, *, predicate=None, distance=None):
+        """Query rows with at least one match, ascending (a
+        :class:`~vibespatial_b200.relation.RowSet`): sindex.query_left_semijoin
+        (src/vibespatial/api/sindex.py:1633)."""
+        return self.query_relation(geometry, predicate=predicate, distance=distance).left_semijoin_rowset()
+
+    def query_left_antijoin(self, geometry, *, predicate=None, distance=None):
+        """Query rows without any match, ascending: sindex.query_left_antijoin
+        (src/vibespatial/api/sindex.py:1660)."""
+        return self.query_left_semijoin(geometry, predicate=predicate, distance=distance).complement()
+
+    def query_right_semijoin(self, geometry, *, predicate=None, distance=None):
+        """Indexed rows matched by at least one query geometry, ascending:
+        sindex.query_right_semijoin (src/vibespatial/api/sindex.py:1714)."""
+        return self.query_relation(geometry, predicate=predicate, distance=distance).right_semijoin_rowset()
+
+    def query_left_match_count_expression(self, geometry, *, predicate=None, distance=None):
+        """Matches per query row (an int64 :class:`~vibespatial_b200.relation.Expression`):
+        sindex.query_left_match_count_expression (src/vibespatial/api/sindex.py:1687)."""
+        from .relation import Expression
+
+        rel = self.query_relation(geometry, predicate=predicate, distance=distance)
+        counts = rel.left_match_count_expression()
+        return Expression("spatial_index.left_match_count", counts.values, source_row_count=counts.source_row_count,
+                          dtype="int64")
+
+    def query_pair_aggregate(self, other, geometry, *, predicate=None, distance=None):
+        """Per indexed row position i of two aligned indexes: the query
+        geometries matching ``self``'s row i (``left_count``), ``other``'s row
+        i (``right_count``), and both (``shared_count``): sindex.query_pair_aggregate
+        (src/vibespatial/api/sindex.py:973; shared pairs as in its host path :1257-1270)."""
+        import pandas as pd
+
+        if not isinstance(other, SpatialIndex):
+            raise TypeError("other must be a SpatialIndex")
+        if other.size != self.size:
+            raise ValueError("query pair aggregate indexes must have equal size")
+        a = self.query_relation(geometry, predicate=predicate, distance=distance)
+        b = other.query_relation(geometry, predicate=predicate, distance=distance)
+        m = self.size
+        nq = max(int(a.left_row_count), 1)
+        left = a.right_match_count_expression().to_numpy()
+        right = b.right_match_count_expression().to_numpy()
+        # pairs are unique, so the pairs of a also present in b are the shared ones
+        if a.is_device and b.is_device:
+            import torch
+
+            ka = a.right_indices.long() * nq + a.left_indices.long()
+            kb = b.right_indices.long() * nq + b.left_indices.long()
+            shared_rows = a.right_indices[torch.isin(ka, kb)] if ka.numel() and kb.numel() else a.right_indices[:0]
+            shared = torch.bincount(shared_rows.long(), minlength=m)[:m].cpu().numpy() if shared_rows.numel() else \
+                np.zeros(m, np.int64)
+        else:
+            ar, al = np.asarray(a.right_indices, np.int64), np.asarray(a.left_indices, np.int64)
+            br, bl = np.asarray(b.right_indices, np.int64), np.asarray(b.left_indices, np.int64)
+            both = np.isin(ar * nq + al, br * nq + bl)
+            shared = np.bincount(ar[both], minlength=m)[:m] if both.any() else np.zeros(m, np.int64)
+        return pd.DataFrame({"left_count": left.astype(np.int64), "right_count": right.astype(np.int64),
+                             "shared_count": np.asarray(shared, np.int64)}, index=pd.RangeIndex(m))
+
+    def nearest_relation(self, geometry, *, return_all=True, max_distance=None, exclusive=False, k=1):
+        """The nearest pairs with their distances as a
+        :class:`~vibespatial_b200.relation.Relation` (sindex.nearest_relation,
+        src/vibespatial/api/sindex.py:2381); same arguments as :meth:`nearest`."""
+        from .relation import Relation
+
+        arr, _ = self._input(geometry)
+        pairs, dist = self.nearest(arr, return_all=return_all, max_distance=max_distance, return_distance=True,
+                                   exclusive=exclusive, k=k)
+        return Relation(pairs[0], pairs[1], predicate="nearest", distances=dist, left_row_count=len(arr),
+                        right_row_count=len(self.geometry), sorted_by_left=True)
 
     def intersection(self, coordinates):
         """Compatibility form of query (rtree's Index.intersection): tree rows
