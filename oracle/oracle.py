@@ -92,6 +92,8 @@ def lib():
         L.orc_wkb_fill.restype = None
         L.orc_wkb_fill.argtypes = [_u8p, _i64p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int8), _i64p, _i32p, _i32p,
                                    _i32p, _dp, _dp, ctypes.c_int]
+        L.orc_point_segment_distance.restype = ctypes.c_double
+        L.orc_point_segment_distance.argtypes = [ctypes.c_double] * 6
         L.orc_point_polygon_distance.restype = ctypes.c_double
         L.orc_point_polygon_distance.argtypes = [ctypes.c_double, ctypes.c_double, _dp, _dp, _i32p, _i32p, _i32p,
                                                  ctypes.c_int64]
@@ -244,6 +246,11 @@ def _dpairs(h):
     finally:
         L.orc_dpairs_free(h)
     return left, right, dist
+
+
+def point_segment_distance(px: float, py: float, ax: float, ay: float, bx: float, by: float) -> float:
+    """Distance from (px, py) to the segment (ax, ay)-(bx, by)."""
+    return float(lib().orc_point_segment_distance(float(px), float(py), float(ax), float(ay), float(bx), float(by)))
 
 
 def point_polygon_distance(px: float, py: float, polys: Polygons, g: int) -> float:
