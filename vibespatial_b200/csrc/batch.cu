@@ -521,7 +521,7 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
     for (int j = 0; j < n_jobs; ++j) {
         const vs_index* ix = indexes[j];
         JobTree& t = jobs[j];
-        memset(&t, 0, sizeof(t));
+        t = JobTree{};
         t.nodes = ix->nodes;
         t.item_geom = ix->item_geom;
         t.geom_off = ix->geom_off;
@@ -551,7 +551,7 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
         for (int j = 0; j < n_jobs; ++j) {
             const vs_index* ix = indexes[j];
             LearnedJob& d = ljobs[j];
-            memset(&d, 0, sizeof(d));
+            d = LearnedJob{};
             const bool has_polys = ix->n_geoms > 0 && ix->h_frame[0] <= ix->h_frame[2];
             if (ix->has_learned) {
                 d = ix->learned.h_desc;
