@@ -816,7 +816,7 @@ def run_nearest_polygons(args, rank, world, local_rank):
     pidx = _abi.point_index(ctx, dx, dy)
     build_wall = time.perf_counter() - t0
     M = len(pol.geom_off) - 1
-    left, right, dist, st = _abi.nearest_polygons(ctx, pidx, P)
+    left, _, _, st = _abi.nearest_polygons(ctx, pidx, P)
     n_pairs = int(left.numel())
     cap = max(n_pairs, 1)
     for _ in range(args.warmup):
@@ -967,17 +967,17 @@ def run_ours(args, rank, world, local_rank):
     left = torch.empty(cap, dtype=torch.int32, device=dev)
     right = torch.empty(cap, dtype=torch.int32, device=dev)
     try:
-        n_pairs, stats = index.join_into(pts, pred, method, left, right)
+        n_pairs, _ = index.join_into(pts, pred, method, left, right)
     except _abi.CapacityError as e:
         cap = e.required
         left = torch.empty(cap, dtype=torch.int32, device=dev)
         right = torch.empty(cap, dtype=torch.int32, device=dev)
-        n_pairs, stats = index.join_into(pts, pred, method, left, right)
+        n_pairs, _ = index.join_into(pts, pred, method, left, right)
     assert join(left, right)[0] == n_pairs
     # plain R-tree on the same GPU, for the learned-vs-plain ratio
     plain = None
     if method == _abi.METHOD_LEARNED:
-        n_plain, st_plain = index.join_into(pts, pred, _abi.METHOD_RTREE, left, right)
+        n_plain, _ = index.join_into(pts, pred, _abi.METHOD_RTREE, left, right)
         assert n_plain == n_pairs, (n_plain, n_pairs)
 
     for _ in range(args.warmup):

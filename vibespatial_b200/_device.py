@@ -186,7 +186,7 @@ def point_index(points, device: int = 0) -> "_abi.DeviceIndex":
     idx = points._cache.get(key)
     if idx is None:
         _torch()
-        pts, t = device_points(points, device)
+        _, t = device_points(points, device)
         idx = points._cache[key] = _abi.point_index(_abi.default_context(device), t["x"], t["y"], t["valid"])
     return idx
 

@@ -9,7 +9,6 @@ src/vibespatial/api/geo_base.py:4461/3314) and ``GeoDataFrame.sjoin``
 """
 from __future__ import annotations
 
-import numpy as np
 import pandas as pd
 
 from .geometry import BaseGeometry, GeometryArray, GeometryDtype

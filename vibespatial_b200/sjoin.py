@@ -18,7 +18,7 @@ import warnings
 import numpy as np
 import pandas as pd
 
-from .frame import GeoDataFrame, GeoSeries
+from .frame import GeoDataFrame
 from .geometry import GeometryArray
 from .query import query_spatial_index
 

@@ -361,7 +361,6 @@ def wkb_polygons(p: PolygonSoA) -> tuple[np.ndarray, np.ndarray]:
     put_u32(offsets[:-1] + 1, np.where(multi, 6, 3))
     put_u32(offsets[:-1][multi] + 5, nparts[multi])
     # part starts
-    part_rank = np.arange(len(part_row)) - geom_off[part_row]
     part_start_in_row = np.zeros(len(part_row), np.int64)
     if len(part_row):
         cum = np.cumsum(part_bytes + part_hdr) - (part_bytes + part_hdr)
