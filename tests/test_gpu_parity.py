@@ -104,8 +104,8 @@ def test_ring_bins(vsabi, ctx, oracle, workload, bin_min):
             assert_same_pairs(gl.cpu().numpy(), gr.cpu().numpy(), el, er)
 
 
-def test_learned_index_is_judged_by_rtree(vsabi, ctx):
-    """Learned lookups and plain traversal give the same pair set (the R-tree is the judge)."""
+def test_learned_index_agrees_with_rtree(vsabi, ctx):
+    """Learned lookups and plain traversal give the same pair set (the R-tree is the arbiter)."""
     from vibespatial_b200.testing import synthetic as syn
 
     w = syn.zipf_join(seed=13, n_points=3_000_000, n_polys=200_000)
