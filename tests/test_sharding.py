@@ -86,3 +86,87 @@ def test_two_rank_gloo_sharded_join(tmp_path, oracle):
     np.testing.assert_array_equal(right[o], er)
     # rank 0 holds the lower half of the points
     assert parts[0]["left"].max() < parts[1]["left"].min()
+
+
+def _distance_worker(rank, world, port, out_dir):
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle as O
+    from vibespatial_b200.geometry import GeometryArray
+    from vibespatial_b200.sharding import sharded_dwithin, sharded_nearest, sharded_nearest_polygons
+    from vibespatial_b200.testing import synthetic as syn
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        w = syn.star_join(seed=33, n_points=8_001, n_polys=201)
+        points = GeometryArray.from_points(w.px, w.py)
+        polys = GeometryArray.from_polygon_buffers(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off,
+                                                   w.polys.geom_off)
+
+        def oracle_args(pts, pg):  # the CPU oracle stands in for the GPU joins here
+            px, py, pv = pts.point_buffers()
+            pb = pg.polygon_buffers()
+            return px, py, pv, O.Polygons(pb.x, pb.y, pb.ring_off, pb.part_off, pb.geom_off, pb.valid)
+
+        def dwithin_fn(pts, pg, distance=0.0, point_distance=None, geom_distance=None):
+            px, py, pv, P = oracle_args(pts, pg)
+            l, r, _ = O.dwithin_join(px, py, pv, P, distance, point_distance=point_distance,
+                                     geom_distance=geom_distance)
+            return l, r
+
+        def nearest_fn(pts, pg, max_distance=None):
+            px, py, pv, P = oracle_args(pts, pg)
+            return O.nearest_join(px, py, pv, P, float("inf") if max_distance is None else max_distance)
+
+        def nearest_polygons_fn(pg, pts, max_distance=None):
+            px, py, pv, P = oracle_args(pts, pg)
+            return O.nearest_polygons_join(px, py, pv, P, float("inf") if max_distance is None else max_distance)
+
+        per_point = np.linspace(0.0, 3.0, len(w.px))
+        out = {}
+        out["dw_l"], out["dw_r"], out["dw_c"] = sharded_dwithin(points, polys, point_distance=per_point,
+                                                                pairs_fn=dwithin_fn)
+        out["nn_l"], out["nn_r"], out["nn_d"], out["nn_c"] = sharded_nearest(points, polys, max_distance=25.0,
+                                                                             pairs_fn=nearest_fn)
+        out["np_l"], out["np_r"], out["np_d"], out["np_c"] = sharded_nearest_polygons(polys, points,
+                                                                                     pairs_fn=nearest_polygons_fn)
+        np.savez(os.path.join(out_dir, f"dist_rank{rank}.npz"), **out)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_sharded_distance_joins(tmp_path, oracle):
+    """dwithin (per-point distances sliced with the points), nearest (points
+    sharded) and reverse nearest (polygons sharded): the ranks' pairs
+    together are the single-process result, the gathered counts locate them."""
+    import torch.multiprocessing as mp
+
+    from vibespatial_b200.testing import synthetic as syn
+
+    world = 2
+    mp.start_processes(_distance_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    parts = [np.load(tmp_path / f"dist_rank{r}.npz") for r in range(world)]
+    w = syn.star_join(seed=33, n_points=8_001, n_polys=201)
+    P = oracle.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+    per_point = np.linspace(0.0, 3.0, len(w.px))
+    expected = {
+        "dw": oracle.dwithin_join(w.px, w.py, None, P, 0.0, point_distance=per_point)[:2],
+        "nn": oracle.nearest_join(w.px, w.py, None, P, 25.0),
+        "np": oracle.nearest_polygons_join(w.px, w.py, None, P),
+    }
+    for key, exp in expected.items():
+        counts = parts[0][f"{key}_c"]
+        assert np.array_equal(counts, parts[1][f"{key}_c"])
+        assert [len(p[f"{key}_l"]) for p in parts] == counts.tolist()
+        got = [np.concatenate([p[f"{key}_{c}"] for p in parts]) for c in ("l", "r", "d")[:len(exp)]]
+        # the ranks hold consecutive slices of the query rows, each sorted: concatenated, they are sorted
+        for g, e in zip(got, exp):
+            np.testing.assert_array_equal(g, e)
+        assert len(got[0]) > 0
