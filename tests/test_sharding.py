@@ -170,3 +170,35 @@ def test_two_rank_gloo_sharded_distance_joins(tmp_path, oracle):
         for g, e in zip(got, exp):
             np.testing.assert_array_equal(g, e)
         assert len(got[0]) > 0
+
+
+@pytest.mark.gpu
+def test_sharded_joins_one_rank_on_the_gpu(oracle):
+    """Without a process group the sharded forms are the whole join on the
+    CUDA path: same pairs and distances as the oracle."""
+    from vibespatial_b200.geometry import GeometryArray
+    from vibespatial_b200.sharding import sharded_dwithin, sharded_join, sharded_nearest, sharded_nearest_polygons
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.star_join(seed=35, n_points=20_000, n_polys=300)
+    points = GeometryArray.from_points(w.px, w.py)
+    polys = GeometryArray.from_polygon_buffers(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off,
+                                               w.polys.geom_off)
+    P = oracle.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
+    l, r, c = sharded_join(points, polys, "within")
+    el, er = oracle.join(w.px, w.py, None, P, "within")
+    np.testing.assert_array_equal(l, el)
+    np.testing.assert_array_equal(r, er)
+    assert c.tolist() == [len(el)]
+    l, r, c = sharded_dwithin(points, polys, distance=1.5)
+    el, er, _ = oracle.dwithin_join(w.px, w.py, None, P, 1.5)
+    np.testing.assert_array_equal(l, el)
+    np.testing.assert_array_equal(r, er)
+    l, r, d, c = sharded_nearest(points, polys, max_distance=30.0)
+    el, er, ed = oracle.nearest_join(w.px, w.py, None, P, 30.0)
+    for g, e in ((l, el), (r, er), (d, ed)):
+        np.testing.assert_array_equal(g, e)
+    l, r, d, c = sharded_nearest_polygons(polys, points)
+    el, er, ed = oracle.nearest_polygons_join(w.px, w.py, None, P)
+    for g, e in ((l, el), (r, er), (d, ed)):
+        np.testing.assert_array_equal(g, e)
