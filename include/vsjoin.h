@@ -241,7 +241,9 @@ int vs_distance_aligned(vs_context* ctx, const vs_points* pts, const vs_polygons
  *   VS_HOW_OUTER  as LEFT, then (-1, row) for every right row without a pair
  * d_out_src (nullable) receives each output row's input pair position (-1
  * for an added row).  *n_out = the number of rows; VS_E_CAPACITY (buffers
- * untouched) when it exceeds capacity.  Up to 2^31 - 1 pairs and rows a side. */
+ * untouched) when it exceeds capacity.  Pairs naming rows outside
+ * [0, n_left) x [0, n_right) give VS_E_ARG before anything is written.
+ * Up to 2^31 - 1 pairs and rows a side. */
 enum { VS_HOW_INNER = 0, VS_HOW_LEFT = 1, VS_HOW_RIGHT = 2, VS_HOW_OUTER = 3 };
 int vs_join_export(vs_context* ctx, const int32_t* d_left, const int32_t* d_right, int64_t n_pairs,
                    int64_t n_left, int64_t n_right, int32_t how, const int64_t* d_left_code,
