@@ -509,6 +509,14 @@ def test_sindex_relation_flow(backend):
     with pytest.raises(ValueError, match="equal size"):
         tree.sindex.query_pair_aggregate(vs.GeometryArray.from_shapes([vs.box(0, 0, 1, 1)]).sindex, q)
 
+    # dwithin: (20, 20) is 12.73 from the third box and 14.14 from the fourth
+    assert tree.sindex.query_left_semijoin(q, predicate="dwithin", distance=10.0).to_numpy().tolist() == [0, 1, 3, 4]
+    assert tree.sindex.query_left_semijoin(q, predicate="dwithin", distance=13.0).to_numpy().tolist() == [0, 1, 2, 3,
+                                                                                                        4]
+    assert tree.sindex.query_right_semijoin(q, predicate="dwithin", distance=13.0).to_numpy().tolist() == [0, 1, 2]
+    counts = tree.sindex.query_left_match_count_expression(q, predicate="dwithin", distance=13.0)
+    assert counts.to_numpy().tolist() == [3, 3, 1, 3, 3]  # at 13 every point but (20, 20) reaches three boxes
+
     near = tree.sindex.nearest_relation(q)
     pairs, dist = tree.sindex.nearest(q, return_distance=True)
     np.testing.assert_array_equal(near.to_numpy(), pairs)
