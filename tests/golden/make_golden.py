@@ -189,6 +189,10 @@ def main(ref_root: str) -> None:
             "value": [213, 4],
             "source": "tests/upstream/geopandas/tools/tests/test_sjoin.py:1039-1044",
         },
+        "cities_countries_shared_first_letter_shape": {
+            "value": [23, 5],
+            "source": "tests/upstream/geopandas/tools/tests/test_sjoin.py:513-526",
+        },
     }
     (HERE / "expected.json").write_text(json.dumps(expected, indent=2) + "\n")
     for f in ("nybb.npz", "naturalearth_lowres.npz", "naturalearth_cities.npz"):

@@ -161,6 +161,24 @@ def test_cities_countries(backend):
     assert sorted(zip(a.index, a["index_right"])) == sorted(zip(b["index_right"], b.index))
 
 
+def test_cities_countries_shared_attribute(backend):
+    """on_attribute: cities and countries joined where they intersect and
+    their names share a first letter (the reference's known answer: 23 rows,
+    5 columns), through the device export when the pairs are on the device."""
+    w = dict(np.load(GOLDEN / "naturalearth_lowres.npz"))
+    c = dict(np.load(GOLDEN / "naturalearth_cities.npz"))
+    countries = vs.GeoDataFrame({"country": w["attr_name"]},
+                                geometry=GeometryArray.from_polygon_buffers(w["x"], w["y"], w["ring_off"],
+                                                                            w["part_off"], w["geom_off"],
+                                                                            geom_type=w["geom_type"]))
+    cities = vs.GeoDataFrame({"name": c["attr_name"]}, geometry=vs.points_from_xy(c["x"], c["y"]))
+    countries["firstLetter"] = countries["country"].astype(str).str[0]
+    cities["firstLetter"] = cities["name"].astype(str).str[0]
+    result = vs.sjoin(cities, countries, on_attribute="firstLetter")
+    assert (result["country"].astype(str).str[0] == result["name"].astype(str).str[0]).all()
+    assert list(result.shape) == EXP["cities_countries_shared_first_letter_shape"]["value"]
+
+
 def _small_frames(index_kind):
     polys = vs.GeoDataFrame({"geometry": [vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11)],
                              "df2": [3, 4, 5]})
