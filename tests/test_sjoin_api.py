@@ -179,6 +179,22 @@ def test_cities_countries_shared_attribute(backend):
     assert list(result.shape) == EXP["cities_countries_shared_first_letter_shape"]["value"]
 
 
+@pytest.mark.parametrize("predicate", ["contains", "contains_properly", "covered_by", "covers", "crosses",
+                                       "intersects", "touches", "within"])
+def test_sjoin_left_order(backend, predicate):
+    """A left join keeps the points' order, whatever the predicate
+    (tests/upstream/geopandas/tools/tests/test_sjoin.py:480-511)."""
+    pts = vs.GeoDataFrame(geometry=vs.points_from_xy([0.1, 0.4, 0.3, 0.7], [0.8, 0.6, 0.9, 0.1]))
+    polys = vs.GeoDataFrame({"id": [1, 2, 3, 4]},
+                            geometry=[vs.box(0, 0, 0.5, 0.5), vs.box(0, 0.5, 0.5, 1), vs.box(0.5, 0, 1, 0.5),
+                                      vs.box(0.5, 0.5, 1, 1)])
+    joined = vs.sjoin(pts, polys, predicate=predicate, how="left")
+    pd.testing.assert_index_equal(joined.index, pts.index)
+    if predicate in ("intersects", "within", "covered_by"):
+        # each point lies inside exactly one box
+        assert joined["id"].tolist() == [2, 2, 2, 3]
+
+
 def _small_frames(index_kind):
     polys = vs.GeoDataFrame({"geometry": [vs.box(0, 0, 5, 5), vs.box(3, 3, 6, 6), vs.box(10, 10, 11, 11)],
                              "df2": [3, 4, 5]})

@@ -154,9 +154,16 @@ class GeoDataFrame(pd.DataFrame):
         else:
             col = "geometry"
             values = _to_geometry_array(geometry, crs=crs)
-            if len(values) != len(self):
-                raise ValueError("geometry length does not match the frame")
-            self[col] = pd.Series(values, index=self.index)
+            if len(self.columns) == 0 and len(self) == 0 and len(values):
+                # no data columns: the frame takes the geometry's rows (and its index, for a series)
+                index = getattr(geometry, "index", None)
+                index = index if isinstance(index, pd.Index) and len(index) == len(values) else \
+                    pd.RangeIndex(len(values))
+                self[col] = pd.Series(values, index=index)
+            else:
+                if len(values) != len(self):
+                    raise ValueError("geometry length does not match the frame")
+                self[col] = pd.Series(values, index=self.index)
         if not isinstance(self[col].dtype, GeometryDtype):
             self[col] = pd.Series(_to_geometry_array(self[col], crs=crs), index=self.index)
         if crs is not None:
