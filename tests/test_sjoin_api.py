@@ -135,6 +135,42 @@ def test_nybb_geometry_name_and_duplicate_columns(backend):
         vs.sjoin(pointdf, polydf, unknown=1)
 
 
+@pytest.mark.parametrize("how", ["left", "right", "inner"])
+def test_nybb_named_index(backend, how):
+    """Index names pass through untouched (tests/upstream/geopandas/tools/tests/test_sjoin.py:911-927)."""
+    pointdf, polydf = nybb_frames()
+    pointdf.index.name = "pointid"
+    polydf.index.name = "polyid"
+    res = vs.sjoin(pointdf, polydf, how=how)
+    assert pointdf.index.name == "pointid" and polydf.index.name == "polyid"
+    assert res.index.name == ("polyid" if how == "right" else "pointid")
+
+
+def test_nybb_values_outer_and_empty_geometries(backend):
+    """test_sjoin.py:929-1008: a non-default polygon index, the outer join's
+    counts, and empty geometries (of another family) that never match."""
+    pointdf, polydf = nybb_frames()
+    relabelled = polydf.copy()
+    relabelled.index = [1, 3, 4, 5, 6]
+    assert vs.sjoin(pointdf, relabelled, how="left").shape == (21, 8)
+    assert vs.sjoin(relabelled, pointdf, how="left").shape == (12, 8)
+
+    df = vs.sjoin(pointdf, polydf, how="outer")
+    left = vs.sjoin(pointdf, polydf, how="left")
+    right = vs.sjoin(pointdf, polydf, how="right")
+    unmatched_left = int(left["index_right"].isna().sum())
+    unmatched_right = int(right["index_left"].isna().sum())
+    assert len(df) == len(left) + unmatched_right
+    assert int(df["index_left"].isna().sum()) == unmatched_right
+    assert int(df["index_right"].isna().sum()) == unmatched_left
+    assert df.geometry.notna().all()
+
+    # the reference uses empty GeometryCollections; empty polygons play that part here
+    empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([vs.Polygon([])] * 3), crs=pointdf.crs)
+    assert vs.sjoin(pd.concat([pointdf, empty]), polydf, how="left").shape == (24, 8)
+    assert vs.sjoin(pointdf, pd.concat([polydf, empty]), how="left").shape == (21, 8)
+
+
 def test_no_valid_geoms(backend):
     pointdf, polydf = nybb_frames()
     empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([]), crs=pointdf.crs)

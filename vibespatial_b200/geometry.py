@@ -462,7 +462,15 @@ class GeometryArray(ExtensionArray):
         return pts | polys
 
     def families(self) -> set:
-        return {int(t) for t in np.unique(self._tags) if t != NULL}
+        """Tags of the rows that can match anything: null and empty rows of any
+        family never match (src/vibespatial/api/tools/sjoin.py:502-544), so
+        they do not decide which side of a join holds the points."""
+        fam = self._cache.get("families")  # the array is immutable
+        if fam is None:
+            live = self._tags[(self._tags != NULL) & ~self.is_empty]
+            present = np.bincount(live.astype(np.int64) + 1, minlength=1)  # tags >= -1: counted, not sorted
+            fam = self._cache["families"] = frozenset(int(t) - 1 for t in np.flatnonzero(present))
+        return set(fam)
 
     def is_points(self) -> bool:
         return self.families() <= {POINT}
