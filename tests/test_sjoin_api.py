@@ -171,6 +171,66 @@ def test_nybb_values_outer_and_empty_geometries(backend):
     assert vs.sjoin(pointdf, pd.concat([polydf, empty]), how="left").shape == (21, 8)
 
 
+@pytest.mark.parametrize("how, lsuffix, rsuffix, expected_cols", [
+    ("left", "left", "right", {"col_left", "col_right", "index_right"}),
+    ("inner", "left", "right", {"col_left", "col_right", "index_right"}),
+    ("right", "left", "right", {"col_left", "col_right", "index_left"}),
+    ("outer", "left", "right", {"col_left", "col_right", "index_left", "index_right"}),
+    ("left", "lft", "rgt", {"col_lft", "col_rgt", "index_rgt"}),
+    ("inner", "lft", "rgt", {"col_lft", "col_rgt", "index_rgt"}),
+    ("right", "lft", "rgt", {"col_lft", "col_rgt", "index_lft"}),
+    ("outer", "lft", "rgt", {"col_lft", "col_rgt", "index_lft", "index_rgt"}),
+])
+def test_suffixes(backend, how, lsuffix, rsuffix, expected_cols):
+    """tests/upstream/geopandas/tools/tests/test_sjoin.py:141-163, with a point
+    and a polygon around it (the reference uses two points)."""
+    left = vs.GeoDataFrame({"col": [1], "geometry": [vs.Point(0, 0)]})
+    right = vs.GeoDataFrame({"col": [1], "geometry": [vs.box(-1, -1, 1, 1)]})
+    joined = vs.sjoin(left, right, how=how, lsuffix=lsuffix, rsuffix=rsuffix)
+    assert set(joined.columns) == expected_cols | {"geometry"}
+
+
+def test_argument_errors_and_crs_warning(backend):
+    """test_sjoin.py:165-181, 325-344: a CRS mismatch warns, unknown keywords
+    and non-frame inputs raise."""
+    left = vs.GeoDataFrame({"col": [1], "geometry": [vs.Point(0, 0)]}, crs="EPSG:3857")
+    right = vs.GeoDataFrame({"col": [1], "geometry": [vs.box(-1, -1, 1, 1)]}, crs="EPSG:4326")
+    with pytest.warns(UserWarning, match="CRS mismatch between the CRS"):
+        vs.sjoin(left, right)
+    right = vs.GeoDataFrame({"col": [1], "geometry": [vs.box(-1, -1, 1, 1)]}, crs="EPSG:3857")
+    with pytest.raises(TypeError, match=r"sjoin\(\) got an unexpected keyword argument 'extra_param'"):
+        vs.sjoin(left, right, extra_param="test")
+    with pytest.raises(ValueError, match="'left_df' should be GeoDataFrame"):
+        vs.sjoin(left.geometry, right)
+    with pytest.raises(ValueError, match="'right_df' should be GeoDataFrame"):
+        vs.sjoin(left, right.geometry)
+
+
+PREDICATES_ALL = ["contains", "contains_properly", "covered_by", "covers", "crosses", "intersects", "touches",
+                  "within"]
+
+
+@pytest.mark.parametrize("predicate", PREDICATES_ALL)
+@pytest.mark.parametrize("empty_kind", ["empty geometries", "no rows"])
+def test_join_with_empty(backend, predicate, empty_kind):
+    """test_sjoin.py:267-323: a point outside both polygons, a frame of empty
+    geometries and a frame without rows give all-missing or empty joins."""
+    polygons = vs.GeoDataFrame({"col2": [1, 2], "geometry": [vs.box(0, 0, 1, 1), vs.box(1, 0, 2, 1)]})
+    not_in = vs.GeoDataFrame({"col1": [1], "geometry": [vs.Point(-0.5, 0.5)]})
+    assert vs.sjoin(not_in, polygons, how="left", predicate=predicate).index_right.isnull().all()
+    assert vs.sjoin(not_in, polygons, how="right", predicate=predicate).index_left.isnull().all()
+    assert vs.sjoin(not_in, polygons, how="inner", predicate=predicate).empty
+    if empty_kind == "empty geometries":
+        empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([vs.Point(), vs.Point()]))
+    else:
+        empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([]))
+    result = vs.sjoin(empty, polygons, how="left", predicate=predicate)
+    assert result.index_right.isnull().all()
+    result = vs.sjoin(empty, polygons, how="right", predicate=predicate)
+    assert result.index_left.isnull().all()
+    assert vs.sjoin(empty, polygons, how="inner", predicate=predicate).empty
+
+
 def test_no_valid_geoms(backend):
     pointdf, polydf = nybb_frames()
     empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([]), crs=pointdf.crs)
