@@ -231,6 +231,55 @@ def test_join_with_empty(backend, predicate, empty_kind):
     assert vs.sjoin(empty, polygons, how="inner", predicate=predicate).empty
 
 
+@pytest.mark.parametrize("how", ["inner", "left", "right"])
+def test_preserve_index_names(backend, how):
+    """test_sjoin.py:610-645 with boxes around the right-hand points: both
+    index names survive, and equal names get the suffixes."""
+    pts = [vs.Point(1, 1), vs.Point(2, 2)]
+    boxes = [vs.box(0.5, 0.5, 1.5, 1.5), vs.box(1.5, 1.6, 2.5, 2.5)]
+    df1 = vs.GeoDataFrame({"geometry": pts}, index=pd.Index([1, 2], name="myidx1"))
+    df2 = vs.GeoDataFrame({"geometry": boxes}, index=pd.Index(["a", "b"], name="myidx2"))
+    result = vs.sjoin(df1, df2, how=how)
+    if how in ("inner", "left"):
+        assert result.index.name == "myidx1" and result.index.tolist() == [1, 2]
+        assert list(result.columns) == ["geometry", "myidx2"] and result["myidx2"].tolist() == ["a", "b"]
+    else:
+        assert result.index.name == "myidx2" and result.index.tolist() == ["a", "b"]
+        assert list(result.columns) == ["myidx1", "geometry"] and result["myidx1"].tolist() == [1, 2]
+    df1.index.name = "myidx"
+    df2.index.name = "myidx"
+    result = vs.sjoin(df1, df2, how=how)
+    if how in ("inner", "left"):
+        assert result.index.name == "myidx_left" and list(result.columns) == ["geometry", "myidx_right"]
+    else:
+        assert result.index.name == "myidx_right" and list(result.columns) == ["myidx_left", "geometry"]
+
+
+@pytest.mark.parametrize("how", ["inner", "left", "right"])
+def test_duplicate_column_index_name(backend, how):
+    """test_sjoin.py:705-739: a left column named like the right index gets
+    the suffixes on both."""
+    pts = [vs.Point(1, 1), vs.Point(2, 2)]
+    boxes = [vs.box(0.5, 0.5, 1.5, 1.5), vs.box(1.5, 1.6, 2.5, 2.5)]
+    df1 = vs.GeoDataFrame({"myidx": [1, 2], "geometry": pts})
+    df2 = vs.GeoDataFrame({"geometry": boxes}, index=pd.Index(["a", "b"], name="myidx"))
+    result = vs.sjoin(df1, df2, how=how)
+    if how in ("inner", "left"):
+        assert list(result.columns) == ["myidx_left", "geometry", "myidx_right"]
+        assert result["myidx_left"].tolist() == [1, 2] and result["myidx_right"].tolist() == ["a", "b"]
+    else:
+        assert result.index.name == "myidx_right" and result.index.tolist() == ["a", "b"]
+        assert list(result.columns) == ["index_left", "myidx_left", "geometry"]
+    result = vs.sjoin(df2, df1, how=how)
+    if how in ("inner", "left"):
+        assert result.index.name == "myidx_left" and result.index.tolist() == ["a", "b"]
+        assert list(result.columns) == ["geometry", "index_right", "myidx_right"]
+        assert result["myidx_right"].tolist() == [1, 2]
+    else:
+        assert list(result.columns) == ["myidx_left", "myidx_right", "geometry"]
+        assert result["myidx_left"].tolist() == ["a", "b"] and result["myidx_right"].tolist() == [1, 2]
+
+
 def test_no_valid_geoms(backend):
     pointdf, polydf = nybb_frames()
     empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([]), crs=pointdf.crs)
