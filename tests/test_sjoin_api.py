@@ -280,6 +280,25 @@ def test_duplicate_column_index_name(backend, how):
         assert result["myidx_left"].tolist() == ["a", "b"] and result["myidx_right"].tolist() == [1, 2]
 
 
+@pytest.mark.parametrize("how", ["inner", "left", "right"])
+def test_conflicting_column_names(backend, how):
+    """test_sjoin.py:792-835: a column named like the generated index column
+    raises; a column named like a suffixed one is kept beside it."""
+    pts = [vs.Point(1, 1), vs.Point(2, 2)]
+    boxes = [vs.box(0.5, 0.5, 1.5, 1.5), vs.box(1.5, 1.6, 2.5, 2.5)]
+    df1 = vs.GeoDataFrame({"index_right": [1, 2], "geometry": pts})
+    df2 = vs.GeoDataFrame({"geometry": boxes})
+    with pytest.raises(ValueError, match="'index_right' cannot be a column name"):
+        vs.sjoin(df1, df2, how=how)
+    df1 = vs.GeoDataFrame({"column": [1, 2], "column_right": ["a", "b"], "geometry": pts})
+    df2 = vs.GeoDataFrame({"column": [0.1, 0.2], "geometry": boxes})
+    result = vs.sjoin(df1, df2, how=how)
+    if how in ("inner", "left"):
+        assert list(result.columns) == ["column_left", "column_right", "geometry", "index_right", "column_right"]
+    else:
+        assert list(result.columns) == ["index_left", "column_left", "column_right", "column_right", "geometry"]
+
+
 def test_no_valid_geoms(backend):
     pointdf, polydf = nybb_frames()
     empty = vs.GeoDataFrame(geometry=GeometryArray.from_shapes([]), crs=pointdf.crs)
