@@ -585,6 +585,49 @@ def test_sjoin_nearest_cities_countries(backend):
     assert set(zip(within.index, within["index_right"])) <= set(zip(zero.index, zero["index_right"]))
 
 
+def _sq(x, y, h=0.1):
+    return vs.box(x - h, y - h, x + h, y + h)
+
+
+def test_sjoin_nearest_empty_frames_and_max_distance(backend):
+    """tests/upstream/geopandas/tools/tests/test_sjoin.py:1045-1176 (TestNearest),
+    with small squares around the reference's right-hand points."""
+    none = vs.GeoDataFrame({"geometry": GeometryArray.from_shapes([])})
+    for kw in ({}, {"how": "inner"}, {"how": "left"}, {"how": "right"}):
+        vs.sjoin_nearest(none, none, **kw)
+    for how in ("outer", "abcde"):
+        with pytest.raises(ValueError, match="`how` was"):
+            vs.sjoin_nearest(none, none, how=how)
+    pts = vs.GeoDataFrame({"geometry": [vs.Point(0, 0), vs.Point(1, 1)]})
+    sqs = vs.GeoDataFrame({"geometry": [_sq(0, 0), _sq(1, 1)]})
+    for col in (None, "distance"):
+        j = vs.sjoin_nearest(pts, none, how="left", distance_col=col)
+        assert len(j) == 2 and j["index_right"].isna().all()
+        assert col is None or j[col].isna().all()
+        j = vs.sjoin_nearest(pts, none, how="right", distance_col=col)
+        assert j.empty and (col is None or col in j)
+        for how in ("inner", "left"):
+            j = vs.sjoin_nearest(none, sqs, how=how, distance_col=col)
+            assert j.empty and (col is None or col in j)
+        j = vs.sjoin_nearest(none, sqs, how="right", distance_col=col)
+        assert len(j) == 2 and j["index_left"].isna().all()
+        assert col is None or j[col].isna().all()
+    # the join empties out under max_distance
+    far = vs.GeoDataFrame({"geometry": [_sq(1, 1), _sq(2, 2)]})
+    for how in ("inner", "left"):
+        j = vs.sjoin_nearest(vs.GeoDataFrame({"geometry": [vs.Point(0, 0)]}), far, how=how, max_distance=1,
+                             distance_col="distances")
+        assert j.empty if how == "inner" else (j["index_right"].isna().all() and j["distances"].isna().all())
+    # max_distance keeps the point inside a square, at distance 0
+    for how in ("inner", "left"):
+        j = vs.sjoin_nearest(pts, far, how=how, max_distance=1, distance_col="distances")
+        if how == "inner":
+            assert j.index.tolist() == [1] and j["index_right"].tolist() == [0] and j["distances"].tolist() == [0.0]
+        else:
+            assert np.isnan(j["index_right"].iloc[0]) and j["index_right"].iloc[1] == 0
+            assert np.isnan(j["distances"].iloc[0]) and j["distances"].iloc[1] == 0.0
+
+
 def test_attribute_codes_and_host_export():
     import importlib
 

@@ -22,7 +22,8 @@ from .frame import GeoDataFrame
 from .geometry import GeometryArray
 from .query import query_spatial_index
 
-_ALLOWED_HOWS = ["left", "right", "inner", "outer"]
+# sjoin allows an outer join; sjoin_nearest does not (src/vibespatial/api/tools/sjoin.py:164, :294-297)
+_SJOIN_HOWS = ["left", "right", "inner", "outer"]
 
 
 def _maybe_make_list(obj):
@@ -33,13 +34,15 @@ def _maybe_make_list(obj):
     return obj
 
 
-def _basic_checks(left_df, right_df, how, lsuffix, rsuffix, on_attribute=None):
+def _basic_checks(left_df, right_df, how, lsuffix, rsuffix, on_attribute=None, allowed_hows=None):
     if not isinstance(left_df, GeoDataFrame):
         raise ValueError(f"'left_df' should be GeoDataFrame, got {type(left_df)}")
     if not isinstance(right_df, GeoDataFrame):
         raise ValueError(f"'right_df' should be GeoDataFrame, got {type(right_df)}")
-    if how not in _ALLOWED_HOWS:
-        raise ValueError(f'`how` was "{how}" but is expected to be in {_ALLOWED_HOWS}')
+    if allowed_hows is None:
+        allowed_hows = ["left", "right", "inner"]
+    if how not in allowed_hows:
+        raise ValueError(f'`how` was "{how}" but is expected to be in {allowed_hows}')
     lcrs, rcrs = left_df.crs, right_df.crs
     if lcrs != rcrs and lcrs is not None and rcrs is not None:
         warnings.warn(f"CRS mismatch between the CRS of left geometries and the CRS of right geometries.\n"
@@ -269,7 +272,7 @@ def sjoin(left_df, right_df, how="inner", predicate="intersects", lsuffix="left"
         first = next(iter(kwargs.keys()))
         raise TypeError(f"sjoin() got an unexpected keyword argument '{first}'")
     on_attribute = _maybe_make_list(on_attribute)
-    _basic_checks(left_df, right_df, how, lsuffix, rsuffix, on_attribute=on_attribute)
+    _basic_checks(left_df, right_df, how, lsuffix, rsuffix, on_attribute=on_attribute, allowed_hows=_SJOIN_HOWS)
     l_idx, r_idx = _geom_predicate_query(left_df, right_df, predicate, distance, method)
     return _frame_join(left_df, right_df, l_idx, r_idx, how, lsuffix, rsuffix, on_attribute)
 
