@@ -152,9 +152,32 @@ def algorithmic_bytes(w, n_pairs: int) -> int:
                + 8 * n_pairs)
 
 
+def join_config(args, w) -> dict:
+    """The workload's configuration, identical in both arms (arm-specific figures live outside it)."""
+    return {"workload": WORKLOAD_DESC[args.workload], "predicate": args.predicate, "n_points_per_gpu": w.n_points,
+            "n_polygons": len(w.polys), "l2": "inputs larger than L2 (126 MB); no flush"}
+
+
+def batched_config(args, jobs) -> dict:
+    return {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate, "n_jobs": len(jobs),
+            "n_points_per_gpu": int(sum(w.n_points for w in jobs)), "n_polygons": int(sum(len(w.polys) for w in jobs)),
+            "l2": "inputs larger than L2 (126 MB); no flush"}
+
+
+def shapely_importable() -> bool:
+    """Whether Shapely (GEOS) imports on this host: the reference's own CPU path needs it."""
+    try:
+        import shapely  # noqa: F401
+    except Exception:
+        return False
+    return True
+
+
 def cpu_sample_rate(w, predicate: str, threads: int, target_s: float = 10.0):
     """Oracle (all host threads) on consecutive 2M-point chunks of the same
-    points until ~target_s of work; points/sec."""
+    points until ~target_s of work; (points/sec, points, seconds, pairs).
+    When the chunks cover every point, `pairs` is the oracle's whole sorted
+    (point row, polygon row) pair set (the checker of the GPU's pairs), else None."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
@@ -162,14 +185,26 @@ def cpu_sample_rate(w, predicate: str, threads: int, target_s: float = 10.0):
     P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
     chunk = min(w.n_points, 2_000_000)
     n, dt, start = 0, 0.0, 0
+    ls, rs = [], []
     while dt < target_s and n < w.n_points:
         stop = min(start + chunk, w.n_points)
         t0 = time.perf_counter()
-        O.join(w.px[start:stop], w.py[start:stop], None, P, predicate, threads)
+        l, r = O.join(w.px[start:stop], w.py[start:stop], None, P, predicate, threads)
         dt += time.perf_counter() - t0
+        ls.append(l.astype(np.int64) + start)
+        rs.append(r.astype(np.int64))
         n += stop - start
         start = stop
-    return n / dt, n, dt
+    pairs = (np.concatenate(ls), np.concatenate(rs)) if n == w.n_points and ls else None
+    return n / dt, n, dt, pairs
+
+
+def pair_mismatches(gl, gr, el, er) -> int:
+    """Pairs in one set and not the other, plus repeated pairs (0 = bit-exact pair sets)."""
+    a = (np.asarray(gl, np.int64) << 32) | np.asarray(gr, np.int64)
+    b = (np.asarray(el, np.int64) << 32) | np.asarray(er, np.int64)
+    ua, ub = np.unique(a), np.unique(b)
+    return int(np.setxor1d(ua, ub, assume_unique=True).size + (len(a) - len(ua)) + (len(b) - len(ub)))
 
 
 def cpu_sample_batched(jobs, predicate: str, threads: int, target_s: float = 10.0):
@@ -200,11 +235,12 @@ def run_reference_batched(args, world):
     import oracle as O
 
     O.build()
-    # a bounded sample: the first jobs up to --ref-sample points
+    # a bounded sample: every stride-th job (the sizes of the whole batch's
+    # log-uniform spread), about --ref-sample points in all
+    total = sum(w.n_points for w in jobs)
+    stride = max(1, -(-total // max(1, args.ref_sample)))
     sample, n = [], 0
-    for w in jobs:
-        if n >= args.ref_sample and sample:
-            break
+    for w in jobs[::stride]:
         sample.append((w, O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)))
         n += w.n_points
 
@@ -225,11 +261,11 @@ def run_reference_batched(args, world):
         "impl": "reference", "metric": "query points/sec", "value": value, "unit": "points/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate, "sample_points": n,
-                   "sample_jobs": len(sample)},
+        "config": batched_config(args, jobs),
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
-                         "sample": f"first {len(sample)} of {len(jobs)} jobs ({n} points), exact CPU oracle "
-                                   "(C + OpenMP): Shapely/GEOS is not installable here"},
+                         "sample": f"every {stride}th job ({len(sample)} of {len(jobs)} jobs, {n} points), exact CPU "
+                                   "oracle (C + OpenMP): Shapely/GEOS is not installable here",
+                         "shapely_importable": shapely_importable()},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -899,13 +935,17 @@ def run_reference(args, rank, world):
 
     O.build()
     P = O.Polygons(w.polys.x, w.polys.y, w.polys.ring_off, w.polys.part_off, w.polys.geom_off)
-    n = min(w.n_points, args.ref_sample)
+    # a strided sample (every stride-th point), so that it follows the whole
+    # workload's distribution (every Zipf site, every cluster) rather than a prefix
+    stride = max(1, -(-w.n_points // max(1, args.ref_sample)))
+    sx, sy = np.ascontiguousarray(w.px[::stride]), np.ascontiguousarray(w.py[::stride])
+    n = len(sx)
     for _ in range(args.warmup):
-        O.join(w.px[:n], w.py[:n], None, P, args.predicate, threads)
+        O.join(sx, sy, None, P, args.predicate, threads)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.join(w.px[:n], w.py[:n], None, P, args.predicate, threads)
+        O.join(sx, sy, None, P, args.predicate, threads)
         times.append(time.perf_counter() - t0)
     tot = sum(times)
     value = n * len(times) / tot
@@ -913,11 +953,11 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": "query points/sec", "value": value, "unit": "points/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "predicate": args.predicate,
-                   "sample_points": n, "n_polygons": len(w.polys)},
+        "config": join_config(args, w),
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
-                         "sample": f"first {n} of {w.n_points} points vs all {len(w.polys)} polygons, "
-                                   "exact CPU oracle (C + OpenMP): Shapely/GEOS is not installable here"},
+                         "sample": f"every {stride}th point ({n} of {w.n_points}) vs all {len(w.polys)} polygons, "
+                                   "exact CPU oracle (C + OpenMP): Shapely/GEOS is not installable here",
+                         "shapely_importable": shapely_importable()},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -1042,6 +1082,14 @@ def run_ours(args, rank, world, local_rank):
             assert n_e == n_pairs, (n_e, n_pairs)
             if k:  # the first call warms the host pipeline
                 e2e_ms.append(a.elapsed_time(b))
+    # the pairs of the benchmarked call and of the e2e call, kept for the check
+    # against the CPU oracle below (outside every timed region)
+    n_chk, _ = join(left, right)
+    gl_chk, gr_chk = left[:n_chk].clone(), right[:n_chk].clone()
+    if n_chk:
+        _abi.sort_pairs(ctx, gl_chk, gr_chk)
+    gl_chk, gr_chk = gl_chk.cpu().numpy(), gr_chk.cpu().numpy()
+    hl_chk, hr_chk = hl[:n_e].numpy().copy(), hr[:n_e].numpy().copy()
     total_ms = float(sum(step_ms))
     if dist:
         t = torch.tensor([total_ms, float(np.median(e2e_ms))], device=dev, dtype=torch.float64)
@@ -1064,26 +1112,35 @@ def run_ours(args, rank, world, local_rank):
         except Exception:
             traffic = None
     cpu = None
+    parity = None
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
-        rate, n_s, dt = cpu_sample_rate(w, args.predicate, threads, args.cpu_seconds)
+        rate, n_s, dt, cpu_pairs = cpu_sample_rate(w, args.predicate, threads, args.cpu_seconds)
         cpu = {"value": rate, "unit": "points/s", "cores": threads, "kind": "port",
                "sample": f"first {n_s} of {N} points vs all {len(w.polys)} polygons ({dt:.1f} s), exact CPU "
-                         "oracle (C + OpenMP); Shapely/GEOS is not installable here"}
+                         "oracle (C + OpenMP); Shapely/GEOS is not installable here",
+               "shapely_importable": shapely_importable()}
+        if cpu_pairs is not None:
+            parity = {"checker": "exact CPU oracle, all points", "oracle_pairs": int(len(cpu_pairs[0])),
+                      "mismatches": pair_mismatches(gl_chk, gr_chk, *cpu_pairs),
+                      "e2e_mismatches": pair_mismatches(hl_chk, hr_chk, *cpu_pairs)}
+    e32, e64 = st.get("fp32_edges", 0), st.get("fp64_edges", 0)
     line = {
         "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "predicate": args.predicate, "method": args.method,
-                   "n_points_per_gpu": N, "n_polygons": len(w.polys), "n_pairs": n_pairs,
-                   "parallelism": f"points sharded over {world} GPU(s), index replicated",
-                   "l2": "inputs (800 MB of points) larger than L2; no flush",
-                   "index_build_ms": info["build_ms"], "index_build_wall_s": build_wall,
-                   "index_device_bytes": info["device_bytes"]},
+        "config": join_config(args, w),
+        "method": args.method, "n_pairs": n_pairs,
+        "parallelism": f"points sharded over {world} GPU(s), index replicated",
+        "index": {"build_ms": info["build_ms"], "build_wall_s": build_wall, "device_bytes": info["device_bytes"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel_ms": kmed,
                      "algorithmic_bytes_per_launch": B},
         "cpu_baseline": cpu,
+        "parity": parity,
+        "split_precision": {"fp32_edges": e32, "fp64_edges": e64,
+                            "fp32_pass_rate": (e32 / (e32 + e64)) if e32 + e64 else None,
+                            "exact_fallbacks": st.get("exact_fallbacks", 0)},
         "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
                 "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int(8 * n_pairs)},
         "gpu_launches": launches,
@@ -1263,13 +1320,11 @@ def run_batched(args, rank, world, local_rank):
         "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate,
-                   "method": ("learned" if learned else "rtree") + ", batched",
-                   "n_jobs": len(jobs), "n_points_per_gpu": N, "n_polygons": n_polys, "n_pairs": n_pairs,
-                   "parallelism": f"jobs replicated per GPU ({world} GPU(s)), independent",
-                   "l2": "inputs (1.1 GB of points) larger than L2; no flush",
-                   "launch_shape": opts, "launch_shape_source": opts_src, "autotune_s": tune_s,
-                   "index_build_ms": build_ms, "index_build_wall_s": build_wall},
+        "config": batched_config(args, jobs),
+        "method": ("learned" if learned else "rtree") + ", batched", "n_pairs": n_pairs,
+        "parallelism": f"jobs replicated per GPU ({world} GPU(s)), independent",
+        "launch_shape": opts, "launch_shape_source": opts_src, "autotune_s": tune_s,
+        "index": {"build_ms": build_ms, "build_wall_s": build_wall},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel_ms": kmed,
                      "algorithmic_bytes_per_launch": B},

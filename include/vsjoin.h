@@ -370,17 +370,19 @@ int vs_wkb_plan_free(vs_wkb_plan* plan);
 
 /* Brute-force point x polygon join that allocates no device memory, for
  * callers that cannot allocate (a host that owns all device memory in a
- * fixed arena, a hard memory budget, a loop that cannot afford an
- * allocation's synchronisation).  No counterpart in the reference: it has no
- * allocation-free join.  Inputs and the pair buffers are the caller's; the
- * kernels' only scratch (one box per polygon and a pair counter) is a fixed
- * 2 MiB device array inside the library, held by every GPU that loads it.
- * At most 65,536 polygon rows (larger inputs: VS_E_ARG).  Runs on `stream`
- * (a cudaStream_t, NULL = legacy default) of the current device; the first
- * call on a device resolves the array's address (cudaGetSymbolAddress), so
- * make it before any stream capture.  Calls that overlap on the GPU share the
- * array and race: serialise them.  Pairs come back unordered; VS_E_CAPACITY
- * reports the required size in *n_pairs. */
+ * fixed arena, a process on a hard memory budget).  No counterpart in the
+ * reference: it has no allocation-free join.  Inputs and the pair buffers are
+ * the caller's; the kernels' only scratch (one box per polygon and a pair
+ * counter) is a fixed 2 MiB device array inside the library, held by every
+ * GPU that loads it.  At most 65,536 polygon rows (larger inputs: VS_E_ARG).
+ * Runs on `stream` (a cudaStream_t, NULL = legacy default) of the current
+ * device and blocks the calling thread until the pair count is back on the
+ * host.  The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress) and keeps it for the life of the process: make that
+ * first call before any stream capture, with the device's primary context
+ * current, and make no call after cudaDeviceReset.  Calls that overlap on the
+ * GPU share the array and race: serialise them.  Pairs come back unordered;
+ * VS_E_CAPACITY reports the required size in *n_pairs. */
 int vs_join_brute_noalloc(const vs_points* pts, const vs_polygons* polys, int32_t predicate,
                           int32_t* d_left, int32_t* d_right, int64_t capacity, int64_t* n_pairs,
                           void* stream);

@@ -1,8 +1,9 @@
 """Generate the golden fixtures under ``tests/golden/`` from the reference's test data.
 
-Run once in a container that has the reference checkout mounted (read-only):
+Run once where a checkout of the reference project is available (read-only),
+passing its root directory:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the vibeSpatial checkout>
 
 It reads the shapefiles the reference's vendored GeoPandas test-suite uses
 (``tests/upstream/geopandas/tests/data/nybb_16a.zip`` and the
@@ -200,4 +201,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the vibeSpatial checkout>")
+    main(sys.argv[1])

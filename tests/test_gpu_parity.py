@@ -308,14 +308,6 @@ def test_full_size_utm_join(vsabi, ctx, oracle, method):
     _check(vsabi, ctx, oracle, w, "within", METHODS[method])
 
 
-def test_full_size_zipf_join(vsabi, ctx, oracle):
-    """The skewed learned-index workload at full size (50M x 1M): learned pairs == oracle pairs."""
-    from vibespatial_b200.testing import synthetic as syn
-
-    w = syn.zipf_join(seed=3)
-    _check(vsabi, ctx, oracle, w, "within", METHODS["learned"])
-
-
 @pytest.mark.parametrize("chunk", [None, 3_000_000])
 @pytest.mark.parametrize("method", ["rtree", "learned"])
 def test_join_host_pipeline(vsabi, ctx, oracle, method, chunk, monkeypatch):

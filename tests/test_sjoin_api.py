@@ -190,6 +190,22 @@ def test_suffixes(backend, how, lsuffix, rsuffix, expected_cols):
     assert set(joined.columns) == expected_cols | {"geometry"}
 
 
+def test_suffix_creating_duplicate_columns_warns(backend):
+    """A suffix that renames an overlapping column onto another column of the same frame warns
+    (GeoPandas' deprecation, src/vibespatial/api/_native_results.py:355-375); plain overlaps do not."""
+    import warnings
+
+    left = vs.GeoDataFrame({"col": [1], "col_left": [2], "geometry": [vs.Point(0, 0)]})
+    right = vs.GeoDataFrame({"col": [3], "geometry": [vs.box(-1, -1, 1, 1)]})
+    with pytest.warns(FutureWarning, match="Passing 'suffixes' which cause duplicate columns {'col_left'}"):
+        joined = vs.sjoin(left, right)
+    assert list(joined.columns).count("col_left") == 2
+    left = vs.GeoDataFrame({"col": [1], "other": [2], "geometry": [vs.Point(0, 0)]})
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", FutureWarning)
+        vs.sjoin(left, right)
+
+
 def test_argument_errors_and_crs_warning(backend):
     """test_sjoin.py:165-181, 325-344: a CRS mismatch warns, unknown keywords
     and non-frame inputs raise."""

@@ -43,6 +43,43 @@ def test_noalloc_matches_vs_join_twice(vsabi, ctx, predicate):
         np.testing.assert_array_equal(gr, er)
 
 
+@pytest.mark.parametrize("predicate", ["within", "intersects", "touches", None])
+def test_noalloc_null_empty_and_nan_rows(vsabi, ctx, predicate):
+    """Null and empty polygons, a polygon with one NaN vertex, null points and NaN points: the same pairs as
+    vs_join (brute), whose index builder also spans a box over the finite coordinates only."""
+    import torch
+    from types import SimpleNamespace
+
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = syn.star_join(seed=23, n_points=30_000, n_polys=400)
+    p = w.polys
+    x, y = p.x.copy(), p.y.copy()
+    x[p.ring_off[p.part_off[p.geom_off[5]]] + 2] = np.nan  # one NaN vertex in polygon 5
+    m = len(p.geom_off) - 1
+    # three empty polygon rows (no parts) appended, and every ninth row null
+    geom_off = np.concatenate([p.geom_off, np.full(3, p.geom_off[-1], np.int32)])
+    gvalid = (np.arange(m + 3) % 9 != 4).astype(np.uint8)
+    polys = SimpleNamespace(x=x, y=y, ring_off=p.ring_off, part_off=p.part_off, geom_off=geom_off, valid=gvalid)
+    px, py = w.px.copy(), w.py.copy()
+    px[::13] = np.nan
+    py[::17] = np.nan
+    pvalid = (np.arange(len(px)) % 7 != 3).astype(np.uint8)
+    el, er, _ = gpu_join(vsabi, ctx, px, py, polys, predicate, method=2, pvalid=pvalid)
+    pts, keep_pts = upload_points(vsabi, px, py, pvalid)
+    dpolys, keep_polys = upload_polys(vsabi, polys)
+    cap = len(el) + 16
+    for _ in range(2):
+        left = torch.full((cap,), -1, dtype=torch.int32, device="cuda")
+        right = torch.full((cap,), -1, dtype=torch.int32, device="cuda")
+        n = vsabi.join_brute_noalloc(pts, dpolys, PRED_CODES[predicate], left, right)
+        gl, gr = _sorted_pairs(left[:n].cpu().numpy(), right[:n].cpu().numpy())
+        assert n == len(el)
+        np.testing.assert_array_equal(gl, el)
+        np.testing.assert_array_equal(gr, er)
+    assert not np.isin(er, np.flatnonzero(gvalid == 0)).any()
+
+
 def test_noalloc_rejects_inputs_over_the_limit(vsabi):
     from vibespatial_b200 import _abi
 

@@ -60,7 +60,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     objs = []
     for src in sources():
         obj = objdir / (src.stem + ".o")
-        cmd = [*base, "-dc" if False else "-c", str(src), "-o", str(obj), "-I", str(INCLUDE)]
+        cmd = [*base, "-c", str(src), "-o", str(obj), "-I", str(INCLUDE)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         r = subprocess.run(cmd, env=env, capture_output=True, text=True)

@@ -2,13 +2,13 @@
 // allocation at all, for callers that cannot allocate.
 //
 // Some hosts own every byte of device memory themselves: an engine that
-// carves one fixed arena at start-up and forbids later cudaMalloc, a process
-// held to a hard memory budget, or a latency-critical loop where an
-// allocation's implicit synchronisation is not acceptable.  This entry point
-// serves them: the caller passes inputs and the output pair buffers, and the
-// only scratch the kernels need (one box per polygon and a pair counter)
-// lives in a file-scope device array of fixed size, reserved when the library
-// is loaded and held by every GPU that loads it until the process exits.
+// carves one fixed arena at start-up and forbids later cudaMalloc, or a
+// process held to a hard memory budget that a hidden allocation would break.
+// This entry point serves them: the caller passes inputs and the output pair
+// buffers, and the only scratch the kernels need (one box per polygon and a
+// pair counter) lives in a file-scope device array of fixed size, reserved
+// when the library is loaded and held by every GPU that loads it until the
+// process exits.
 //
 // Limits and rules:
 //   * at most kNoAllocMaxPolygons (65,536) polygon rows; larger inputs are
@@ -17,9 +17,17 @@
 //     overlap on the GPU (different streams, threads or processes sharing a
 //     context) race on it and must be serialised by the caller; each call
 //     clears the counter it needs before use;
+//   * every call blocks the calling thread: it ends by copying the pair count
+//     back to the host and waiting for `stream`;
 //   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current); make that first call
-//     before any stream capture;
+//     cudaGetSymbolAddress (with that device current) and keeps it for the
+//     life of the process; make that first call before any stream capture.
+//     The address belongs to the device's primary context: call this entry
+//     point with the primary context current (the CUDA runtime's default),
+//     and not after cudaDeviceReset, which invalidates the kept address;
+//   * a polygon's box spans its finite coordinates (fmin/fmax skip NaN), as
+//     the index builder computes it; null and empty rows get a box that
+//     contains nothing;
 //   * pairs come back unordered (left = point row, right = polygon row).
 #include <cuda_runtime.h>
 #include <stdint.h>

@@ -137,6 +137,16 @@ def _suffix_overlaps(left_cols, right_cols, lsuffix, rsuffix, lgeom, rgeom):
         raise ValueError(f"columns overlap but no suffix specified: {sorted(map(str, overlap))}")
     left = [f"{c}_{lsuffix}" if c in overlap and c != lgeom and lsuffix is not None else c for c in left_cols]
     right = [f"{c}_{rsuffix}" if c in overlap and c != rgeom and rsuffix is not None else c for c in right_cols]
+    # a suffixed name that collides with another column of the same side
+    # (one that was not already repeated before renaming) is deprecated in
+    # GeoPandas (src/vibespatial/api/_native_results.py:355-375)
+    made = set()
+    for before, after in ((left_cols, left), (right_cols, right)):
+        b, a = pd.Index(before), pd.Index(after)
+        made.update(a[a.duplicated() & ~b.duplicated()].tolist())
+    if made:
+        warnings.warn(f"Passing 'suffixes' which cause duplicate columns {made} in the result is deprecated and "
+                      "will raise a MergeError in a future version.", FutureWarning, stacklevel=4)
     return left, right
 
 
