@@ -152,6 +152,31 @@ def algorithmic_bytes(w, n_pairs: int) -> int:
                + 8 * n_pairs)
 
 
+def plan_median_ms(plan, pred, left, right, n_expect, use_graph=True, reps=5, warm=2):
+    """Median device time (CUDA events inside vs_batch_run) of a batch plan's join."""
+    ms = []
+    for k in range(warm + reps):
+        n_k, st_k = plan.run_into(pred, left, right, use_graph=use_graph)
+        assert n_k == n_expect, (n_k, n_expect)
+        if k >= warm:
+            ms.append(st_k["kernel_ms"])
+    return float(np.median(ms))
+
+
+def learned_ablations(_abi, ctx, indexes, pts, job_start, pred, left, right, n_pairs, base_opts, reps):
+    """What each choice of the learned pipeline buys: the same batch plan with the RMI replaced by a binary
+    search over every cell key, with FP64 ring walks instead of the FP32 stage, and launched directly instead
+    of replayed from a CUDA graph (median device ms of each; same pairs)."""
+    out = {}
+    for name, extra, graph in (("graph_ms", {}, True), ("direct_launch_ms", {}, False),
+                               ("rmi_replaced_by_bsearch_ms", {"learned_flags": _abi.JOIN_LEARNED_BSEARCH}, True),
+                               ("fp64_walk_ms", {"learned_flags": _abi.JOIN_LEARNED_FP64_WALK}, True)):
+        plan = _abi.BatchPlan(ctx, indexes, pts, job_start, options=dict(base_opts, **extra))
+        out[name] = plan_median_ms(plan, pred, left, right, n_pairs, use_graph=graph, reps=reps)
+        plan.close()
+    return out
+
+
 def join_config(args, w) -> dict:
     """The workload's configuration, identical in both arms (arm-specific figures live outside it)."""
     return {"workload": WORKLOAD_DESC[args.workload], "predicate": args.predicate, "n_points_per_gpu": w.n_points,
@@ -1059,6 +1084,7 @@ def run_ours(args, rank, world, local_rank):
                 _, stb = index.join_into(pts, pred, _abi.METHOD_RTREE, left, right, flags=_abi.JOIN_BULK_LEAVES)
                 pb.append(stb["kernel_ms"])
             plain_bulk = float(np.median(pb))
+        ablations = None
         if batched:
             # per-phase device times of the same learned pipeline, launched
             # directly (a graph replay records no phase marks)
@@ -1066,6 +1092,10 @@ def run_ours(args, rank, world, local_rank):
             for _ in range(max(3, args.steps // 2)):
                 dph.append(index.join_into(pts, pred, _abi.METHOD_LEARNED, left, right)[1]["phase_ms"])
             phases = dph
+            ablations = learned_ablations(_abi, ctx, [index], pts, [0, N], pred, left, right, n_pairs,
+                                          {"method": _abi.METHOD_LEARNED}, max(3, args.steps // 2))
+            if plain is not None:
+                ablations["plain_rtree_ms"] = plain
         # e2e through the C-ABI with HOST buffers (vs_join_host): pinned host
         # points in, pinned host pairs out, the chunked copies overlapping the join
         hx = torch.from_numpy(w.px).pin_memory()
@@ -1148,6 +1178,8 @@ def run_ours(args, rank, world, local_rank):
         "join_stats": st,
         "index_info": info,
     }
+    if ablations is not None:
+        line["ablations"] = ablations
     if plain is not None:
         line["plain_rtree_ms"] = plain
         line["plain_rtree_bulk_leaves_ms"] = plain_bulk
@@ -1241,6 +1273,7 @@ def run_batched(args, rank, world, local_rank):
         step_ms = [a.elapsed_time(b) for a, b in ev]
         # the R-tree batch on the same jobs, for the learned-vs-plain ratio
         rtree_batch_ms = None
+        ablations = None
         if learned:
             rplan = _abi.BatchPlan(ctx, indexes, pts, job_start,
                                    options=dict(autotune.lookup(key) or autotune.DEFAULTS, method=_abi.METHOD_RTREE))
@@ -1252,6 +1285,9 @@ def run_batched(args, rank, world, local_rank):
                     rms.append(st_r["kernel_ms"])
             rplan.close()
             rtree_batch_ms = float(np.median(rms))
+            ablations = learned_ablations(_abi, ctx, indexes, pts, job_start, pred, left, right, n_pairs,
+                                          dict(opts, method=bmethod), max(3, args.steps // 2))
+            ablations["plain_rtree_batched_ms"] = rtree_batch_ms
         # the same jobs one vs_join call at a time (how a caller without the
         # batch API runs them), after the timed region
         loop_ms = []
@@ -1336,6 +1372,8 @@ def run_batched(args, rank, world, local_rank):
         "per_job_loop_ms": loop_med,
         "batched_vs_loop": loop_med / kmed,
     }
+    if ablations is not None:
+        line["ablations"] = ablations
     if rtree_batch_ms is not None:
         line["plain_rtree_batched_ms"] = rtree_batch_ms
         line["learned_vs_plain"] = rtree_batch_ms / kmed

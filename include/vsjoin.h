@@ -67,6 +67,9 @@ enum vs_method {
 #define VS_JOIN_SORT 1u        /* return pairs sorted by (left, right) */
 #define VS_JOIN_BULK_LEAVES 2u /* R-tree method: load leaf blocks with bulk copies (TMA, cp.async.bulk) into
                                   shared memory instead of lane loads (same pairs; measured ~2% slower) */
+/* Ablations of the learned method (same pairs; for measuring what each choice buys): */
+#define VS_JOIN_LEARNED_BSEARCH 4u   /* cell lookup by binary search over every cell key instead of the RMI */
+#define VS_JOIN_LEARNED_FP64_WALK 8u /* ring walks in FP64 (the plain method's filter) instead of FP32 first */
 
 typedef struct vs_context vs_context;
 typedef struct vs_index vs_index;
@@ -305,6 +308,10 @@ typedef struct vs_batch_options {
     int32_t sort_levels;      /* R-tree: Hilbert levels the points of a job are sorted by (0 = 8) */
     int32_t method;           /* VS_METHOD_RTREE (0) or VS_METHOD_LEARNED: every index with polygons
                                  must then have its learned part (VS_E_ARG otherwise) */
+    int32_t learned_map_blocks_per_sm;    /* learned: map pass blocks per SM (0 = 8) */
+    int32_t learned_refine_blocks_per_sm; /* learned: refine pass blocks per SM (0 = as many as fit) */
+    int32_t learned_grab;     /* learned: grouped points a refine warp takes per grab (0 = 32; rounded up to 32s) */
+    uint32_t learned_flags;   /* learned: VS_JOIN_LEARNED_BSEARCH | VS_JOIN_LEARNED_FP64_WALK (ablations) */
 } vs_batch_options;
 
 /* At most 4096 jobs and 2^31-1 points in total. */

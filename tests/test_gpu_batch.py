@@ -207,6 +207,33 @@ def test_learned_batch_matches_oracle(lbatch, oracle, predicate, use_graph):
         np.testing.assert_array_equal(r, er)
 
 
+@pytest.mark.parametrize("options", [
+    {"learned_map_blocks_per_sm": 1, "learned_refine_blocks_per_sm": 1, "learned_grab": 32},
+    {"learned_map_blocks_per_sm": 3, "learned_refine_blocks_per_sm": 2, "learned_grab": 100},
+    {"learned_grab": 4096, "learned_flags": 4},
+    {"learned_refine_blocks_per_sm": 8, "learned_flags": 8},
+])
+def test_learned_batch_launch_shapes_do_not_change_pairs(vsabi, ctx, oracle, options):
+    """Learned batch plans give the oracle's pairs whatever their launch shape (the autotuner's search space)
+    and with either ablation switch, graph-replayed and launched directly."""
+    jobs = _jobs(seed=12, n_jobs=5)
+    b = _Batch(vsabi, ctx, jobs, options=options, learned=True)
+    for use_graph in (True, False):
+        left, right, _ = _run(b, "intersects", use_graph=use_graph)
+        for j, (l, r) in enumerate(b.split(left, right)):
+            w = jobs[j]
+            el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), "intersects")
+            np.testing.assert_array_equal(l, el)
+            np.testing.assert_array_equal(r, er)
+
+
+def test_learned_batch_rejects_bad_shapes(vsabi, ctx, lbatch):
+    for bad in ({"learned_grab": -1}, {"learned_map_blocks_per_sm": 9}, {"learned_flags": 1}):
+        with pytest.raises(ValueError):
+            vsabi.BatchPlan(ctx, lbatch.indexes, lbatch.pts, lbatch.job_start,
+                            options=dict(bad, method=vsabi.METHOD_LEARNED))
+
+
 def test_learned_batch_single_job_equals_vs_join(vsabi, ctx):
     from vibespatial_b200.testing import synthetic as syn
 

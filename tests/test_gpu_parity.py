@@ -357,3 +357,27 @@ def test_join_host_grows_chunk_pair_buffer(vsabi, ctx, oracle):
         n, _ = index.join_host(w.px, w.py, PRED_CODES[predicate], vsabi.METHOD_RTREE, hl, hr, sort=True)
         assert n == len(el) > w.n_points  # more pairs than the first chunk buffer holds
         assert_same_pairs(hl, hr, el, er)
+
+
+@pytest.mark.parametrize("flags", ["bsearch", "fp64_walk", "both"])
+@pytest.mark.parametrize("workload", ["zipf", "degenerate"])
+def test_learned_ablation_switches(vsabi, ctx, oracle, workload, flags):
+    """The learned method with its RMI replaced by a binary search over every cell key, or with FP64 ring walks
+    instead of the FP32 stage (the ablations the benchmark times), still gives the oracle's pairs."""
+    from vibespatial_b200.testing import synthetic as syn
+
+    w = (syn.zipf_join(seed=14, n_points=1_000_000, n_polys=50_000) if workload == "zipf"
+         else syn.degenerate_join(seed=15, n_points=300_000, n_polys=3_000))
+    f = {"bsearch": vsabi.JOIN_LEARNED_BSEARCH, "fp64_walk": vsabi.JOIN_LEARNED_FP64_WALK,
+         "both": vsabi.JOIN_LEARNED_BSEARCH | vsabi.JOIN_LEARNED_FP64_WALK}[flags]
+    pts, _k1 = upload_points(vsabi, w.px, w.py)
+    P, _k2 = upload_polys(vsabi, w.polys)
+    index = vsabi.DeviceIndex(ctx, P, learned=True)
+    for predicate in ("within", "intersects"):
+        el, er = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), predicate)
+        gl, gr, st = index.join(pts, PRED_CODES[predicate], vsabi.METHOD_LEARNED, flags=f)
+        assert_same_pairs(gl.cpu().numpy(), gr.cpu().numpy(), el, er)
+        if f & vsabi.JOIN_LEARNED_FP64_WALK:
+            assert st["fp32_edges"] == 0
+        if f & vsabi.JOIN_LEARNED_BSEARCH:
+            assert st["rmi_fallbacks"] == 0

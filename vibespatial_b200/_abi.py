@@ -20,6 +20,8 @@ PRED_BBOX, PRED_INTERSECTS, PRED_WITHIN, PRED_COVERED_BY, PRED_TOUCHES = range(5
 METHOD_RTREE, METHOD_LEARNED, METHOD_BRUTE = range(3)
 JOIN_SORT = 1
 JOIN_BULK_LEAVES = 2
+JOIN_LEARNED_BSEARCH = 4
+JOIN_LEARNED_FP64_WALK = 8
 
 # Every function the header declares; tests check the library exports them.
 EXPORTED = (
@@ -87,7 +89,9 @@ class JoinStats(ctypes.Structure):
 
 class BatchOptions(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_int32), ("packets_per_grab", ctypes.c_int32),
-                ("sort_levels", ctypes.c_int32), ("method", ctypes.c_int32)]
+                ("sort_levels", ctypes.c_int32), ("method", ctypes.c_int32),
+                ("learned_map_blocks_per_sm", ctypes.c_int32), ("learned_refine_blocks_per_sm", ctypes.c_int32),
+                ("learned_grab", ctypes.c_int32), ("learned_flags", ctypes.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

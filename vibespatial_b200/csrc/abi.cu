@@ -283,6 +283,9 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
     // Pairs the filters cannot certify go to the context's deferred buffer
     // and are resolved exactly after the join kernel; if more were deferred
     // than the buffer holds, the join runs once more with a buffer that fits.
+    LearnedShape shape{};
+    shape.flags = ((flags & VS_JOIN_LEARNED_BSEARCH) ? kLearnedBsearch : 0u) |
+                  ((flags & VS_JOIN_LEARNED_FP64_WALK) ? kLearnedFp64Walk : 0u);
     unsigned long long want = (unsigned long long)(pts->n / 64 + 65536);
     for (int attempt = 0; attempt < 2; ++attempt) {
         VS_TRY(ensure_defer_capacity(ctx, want));
@@ -293,7 +296,7 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
         phase_mark(ctx, 0);
         int st;
         if (method == VS_METHOD_LEARNED)
-            st = launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity, ds);
+            st = launch_learned_join(ctx, idx, pts, mask, d_left, d_right, capacity, ds, 0, shape);
         else
             st = launch_rtree_join(ctx, idx, pts, mask, method == VS_METHOD_BRUTE, (flags & VS_JOIN_BULK_LEAVES) != 0,
                                    d_left, d_right, capacity, ds);

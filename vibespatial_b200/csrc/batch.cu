@@ -401,6 +401,11 @@ int enqueue_batch(vs_batch_plan* p, cudaStream_t s, int mask, int32_t* left, int
         q.n_cells = p->n_cells;
         q.accept_mask = mask;
         q.has_ring_bins = p->has_ring_bins;
+        q.shape.map_blocks_per_sm = p->opts.learned_map_blocks_per_sm;
+        q.shape.refine_blocks_per_sm = p->opts.learned_refine_blocks_per_sm;
+        q.shape.grab = p->opts.learned_grab;
+        q.shape.flags = ((p->opts.learned_flags & VS_JOIN_LEARNED_BSEARCH) ? kLearnedBsearch : 0u) |
+                        ((p->opts.learned_flags & VS_JOIN_LEARNED_FP64_WALK) ? kLearnedFp64Walk : 0u);
         VS_TRY(enqueue_learned(s, nullptr, q, p->n_jobs == 1 ? &p->h_single : nullptr, p->lsc, a.sink, a.defer,
                                a.counters, &p->d_work[0]));
         if (mask) {
@@ -510,6 +515,14 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
     if (p->opts.blocks_per_sm > 8) p->opts.blocks_per_sm = 8;
     if (p->opts.packets_per_grab <= 0) p->opts.packets_per_grab = 4;
     if (p->opts.sort_levels <= 0) p->opts.sort_levels = 8;
+    if (p->opts.learned_map_blocks_per_sm < 0 || p->opts.learned_map_blocks_per_sm > 8 ||
+        p->opts.learned_refine_blocks_per_sm < 0 || p->opts.learned_refine_blocks_per_sm > 8 ||
+        p->opts.learned_grab < 0 || p->opts.learned_grab > 4096 ||
+        (p->opts.learned_flags & ~(VS_JOIN_LEARNED_BSEARCH | VS_JOIN_LEARNED_FP64_WALK)) != 0) {
+        set_error("learned launch shape out of range (blocks per SM 0..8, grab 0..4096, flags 4|8)");
+        delete p;
+        return VS_E_ARG;
+    }
     // key = job id in the top bits, Hilbert cell below; 2^job_bits > n_jobs,
     // so the all-ones sentinel never collides with a valid key
     const int job_bits = bits_needed(n_jobs);

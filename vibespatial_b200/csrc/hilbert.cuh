@@ -74,6 +74,28 @@ __device__ __forceinline__ uint32_t hilbert_key_lut(uint32_t x, uint32_t y, int 
     return d >> (2 * (4 * chunks - levels));
 }
 
+// Inverse of hilbert_key at `levels` levels: the cell (cx, cy) of the
+// level-`levels` grid (so hilbert_key(cx << (32 - levels), cy << (32 - levels),
+// levels) == key).  The walk reads the key's base-4 digits MSB first under the
+// same swap / complement state as the table above: digit d = (3 rx) ^ ry gives
+// rx = d >> 1 and ry = (d ^ rx) & 1 in the transformed frame.
+__host__ __device__ __forceinline__ void hilbert_cell(uint32_t key, int levels, uint32_t& cx, uint32_t& cy) {
+    uint32_t sw = 0, inv = 0, x = 0, y = 0;
+    for (int lv = levels - 1; lv >= 0; --lv) {
+        const uint32_t d = (key >> (2 * lv)) & 3u;
+        const uint32_t rx = d >> 1, ry = (d ^ rx) & 1u;
+        const uint32_t a = rx ^ inv, b = ry ^ inv;
+        x = (x << 1) | (sw ? b : a);
+        y = (y << 1) | (sw ? a : b);
+        if (ry == 0) {
+            if (rx == 1) inv ^= 1u;
+            sw ^= 1u;
+        }
+    }
+    cx = x;
+    cy = y;
+}
+
 // Quantise a coordinate to the 2^32 grid spanning [lo, lo + span] with scale
 // = (2^32 - 1) / span; values outside clamp to the border cells.
 __host__ __device__ __forceinline__ uint32_t quantize(double v, double lo, double scale) {

@@ -19,18 +19,32 @@ constexpr int kMaxLevels = 16;   // 16^15 > 2^31 items
 // error window bounds the search, so every lookup is exact.
 constexpr int kRmiHidden = 32;
 
-// Everything the learned join needs about one polygon slot, in three 16-byte
-// words: the FP64 origin, the FP32 box relative to it (rounded outward), the
-// bound on the FP32 vertex rounding error, the slot (its original row is
-// item_geom[slot]), and for a single-ring polygon its coordinate range
-// (c0 = -1 for multi-ring shapes).  The learned index stores one record per
-// (cell, polygon) entry, in cell order, so a candidate is one 48-byte read.
-struct __align__(16) SlotRecord {
-    double ox, oy;
+// Everything the learned join needs about one (cell, polygon) entry of the
+// learned index, in two 16-byte words.  Coordinates are FP32 offsets from
+// the cell's anchor (its centre, cell_anchor below):
+//   box       the polygon's box relative to the anchor, rounded outward
+//   off       fl32(anchor - slot origin): a query point q relative to the
+//             anchor is q + off relative to the slot origin, the frame of
+//             the slot's FP32 vertices (xy32)
+//   err       bound on |FP32 vertex - (vertex - origin)| of the slot plus
+//             |off - (anchor - origin)|
+//   slot      the polygon's slot (its original row is item_geom[slot])
+// The learned index stores one record per entry, in cell order, so a
+// candidate is one 32-byte read.
+struct __align__(16) EntryRecord {
     float4 box;
+    float offx, offy;
     float err;
     int32_t slot;
-    int32_t c0, c1;
+};
+
+// A query point matched to a cell: FP32 offsets from the cell's anchor, its
+// row, and its batch-wide cell number.  The map pass stages these, the place
+// pass permutes them into cell order, and the refine pass reads them.
+struct __align__(16) CellPoint {
+    float qx, qy;
+    int32_t row;
+    uint32_t gcell;
 };
 
 // Leaf of the RMI: position = floor(a + b * key), error window [lo, hi].
@@ -59,6 +73,7 @@ struct LearnedJob {
     // frame and quantisation scales, computed on the device exactly as the
     // build computed them
     double lox, loy, hix, hiy, sx, sy;
+    double cwx, cwy;     // level-L cell width per axis (cell_anchor)
     int32_t L;
     int32_t occ_shift;   // cell key >> occ_shift = occupancy bit
     int32_t root_shift;  // cell key >> root_shift = root-table index
@@ -69,7 +84,8 @@ struct LearnedJob {
     const RmiLeaf* leaves;
     const uint32_t* cell_keys;
     const uint32_t* cell_start;
-    const SlotRecord* recs;  // [n_entries] per-entry slot records, cell order
+    const EntryRecord* recs;  // [n_entries] per-entry records, cell order
+    const int2* c01;          // [n_geoms] coordinate range of a single-ring slot, (-1, -1) otherwise
     const float2* xy32;
     const double2* xy;
     const int32_t* item_geom;
@@ -79,6 +95,24 @@ struct LearnedJob {
     const vs_box* boxes;     // FP64 slot boxes (R-tree level 0)
     RingIndex rings;         // y-bins of the index's long rings
 };
+
+// Launch shape of the learned pipeline (every field 0 = the default), and the
+// ablation switches that replace one of its choices by the plain method.
+struct LearnedShape {
+    int32_t map_blocks_per_sm;     // map pass blocks per SM (0 = 8)
+    int32_t refine_blocks_per_sm;  // refine pass blocks per SM (0 = as many as fit)
+    int32_t grab;                  // grouped points a refine warp takes per work grab (0 = 32; multiple of 32)
+    uint32_t flags;                // kLearnedBsearch | kLearnedFp64Walk
+};
+constexpr uint32_t kLearnedBsearch = 1u;   // cell lookup by binary search over all cell keys (no RMI)
+constexpr uint32_t kLearnedFp64Walk = 2u;  // ring walks in FP64 (no FP32 edge stage)
+
+// Centre of level-L grid cell c on one axis: lo + (c + 0.5) * cell width,
+// one fused multiply-add, so the index build (from a cell's key) and the
+// query (from a point's quantised coordinates) compute the same bits.
+__device__ __forceinline__ double cell_anchor(double lo, double cw, uint32_t c) {
+    return __fma_rn((double)c + 0.5, cw, lo);
+}
 
 struct LearnedIndex {
     int32_t level = 0;               // grid level L (cells of frame / 2^L per axis)
@@ -102,12 +136,12 @@ struct LearnedIndex {
     int2* leaf_err = nullptr;        // [n_leaves] inclusive error window (lo, hi)
     RmiLeaf* leaves = nullptr;       // [n_leaves] the two above packed for queries
     int32_t n_leaves = 0;
-    SlotRecord* recs = nullptr;      // [n_entries] record of each entry's slot, cell order
+    EntryRecord* recs = nullptr;     // [n_entries] record of each entry, cell order
+    int2* c01 = nullptr;             // [n_geoms] single-ring coordinate range per slot
     LearnedJob* desc = nullptr;      // device: this index as the query kernels see it
     LearnedJob h_desc{};             // host copy of *desc
     // FP32 tile-relative copies used by the split-precision filter
     double2* origin = nullptr;       // [n_geoms] slot origin (box centre, FP64)
-    float4* box32 = nullptr;         // [n_geoms] slot box relative to the origin, rounded outward
     float* err32 = nullptr;          // [n_geoms] bound on |vertex rounding error| of the slot
     float2* xy32 = nullptr;          // [n_coords] vertices relative to their slot origin (nearest)
     float rmi_train_ms = 0.f;

@@ -24,7 +24,7 @@ int launch_rtree_join(vs_context* ctx, const vs_index* idx, const vs_points* pts
                       int64_t row_base = 0);
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
                         int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink,
-                        int64_t row_base = 0);
+                        int64_t row_base = 0, const LearnedShape& shape = LearnedShape{});
 // Exact pass over the pairs the filtered kernels deferred (count read on device).
 int launch_resolve_deferred(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask,
                             int32_t* d_left, int32_t* d_right, int64_t capacity, const DeferSink& dsink,

@@ -142,7 +142,7 @@ __global__ void occ_kernel(const uint32_t* __restrict__ cell_keys, int64_t n, in
 __global__ void split_copy_kernel(const vs_box* __restrict__ box, int64_t M, const int32_t* __restrict__ geom_off,
                                   const int32_t* __restrict__ part_off, const int32_t* __restrict__ ring_off,
                                   const double2* __restrict__ xy, double2* __restrict__ origin,
-                                  float4* __restrict__ box32, float* __restrict__ err32, float2* __restrict__ xy32) {
+                                  float* __restrict__ err32, float2* __restrict__ xy32) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -168,51 +168,64 @@ __global__ void split_copy_kernel(const vs_box* __restrict__ box, int64_t M, con
         if (lane == 0) {
             origin[s] = make_double2(ox, oy);
             err32[s] = __double2float_ru(emax * (1.0 + 1e-6));
-            if (ok) {
-                const double a = b.minx - ox, c = b.miny - oy, d = b.maxx - ox, e = b.maxy - oy;
-                box32[s] = make_float4(__double2float_rd(a - fabs(a) * u64), __double2float_rd(c - fabs(c) * u64),
-                                       __double2float_ru(d + fabs(d) * u64), __double2float_ru(e + fabs(e) * u64));
-            } else {
-                box32[s] = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
-            }
         }
     }
 }
 
-__global__ void pack_slots_kernel(int64_t M, const double2* __restrict__ origin, const float4* __restrict__ box32,
-                                  const float* __restrict__ err32, const int32_t* __restrict__ item_geom,
-                                  const int32_t* __restrict__ geom_off, const int32_t* __restrict__ part_off,
-                                  const int32_t* __restrict__ ring_off, const int32_t* __restrict__ ring_bin,
-                                  SlotRecord* __restrict__ out) {
+// Coordinate range of every single-ring slot: such polygons take the short
+// ring walk (c0 >= 0) unless the split walk would use the ring's y-bins.
+__global__ void slot_c01_kernel(int64_t M, const int32_t* __restrict__ geom_off, const int32_t* __restrict__ part_off,
+                                const int32_t* __restrict__ ring_off, const int32_t* __restrict__ ring_bin,
+                                int2* __restrict__ out) {
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M; s += (int64_t)gridDim.x * blockDim.x) {
-        SlotRecord r;
-        r.ox = origin[s].x;
-        r.oy = origin[s].y;
-        r.box = box32[s];
-        r.err = err32[s];
-        r.slot = (int32_t)s;
+        int2 r = make_int2(-1, -1);
         const int32_t p0 = geom_off[s], p1 = geom_off[s + 1];
-        r.c0 = -1;
-        r.c1 = -1;
-        // single-ring polygons take the short path (c0 >= 0) unless the split
-        // walk would use the ring's y-bins
         if (p1 - p0 == 1 && part_off[p0 + 1] - part_off[p0] == 1) {
             const int ring = part_off[p0];
             const int c0 = ring_off[ring], c1 = ring_off[ring + 1];
-            if (ring_bin == nullptr || ring_bin[ring] < 0 || c1 - c0 < kSplitBinMinVertices) {
-                r.c0 = c0;
-                r.c1 = c1;
-            }
+            if (ring_bin == nullptr || ring_bin[ring] < 0 || c1 - c0 < kSplitBinMinVertices) r = make_int2(c0, c1);
         }
         out[s] = r;
     }
 }
 
-// One record per (cell, polygon) entry, in cell order.
-__global__ void entry_recs_kernel(int64_t E, const uint32_t* __restrict__ entries,
-                                  const SlotRecord* __restrict__ slots, SlotRecord* __restrict__ out) {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
-        out[e] = slots[entries[e]];
+// One record per (cell, polygon) entry, in cell order, relative to the cell's
+// anchor.  The cell comes from the entry's sorted key (Hilbert decode); a
+// decode that does not re-encode to the key sets *bad (the build then fails).
+__global__ void entry_recs_kernel(int64_t E, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ entries,
+                                  const LearnedJob* __restrict__ d, const vs_box* __restrict__ boxes,
+                                  const double2* __restrict__ origin, const float* __restrict__ err32,
+                                  EntryRecord* __restrict__ out, unsigned* __restrict__ bad) {
+    const double u64 = 1.1102230246251565e-16;  // 2^-53
+    const int L = d->L, sh = 32 - L;
+    const double lox = d->lox, loy = d->loy, cwx = d->cwx, cwy = d->cwy;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t key = keys[e];
+        uint32_t cx, cy;
+        hilbert_cell(key, L, cx, cy);
+        if ((uint32_t)hilbert_key(cx << sh, cy << sh, L) != key) atomicOr(bad, 1u);
+        const double ax = cell_anchor(lox, cwx, cx), ay = cell_anchor(loy, cwy, cy);
+        const int32_t slot = (int32_t)entries[e];
+        const vs_box b = boxes[slot];
+        const double2 o = origin[slot];
+        EntryRecord r;
+        if (b.minx <= b.maxx && b.miny <= b.maxy) {
+            // each FP64 difference is within u64 |v| of the real one; widen by that, then round outward
+            const double a = b.minx - ax, c = b.miny - ay, f = b.maxx - ax, g = b.maxy - ay;
+            r.box = make_float4(__double2float_rd(a - fabs(a) * u64), __double2float_rd(c - fabs(c) * u64),
+                                __double2float_ru(f + fabs(f) * u64), __double2float_ru(g + fabs(g) * u64));
+        } else {
+            r.box = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
+        }
+        const double dx = ax - o.x, dy = ay - o.y;
+        r.offx = __double2float_rn(dx);
+        r.offy = __double2float_rn(dy);
+        const double ex = fabs((double)r.offx - dx) + fabs(dx) * u64;
+        const double ey = fabs((double)r.offy - dy) + fabs(dy) * u64;
+        r.err = __double2float_ru(((double)err32[slot] + fmax(ex, ey)) * (1.0 + 1e-6));
+        r.slot = slot;
+        out[e] = r;
+    }
 }
 
 __global__ void pack_leaves_kernel(int nl, const double2* __restrict__ ab, const int2* __restrict__ err,
@@ -439,6 +452,10 @@ __global__ void learned_desc_kernel(const double* __restrict__ fr, LearnedJob* _
     d->hiy = fr[3];
     d->sx = sx;
     d->sy = sy;
+    // a level-L cell spans 2^(32-L) grid units of 1/scale each
+    const double units = ldexp(1.0, 32 - d->L);
+    d->cwx = units / sx;
+    d->cwy = units / sy;
 }
 
 template <class T>
@@ -573,8 +590,8 @@ void free_learned_index(vs_index* idx) {
     cudaFree(li.leaf_ab);
     cudaFree(li.leaf_err);
     cudaFree(li.origin);
-    cudaFree(li.box32);
     cudaFree(li.err32);
+    cudaFree(li.c01);
     cudaFree(li.xy32);
     cudaFree(li.leaves);
     cudaFree(li.recs);
@@ -673,23 +690,8 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     VS_TRY(st);
-    // 6. FP32 tile-relative copies
-    VS_TRY(dalloc(&li.origin, (size_t)M, bytes));
-    VS_TRY(dalloc(&li.box32, (size_t)M, bytes));
-    VS_TRY(dalloc(&li.err32, (size_t)M, bytes));
-    VS_TRY(dalloc(&li.xy32, (size_t)std::max<int64_t>(idx->n_coords, 1), bytes));
-    split_copy_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
-                                                            idx->xy, li.origin, li.box32, li.err32, li.xy32);
-    VS_CUDA_TRY(cudaGetLastError());
-    Scratch<SlotRecord> slots;
-    VS_TRY(slots.alloc((size_t)M, s));
-    VS_TRY(dalloc(&li.recs, (size_t)E, bytes));
-    pack_slots_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, li.origin, li.box32, li.err32, idx->item_geom, idx->geom_off,
-                                                       idx->part_off, idx->ring_off, idx->ring_bin, slots.p);
-    VS_CUDA_TRY(cudaGetLastError());
-    entry_recs_kernel<<<grid_for(E, 256), 256, 0, s>>>((int64_t)E, li.entries, slots.p, li.recs);
-    VS_CUDA_TRY(cudaGetLastError());
-    // 7. the query descriptor (one job, cells numbered from 0)
+    // 6. the query descriptor (one job, cells numbered from 0); its frame
+    // fields and cell widths are computed on the device
     LearnedJob d{};
     d.L = L;
     d.occ_shift = 2 * (L - li.occ_level);
@@ -701,8 +703,6 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     d.leaves = li.leaves;
     d.cell_keys = li.cell_keys;
     d.cell_start = li.cell_start;
-    d.recs = li.recs;
-    d.xy32 = li.xy32;
     d.xy = idx->xy;
     d.item_geom = idx->item_geom;
     d.geom_off = idx->geom_off;
@@ -710,12 +710,39 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     d.ring_off = idx->ring_off;
     d.boxes = idx->nodes;
     d.rings = idx->ring_index();
+    // 7. FP32 slot-relative vertices, per-slot ring ranges, per-entry records
+    VS_TRY(dalloc(&li.origin, (size_t)M, bytes));
+    VS_TRY(dalloc(&li.err32, (size_t)M, bytes));
+    VS_TRY(dalloc(&li.c01, (size_t)M, bytes));
+    VS_TRY(dalloc(&li.xy32, (size_t)std::max<int64_t>(idx->n_coords, 1), bytes));
+    VS_TRY(dalloc(&li.recs, (size_t)E, bytes));
     VS_TRY(dalloc(&li.desc, 1, bytes));
+    d.recs = li.recs;
+    d.c01 = li.c01;
+    d.xy32 = li.xy32;
     VS_CUDA_TRY(cudaMemcpyAsync(li.desc, &d, sizeof(d), cudaMemcpyHostToDevice, s));
     learned_desc_kernel<<<1, 1, 0, s>>>(idx->frame, li.desc);
     VS_CUDA_TRY(cudaGetLastError());
+    split_copy_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
+                                                            idx->xy, li.origin, li.err32, li.xy32);
+    VS_CUDA_TRY(cudaGetLastError());
+    slot_c01_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, idx->geom_off, idx->part_off, idx->ring_off, idx->ring_bin,
+                                                     li.c01);
+    VS_CUDA_TRY(cudaGetLastError());
+    Scratch<unsigned> bad;
+    VS_TRY(bad.alloc(1, s));
+    VS_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(unsigned), s));
+    entry_recs_kernel<<<grid_for(E, 256), 256, 0, s>>>((int64_t)E, keys.p, li.entries, li.desc, boxes, li.origin,
+                                                       li.err32, li.recs, bad.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    unsigned h_bad = 0;
+    VS_CUDA_TRY(cudaMemcpyAsync(&h_bad, bad.p, sizeof(h_bad), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaMemcpyAsync(&li.h_desc, li.desc, sizeof(LearnedJob), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h_bad) {
+        set_error("learned index: a cell key did not decode to its cell");
+        return VS_E_CUDA;
+    }
     idx->has_learned = true;
     return VS_OK;
 }

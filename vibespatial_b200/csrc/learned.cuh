@@ -11,11 +11,11 @@ namespace vs {
 
 // Per-query scratch of the learned pipeline (points n, batch-wide cells).
 struct LearnedScratch {
-    void* staged = nullptr;          // striped staging regions of matched points
+    void* staged = nullptr;          // striped staging regions of matched points (CellPoint)
     uint32_t* stripe_count = nullptr;
     int64_t stripe_cap = 0;
     uint32_t* cell_count = nullptr;  // counts, then start offsets after the scan
-    void* grouped = nullptr;         // matched points in cell order
+    void* grouped = nullptr;         // matched points in cell order (CellPoint)
     uint32_t* n_grouped = nullptr;
 };
 
@@ -37,9 +37,10 @@ struct LearnedQuery {
     int accept_mask;
     bool has_ring_bins;  // some job's index has y-binned rings long enough for the split walk
     int64_t row_base;    // added to every emitted / deferred point row (chunked joins)
+    LearnedShape shape;  // launch shape and ablation switches (zero = defaults)
 };
 
-// Enqueue map -> scan -> scatter -> refine on stream s (no host
+// Enqueue map -> scan -> place -> refine on stream s (no host
 // synchronisation; capturable).  For one job, `single` is its descriptor
 // (host copy, passed as a kernel parameter); q.jobs is used for batches.
 // ctx (may be null) receives phase marks 1, 2.

@@ -5,21 +5,23 @@
 // own positions, so no general sort is needed):
 //   map      input order: the point's job (batch) -> level-L cell key ->
 //            occupancy bit -> root table -> leaf model -> binary search inside
-//            the leaf's error window -> cell index (or none); warp-aggregated
-//            atomics on the per-cell counts return each point's rank within
-//            its cell, and the matched points are appended to striped staging
-//            regions
-//   scatter  after an exclusive scan of the counts, every staged point writes
-//            one aligned 32-byte record at start[cell] + rank, carrying its
-//            cell's candidate range
-//   refine   a warp takes 32 consecutive records, which share a candidate
-//            list except at cell boundaries, so the lanes read each polygon's
-//            data together (broadcast); each candidate is box-filtered in
-//            FP32 (rounded outward); survivors are queued per warp and
-//            refined 32 at a time with the FP32 crossing test on
-//            tile-relative coordinates; only edges whose FP32 decision lies
-//            within the rounding-error bound are re-decided in FP64, and a
-//            pair the FP64 filter cannot certify is deferred to the exact pass.
+//            the leaf's error window -> cell index (or none); the per-cell
+//            counts are incremented, and every matched point is appended to
+//            a striped staging region as one 16-byte CellPoint: its FP32
+//            offsets from the cell's anchor, its row and its cell
+//   place    after an exclusive scan of the counts, every staged CellPoint is
+//            copied to its cell's next free position (per-cell cursors), so
+//            the points end up grouped by cell
+//   refine   a warp takes 32 consecutive grouped points, which share a
+//            candidate list except at cell boundaries, so the lanes read each
+//            entry record together (broadcast); each candidate is box-filtered
+//            in FP32 against the entry's box relative to the same anchor
+//            (rounded outward); survivors are queued per warp and refined 32
+//            at a time with the FP32 crossing test on slot-relative
+//            coordinates; only edges whose FP32 decision lies within the
+//            rounding-error bound are re-decided in FP64 (the point's FP64
+//            coordinates are read back by row only then), and a pair the FP64
+//            filter cannot certify is deferred to the exact pass.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -38,57 +40,39 @@ namespace {
 
 constexpr int kThreads = 256;
 
-// A matched query point as the map pass leaves it: coordinates, row, its
-// job's cell index, its rank among the cell's points, and the job.
-struct __align__(32) StagedPoint {
-    double x, y;
-    int32_t row;
-    int32_t cell;
-    uint32_t rank;
-    int32_t job;
-};
-
 // The map pass appends matched points to kStripes regions of the staging
 // array, region s taking the packets p with p % kStripes == s, so each
 // region's append counter sees 1/kStripes of the atomics and a region never
 // holds more than 32 * ceil(packets / kStripes) points.
 constexpr int kStripes = 2048;
 
-// A query point in cell order, with its cell's candidate range
-// [lo, lo + len) of its job's per-entry records.  A full 32-byte sector, so
-// the scatter writes whole sectors.
-struct __align__(32) GroupedPoint {
-    double x, y;
-    int32_t row;
-    uint32_t lo;
-    uint32_t len;
-    int32_t job;
-};
-
 // A (point, candidate) pair that passed the FP32 box filter, queued for the
-// ring walk.
+// ring walk: the point relative to the slot origin, the tolerance of every
+// FP32 coordinate difference, and what the walk and the emission need.
 struct __align__(16) QueuedPair {
-    double x, y;
+    float qx, qy;
+    float t;
     int32_t row;
-    uint32_t rec;  // index into the job's per-entry records
+    int32_t slot;
     int32_t job;
-    int32_t pad;
+    int32_t pad0, pad1;
 };
 constexpr int kQueue = 64;  // >= 31 left over + 32 appended in one step
 
 struct LqArgs {
     LearnedQuery q;
     LearnedJob single;  // the one job of a single join (kernel parameter space)
-    StagedPoint* staged;
+    CellPoint* staged;
     uint32_t* stripe_count;
     int64_t stripe_cap;
     uint32_t* cell_count;
-    GroupedPoint* grouped;
+    CellPoint* grouped;
     const uint32_t* n_grouped;
     PairSink sink;
     DeferSink defer;
     unsigned long long* counters;
     unsigned long long* work;  // refine work queue (grouped points handed out)
+    int64_t grab;              // grouped points a refine warp takes per grab (multiple of 32)
 };
 
 // Job descriptor of a batch query (global memory) or of a single join (the
@@ -97,6 +81,19 @@ template <bool kMulti>
 __device__ __forceinline__ const LearnedJob& job_desc(const LqArgs& a, int job) {
     if constexpr (kMulti) return a.q.jobs[job];
     else return a.single;
+}
+
+// Job of query point pi (its index in the query's point arrays).
+template <bool kMulti>
+__device__ __forceinline__ int point_job(const LearnedQuery& q, int64_t pi) {
+    if (!kMulti || q.n_jobs <= 1) return 0;
+    int lo = 0, hi = q.n_jobs;  // last job with job_start[job] <= pi
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (q.job_start[mid] <= pi) lo = mid;
+        else hi = mid;
+    }
+    return lo;
 }
 
 // ------------------------------------------------------- split refine ---
@@ -135,31 +132,38 @@ __device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, flo
 }
 
 // One edge (vertex ia -> vertex ib) of the split ring walk: FP32 first, the
-// FP64 filter when the FP32 bound is inconclusive.  0: go on, 1: on the
-// edge, 2: undecided by the FP64 filter too.
-__device__ __forceinline__ int split_edge(double px, double py, float qx, float qy, float t, float2 a, float2 b,
-                                          const double2* __restrict__ xy, int ia, int ib, bool& inside,
-                                          unsigned& n32, unsigned& n64) {
+// FP64 filter when the FP32 bound is inconclusive.  The FP64 point is read
+// from the query arrays (X, Y at pi) only then.  0: go on, 1: on the edge,
+// 2: undecided by the FP64 filter too.
+struct PointRef {
+    const double* X;
+    const double* Y;
+    int64_t pi;
+};
+
+__device__ __forceinline__ int split_edge(float qx, float qy, float t, float2 a, float2 b,
+                                          const double2* __restrict__ xy, int ia, int ib, const PointRef& P,
+                                          bool& inside, unsigned& n32, unsigned& n64) {
     if (edge_step_fp32(a.x, a.y, b.x, b.y, qx, qy, t, inside)) {
         ++n32;
         return 0;
     }
     ++n64;
     const double2 A = xy[ia], B = xy[ib];
-    return edge_step_filtered(A.x, A.y, B.x, B.y, px, py, inside);
+    return edge_step_filtered(A.x, A.y, B.x, B.y, P.X[P.pi], P.Y[P.pi], inside);
 }
 
 // Split-precision location of a point in one ring, every edge.
-__device__ __forceinline__ int ring_location_split(double px, double py, float qx, float qy, float t,
-                                                   const float2* __restrict__ xy32, const double2* __restrict__ xy,
-                                                   int start, int end, unsigned& n32, unsigned& n64) {
+__device__ __forceinline__ int ring_location_split(float qx, float qy, float t, const float2* __restrict__ xy32,
+                                                   const double2* __restrict__ xy, int start, int end,
+                                                   const PointRef& P, unsigned& n32, unsigned& n64) {
     if (end - start < 2) return LOC_OUTSIDE;
     bool inside = false;
     float2 a = xy32[end - 1];
     int ia = end - 1;
     for (int i = start; i < end; ++i) {
         const float2 b = xy32[i];
-        const int r = split_edge(px, py, qx, qy, t, a, b, xy, ia, i, inside, n32, n64);
+        const int r = split_edge(qx, qy, t, a, b, xy, ia, i, P, inside, n32, n64);
         if (r == 1) return LOC_BOUNDARY;
         if (r == 2) return LOC_UNDECIDED;
         a = b;
@@ -169,14 +173,15 @@ __device__ __forceinline__ int ring_location_split(double px, double py, float q
 }
 
 // The same for a ring with y-bins: only the edges of the point's bin, in ring
-// order; an edge that continues the previous one reuses its end vertex.
-__device__ __forceinline__ int ring_location_split_binned(double px, double py, float qx, float qy, float t,
+// order; an edge that continues the previous one reuses its end vertex.  The
+// bin is chosen from the point's FP64 y (bins are defined on FP64 y).
+__device__ __forceinline__ int ring_location_split_binned(float qx, float qy, float t,
                                                           const float2* __restrict__ xy32,
                                                           const double2* __restrict__ xy, int start, int end,
                                                           const RingBins& bins, const uint16_t* __restrict__ edges,
-                                                          unsigned& n32, unsigned& n64) {
+                                                          const PointRef& P, unsigned& n32, unsigned& n64) {
     bool inside = false;
-    const int k = ring_bin_of(py, bins.y0, bins.scale);
+    const int k = ring_bin_of(P.Y[P.pi], bins.y0, bins.scale);
     const uint32_t e1 = bins.off[k + 1];
     int last = -2;
     float2 lb = make_float2(0.f, 0.f);
@@ -185,7 +190,7 @@ __device__ __forceinline__ int ring_location_split_binned(double px, double py, 
         const int ia = i == start ? end - 1 : i - 1;
         const float2 a = ia == last ? lb : xy32[ia];
         const float2 b = xy32[i];
-        const int r = split_edge(px, py, qx, qy, t, a, b, xy, ia, i, inside, n32, n64);
+        const int r = split_edge(qx, qy, t, a, b, xy, ia, i, P, inside, n32, n64);
         if (r == 1) return LOC_BOUNDARY;
         if (r == 2) return LOC_UNDECIDED;
         last = i;
@@ -197,8 +202,8 @@ __device__ __forceinline__ int ring_location_split_binned(double px, double py, 
 // kBins: the index has y-binned rings (kernels without bins carry no binned
 // walk, which keeps their registers for the common short rings).
 template <bool kBins>
-__device__ __forceinline__ int geometry_location_split(double px, double py, float qx, float qy, float t,
-                                                       const LearnedJob& J, int g, unsigned& n32, unsigned& n64) {
+__device__ __forceinline__ int geometry_location_split(float qx, float qy, float t, const LearnedJob& J, int g,
+                                                       const PointRef& P, unsigned& n32, unsigned& n64) {
     const int p0 = J.geom_off[g], p1 = J.geom_off[g + 1];
     for (int part = p0; part < p1; ++part) {
         bool inside = false;
@@ -207,10 +212,9 @@ __device__ __forceinline__ int geometry_location_split(double px, double py, flo
             const int c0 = J.ring_off[ring], c1 = J.ring_off[ring + 1];
             // the FP32 walk is cheap per edge, so bins pay off only on longer rings than for the FP64 walk
             const int rb = (kBins && J.rings.ring_bin && c1 - c0 >= kSplitBinMinVertices) ? J.rings.ring_bin[ring] : -1;
-            const int k = rb >= 0
-                              ? ring_location_split_binned(px, py, qx, qy, t, J.xy32, J.xy, c0, c1, J.rings.bins[rb],
-                                                           J.rings.edges, n32, n64)
-                              : ring_location_split(px, py, qx, qy, t, J.xy32, J.xy, c0, c1, n32, n64);
+            const int k = rb >= 0 ? ring_location_split_binned(qx, qy, t, J.xy32, J.xy, c0, c1, J.rings.bins[rb],
+                                                               J.rings.edges, P, n32, n64)
+                                  : ring_location_split(qx, qy, t, J.xy32, J.xy, c0, c1, P, n32, n64);
             if (k == LOC_BOUNDARY || k == LOC_UNDECIDED) return k;
             if (k == LOC_INTERIOR) inside = !inside;
         }
@@ -220,22 +224,29 @@ __device__ __forceinline__ int geometry_location_split(double px, double py, flo
 }
 
 // ---------------------------------------------------------------- map ---
-// Exact lookup of a point's cell in job J's learned index: level-L cell key ->
-// occupancy bit -> root table -> leaf model -> binary search inside the
-// leaf's error window.  Returns the cell's index, or -1 when no stored cell
-// matches (no polygon box overlaps the point's cell).
-__device__ __forceinline__ int learned_lookup(const LearnedJob& J, double x, double y, const uint16_t* lut,
+// Exact lookup of grid cell (gx, gy) (32-bit grid coordinates) in job J's
+// learned index: level-L cell key -> occupancy bit -> root table -> leaf
+// model -> binary search inside the leaf's error window.  Returns the cell's
+// index, or -1 when no stored cell matches (no polygon box overlaps it).
+// kBsearch (an ablation): the model is skipped and the search covers every
+// stored key.
+template <bool kBsearch>
+__device__ __forceinline__ int learned_lookup(const LearnedJob& J, uint32_t gx, uint32_t gy, const uint16_t* lut,
                                               unsigned long long& n_wide) {
-    const uint32_t cell = hilbert_key_lut(quantize(x, J.lox, J.sx), quantize(y, J.loy, J.sy), J.L, lut);
+    const uint32_t cell = hilbert_key_lut(gx, gy, J.L, lut);
     const uint32_t ob = cell >> J.occ_shift;
     if (!((J.occ[ob >> 5] >> (ob & 31)) & 1u)) return -1;
-    const RmiLeaf lf = J.leaves[J.root_table[cell >> J.root_shift]];
-    if (lf.lo > lf.hi) return -1;  // no stored key routes to this leaf
-    const long long pred = rmi_predict(make_double2(lf.a, lf.b), cell);
-    long long l0 = pred + lf.lo, h0 = pred + lf.hi + 1;  // search [l0, h0)
-    l0 = l0 < 0 ? 0 : l0;
-    h0 = h0 > J.n_cells ? J.n_cells : h0;
-    if (h0 - l0 > 256) ++n_wide;
+    long long l0 = 0, h0 = J.n_cells;  // search [l0, h0)
+    if constexpr (!kBsearch) {
+        const RmiLeaf lf = J.leaves[J.root_table[cell >> J.root_shift]];
+        if (lf.lo > lf.hi) return -1;  // no stored key routes to this leaf
+        const long long pred = rmi_predict(make_double2(lf.a, lf.b), cell);
+        l0 = pred + lf.lo;
+        h0 = pred + lf.hi + 1;
+        l0 = l0 < 0 ? 0 : l0;
+        h0 = h0 > J.n_cells ? J.n_cells : h0;
+        if (h0 - l0 > 256) ++n_wide;
+    }
     const long long h1 = h0;
     while (l0 < h0) {
         const long long mid = (l0 + h0) >> 1;
@@ -251,25 +262,17 @@ template <bool kMulti>
 __device__ __forceinline__ int packet_job(const LearnedQuery& q, int64_t b0, int64_t i, int lane) {
     if (!kMulti || q.n_jobs <= 1) return 0;
     int j = 0;
-    if (lane == 0) {
-        int lo = 0, hi = q.n_jobs;  // last job with job_start[job] <= b0
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (q.job_start[mid] <= b0) lo = mid;
-            else hi = mid;
-        }
-        j = lo;
-    }
+    if (lane == 0) j = point_job<kMulti>(q, b0);
     j = __shfl_sync(0xffffffffu, j, 0);
     if (i < q.n)
         while (j + 1 < q.n_jobs && i >= q.job_start[j + 1]) ++j;
     return j;
 }
 
-// Pass 1 (map), points in input order: each point's cell and its rank among
-// the cell's points (warp-aggregated atomics on the per-cell counts); the
-// matched points are appended to the staging regions.
-template <bool kMulti>
+// Pass 1 (map), points in input order: each point's cell, the per-cell
+// counts, and the matched points appended to the staging regions as
+// CellPoints (FP32 offsets from the cell's anchor: |offset| <= half a cell).
+template <bool kMulti, bool kBsearch>
 __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LqArgs a) {
     __shared__ uint16_t s_lut[kHilbertLutSize];
     hilbert_lut_init(s_lut);
@@ -280,26 +283,28 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LqArgs a
     const unsigned lt = (1u << lane) - 1u;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    // Warp-uniform loop: the whole warp reaches the match and shuffle together.
+    // Warp-uniform loop: the whole warp reaches the ballot and shuffle together.
     for (int64_t b0 = gw * 32; b0 < q.n; b0 += nw * 32) {
         const int64_t i = b0 + lane;
         const int job = packet_job<kMulti>(q, b0, i, lane);
-        int c = -1, gc = -1;
-        double x = 0.0, y = 0.0;
+        int gc = -1;
+        float qx = 0.f, qy = 0.f;
         if (i < q.n) {
             const LearnedJob& J = job_desc<kMulti>(a, job);
-            x = q.px[i];
-            y = q.py[i];
+            const double x = q.px[i], y = q.py[i];
             if ((q.pvalid == nullptr || q.pvalid[i]) && J.n_cells > 0 && x >= J.lox && x <= J.hix && y >= J.loy &&
-                y <= J.hiy)
-                c = learned_lookup(J, x, y, s_lut, n_wide);
-            if (c >= 0) gc = (int)(J.cell_base + (uint32_t)c);
+                y <= J.hiy) {
+                const uint32_t gx = quantize(x, J.lox, J.sx), gy = quantize(y, J.loy, J.sy);
+                const int c = learned_lookup<kBsearch>(J, gx, gy, s_lut, n_wide);
+                if (c >= 0) {
+                    gc = (int)(J.cell_base + (uint32_t)c);
+                    const int sh = 32 - J.L;
+                    qx = __double2float_rn(__dsub_rn(x, cell_anchor(J.lox, J.cwx, gx >> sh)));
+                    qy = __double2float_rn(__dsub_rn(y, cell_anchor(J.loy, J.cwy, gy >> sh)));
+                }
+            }
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, gc);
-        const int leader = __ffs(peers) - 1;
-        uint32_t base = 0;
-        if (gc >= 0 && lane == leader) base = atomicAdd(&a.cell_count[gc], (uint32_t)__popc(peers));
-        base = __shfl_sync(0xffffffffu, base, leader);
+        if (gc >= 0) atomicAdd(&a.cell_count[gc], 1u);
         // append the matched points of this packet to its stripe region
         const unsigned mm = __ballot_sync(0xffffffffu, gc >= 0);
         if (mm) {
@@ -308,13 +313,11 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LqArgs a
             if (lane == 0) sb = atomicAdd(&a.stripe_count[stripe], (uint32_t)__popc(mm));
             sb = __shfl_sync(0xffffffffu, sb, 0);
             if (gc >= 0) {
-                StagedPoint p;
-                p.x = x;
-                p.y = y;
+                CellPoint p;
+                p.qx = qx;
+                p.qy = qy;
                 p.row = (int32_t)(i + q.row_base);
-                p.cell = c;
-                p.rank = base + __popc(peers & lt);
-                p.job = job;
+                p.gcell = (uint32_t)gc;
                 a.staged[stripe * a.stripe_cap + sb + __popc(mm & lt)] = p;
             }
         }
@@ -322,51 +325,51 @@ __global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LqArgs a
     add_counter(a.counters, 6, n_wide);
 }
 
-// ------------------------------------------------------------ scatter ---
-// Pass 2 (scatter): after the exclusive scan of the counts, every staged
-// point writes one aligned 32-byte record at start[cell] + rank, carrying its
-// cell's candidate range.  A block walks whole stripe regions (coalesced
-// reads, every lane busy); each thread keeps kScatterUnroll records in flight.
-#ifndef VS_SCATTER_UNROLL
-#define VS_SCATTER_UNROLL 4
+// -------------------------------------------------------------- place ---
+// Pass 2 (place): after the exclusive scan of the counts (cell_count[c] is
+// then the first position of cell c), every staged point takes the next
+// position of its cell (warp-aggregated cursor increments) and is copied
+// there.  A block walks whole stripe regions; a warp keeps kPlaceUnroll
+// groups of 32 records in flight (loads, then cursor increments, then stores).
+#ifndef VS_PLACE_UNROLL
+#define VS_PLACE_UNROLL 4
 #endif
-constexpr int kScatterUnroll = VS_SCATTER_UNROLL;
+constexpr int kPlaceUnroll = VS_PLACE_UNROLL;
 
-#ifndef VS_SCATTER_MIN_BLOCKS
-#define VS_SCATTER_MIN_BLOCKS 1
-#endif
-template <bool kMulti>
-__global__ void __launch_bounds__(kThreads, VS_SCATTER_MIN_BLOCKS) learned_scatter_kernel(const LqArgs a) {
+__global__ void __launch_bounds__(kThreads) learned_place_kernel(const LqArgs a) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    constexpr uint32_t kStep = 32u * kPlaceUnroll;
     for (int stripe = blockIdx.x; stripe < kStripes; stripe += gridDim.x) {
         const uint32_t cnt = a.stripe_count[stripe];
-        const StagedPoint* src = a.staged + (int64_t)stripe * a.stripe_cap;
-        for (uint32_t k0 = threadIdx.x; k0 < cnt; k0 += blockDim.x * kScatterUnroll) {
-            StagedPoint p[kScatterUnroll];
+        const CellPoint* src = a.staged + (int64_t)stripe * a.stripe_cap;
+        // warp-uniform loop: every lane runs the same iterations
+        for (uint32_t k0 = (uint32_t)warp * kStep; k0 < cnt; k0 += (kThreads / 32) * kStep) {
+            CellPoint p[kPlaceUnroll];
+            int gc[kPlaceUnroll];
 #pragma unroll
-            for (int u = 0; u < kScatterUnroll; ++u) {
-                const uint32_t k = k0 + u * blockDim.x;
-                if (k < cnt) p[u] = src[k];
-            }
-            GroupedPoint g[kScatterUnroll];
-            uint32_t pos[kScatterUnroll];
-#pragma unroll
-            for (int u = 0; u < kScatterUnroll; ++u) {
-                const uint32_t k = k0 + u * blockDim.x;
+            for (int u = 0; u < kPlaceUnroll; ++u) {
+                const uint32_t k = k0 + u * 32 + lane;
+                gc[u] = -1;
                 if (k < cnt) {
-                    const LearnedJob& J = job_desc<kMulti>(a, p[u].job);
-                    const int c = p[u].cell;
-                    g[u].x = p[u].x;
-                    g[u].y = p[u].y;
-                    g[u].row = p[u].row;
-                    g[u].lo = J.cell_start[c];
-                    g[u].len = J.cell_start[c + 1] - g[u].lo;
-                    g[u].job = p[u].job;
-                    pos[u] = a.cell_count[J.cell_base + (uint32_t)c] + p[u].rank;
+                    p[u] = src[k];
+                    gc[u] = (int)p[u].gcell;
                 }
             }
+            unsigned peers[kPlaceUnroll];
+            uint32_t base[kPlaceUnroll];
 #pragma unroll
-            for (int u = 0; u < kScatterUnroll; ++u)
-                if (k0 + u * blockDim.x < cnt) a.grouped[pos[u]] = g[u];
+            for (int u = 0; u < kPlaceUnroll; ++u) {
+                peers[u] = __match_any_sync(0xffffffffu, gc[u]);
+                base[u] = 0;
+                if (gc[u] >= 0 && lane == __ffs(peers[u]) - 1)
+                    base[u] = atomicAdd(&a.cell_count[gc[u]], (uint32_t)__popc(peers[u]));
+            }
+#pragma unroll
+            for (int u = 0; u < kPlaceUnroll; ++u) {
+                const uint32_t b = __shfl_sync(0xffffffffu, base[u], __ffs(peers[u]) - 1);
+                if (gc[u] >= 0) a.grouped[b + __popc(peers[u] & lt)] = p[u];
+            }
         }
     }
 }
@@ -375,25 +378,55 @@ __global__ void __launch_bounds__(kThreads, VS_SCATTER_MIN_BLOCKS) learned_scatt
 #ifndef VS_JOIN_MIN_BLOCKS
 #define VS_JOIN_MIN_BLOCKS 5
 #endif
-#ifndef VS_JOIN_GRAB
-#define VS_JOIN_GRAB 32
-#endif
-constexpr int64_t kJoinGrab = VS_JOIN_GRAB;  // grouped points per work-queue grab (multiple of 32)
+constexpr int64_t kJoinGrab = 32;  // default grouped points per work-queue grab (multiple of 32)
 
-// FP32 box filter of one candidate record (rounded outward: never rejects a
-// point of the box).
-__device__ __forceinline__ bool box_filter_fp32(const SlotRecord* rp, double x, double y) {
-    const double2 o = *reinterpret_cast<const double2*>(&rp->ox);
-    const float4 bx = rp->box;
-    const float qx = __double2float_rn(x - o.x), qy = __double2float_rn(y - o.y);
-    const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-    return !(__fadd_ru(qx, dp) < bx.x || __fsub_rd(qx, dp) > bx.z || __fadd_ru(qy, dp) < bx.y ||
-             __fsub_rd(qy, dp) > bx.w);
+// A grouped point's candidate range and conversion-error bound.  The bound
+// dq covers |q - (p - anchor)|: the FP64 subtraction (2^-53 relative) and the
+// FP32 rounding (2^-24 relative, or the subnormal spacing).
+struct GroupedLane {
+    CellPoint p;
+    uint32_t lo, len;
+    int job;
+    float dq;
+};
+
+template <bool kMulti>
+__device__ __forceinline__ GroupedLane load_grouped(const LqArgs& a, int64_t j, int64_t e0) {
+    GroupedLane g;
+    g.p = CellPoint{0.f, 0.f, 0, 0u};
+    g.lo = g.len = 0;
+    g.job = 0;
+    if (j < e0) {
+        g.p = a.grouped[j];
+        g.job = point_job<kMulti>(a.q, (int64_t)g.p.row - a.q.row_base);
+        const LearnedJob& J = job_desc<kMulti>(a, g.job);
+        const uint32_t c = g.p.gcell - J.cell_base;
+        g.lo = J.cell_start[c];
+        g.len = J.cell_start[c + 1] - g.lo;
+    }
+    g.dq = __fmaf_ru(fmaxf(fabsf(g.p.qx), fabsf(g.p.qy)), 6.1e-8f, 1e-37f);
+    return g;
+}
+
+// FP32 box filter of one candidate (the box is rounded outward and the point
+// widened by its error bound: never rejects a point of the polygon's box).
+__device__ __forceinline__ bool box_filter_fp32(const float4& bx, float qx, float qy, float dq) {
+    return !(__fadd_ru(qx, dq) < bx.x || __fsub_rd(qx, dq) > bx.z || __fadd_ru(qy, dq) < bx.y ||
+             __fsub_rd(qy, dq) > bx.w);
+}
+
+__device__ __forceinline__ unsigned warp_max_u32(unsigned v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = t > v ? t : v;
+    }
+    return v;
 }
 
 // Box candidates only (predicate BBOX): a warp takes 32 consecutive grouped
 // points and walks their candidate lists; the FP32 filter's survivors are
-// decided exactly on the FP64 box.
+// decided exactly on the FP64 box with the point's FP64 coordinates.
 template <bool kMulti>
 __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_bbox_kernel(const LqArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
@@ -405,36 +438,30 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_bbox_ker
     const int64_t n = (int64_t)*a.n_grouped;
     unsigned long long n_cand = 0;
     for (;;) {
-        const int64_t b0 = warp_grab(a.work, kJoinGrab);
+        const int64_t b0 = warp_grab(a.work, a.grab);
         if (b0 >= n) break;
-        const int64_t e0 = b0 + kJoinGrab < n ? b0 + kJoinGrab : n;
+        const int64_t e0 = b0 + a.grab < n ? b0 + a.grab : n;
         for (int64_t base = b0; base < e0; base += 32) {
-            const int64_t j = base + lane;
-            GroupedPoint g{0.0, 0.0, 0, 0, 0, 0};
-            if (j < e0) g = a.grouped[j];
-            uint32_t maxlen = g.len;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
-                maxlen = t > maxlen ? t : maxlen;
-            }
+            const GroupedLane g = load_grouped<kMulti>(a, base + lane, e0);
+            const uint32_t maxlen = warp_max_u32(g.len);
+            const LearnedJob& J = job_desc<kMulti>(a, g.job);
+            const int64_t pi = (int64_t)g.p.row - a.q.row_base;
             for (uint32_t k = 0; k < maxlen; ++k) {
                 bool want = false;
                 int32_t right = 0;
                 if (k < g.len) {
-                    const LearnedJob& J = job_desc<kMulti>(a, g.job);
-                    const SlotRecord* rp = J.recs + g.lo + k;
-                    if (box_filter_fp32(rp, g.x, g.y)) {
-                        const int slot = rp->slot;
-                        const vs_box bb = J.boxes[slot];
-                        if (g.x >= bb.minx && g.x <= bb.maxx && g.y >= bb.miny && g.y <= bb.maxy) {
+                    const EntryRecord r = J.recs[g.lo + k];
+                    if (box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq)) {
+                        const vs_box bb = J.boxes[r.slot];
+                        const double x = a.q.px[pi], y = a.q.py[pi];
+                        if (x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy) {
                             ++n_cand;
                             want = true;
-                            right = J.item_geom[slot];
+                            right = J.item_geom[r.slot];
                         }
                     }
                 }
-                wemit_sync(out, a.sink, want, g.row, right);
+                wemit_sync(out, a.sink, want, g.p.row, right);
             }
             wflush(out, a.sink, false);
         }
@@ -444,7 +471,9 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_bbox_ker
 }
 
 // Ring walks of up to 32 queued pairs, one per lane.
-template <bool kMulti, bool kBins>
+// kF64 (an ablation): the walk is the plain method's FP64 filtered walk on
+// the point's FP64 coordinates, with no FP32 edge stage.
+template <bool kMulti, bool kBins, bool kF64>
 __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& out, const QueuedPair* qp, int nq,
                                               int lane, unsigned& n32, unsigned& n64) {
     bool want = false;
@@ -453,17 +482,21 @@ __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& ou
         const QueuedPair jb = qp[lane];
         const LearnedJob& J = job_desc<kMulti>(a, jb.job);
         row = jb.row;
-        const SlotRecord r = J.recs[jb.rec];
-        const float qx = __double2float_rn(jb.x - r.ox), qy = __double2float_rn(jb.y - r.oy);
-        const float dp = __fmaf_ru(fmaxf(fabsf(qx), fabsf(qy)), 6.1e-8f, 1e-37f);
-        const float t = __fmul_ru(__fadd_ru(r.err, dp), 1.0001f);
-        const int loc = r.c0 >= 0 ? ring_location_split(jb.x, jb.y, qx, qy, t, J.xy32, J.xy, r.c0, r.c1, n32, n64)
-                                  : geometry_location_split<kBins>(jb.x, jb.y, qx, qy, t, J, r.slot, n32, n64);
+        const PointRef P{a.q.px, a.q.py, (int64_t)jb.row - a.q.row_base};
+        int loc;
+        if constexpr (kF64) {
+            loc = geometry_location_filtered(P.X[P.pi], P.Y[P.pi], J.xy, J.ring_off, J.part_off, J.geom_off, jb.slot,
+                                             J.rings);
+        } else {
+            const int2 cr = J.c01[jb.slot];
+            loc = cr.x >= 0 ? ring_location_split(jb.qx, jb.qy, jb.t, J.xy32, J.xy, cr.x, cr.y, P, n32, n64)
+                            : geometry_location_split<kBins>(jb.qx, jb.qy, jb.t, J, jb.slot, P, n32, n64);
+        }
         if (loc == LOC_UNDECIDED) {
-            defer(a.defer, jb.row, r.slot);  // a batch's exact pass finds the job from the row
+            defer(a.defer, jb.row, jb.slot);  // a batch's exact pass finds the job from the row
         } else if ((a.q.accept_mask >> loc) & 1) {
             want = true;
-            right = J.item_geom[r.slot];
+            right = J.item_geom[jb.slot];
         }
     }
     wemit_sync(out, a.sink, want, row, right);
@@ -471,12 +504,13 @@ __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& ou
 
 // Pass 3 with a location test: the warp walks its grouped points' candidate
 // lists, and every (point, candidate) pair that passes the FP32 box filter is
-// appended to a warp-local queue in shared memory.  Each time 32 pairs are
-// queued, every lane refines one of them, so the ring walks, which dominate,
-// run with all lanes busy instead of only the lanes whose point lies in the
+// appended to a warp-local queue in shared memory, converted to the slot's
+// frame (q + off) with its error tolerance.  Each time 32 pairs are queued,
+// every lane refines one of them, so the ring walks, which dominate, run
+// with all lanes busy instead of only the lanes whose point lies in the
 // current candidate's box.  Neighbouring queue entries mostly share a
 // polygon, so vertex reads stay broadcasts.
-template <bool kMulti, bool kBins>
+template <bool kMulti, bool kBins, bool kF64>
 __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_kernel(const LqArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
     __shared__ unsigned s_cnt[kThreads / 32];
@@ -492,36 +526,40 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_k
     unsigned n32 = 0, n64 = 0;
     int nq = 0;  // warp-uniform queue length
     for (;;) {
-        const int64_t b0 = warp_grab(a.work, kJoinGrab);
+        const int64_t b0 = warp_grab(a.work, a.grab);
         if (b0 >= n) break;
-        const int64_t e0 = b0 + kJoinGrab < n ? b0 + kJoinGrab : n;
+        const int64_t e0 = b0 + a.grab < n ? b0 + a.grab : n;
         for (int64_t base = b0; base < e0; base += 32) {
-            const int64_t j = base + lane;
-            GroupedPoint g{0.0, 0.0, 0, 0, 0, 0};
-            if (j < e0) g = a.grouped[j];
-            uint32_t maxlen = g.len;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const uint32_t t = __shfl_xor_sync(0xffffffffu, maxlen, o);
-                maxlen = t > maxlen ? t : maxlen;
-            }
-            const SlotRecord* recs = job_desc<kMulti>(a, g.job).recs;
+            const GroupedLane g = load_grouped<kMulti>(a, base + lane, e0);
+            const uint32_t maxlen = warp_max_u32(g.len);
+            const EntryRecord* recs = job_desc<kMulti>(a, g.job).recs;
             for (uint32_t k = 0; k < maxlen; ++k) {
-                const bool inbox = k < g.len && box_filter_fp32(recs + g.lo + k, g.x, g.y);
+                bool inbox = false;
+                EntryRecord r;
+                if (k < g.len) {
+                    r = recs[g.lo + k];
+                    inbox = box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq);
+                }
                 const unsigned m = __ballot_sync(0xffffffffu, inbox);
                 if (inbox) {
                     QueuedPair& e = qp[nq + __popc(m & lt)];
-                    e.x = g.x;
-                    e.y = g.y;
-                    e.row = g.row;
-                    e.rec = g.lo + k;
+                    // the point in the slot's frame; its error against the real
+                    // p - origin is at most dq + |off error| (in r.err with the
+                    // vertex error) + the rounding of this addition (es)
+                    const float sx = __fadd_rn(g.p.qx, r.offx), sy = __fadd_rn(g.p.qy, r.offy);
+                    const float es = __fmaf_ru(fmaxf(fabsf(sx), fabsf(sy)), 6.1e-8f, 1e-37f);
+                    e.qx = sx;
+                    e.qy = sy;
+                    e.t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, g.dq), es), 1.0001f);
+                    e.row = g.p.row;
+                    e.slot = r.slot;
                     e.job = g.job;
                     ++n_cand;
                 }
                 nq += __popc(m);
                 __syncwarp();
                 if (nq >= 32) {
-                    refine_queued<kMulti, kBins>(a, out, qp, 32, lane, n32, n64);
+                    refine_queued<kMulti, kBins, kF64>(a, out, qp, 32, lane, n32, n64);
                     __syncwarp();
                     if (lane < nq - 32) qp[lane] = qp[32 + lane];
                     nq -= 32;
@@ -531,7 +569,7 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_k
             wflush(out, a.sink, false);
         }
     }
-    if (nq > 0) refine_queued<kMulti, kBins>(a, out, qp, nq, lane, n32, n64);
+    if (nq > 0) refine_queued<kMulti, kBins, kF64>(a, out, qp, nq, lane, n32, n64);
     wflush(out, a.sink, true);
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 2, n32);
@@ -549,49 +587,71 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 size_t learned_scratch_bytes(int64_t n, int64_t n_cells) {
     const int64_t cap = stripe_cap_for(n);
-    return align256(sizeof(StagedPoint) * (size_t)(kStripes * cap)) + align256(sizeof(uint32_t) * kStripes) +
+    return align256(sizeof(CellPoint) * (size_t)(kStripes * cap)) + align256(sizeof(uint32_t) * kStripes) +
            align256(sizeof(uint32_t) * (size_t)(n_cells > 0 ? n_cells : 1)) +
-           align256(sizeof(GroupedPoint) * (size_t)(n > 0 ? n : 1)) + align256(sizeof(uint32_t));
+           align256(sizeof(CellPoint) * (size_t)(n > 0 ? n : 1)) + align256(sizeof(uint32_t));
 }
 
 void learned_scratch_carve(void* base, int64_t n, int64_t n_cells, LearnedScratch& sc) {
     char* p = (char*)base;
     sc.stripe_cap = stripe_cap_for(n);
     sc.staged = p;
-    p += align256(sizeof(StagedPoint) * (size_t)(kStripes * sc.stripe_cap));
+    p += align256(sizeof(CellPoint) * (size_t)(kStripes * sc.stripe_cap));
     sc.stripe_count = (uint32_t*)p;
     p += align256(sizeof(uint32_t) * kStripes);
     sc.cell_count = (uint32_t*)p;
     p += align256(sizeof(uint32_t) * (size_t)(n_cells > 0 ? n_cells : 1));
     sc.grouped = p;
-    p += align256(sizeof(GroupedPoint) * (size_t)(n > 0 ? n : 1));
+    p += align256(sizeof(CellPoint) * (size_t)(n > 0 ? n : 1));
     sc.n_grouped = (uint32_t*)p;
 }
 
 namespace {
 
-#ifndef VS_LEARNED_BLOCKS_PER_SM
-#define VS_LEARNED_BLOCKS_PER_SM 8  // map blocks per SM (0: one resident wave)
-#endif
+template <bool kMulti, bool kBins>
+void* pick_refine(uint32_t flags) {
+    return (flags & kLearnedFp64Walk) ? (void*)learned_refine_kernel<kMulti, kBins, true>
+                                      : (void*)learned_refine_kernel<kMulti, kBins, false>;
+}
+
+// Grid of a persistent kernel: blocks_per_sm per SM when given (capped at the
+// occupancy limit), else every block that fits; never more than the work needs.
+int persistent_grid(const void* kernel, int64_t n, int blocks_per_sm) {
+    int dev = 0, sms = 1, fit = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kernel, kThreads, 0);
+    fit = fit > 0 ? fit : 1;
+    const int per = blocks_per_sm > 0 && blocks_per_sm < fit ? blocks_per_sm : fit;
+    const int64_t need = (n + kThreads - 1) / kThreads;
+    const int64_t g = (int64_t)per * sms;
+    return (int)(need < 1 ? 1 : (need < g ? need : g));
+}
 
 template <bool kMulti>
 int launch_passes(cudaStream_t s, vs_context* ctx, const LqArgs& a) {
     const int64_t n = a.q.n;
-    const int map_grid = VS_LEARNED_BLOCKS_PER_SM > 0 ? grid_for(n, kThreads, VS_LEARNED_BLOCKS_PER_SM)
-                                                      : resident_grid(learned_map_kernel<kMulti>, n, kThreads);
-    learned_map_kernel<kMulti><<<map_grid, kThreads, 0, s>>>(a);
+    const LearnedShape& sh = a.q.shape;
+    const int map_grid = grid_for(n, kThreads, sh.map_blocks_per_sm > 0 ? sh.map_blocks_per_sm : 8);
+    if (sh.flags & kLearnedBsearch) learned_map_kernel<kMulti, true><<<map_grid, kThreads, 0, s>>>(a);
+    else learned_map_kernel<kMulti, false><<<map_grid, kThreads, 0, s>>>(a);
     VS_LAUNCHED("learned_map", s);
     VS_TRY(exclusive_scan_u32(a.cell_count, a.cell_count, a.q.n_cells, (uint32_t*)a.n_grouped, s));
     if (ctx) phase_mark(ctx, 1);
-    learned_scatter_kernel<kMulti><<<kStripes, kThreads, 0, s>>>(a);
-    VS_LAUNCHED("learned_scatter", s);
+    learned_place_kernel<<<kStripes, kThreads, 0, s>>>(a);
+    VS_LAUNCHED("learned_place", s);
     if (ctx) phase_mark(ctx, 2);
     if (a.q.accept_mask) {
-        auto* kernel = a.q.has_ring_bins ? learned_refine_kernel<kMulti, true> : learned_refine_kernel<kMulti, false>;
-        kernel<<<resident_grid(kernel, n, kThreads), kThreads, 0, s>>>(a);
+        const void* kernel = a.q.has_ring_bins ? pick_refine<kMulti, true>(sh.flags) : pick_refine<kMulti, false>(sh.flags);
+        const int grid = persistent_grid(kernel, n, sh.refine_blocks_per_sm);
+        void* args[] = {(void*)&a};
+        VS_CUDA_TRY(cudaLaunchKernel(kernel, dim3(grid), dim3(kThreads), args, 0, s));
         VS_LAUNCHED("learned_refine", s);
     } else {
-        learned_bbox_kernel<kMulti><<<resident_grid(learned_bbox_kernel<kMulti>, n, kThreads), kThreads, 0, s>>>(a);
+        const void* kernel = (const void*)learned_bbox_kernel<kMulti>;
+        const int grid = persistent_grid(kernel, n, sh.refine_blocks_per_sm);
+        void* args[] = {(void*)&a};
+        VS_CUDA_TRY(cudaLaunchKernel(kernel, dim3(grid), dim3(kThreads), args, 0, s));
         VS_LAUNCHED("learned_bbox", s);
     }
     return VS_OK;
@@ -605,25 +665,26 @@ int enqueue_learned(cudaStream_t s, vs_context* ctx, const LearnedQuery& q, cons
     LqArgs a{};
     a.q = q;
     if (single) a.single = *single;
-    a.staged = (StagedPoint*)sc.staged;
+    a.staged = (CellPoint*)sc.staged;
     a.stripe_count = sc.stripe_count;
     a.stripe_cap = sc.stripe_cap;
     a.cell_count = sc.cell_count;
-    a.grouped = (GroupedPoint*)sc.grouped;
+    a.grouped = (CellPoint*)sc.grouped;
     a.n_grouped = sc.n_grouped;
     a.sink = sink;
     a.defer = defer;
     a.counters = counters;
     a.work = work;
+    a.grab = q.shape.grab > 0 ? (int64_t)((q.shape.grab + 31) / 32 * 32) : kJoinGrab;
     VS_CUDA_TRY(cudaMemsetAsync(sc.cell_count, 0, (size_t)(q.n_cells > 0 ? q.n_cells : 1) * sizeof(uint32_t), s));
     VS_CUDA_TRY(cudaMemsetAsync(sc.stripe_count, 0, (size_t)kStripes * sizeof(uint32_t), s));
     if (q.n_jobs > 1) return launch_passes<true>(s, ctx, a);
     return launch_passes<false>(s, ctx, a);
-    return VS_OK;
 }
 
 int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int accept_mask, int32_t* d_left,
-                        int32_t* d_right, int64_t capacity, const DeferSink& dsink, int64_t row_base) {
+                        int32_t* d_right, int64_t capacity, const DeferSink& dsink, int64_t row_base,
+                        const LearnedShape& shape) {
     const LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
     Scratch<char> buf;
@@ -642,6 +703,7 @@ int launch_learned_join(vs_context* ctx, const vs_index* idx, const vs_points* p
     q.accept_mask = accept_mask;
     q.has_ring_bins = idx->n_split_binned_rings > 0;
     q.row_base = row_base;
+    q.shape = shape;
     const PairSink sink{d_left, d_right, (unsigned long long)(capacity > 0 ? capacity : 0), &ctx->d_counters[0]};
     return enqueue_learned(s, ctx, q, &li.h_desc, sc, sink, dsink, ctx->d_counters, &ctx->d_counters[kWorkCounter]);
 }
