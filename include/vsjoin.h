@@ -375,6 +375,40 @@ int vs_wkb_plan_create(vs_context* ctx, const uint8_t* d_wkb, const int64_t* d_o
 int vs_wkb_plan_decode(vs_wkb_plan* plan, const vs_wkb_out* out);
 int vs_wkb_plan_free(vs_wkb_plan* plan);
 
+/* ---------------------------------------------------------------------- */
+/* Row reductions of a join's pairs on the device (the relation flow of the
+ * index without exported pairs).  Replace the reference's native relation
+ * reductions: sindex.query_left_match_count_expression,
+ * query_left_semijoin / query_left_antijoin / query_right_semijoin
+ * (src/vibespatial/api/sindex.py:1592-1760), query_aggregate's size and sum
+ * (:505) and query_pair_aggregate's shared counts (:973, host path
+ * :1257-1270).  Rows outside their range: VS_E_ARG.  Each call returns when
+ * its outputs are complete. */
+
+/* d_counts[r] (int64, n_rows of them) = pairs whose row is r, counting only
+ * the pairs whose d_mask byte is non-zero when d_mask is given. */
+int vs_row_counts(vs_context* ctx, const int32_t* d_rows, const uint8_t* d_mask, int64_t n_pairs, int64_t n_rows,
+                  int64_t* d_counts);
+
+/* d_sums[r] = sum of d_values[d_cols[k]] over the pairs k with d_rows[k] == r,
+ * added in pair order (so equal to numpy's bincount(rows, weights=...)); the
+ * rows must ascend (VS_E_ARG otherwise), as a join's sorted pairs do. */
+int vs_row_sums(vs_context* ctx, const int32_t* d_rows, const int32_t* d_cols, int64_t n_pairs, int64_t n_rows,
+                const double* d_values, int64_t n_values, double* d_sums);
+
+/* The rows r in ascending order whose d_counts[r] > 0 (matched != 0: a
+ * semijoin) or == 0 (matched == 0: an antijoin), into d_out (n_rows
+ * capacity); their number in *n_out. */
+int vs_select_rows(vs_context* ctx, const int64_t* d_counts, int64_t n_rows, int32_t matched, int32_t* d_out,
+                   int64_t* n_out);
+
+/* d_flags[k] = 1 when pair k of relation a is also a pair of relation b, else
+ * 0.  b's pairs must be sorted by (left, right) (VS_E_ARG otherwise), as a
+ * join's sorted output is; left rows lie in [0, n_left_rows). */
+int vs_pairs_member(vs_context* ctx, const int32_t* d_a_left, const int32_t* d_a_right, int64_t n_a,
+                    const int32_t* d_b_left, const int32_t* d_b_right, int64_t n_b, int64_t n_left_rows,
+                    uint8_t* d_flags);
+
 /* Brute-force point x polygon join that allocates no device memory, for
  * callers that cannot allocate (a host that owns all device memory in a
  * fixed arena, a process on a hard memory budget).  No counterpart in the

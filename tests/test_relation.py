@@ -1,6 +1,6 @@
 """Row-flow carriers (Relation, RowSet, Expression) over numpy arrays and
-over torch tensors (the join's device output; CPU tensors here run the same
-torch code as CUDA ones), and SpatialIndex.query_pair_aggregate on tensor pairs."""
+over CUDA tensors (the join's device output, reduced by the library's
+row-reduction kernels), and SpatialIndex.query_pair_aggregate on device pairs."""
 import numpy as np
 import pytest
 import torch
@@ -10,12 +10,15 @@ from vibespatial_b200 import query
 from vibespatial_b200.relation import Expression, Relation, RowSet
 
 
-@pytest.mark.parametrize("kind", ["numpy", "torch"])
+KINDS = ["numpy", pytest.param("torch", marks=pytest.mark.gpu)]
+
+
+@pytest.mark.parametrize("kind", KINDS)
 def test_relation_reductions(kind):
     left = np.array([0, 0, 2, 2, 2, 5], np.int32)
     right = np.array([1, 3, 0, 1, 3, 3], np.int32)
     if kind == "torch":
-        left, right = torch.from_numpy(left), torch.from_numpy(right)
+        left, right = torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda()
     rel = Relation(left, right, predicate="intersects", left_row_count=7, right_row_count=4, sorted_by_left=True)
     assert len(rel) == 6 and rel.is_device == (kind == "torch")
     assert rel.left_match_count_expression().to_numpy().tolist() == [2, 0, 3, 0, 0, 1, 0]
@@ -23,14 +26,15 @@ def test_relation_reductions(kind):
     semi = rel.left_semijoin_rowset()
     assert semi.to_numpy().tolist() == [0, 2, 5] and semi.source_row_count == 7
     assert semi.complement().to_numpy().tolist() == [1, 3, 4, 6]
+    assert rel.left_antijoin_rowset().to_numpy().tolist() == [1, 3, 4, 6]
     assert rel.right_semijoin_rowset().to_numpy().tolist() == [0, 1, 3]
     assert rel.to_numpy().tolist() == [[0, 0, 2, 2, 2, 5], [1, 3, 0, 1, 3, 3]]
 
 
-@pytest.mark.parametrize("kind", ["numpy", "torch"])
+@pytest.mark.parametrize("kind", KINDS)
 def test_empty_relation(kind):
     e = np.zeros(0, np.int32)
-    left, right = (e, e.copy()) if kind == "numpy" else (torch.from_numpy(e), torch.from_numpy(e.copy()))
+    left, right = (e, e.copy()) if kind == "numpy" else (torch.from_numpy(e).cuda(), torch.from_numpy(e.copy()).cuda())
     rel = Relation(left, right, left_row_count=3, right_row_count=2)
     assert len(rel) == 0 and rel.to_numpy().shape == (2, 0)
     assert rel.left_semijoin_rowset().to_numpy().tolist() == []
@@ -49,9 +53,10 @@ def test_expression_and_rowset_checks():
     assert rs.complement().to_numpy().tolist() == [0, 2, 3]
 
 
+@pytest.mark.gpu
 def test_pair_aggregate_on_tensor_pairs(monkeypatch):
-    """The tensor branch of query_pair_aggregate (torch.isin over pair keys)
-    gives the numpy branch's counts."""
+    """The device branch of query_pair_aggregate (vs_pairs_member and masked
+    vs_row_counts on the pairs) gives the numpy branch's counts."""
     a_pairs = {"l": np.array([0, 1, 1, 3, 4, 4]), "r": np.array([0, 0, 1, 2, 0, 1])}
     b_pairs = {"l": np.array([0, 1, 1, 3]), "r": np.array([0, 0, 1, 3])}
     tree_a = vs.GeometryArray.from_shapes([vs.box(0, 0, 1, 1)] * 4)
@@ -62,7 +67,7 @@ def test_pair_aggregate_on_tensor_pairs(monkeypatch):
         def rows(self, arr, predicate, distance):
             p = a_pairs if self.geometry is tree_a else b_pairs
             l, r = p["l"].astype(np.int32), p["r"].astype(np.int32)
-            return (torch.from_numpy(l), torch.from_numpy(r)) if as_tensor else (l, r)
+            return (torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) if as_tensor else (l, r)
         return rows
 
     out = {}

@@ -25,6 +25,45 @@ def test_shard_range_covers_everything_once():
         shard_range(10, 2, 2)
 
 
+def test_hilbert_keys_follow_the_device_curve():
+    """The host keys that cut Hilbert-range shards are the device curve's keys (16 levels)."""
+    from vibespatial_b200 import _abi
+    from vibespatial_b200.sharding import hilbert_keys_np
+
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-5, 5, 2000)
+    y = rng.uniform(10, 30, 2000)
+    frame = (-5.0, 10.0, 5.0, 30.0)
+    keys = hilbert_keys_np(x, y, frame)
+    side = (1 << 16) - 1
+    gx = np.clip((x + 5.0) / 10.0 * side, 0, side).astype(np.uint32)
+    gy = np.clip((y - 10.0) / 20.0 * side, 0, side).astype(np.uint32)
+    exp = [_abi.hilbert_key_host(int(a) << 16, int(b) << 16, 16) for a, b in zip(gx, gy)]
+    np.testing.assert_array_equal(keys, np.array(exp, np.uint32))
+    x[::5] = np.nan
+    assert (hilbert_keys_np(x, y, frame)[::5] == 0xFFFFFFFF).all()
+
+
+def test_hilbert_shards_partition_rows_and_stay_compact():
+    from vibespatial_b200.sharding import hilbert_shard_rows
+
+    rng = np.random.default_rng(5)
+    x = rng.uniform(0, 1000, 100_003)
+    y = rng.uniform(0, 1000, 100_003)
+    x[::97] = np.nan  # empty points go to the last shard
+    for world in (1, 2, 3, 4, 8):
+        shards = [hilbert_shard_rows(x, y, r, world) for r in range(world)]
+        allr = np.concatenate(shards)
+        assert len(allr) == len(x) and len(np.unique(allr)) == len(x)
+        sizes = [len(s) for s in shards]
+        assert max(sizes) - min(sizes) <= 1
+        if world == 4:  # a quarter of uniform points covers well under the whole frame's box
+            for s in shards[:-1]:
+                area = np.ptp(x[s]) * np.ptp(y[s])
+                assert area < 0.6 * 1000 * 1000, area
+    assert np.isnan(x[hilbert_shard_rows(x, y, 3, 4)[-1]])
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -59,6 +98,12 @@ def _worker(rank, world, port, out_dir):
 
         left, right, counts = sharded_join(points, polys, "within", pairs_fn=pairs_fn)
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), left=left, right=right, counts=counts)
+        # Hilbert-range shards, pairs assembled on rank 0 (None elsewhere)
+        al, ar, ac = sharded_join(points, polys, "within", pairs_fn=pairs_fn, shard="hilbert", assemble=True)
+        if rank == 0:
+            np.savez(os.path.join(out_dir, "assembled.npz"), left=al, right=ar, counts=ac)
+        else:
+            assert al is None and ar is None
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -86,6 +131,11 @@ def test_two_rank_gloo_sharded_join(tmp_path, oracle):
     np.testing.assert_array_equal(right[o], er)
     # rank 0 holds the lower half of the points
     assert parts[0]["left"].max() < parts[1]["left"].min()
+    # Hilbert-range shards assembled on rank 0: the single-process pair set, sorted
+    a = np.load(tmp_path / "assembled.npz")
+    np.testing.assert_array_equal(a["left"], el)
+    np.testing.assert_array_equal(a["right"], er)
+    assert a["counts"].sum() == len(el) and (a["counts"] > 0).all()
 
 
 def _distance_worker(rank, world, port, out_dir):
@@ -135,6 +185,12 @@ def _distance_worker(rank, world, port, out_dir):
                                                                              pairs_fn=nearest_fn)
         out["np_l"], out["np_r"], out["np_d"], out["np_c"] = sharded_nearest_polygons(polys, points,
                                                                                      pairs_fn=nearest_polygons_fn)
+        # distances travel with their pairs through the assembly
+        hl, hr, hd, hc = sharded_nearest(points, polys, max_distance=25.0, pairs_fn=nearest_fn, shard="hilbert",
+                                         assemble=True)
+        if rank == 0:
+            out["hn_l"], out["hn_r"], out["hn_d"] = hl, hr, hd
+        dist.barrier()
         np.savez(os.path.join(out_dir, f"dist_rank{rank}.npz"), **out)
         dist.barrier()
     finally:
@@ -170,6 +226,8 @@ def test_two_rank_gloo_sharded_distance_joins(tmp_path, oracle):
         for g, e in zip(got, exp):
             np.testing.assert_array_equal(g, e)
         assert len(got[0]) > 0
+    for g, e in zip((parts[0]["hn_l"], parts[0]["hn_r"], parts[0]["hn_d"]), expected["nn"]):
+        np.testing.assert_array_equal(g, e)
 
 
 @pytest.mark.gpu

@@ -31,7 +31,8 @@ EXPORTED = (
     "vs_join_brute_noalloc", "vs_batch_plan_create", "vs_batch_run", "vs_batch_plan_free",
     "vs_wkb_plan_create", "vs_wkb_plan_decode", "vs_wkb_plan_free", "vs_join_host",
     "vs_thread_kernel_launches", "vs_join_dwithin", "vs_join_nearest", "vs_join_export",
-    "vs_distance_aligned", "vs_join_nearest_polygons",
+    "vs_distance_aligned", "vs_join_nearest_polygons", "vs_row_counts", "vs_row_sums", "vs_select_rows",
+    "vs_pairs_member",
 )
 
 
@@ -182,6 +183,10 @@ def load(path: Path | str | None = None):
             "vs_wkb_plan_free": (ctypes.c_int, [vp]),
             "vs_join_host": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i32, i32, u32, vp, vp, i64, ctypes.POINTER(i64),
                                             ctypes.POINTER(JoinStats)]),
+            "vs_row_counts": (ctypes.c_int, [vp, vp, vp, i64, i64, vp]),
+            "vs_row_sums": (ctypes.c_int, [vp, vp, vp, i64, i64, vp, i64, vp]),
+            "vs_select_rows": (ctypes.c_int, [vp, vp, i64, i32, vp, ctypes.POINTER(i64)]),
+            "vs_pairs_member": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, i64, i64, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -619,6 +624,60 @@ def join_brute_noalloc(pts: Points, polys: Polygons, predicate: int, left, right
                                           _ptr(right), cap, ctypes.byref(n), ctypes.c_void_p(stream))
     check(status, required=int(n.value))
     return int(n.value)
+
+
+def _i32_dev(a):
+    """The int32 contiguous form of a device row array (no copy when it already is)."""
+    import torch
+
+    return a.contiguous() if a.dtype == torch.int32 else a.to(torch.int32).contiguous()
+
+
+def row_counts(ctx: Context, rows, n_rows: int, mask=None):
+    """int64 device tensor: pairs per row 0..n_rows-1, over the pairs where ``mask`` (bool / uint8 device
+    tensor) is set when given (vs_row_counts)."""
+    import torch
+
+    r = _i32_dev(rows)
+    m = None if mask is None else mask.to(torch.uint8).contiguous()
+    out = torch.empty(max(int(n_rows), 0), dtype=torch.int64, device=r.device)
+    check(load().vs_row_counts(ctx.handle, _ptr(r), _ptr(m), int(r.numel()), int(n_rows), _ptr(out)))
+    return out
+
+
+def row_sums(ctx: Context, rows, cols, values, n_rows: int):
+    """float64 device tensor: per row, the sum of values[cols] over its pairs in pair order (rows ascending;
+    vs_row_sums)."""
+    import torch
+
+    r, c = _i32_dev(rows), _i32_dev(cols)
+    v = values.to(device=r.device, dtype=torch.float64).contiguous()
+    out = torch.empty(max(int(n_rows), 0), dtype=torch.float64, device=r.device)
+    check(load().vs_row_sums(ctx.handle, _ptr(r), _ptr(c), int(r.numel()), int(n_rows), _ptr(v), int(v.numel()),
+                             _ptr(out)))
+    return out
+
+
+def select_rows(ctx: Context, counts, matched: bool = True):
+    """int32 device tensor: ascending rows whose count is > 0 (matched) or == 0 (vs_select_rows)."""
+    import torch
+
+    c = counts.to(torch.int64).contiguous()
+    out = torch.empty(max(int(c.numel()), 1), dtype=torch.int32, device=c.device)
+    n = ctypes.c_int64(0)
+    check(load().vs_select_rows(ctx.handle, _ptr(c), int(c.numel()), 1 if matched else 0, _ptr(out), ctypes.byref(n)))
+    return out[:n.value]
+
+
+def pairs_member(ctx: Context, a_left, a_right, b_left, b_right, n_left_rows: int):
+    """bool device tensor: pair k of a is also a pair of b (b sorted by (left, right); vs_pairs_member)."""
+    import torch
+
+    al, ar, bl, br = (_i32_dev(t) for t in (a_left, a_right, b_left, b_right))
+    flags = torch.empty(max(int(al.numel()), 1), dtype=torch.uint8, device=al.device)
+    check(load().vs_pairs_member(ctx.handle, _ptr(al), _ptr(ar), int(al.numel()), _ptr(bl), _ptr(br),
+                                 int(bl.numel()), int(n_left_rows), _ptr(flags)))
+    return flags[:al.numel()].bool()
 
 
 def sort_pairs(ctx: Context, left, right) -> None:

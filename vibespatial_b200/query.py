@@ -250,16 +250,11 @@ class SpatialIndex:
         sindex.query_any (src/vibespatial/api/sindex.py:594)."""
         import pandas as pd
 
+        from .relation import _counts, _to_numpy
+
         arr, index = self._input(geometry)
         rows, _ = self._pair_rows(arr, predicate, distance)
-        n = len(arr)
-        if isinstance(rows, np.ndarray):
-            hit = np.bincount(rows, minlength=n)[:n] > 0 if len(rows) else np.zeros(n, bool)
-        else:
-            import torch
-
-            hit = (torch.bincount(rows.long(), minlength=n)[:n] > 0).cpu().numpy() if rows.numel() else \
-                np.zeros(n, bool)
+        hit = _to_numpy(_counts(rows, len(arr))) > 0
         return pd.Series(hit, index=index)
 
     def query_aggregate(self, geometry, aggregations, *, predicate=None, distance=None):
@@ -312,19 +307,19 @@ class SpatialIndex:
                 else:
                     out[name] = np.bincount(rows, weights=v[trows], minlength=n)[:n] if len(rows) else np.zeros(n)
         else:
+            # the library's row-reduction kernels on the join's device pairs
+            # (sorted by query row, as the sums need): vs_row_counts, vs_row_sums
             import torch
 
-            r = rows.long()
+            from . import _abi
+
+            ctx = _abi.default_context(rows.device.index if rows.device.index is not None else 0)
             for name, v in specs.items():
                 if v is None:
-                    c = torch.bincount(r, minlength=n)[:n] if r.numel() else torch.zeros(n, dtype=torch.int64)
-                    out[name] = c.cpu().numpy().astype(np.int64)
+                    out[name] = _abi.row_counts(ctx, rows, n).cpu().numpy()
                 else:
-                    acc = torch.zeros(n, dtype=torch.float64, device=r.device)
-                    if r.numel():
-                        dv = torch.from_numpy(v).to(r.device)
-                        acc.index_add_(0, r, dv[trows.long()])
-                    out[name] = acc.cpu().numpy()
+                    dv = torch.from_numpy(v).to(rows.device)
+                    out[name] = _abi.row_sums(ctx, rows, trows, dv, n).cpu().numpy()
         return pd.DataFrame(out, index=index)
 
     # -- row flow without exported pairs (the reference's private relation
@@ -355,7 +350,7 @@ class SpatialIndex:
     def query_left_antijoin(self, geometry, *, predicate=None, distance=None):
         """Query rows without any match, ascending: sindex.query_left_antijoin
         (src/vibespatial/api/sindex.py:1660)."""
-        return self.query_left_semijoin(geometry, predicate=predicate, distance=distance).complement()
+        return self.query_relation(geometry, predicate=predicate, distance=distance).left_antijoin_rowset()
 
     def query_right_semijoin(self, geometry, *, predicate=None, distance=None):
         """Indexed rows matched by at least one query geometry, ascending:
@@ -391,13 +386,15 @@ class SpatialIndex:
         right = b.right_match_count_expression().to_numpy()
         # pairs are unique, so the pairs of a also present in b are the shared ones
         if a.is_device and b.is_device:
-            import torch
+            # membership of a's pairs among b's (b sorted by (query row, indexed
+            # row), as the join returns them), then counts of the shared pairs'
+            # indexed rows: vs_pairs_member, vs_row_counts
+            from . import _abi
 
-            ka = a.right_indices.long() * nq + a.left_indices.long()
-            kb = b.right_indices.long() * nq + b.left_indices.long()
-            shared_rows = a.right_indices[torch.isin(ka, kb)] if ka.numel() and kb.numel() else a.right_indices[:0]
-            shared = torch.bincount(shared_rows.long(), minlength=m)[:m].cpu().numpy() if shared_rows.numel() else \
-                np.zeros(m, np.int64)
+            dev = a.left_indices.device.index if a.left_indices.device.index is not None else 0
+            ctx = _abi.default_context(dev)
+            flags = _abi.pairs_member(ctx, a.left_indices, a.right_indices, b.left_indices, b.right_indices, nq)
+            shared = _abi.row_counts(ctx, a.right_indices, m, mask=flags).cpu().numpy()
         else:
             ar, al = np.asarray(a.right_indices, np.int64), np.asarray(a.left_indices, np.int64)
             br, bl = np.asarray(b.right_indices, np.int64), np.asarray(b.left_indices, np.int64)

@@ -27,16 +27,30 @@ def _size(a) -> int:
     return int(a.shape[0]) if _is_numpy(a) else int(a.numel())
 
 
-def _counts(rows, n: int):
-    """Occurrences of 0..n-1 in ``rows`` (int64, same device as ``rows``)."""
-    if _is_numpy(rows):
-        return np.bincount(rows.astype(np.int64), minlength=n)[:n].astype(np.int64) if len(rows) else \
-            np.zeros(n, np.int64)
-    import torch
+def _ctx(t):
+    from . import _abi
 
-    if rows.numel() == 0:
-        return torch.zeros(n, dtype=torch.int64, device=rows.device)
-    return torch.bincount(rows.long(), minlength=n)[:n]
+    return _abi, _abi.default_context(t.device.index if t.device.index is not None else 0)
+
+
+def _counts(rows, n: int, mask=None):
+    """Occurrences of 0..n-1 in ``rows`` (int64, same device as ``rows``), over
+    the pairs where ``mask`` is set when given; device arrays are counted by
+    the library's row-count kernel (vs_row_counts)."""
+    if _is_numpy(rows):
+        r = rows.astype(np.int64) if mask is None else rows[np.asarray(mask, bool)].astype(np.int64)
+        return np.bincount(r, minlength=n)[:n].astype(np.int64) if len(r) else np.zeros(n, np.int64)
+    abi, ctx = _ctx(rows)
+    return abi.row_counts(ctx, rows, n, mask)
+
+
+def _matched_rows(counts, matched: bool = True):
+    """Ascending rows whose count is > 0 (``matched``) or == 0: the
+    semijoin / antijoin row sets (vs_select_rows on the device)."""
+    if _is_numpy(counts):
+        return np.flatnonzero(counts > 0 if matched else counts == 0).astype(np.int64)
+    abi, ctx = _ctx(counts)
+    return abi.select_rows(ctx, counts, matched)
 
 
 def _nonzero(flags):
@@ -82,12 +96,17 @@ class Relation:
     def left_semijoin_rowset(self) -> "RowSet":
         """Query rows with at least one match, ascending."""
         c = self.left_match_count_expression().values
-        return RowSet(_nonzero(c > 0), source_row_count=int(self.left_row_count), unique=True)
+        return RowSet(_matched_rows(c, True), source_row_count=int(self.left_row_count), unique=True)
+
+    def left_antijoin_rowset(self) -> "RowSet":
+        """Query rows without any match, ascending."""
+        c = self.left_match_count_expression().values
+        return RowSet(_matched_rows(c, False), source_row_count=int(self.left_row_count), unique=True)
 
     def right_semijoin_rowset(self) -> "RowSet":
         """Indexed rows with at least one match, ascending."""
         c = self.right_match_count_expression().values
-        return RowSet(_nonzero(c > 0), source_row_count=int(self.right_row_count), unique=True)
+        return RowSet(_matched_rows(c, True), source_row_count=int(self.right_row_count), unique=True)
 
     def to_numpy(self) -> np.ndarray:
         """The (2, K) intp pairs of sindex.query."""
