@@ -145,10 +145,10 @@ WORKLOAD_DESC = {
 }
 
 
-def algorithmic_bytes(w, n_pairs: int) -> int:
+def algorithmic_bytes(w, n_pairs: int, n_points: int | None = None) -> int:
     """Bytes the join must move at least once: points, polygon SoA, pair output."""
     p = w.polys
-    return int(16 * w.n_points + 16 * p.n_coords + 4 * (len(p.ring_off) + len(p.part_off) + len(p.geom_off))
+    return int(16 * (w.n_points if n_points is None else n_points) + 16 * p.n_coords + 4 * (len(p.ring_off) + len(p.part_off) + len(p.geom_off))
                + 8 * n_pairs)
 
 
@@ -633,7 +633,9 @@ def run_distance(args, rank, world, local_rank):
         total_ms, e2e_med = float(t[0]), float(t[1])
     else:
         e2e_med = float(np.median(e2e_ms))
-    value = world * N * args.steps / (total_ms / 1e3)
+    # points every rank processed per step: N each (weak), or the one dataset (sharded)
+    n_job = w.n_points if sharded else world * N
+    value = n_job * args.steps / (total_ms / 1e3)
     if rank != 0:
         return
     peak, peak_kind = _peaks()
@@ -999,8 +1001,19 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         import torch.distributed as tdist
 
-    w = make_workload(args.workload, rank, args.scale)
-    N = w.n_points
+    # default: every rank joins a dataset of its own (weak scaling); with
+    # --shard hilbert all ranks hold one dataset and each joins its
+    # Hilbert-range shard of the points (strong scaling), pairs assembled on rank 0
+    sharded = args.shard == "hilbert"
+    w = make_workload(args.workload, 0 if sharded else rank, args.scale)
+    rows = None
+    px, py = w.px, w.py
+    if sharded:
+        from vibespatial_b200.sharding import hilbert_shard_rows
+
+        rows = hilbert_shard_rows(w.px, w.py, rank, world)
+        px, py = np.ascontiguousarray(w.px[rows]), np.ascontiguousarray(w.py[rows])
+    N = len(px)
     ctx = _abi.Context(dev)
     stream = ctx.torch_stream
     pol = w.polys
@@ -1015,8 +1028,8 @@ def run_ours(args, rank, world, local_rank):
     build_wall = time.perf_counter() - t0
     info = index.info()
     del d_poly
-    dx = torch.from_numpy(w.px).to(dev)
-    dy = torch.from_numpy(w.py).to(dev)
+    dx = torch.from_numpy(px).to(dev)
+    dy = torch.from_numpy(py).to(dev)
     pts = _abi.make_points(dx, dy)
     # learned + batched: the join as a one-job batch plan (the persistent
     # learned pipeline replayed from a CUDA graph)
@@ -1026,6 +1039,31 @@ def run_ours(args, rank, world, local_rank):
         if plan is not None:
             return plan.run_into(pred, lft, rgt, use_graph=True)
         return index.join_into(pts, pred, method, lft, rgt)
+
+    assembled = {}
+
+    def assemble(lft, rgt, n_local):
+        """Sharded mode, N > 1: every rank's pairs (shard-local point rows)
+        sent to rank 0 over NCCL, sized by an all-gather of the counts."""
+        with torch.cuda.stream(stream):
+            cnt = torch.tensor([n_local], dtype=torch.int64, device=dev)
+            allc = [torch.zeros(1, dtype=torch.int64, device=dev) for _ in range(world)]
+            tdist.all_gather(allc, cnt)
+            counts = [int(c.item()) for c in allc]
+            if rank == 0:
+                if "l" not in assembled:
+                    assembled["l"] = torch.empty(max(1, sum(counts)), dtype=torch.int32, device=dev)
+                    assembled["r"] = torch.empty(max(1, sum(counts)), dtype=torch.int32, device=dev)
+                off = counts[0]
+                for r in range(1, world):
+                    if counts[r]:
+                        tdist.recv(assembled["l"][off:off + counts[r]], src=r)
+                        tdist.recv(assembled["r"][off:off + counts[r]], src=r)
+                    off += counts[r]
+            elif n_local:
+                tdist.send(lft[:n_local], dst=0)
+                tdist.send(rgt[:n_local], dst=0)
+        return counts
 
     # size the pair buffers once (exact count from a first join)
     cap = max(1024, N)
@@ -1046,7 +1084,9 @@ def run_ours(args, rank, world, local_rank):
         assert n_plain == n_pairs, (n_plain, n_pairs)
 
     for _ in range(args.warmup):
-        join(left, right)
+        n_w, _ = join(left, right)
+        if sharded and dist:
+            assemble(left, right, n_w)
     if dist:
         tdist.barrier()
     torch.cuda.synchronize()
@@ -1060,6 +1100,8 @@ def run_ours(args, rank, world, local_rank):
         for k in range(args.steps):
             ev[k][0].record(stream)
             n_k, st = join(left, right)
+            if sharded and dist:
+                assemble(left, right, n_k)
             ev[k][1].record(stream)
             kernel_ms.append(st["kernel_ms"])
             phases.append(st["phase_ms"])
@@ -1098,8 +1140,8 @@ def run_ours(args, rank, world, local_rank):
                 ablations["plain_rtree_ms"] = plain
         # e2e through the C-ABI with HOST buffers (vs_join_host): pinned host
         # points in, pinned host pairs out, the chunked copies overlapping the join
-        hx = torch.from_numpy(w.px).pin_memory()
-        hy = torch.from_numpy(w.py).pin_memory()
+        hx = torch.from_numpy(px).pin_memory()
+        hy = torch.from_numpy(py).pin_memory()
         hl = torch.empty(cap, dtype=torch.int32).pin_memory()
         hr = torch.empty(cap, dtype=torch.int32).pin_memory()
         e2e_ms = []
@@ -1120,6 +1162,8 @@ def run_ours(args, rank, world, local_rank):
         _abi.sort_pairs(ctx, gl_chk, gr_chk)
     gl_chk, gr_chk = gl_chk.cpu().numpy(), gr_chk.cpu().numpy()
     hl_chk, hr_chk = hl[:n_e].numpy().copy(), hr[:n_e].numpy().copy()
+    if rows is not None:  # shard-local point rows -> the dataset's rows
+        gl_chk, hl_chk = rows[gl_chk], rows[hl_chk]
     total_ms = float(sum(step_ms))
     if dist:
         t = torch.tensor([total_ms, float(np.median(e2e_ms))], device=dev, dtype=torch.float64)
@@ -1127,12 +1171,14 @@ def run_ours(args, rank, world, local_rank):
         total_ms, e2e_med = float(t[0]), float(t[1])
     else:
         e2e_med = float(np.median(e2e_ms))
-    value = world * N * args.steps / (total_ms / 1e3)
+    # points every rank processed per step: N each (weak), or the one dataset (sharded)
+    n_job = w.n_points if sharded else world * N
+    value = n_job * args.steps / (total_ms / 1e3)
     if rank != 0:
         return
     peak, peak_kind = _peaks()
     kmed = float(np.median(kernel_ms))
-    B = algorithmic_bytes(w, n_pairs)
+    B = algorithmic_bytes(w, n_pairs, N)
     achieved = B / (kmed / 1e3) / 1e9
     traffic = None
     prof = ROOT / "profiles" / f"traffic_{args.workload}_{args.method}.json"
@@ -1157,11 +1203,14 @@ def run_ours(args, rank, world, local_rank):
     e32, e64 = st.get("fp32_edges", 0), st.get("fp64_edges", 0)
     line = {
         "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if sharded else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": join_config(args, w),
         "method": args.method, "n_pairs": n_pairs,
-        "parallelism": f"points sharded over {world} GPU(s), index replicated",
+        "parallelism": (f"one dataset, Hilbert-range shards of the points over {world} GPU(s), index replicated, "
+                        "pairs assembled on rank 0 (NCCL send/recv) every step" if sharded else
+                        f"points sharded over {world} GPU(s), index replicated"),
         "index": {"build_ms": info["build_ms"], "build_wall_s": build_wall, "device_bytes": info["device_bytes"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel_ms": kmed,
@@ -1171,7 +1220,7 @@ def run_ours(args, rank, world, local_rank):
         "split_precision": {"fp32_edges": e32, "fp64_edges": e64,
                             "fp32_pass_rate": (e32 / (e32 + e64)) if e32 + e64 else None,
                             "exact_fallbacks": st.get("exact_fallbacks", 0)},
-        "e2e": {"value": world * N / (e2e_med / 1e3), "unit": "points/s",
+        "e2e": {"value": n_job / (e2e_med / 1e3), "unit": "points/s",
                 "h2d_bytes_per_step": int(16 * N), "d2h_bytes_per_step": int(8 * n_pairs)},
         "gpu_launches": launches,
         "phases_ms": dict(zip(PHASES, (float(v) for v in np.median(np.array(phases), axis=0)))),
@@ -1395,6 +1444,9 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-sample", type=int, default=4_000_000)
+    ap.add_argument("--shard", choices=["none", "hilbert"], default="none",
+                    help="none: each rank joins its own dataset (weak scaling); hilbert: one dataset, each rank "
+                         "joins a Hilbert-range shard of its points and rank 0 assembles the pairs (strong scaling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ring-bin-min", type=int, default=0,
                     help="rings with at least this many vertices get y-bins (0: library default, <0: none)")

@@ -160,13 +160,16 @@ __device__ __forceinline__ int ring_location_split(float qx, float qy, float t, 
     if (end - start < 2) return LOC_OUTSIDE;
     bool inside = false;
     float2 a = xy32[end - 1];
+    float2 b = xy32[start];
     int ia = end - 1;
     for (int i = start; i < end; ++i) {
-        const float2 b = xy32[i];
+        // the next vertex's load is in flight while this edge is decided
+        const float2 nb = xy32[i + 1 < end ? i + 1 : i];
         const int r = split_edge(qx, qy, t, a, b, xy, ia, i, P, inside, n32, n64);
         if (r == 1) return LOC_BOUNDARY;
         if (r == 2) return LOC_UNDECIDED;
         a = b;
+        b = nb;
         ia = i;
     }
     return inside ? LOC_INTERIOR : LOC_OUTSIDE;
