@@ -1033,7 +1033,23 @@ def run_ours(args, rank, world, local_rank):
     pts = _abi.make_points(dx, dy)
     # learned + batched: the join as a one-job batch plan (the persistent
     # learned pipeline replayed from a CUDA graph)
-    plan = _abi.BatchPlan(ctx, [index], pts, [0, N], options={"method": _abi.METHOD_LEARNED}) if batched else None
+    plan = None
+    plan_opts, plan_opts_src = None, None
+    if batched:
+        from vibespatial_b200 import autotune
+
+        # launch shape from the autotuner (cached, else searched now, before any timing)
+        probe_cap = max(1024, N)
+        pl = torch.empty(probe_cap, dtype=torch.int32, device=dev)
+        pr = torch.empty(probe_cap, dtype=torch.int32, device=dev)
+        try:
+            plan_opts, plan_opts_src = autotune.tuned_options(
+                ctx, [index], pts, [0, N], pred, len(w.polys), left=pl, right=pr, use_cache=not args.autotune,
+                method=_abi.METHOD_LEARNED, with_source=True)
+        except _abi.CapacityError:  # more pairs than points: keep the defaults
+            plan_opts, plan_opts_src = dict(autotune.LEARNED_DEFAULTS), "defaults (pairs exceed the probe buffer)"
+        del pl, pr
+        plan = _abi.BatchPlan(ctx, [index], pts, [0, N], options=dict(plan_opts, method=_abi.METHOD_LEARNED))
 
     def join(lft, rgt):
         if plan is not None:
@@ -1135,7 +1151,7 @@ def run_ours(args, rank, world, local_rank):
                 dph.append(index.join_into(pts, pred, _abi.METHOD_LEARNED, left, right)[1]["phase_ms"])
             phases = dph
             ablations = learned_ablations(_abi, ctx, [index], pts, [0, N], pred, left, right, n_pairs,
-                                          {"method": _abi.METHOD_LEARNED}, max(3, args.steps // 2))
+                                          dict(plan_opts, method=_abi.METHOD_LEARNED), max(3, args.steps // 2))
             if plain is not None:
                 ablations["plain_rtree_ms"] = plain
         # e2e through the C-ABI with HOST buffers (vs_join_host): pinned host
@@ -1229,6 +1245,9 @@ def run_ours(args, rank, world, local_rank):
     }
     if ablations is not None:
         line["ablations"] = ablations
+    if plan_opts is not None:
+        line["launch_shape"] = plan_opts
+        line["launch_shape_source"] = plan_opts_src
     if plain is not None:
         line["plain_rtree_ms"] = plain
         line["plain_rtree_bulk_leaves_ms"] = plain_bulk
@@ -1284,19 +1303,12 @@ def run_batched(args, rank, world, local_rank):
     right = torch.empty(cap, dtype=torch.int32, device=dev)
     name, sms = autotune.device_identity(dev)
     key = autotune.cache_key(name, sms, autotune.shape_class(len(jobs), N, n_polys), pred)
-    tune_s = None
-    if learned:
-        opts, opts_src = {}, "learned pipeline (no R-tree launch shape)"
-    elif args.autotune:
-        t1 = time.perf_counter()
-        opts = autotune.tuned_options(ctx, indexes, pts, job_start, pred, n_polys, left=left, right=right,
-                                      use_cache=False)
-        tune_s = time.perf_counter() - t1
-        opts_src = "searched"
-    else:
-        opts = autotune.lookup(key)
-        opts_src = "cache" if opts else "defaults"
-        opts = opts or dict(autotune.DEFAULTS)
+    # launch shape of the timed plan: the autotuner's (cached, else searched
+    # now, before the timed region); --autotune forces a fresh search
+    t1 = time.perf_counter()
+    opts, opts_src = autotune.tuned_options(ctx, indexes, pts, job_start, pred, n_polys, left=left, right=right,
+                                            use_cache=not args.autotune, method=bmethod, with_source=True)
+    tune_s = time.perf_counter() - t1
     plan = _abi.BatchPlan(ctx, indexes, pts, job_start, options=dict(opts, method=bmethod))
     for _ in range(args.warmup):
         n_w, _ = plan.run_into(pred, left, right, use_graph=True)
@@ -1324,8 +1336,9 @@ def run_batched(args, rank, world, local_rank):
         rtree_batch_ms = None
         ablations = None
         if learned:
-            rplan = _abi.BatchPlan(ctx, indexes, pts, job_start,
-                                   options=dict(autotune.lookup(key) or autotune.DEFAULTS, method=_abi.METHOD_RTREE))
+            ropts = autotune.tuned_options(ctx, indexes, pts, job_start, pred, n_polys, left=left, right=right,
+                                           use_cache=not args.autotune, method=_abi.METHOD_RTREE)
+            rplan = _abi.BatchPlan(ctx, indexes, pts, job_start, options=dict(ropts, method=_abi.METHOD_RTREE))
             rms = []
             for k in range(3 + max(3, args.steps // 2)):
                 n_r, st_r = rplan.run_into(pred, left, right, use_graph=True)

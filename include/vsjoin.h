@@ -312,6 +312,7 @@ typedef struct vs_batch_options {
     int32_t learned_refine_blocks_per_sm; /* learned: refine pass blocks per SM (0 = as many as fit) */
     int32_t learned_grab;     /* learned: grouped points a refine warp takes per grab (0 = 32; rounded up to 32s) */
     uint32_t learned_flags;   /* learned: VS_JOIN_LEARNED_BSEARCH | VS_JOIN_LEARNED_FP64_WALK (ablations) */
+    int32_t learned_map_packets; /* learned: 32-point packets a map warp looks up together, 1 or 2 (0 = 1) */
 } vs_batch_options;
 
 /* At most 4096 jobs and 2^31-1 points in total. */

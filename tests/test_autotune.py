@@ -54,3 +54,22 @@ def test_cache_tolerates_garbage_and_partial_entries(tmp_path, monkeypatch):
     assert at.lookup("k", p) == {**at.DEFAULTS, "sort_levels": 12}
     monkeypatch.setenv(at.CACHE_ENV, str(p))
     assert at.cache_path() == p
+
+
+def test_learned_space_and_keys(tmp_path):
+    """The learned pipeline has its own defaults, search space and cache entries (the R-tree's stay apart)."""
+    d, sp = at.space_for(at.METHOD_LEARNED)
+    assert d == at.LEARNED_DEFAULTS and sp == at.LEARNED_SPACE
+    assert all(d[k] in sp[k] for k in d)
+    kr = at.cache_key("NVIDIA B200", 148, "j8-p17-g12", 2)
+    kl = at.cache_key("NVIDIA B200", 148, "j8-p17-g12", 2, at.METHOD_LEARNED)
+    assert kr != kl
+    p = tmp_path / "tune.json"
+    at.store(kl, {"learned_map_blocks_per_sm": 4, "learned_refine_blocks_per_sm": 5, "learned_grab": 64}, 3.4, p)
+    assert at.lookup(kr, p) is None
+    assert at.lookup(kl, p, at.METHOD_LEARNED) == {"learned_map_blocks_per_sm": 4, "learned_map_packets": 1,
+                                                   "learned_refine_blocks_per_sm": 5, "learned_grab": 64}
+    target = {"learned_map_blocks_per_sm": 4, "learned_map_packets": 2, "learned_refine_blocks_per_sm": 3,
+              "learned_grab": 128}
+    best, ms, _ = at.search(lambda o: sum((o[k] - target[k]) ** 2 for k in target), space=sp, start=d)
+    assert best == target and ms == 0

@@ -209,7 +209,8 @@ def test_learned_batch_matches_oracle(lbatch, oracle, predicate, use_graph):
 
 @pytest.mark.parametrize("options", [
     {"learned_map_blocks_per_sm": 1, "learned_refine_blocks_per_sm": 1, "learned_grab": 32},
-    {"learned_map_blocks_per_sm": 3, "learned_refine_blocks_per_sm": 2, "learned_grab": 100},
+    {"learned_map_blocks_per_sm": 3, "learned_refine_blocks_per_sm": 2, "learned_grab": 100, "learned_map_packets": 2},
+    {"learned_refine_blocks_per_sm": 5, "learned_map_packets": 2},
     {"learned_grab": 4096, "learned_flags": 4},
     {"learned_refine_blocks_per_sm": 8, "learned_flags": 8},
 ])
@@ -227,8 +228,38 @@ def test_learned_batch_launch_shapes_do_not_change_pairs(vsabi, ctx, oracle, opt
             np.testing.assert_array_equal(r, er)
 
 
+def test_learned_autotune_round_trip(vsabi, ctx, lbatch, tmp_path):
+    """The autotuner searches the learned pipeline's launch shape, caches it, and the tuned plan gives the
+    default plan's pairs."""
+    import torch
+
+    from vibespatial_b200 import autotune as at
+
+    left = torch.empty(1 << 20, dtype=torch.int32, device="cuda")
+    right = torch.empty(1 << 20, dtype=torch.int32, device="cuda")
+    n_polys = sum(len(w.polys.geom_off) - 1 for w in lbatch.jobs)
+    path = tmp_path / "tune.json"
+    opts, src = at.tuned_options(ctx, lbatch.indexes, lbatch.pts, lbatch.job_start, PRED_CODES["within"], n_polys,
+                                 left=left, right=right, passes=1, path=path, method=vsabi.METHOD_LEARNED,
+                                 with_source=True)
+    assert src == "searched" and set(opts) == set(at.LEARNED_DEFAULTS)
+    again, src2 = at.tuned_options(ctx, lbatch.indexes, lbatch.pts, lbatch.job_start, PRED_CODES["within"],
+                                   n_polys, left=left, right=right, path=path, method=vsabi.METHOD_LEARNED,
+                                   with_source=True)
+    assert (again, src2) == (opts, "cache")
+    plan = vsabi.BatchPlan(ctx, lbatch.indexes, lbatch.pts, lbatch.job_start,
+                           options=dict(opts, method=vsabi.METHOD_LEARNED))
+    l1, r1, _ = plan.run(PRED_CODES["within"])
+    l0, r0, _ = _run(lbatch, "within")
+    for x, y in zip(lbatch.split(l1.cpu().numpy().astype(np.int64), r1.cpu().numpy().astype(np.int64)),
+                    lbatch.split(l0, r0)):
+        np.testing.assert_array_equal(x[0], y[0])
+        np.testing.assert_array_equal(x[1], y[1])
+
+
 def test_learned_batch_rejects_bad_shapes(vsabi, ctx, lbatch):
-    for bad in ({"learned_grab": -1}, {"learned_map_blocks_per_sm": 9}, {"learned_flags": 1}):
+    for bad in ({"learned_grab": -1}, {"learned_map_blocks_per_sm": 9}, {"learned_flags": 1},
+                {"learned_map_packets": 3}):
         with pytest.raises(ValueError):
             vsabi.BatchPlan(ctx, lbatch.indexes, lbatch.pts, lbatch.job_start,
                             options=dict(bad, method=vsabi.METHOD_LEARNED))

@@ -92,7 +92,8 @@ class BatchOptions(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_int32), ("packets_per_grab", ctypes.c_int32),
                 ("sort_levels", ctypes.c_int32), ("method", ctypes.c_int32),
                 ("learned_map_blocks_per_sm", ctypes.c_int32), ("learned_refine_blocks_per_sm", ctypes.c_int32),
-                ("learned_grab", ctypes.c_int32), ("learned_flags", ctypes.c_uint32)]
+                ("learned_grab", ctypes.c_int32), ("learned_flags", ctypes.c_uint32),
+                ("learned_map_packets", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

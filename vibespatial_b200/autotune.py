@@ -1,12 +1,16 @@
 """Autotuner for the batched join's launch shape.
 
-The batched join (``vs_batch_run``) has three shape parameters: join-kernel
-blocks per SM, 32-point packets a warp takes per grab of the work counter, and
-the Hilbert levels the points of a job are sorted by (more levels: coherent
-packets but more radix passes).  The best values depend on the device and on
-the batch's shape (job count, points per job, polygons per job), so they are
-searched by timing the real kernels and cached on disk per
-(device, shape class, predicate).
+The R-tree batch (``vs_batch_run`` with ``VS_METHOD_RTREE``) has three shape
+parameters: join-kernel blocks per SM, 32-point packets a warp takes per grab
+of the work counter, and the Hilbert levels the points of a job are sorted by
+(more levels: coherent packets but more radix passes).  The learned batch
+(``VS_METHOD_LEARNED``) has four of its own: map-pass blocks per SM, the
+32-point packets a map warp looks up together (1 or 2), refine blocks per SM
+(4 or fewer run the 64-register refine build, 5 the 48-register one), and the
+grouped points a refine warp takes per grab of its work counter.  The best values depend on the device and on the batch's shape
+(job count, points per job, polygons per job), so they are searched by timing
+the real kernels and cached on disk per (device, shape class, predicate,
+method).
 
 The search is coordinate descent over a small grid: starting from the
 defaults, each parameter in turn is swept with the others held, and the sweep
@@ -32,6 +36,20 @@ SPACE = {
     "packets_per_grab": (1, 2, 4, 8, 16),
     "sort_levels": (6, 8, 10, 12),
 }
+LEARNED_DEFAULTS = {"learned_map_blocks_per_sm": 8, "learned_map_packets": 1, "learned_refine_blocks_per_sm": 4,
+                    "learned_grab": 32}
+LEARNED_SPACE = {
+    "learned_map_blocks_per_sm": (2, 4, 6, 8),
+    "learned_map_packets": (1, 2),
+    "learned_refine_blocks_per_sm": (2, 3, 4, 5),
+    "learned_grab": (32, 64, 128, 256),
+}
+METHOD_RTREE, METHOD_LEARNED = 0, 1
+
+
+def space_for(method: int) -> tuple[dict, dict]:
+    """(defaults, search space) of a batch method's launch shape."""
+    return (LEARNED_DEFAULTS, LEARNED_SPACE) if int(method) == METHOD_LEARNED else (DEFAULTS, SPACE)
 CACHE_ENV = "VIBESPATIAL_B200_AUTOTUNE_CACHE"
 _lock = threading.Lock()
 
@@ -53,8 +71,9 @@ def shape_class(n_jobs: int, n_points: int, n_polygons: int) -> str:
     return f"j{lg(n_jobs)}-p{lg(n_points / n_jobs)}-g{lg(n_polygons / n_jobs)}"
 
 
-def cache_key(device_name: str, sm_count: int, shape: str, predicate: int) -> str:
-    return f"{device_name}|sm{int(sm_count)}|{shape}|pred{int(predicate)}"
+def cache_key(device_name: str, sm_count: int, shape: str, predicate: int, method: int = METHOD_RTREE) -> str:
+    key = f"{device_name}|sm{int(sm_count)}|{shape}|pred{int(predicate)}"
+    return key if int(method) == METHOD_RTREE else f"{key}|learned"
 
 
 def load_cache(path: Path | None = None) -> dict:
@@ -80,12 +99,13 @@ def store(key: str, options: dict, ms: float, path: Path | None = None) -> None:
         os.replace(tmp, p)
 
 
-def lookup(key: str, path: Path | None = None) -> dict | None:
+def lookup(key: str, path: Path | None = None, method: int = METHOD_RTREE) -> dict | None:
     ent = load_cache(path).get(key)
     if not ent or not isinstance(ent.get("options"), dict):
         return None
-    opts = dict(DEFAULTS)
-    opts.update({k: int(v) for k, v in ent["options"].items() if k in DEFAULTS})
+    defaults, _ = space_for(method)
+    opts = dict(defaults)
+    opts.update({k: int(v) for k, v in ent["options"].items() if k in defaults})
     return opts
 
 
@@ -141,28 +161,31 @@ def time_plan(plan, predicate: int, left, right, *, warmup: int = 2, reps: int =
 
 
 def tuned_options(ctx, indexes, pts, job_start, predicate: int, n_polygons: int, *, left, right,
-                  use_cache: bool = True, passes: int = 2, path: Path | None = None) -> dict:
-    """Launch shape for this batch: from the cache, else searched and stored.
+                  use_cache: bool = True, passes: int = 2, path: Path | None = None,
+                  method: int = METHOD_RTREE, with_source: bool = False):
+    """Launch shape for this batch and method: from the cache, else searched
+    and stored.  With ``with_source``, returns (options, "cache"|"searched").
 
     ``left`` / ``right`` are pair buffers large enough for the batch (the
-    search runs the real join into them).
+    search runs the real join into them).  The options exclude ``method``.
     """
     from ._abi import BatchPlan
 
+    defaults, space = space_for(method)
     name, sms = device_identity(ctx.device)
-    key = cache_key(name, sms, shape_class(len(indexes), int(pts.n), n_polygons), predicate)
+    key = cache_key(name, sms, shape_class(len(indexes), int(pts.n), n_polygons), predicate, method)
     if use_cache:
-        hit = lookup(key, path)
+        hit = lookup(key, path, method)
         if hit is not None:
-            return hit
+            return (hit, "cache") if with_source else hit
 
     def measure(opts):
-        plan = BatchPlan(ctx, indexes, pts, job_start, options=opts)
+        plan = BatchPlan(ctx, indexes, pts, job_start, options=dict(opts, method=int(method)))
         try:
             return time_plan(plan, predicate, left, right)
         finally:
             plan.close()
 
-    best, ms, _ = search(measure, passes=passes)
+    best, ms, _ = search(measure, space=space, start=defaults, passes=passes)
     store(key, best, ms, path)
-    return best
+    return (best, "searched") if with_source else best

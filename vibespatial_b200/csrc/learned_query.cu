@@ -6,12 +6,13 @@
 //   map      input order: the point's job (batch) -> level-L cell key ->
 //            occupancy bit -> root table -> leaf model -> binary search inside
 //            the leaf's error window -> cell index (or none); the per-cell
-//            counts are incremented, and every matched point is appended to
-//            a striped staging region as one 16-byte CellPoint: its FP32
-//            offsets from the cell's anchor, its row and its cell
+//            count increment returns the point's rank in its cell, and every
+//            matched point is appended to a striped staging region as one
+//            16-byte CellPoint (its FP32 offsets from the cell's anchor, its
+//            row and its cell) with its rank beside it
 //   place    after an exclusive scan of the counts, every staged CellPoint is
-//            copied to its cell's next free position (per-cell cursors), so
-//            the points end up grouped by cell
+//            copied to its cell's start + its rank, so the points end up
+//            grouped by cell
 //   refine   a warp takes 32 consecutive grouped points, which share a
 //            candidate list except at cell boundaries, so the lanes read each
 //            entry record together (broadcast); each candidate is box-filtered
@@ -34,6 +35,7 @@
 #include "learned.cuh"
 #include "primitives.cuh"
 #include "rmi.cuh"
+#include "tma.cuh"
 
 namespace vs {
 namespace {
@@ -63,6 +65,7 @@ struct LqArgs {
     LearnedQuery q;
     LearnedJob single;  // the one job of a single join (kernel parameter space)
     CellPoint* staged;
+    uint32_t* staged_rank;  // each staged point's rank among its cell's points (same layout as staged)
     uint32_t* stripe_count;
     int64_t stripe_cap;
     uint32_t* cell_count;
@@ -272,114 +275,126 @@ __device__ __forceinline__ int packet_job(const LearnedQuery& q, int64_t b0, int
     return j;
 }
 
+// One point of the map pass: its batch-wide cell (-1: none) and its FP32
+// offsets from the cell's anchor (|offset| <= half a cell).
+template <bool kMulti, bool kBsearch>
+__device__ __forceinline__ int map_point(const LqArgs& a, int64_t i, int job, const uint16_t* lut,
+                                         unsigned long long& n_wide, float& qx, float& qy) {
+    const LearnedQuery& q = a.q;
+    if (i >= q.n) return -1;
+    const LearnedJob& J = job_desc<kMulti>(a, job);
+    const double x = q.px[i], y = q.py[i];
+    if (!((q.pvalid == nullptr || q.pvalid[i]) && J.n_cells > 0 && x >= J.lox && x <= J.hix && y >= J.loy &&
+          y <= J.hiy))
+        return -1;
+    const uint32_t gx = quantize(x, J.lox, J.sx), gy = quantize(y, J.loy, J.sy);
+    const int c = learned_lookup<kBsearch>(J, gx, gy, lut, n_wide);
+    if (c < 0) return -1;
+    const int sh = 32 - J.L;
+    qx = __double2float_rn(__dsub_rn(x, cell_anchor(J.lox, J.cwx, gx >> sh)));
+    qy = __double2float_rn(__dsub_rn(y, cell_anchor(J.loy, J.cwy, gy >> sh)));
+    return (int)(J.cell_base + (uint32_t)c);
+}
+
+// Count a packet's matched points (each point's count increment returns its
+// rank among its cell's points) and append them, with their ranks, to the
+// packet's stripe region.  The rank and stripe increments are independent,
+// so both round trips overlap.  Whole warp, converged.
+__device__ __forceinline__ void map_emit(const LqArgs& a, int64_t b0, int lane, int gc, float qx, float qy) {
+    uint32_t rank = 0;
+    if (gc >= 0) rank = atomicAdd(&a.cell_count[gc], 1u);
+    const unsigned mm = __ballot_sync(0xffffffffu, gc >= 0);
+    if (!mm) return;
+    const int64_t stripe = (b0 >> 5) % kStripes;
+    uint32_t sb = 0;
+    if (lane == 0) sb = atomicAdd(&a.stripe_count[stripe], (uint32_t)__popc(mm));
+    sb = __shfl_sync(0xffffffffu, sb, 0);
+    if (gc >= 0) {
+        CellPoint p;
+        p.qx = qx;
+        p.qy = qy;
+        p.row = (int32_t)(b0 + lane + a.q.row_base);
+        p.gcell = (uint32_t)gc;
+        const int64_t slot = stripe * a.stripe_cap + sb + __popc(mm & ((1u << lane) - 1u));
+        a.staged[slot] = p;
+        a.staged_rank[slot] = rank;
+    }
+}
+
 // Pass 1 (map), points in input order: each point's cell, the per-cell
 // counts, and the matched points appended to the staging regions as
-// CellPoints (FP32 offsets from the cell's anchor: |offset| <= half a cell).
-template <bool kMulti, bool kBsearch>
-__global__ void __launch_bounds__(kThreads, 8) learned_map_kernel(const LqArgs a) {
+// CellPoints.  A warp takes kPackets packets of 32 points per iteration and
+// runs their lookups together, so that many independent chains of dependent
+// index loads (occupancy bit, root table, leaf, binary search) are in flight.
+template <bool kMulti, bool kBsearch, int kPackets>
+__global__ void __launch_bounds__(kThreads, kPackets == 1 ? 8 : 6) learned_map_kernel(const LqArgs a) {
     __shared__ uint16_t s_lut[kHilbertLutSize];
     hilbert_lut_init(s_lut);
     __syncthreads();
     const LearnedQuery& q = a.q;
     unsigned long long n_wide = 0;
     const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    // Warp-uniform loop: the whole warp reaches the ballot and shuffle together.
-    for (int64_t b0 = gw * 32; b0 < q.n; b0 += nw * 32) {
-        const int64_t i = b0 + lane;
-        const int job = packet_job<kMulti>(q, b0, i, lane);
-        int gc = -1;
-        float qx = 0.f, qy = 0.f;
-        if (i < q.n) {
-            const LearnedJob& J = job_desc<kMulti>(a, job);
-            const double x = q.px[i], y = q.py[i];
-            if ((q.pvalid == nullptr || q.pvalid[i]) && J.n_cells > 0 && x >= J.lox && x <= J.hix && y >= J.loy &&
-                y <= J.hiy) {
-                const uint32_t gx = quantize(x, J.lox, J.sx), gy = quantize(y, J.loy, J.sy);
-                const int c = learned_lookup<kBsearch>(J, gx, gy, s_lut, n_wide);
-                if (c >= 0) {
-                    gc = (int)(J.cell_base + (uint32_t)c);
-                    const int sh = 32 - J.L;
-                    qx = __double2float_rn(__dsub_rn(x, cell_anchor(J.lox, J.cwx, gx >> sh)));
-                    qy = __double2float_rn(__dsub_rn(y, cell_anchor(J.loy, J.cwy, gy >> sh)));
-                }
-            }
+    // Warp-uniform loop: the whole warp reaches the ballots and shuffles together.
+    for (int64_t b0 = gw * 32 * kPackets; b0 < q.n; b0 += nw * 32 * kPackets) {
+        int gc[kPackets];
+        float qx[kPackets], qy[kPackets];
+#pragma unroll
+        for (int u = 0; u < kPackets; ++u) {
+            const int64_t bu = b0 + 32 * u;
+            const int job = packet_job<kMulti>(q, bu < q.n ? bu : b0, bu + lane, lane);
+            qx[u] = qy[u] = 0.f;
+            gc[u] = map_point<kMulti, kBsearch>(a, bu + lane, job, s_lut, n_wide, qx[u], qy[u]);
         }
-        if (gc >= 0) atomicAdd(&a.cell_count[gc], 1u);
-        // append the matched points of this packet to its stripe region
-        const unsigned mm = __ballot_sync(0xffffffffu, gc >= 0);
-        if (mm) {
-            const int64_t stripe = (b0 >> 5) % kStripes;
-            uint32_t sb = 0;
-            if (lane == 0) sb = atomicAdd(&a.stripe_count[stripe], (uint32_t)__popc(mm));
-            sb = __shfl_sync(0xffffffffu, sb, 0);
-            if (gc >= 0) {
-                CellPoint p;
-                p.qx = qx;
-                p.qy = qy;
-                p.row = (int32_t)(i + q.row_base);
-                p.gcell = (uint32_t)gc;
-                a.staged[stripe * a.stripe_cap + sb + __popc(mm & lt)] = p;
-            }
-        }
+#pragma unroll
+        for (int u = 0; u < kPackets; ++u) map_emit(a, b0 + 32 * u, lane, gc[u], qx[u], qy[u]);
     }
     add_counter(a.counters, 6, n_wide);
 }
 
 // -------------------------------------------------------------- place ---
 // Pass 2 (place): after the exclusive scan of the counts (cell_count[c] is
-// then the first position of cell c), every staged point takes the next
-// position of its cell (warp-aggregated cursor increments) and is copied
-// there.  A block walks whole stripe regions; a warp keeps kPlaceUnroll
-// groups of 32 records in flight (loads, then cursor increments, then stores).
+// then the first position of cell c), every staged point is copied to
+// cell_count[cell] + its rank: a permutation with no atomics.  A block walks
+// whole stripe regions; a warp keeps kPlaceUnroll groups of 32 records in
+// flight (record and rank loads, then cell starts, then stores).
 #ifndef VS_PLACE_UNROLL
-#define VS_PLACE_UNROLL 4
+#define VS_PLACE_UNROLL 8
 #endif
 constexpr int kPlaceUnroll = VS_PLACE_UNROLL;
 
 __global__ void __launch_bounds__(kThreads) learned_place_kernel(const LqArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
     constexpr uint32_t kStep = 32u * kPlaceUnroll;
     for (int stripe = blockIdx.x; stripe < kStripes; stripe += gridDim.x) {
         const uint32_t cnt = a.stripe_count[stripe];
-        const CellPoint* src = a.staged + (int64_t)stripe * a.stripe_cap;
-        // warp-uniform loop: every lane runs the same iterations
-        for (uint32_t k0 = (uint32_t)warp * kStep; k0 < cnt; k0 += (kThreads / 32) * kStep) {
+        const int64_t off = (int64_t)stripe * a.stripe_cap;
+        for (uint32_t k0 = (uint32_t)warp * kStep + lane; k0 < cnt; k0 += (kThreads / 32) * kStep) {
             CellPoint p[kPlaceUnroll];
-            int gc[kPlaceUnroll];
+            uint32_t rank[kPlaceUnroll];
 #pragma unroll
             for (int u = 0; u < kPlaceUnroll; ++u) {
-                const uint32_t k = k0 + u * 32 + lane;
-                gc[u] = -1;
+                const uint32_t k = k0 + u * 32;
                 if (k < cnt) {
-                    p[u] = src[k];
-                    gc[u] = (int)p[u].gcell;
+                    p[u] = a.staged[off + k];
+                    rank[u] = a.staged_rank[off + k];
                 }
             }
-            unsigned peers[kPlaceUnroll];
-            uint32_t base[kPlaceUnroll];
+            uint32_t start[kPlaceUnroll];
 #pragma unroll
-            for (int u = 0; u < kPlaceUnroll; ++u) {
-                peers[u] = __match_any_sync(0xffffffffu, gc[u]);
-                base[u] = 0;
-                if (gc[u] >= 0 && lane == __ffs(peers[u]) - 1)
-                    base[u] = atomicAdd(&a.cell_count[gc[u]], (uint32_t)__popc(peers[u]));
-            }
+            for (int u = 0; u < kPlaceUnroll; ++u)
+                if (k0 + u * 32 < cnt) start[u] = a.cell_count[p[u].gcell];
 #pragma unroll
-            for (int u = 0; u < kPlaceUnroll; ++u) {
-                const uint32_t b = __shfl_sync(0xffffffffu, base[u], __ffs(peers[u]) - 1);
-                if (gc[u] >= 0) a.grouped[b + __popc(peers[u] & lt)] = p[u];
-            }
+            for (int u = 0; u < kPlaceUnroll; ++u)
+                if (k0 + u * 32 < cnt) a.grouped[start[u] + rank[u]] = p[u];
         }
     }
 }
 
 // ------------------------------------------------------------- refine ---
 #ifndef VS_JOIN_MIN_BLOCKS
-#define VS_JOIN_MIN_BLOCKS 5
+#define VS_JOIN_MIN_BLOCKS 5  // the bbox kernel's register cap (blocks per SM)
 #endif
 constexpr int64_t kJoinGrab = 32;  // default grouped points per work-queue grab (multiple of 32)
 
@@ -513,16 +528,32 @@ __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& ou
 // with all lanes busy instead of only the lanes whose point lies in the
 // current candidate's box.  Neighbouring queue entries mostly share a
 // polygon, so vertex reads stay broadcasts.
-template <bool kMulti, bool kBins, bool kF64>
-__global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_kernel(const LqArgs a) {
+// Entry records a warp stages in shared memory for one packet of 32 grouped
+// points: the lanes' cells ascend, so their candidate lists lie in one
+// contiguous run of the job's records, from the first lane's first record to
+// the last lane's last; a run of at most kStageRecs records arrives by one
+// bulk copy (TMA), and longer runs are read from global memory.
+constexpr int kStageRecs = 64;
+
+// kMinBlocks: resident blocks per SM the registers are capped for (4: 64
+// registers, no spills; 5: 48 registers, more warps, a few spills).
+template <bool kMulti, bool kBins, bool kF64, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(const LqArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
     __shared__ unsigned s_cnt[kThreads / 32];
     __shared__ QueuedPair s_q[kThreads / 32][kQueue];
+    __shared__ __align__(128) EntryRecord s_recs[kThreads / 32][kStageRecs];
+    __shared__ uint64_t s_bar[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) s_cnt[warp] = 0;
+    if (lane == 0) {
+        s_cnt[warp] = 0;
+        mbar_init(&s_bar[warp]);
+    }
     __syncwarp();
+    uint32_t phase = 0;
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
     QueuedPair* qp = s_q[warp];
+    const EntryRecord* st = s_recs[warp];
     const unsigned lt = (1u << lane) - 1u;
     const int64_t n = (int64_t)*a.n_grouped;
     unsigned long long n_cand = 0;
@@ -536,11 +567,30 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_refine_k
             const GroupedLane g = load_grouped<kMulti>(a, base + lane, e0);
             const uint32_t maxlen = warp_max_u32(g.len);
             const EntryRecord* recs = job_desc<kMulti>(a, g.job).recs;
+            // stage the packet's run of records (warp-uniform decision)
+            const unsigned has = __ballot_sync(0xffffffffu, g.len > 0);
+            const int first = has ? __ffs(has) - 1 : 0, last = has ? 31 - __clz(has) : 0;
+            const uint32_t run_lo = __shfl_sync(0xffffffffu, g.lo, first);
+            const uint32_t run_hi = __shfl_sync(0xffffffffu, g.lo + g.len, last);
+            const bool one_job = !kMulti || __all_sync(0xffffffffu, g.len == 0 || g.job == __shfl_sync(0xffffffffu, g.job, first));
+            const bool staged = has != 0 && one_job && run_hi - run_lo <= (uint32_t)kStageRecs;
+            if (staged) {
+                __syncwarp();  // every lane is done with the buffer's previous run
+                if (lane == 0) bulk_load(s_recs[warp], recs + run_lo, (run_hi - run_lo) * (uint32_t)sizeof(EntryRecord),
+                                         &s_bar[warp]);
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&s_bar[warp], phase))) {
+                    // record the timeout, give the copy one more bounded wait, stop this warp
+                    if (lane == 0) atomicOr(&a.counters[4], 2ull);
+                    mbar_wait_bounded(&s_bar[warp], phase);
+                    return;
+                }
+                phase ^= 1u;
+            }
             for (uint32_t k = 0; k < maxlen; ++k) {
                 bool inbox = false;
                 EntryRecord r;
                 if (k < g.len) {
-                    r = recs[g.lo + k];
+                    r = staged ? st[g.lo + k - run_lo] : recs[g.lo + k];
                     inbox = box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq);
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, inbox);
@@ -590,7 +640,8 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 size_t learned_scratch_bytes(int64_t n, int64_t n_cells) {
     const int64_t cap = stripe_cap_for(n);
-    return align256(sizeof(CellPoint) * (size_t)(kStripes * cap)) + align256(sizeof(uint32_t) * kStripes) +
+    return align256(sizeof(CellPoint) * (size_t)(kStripes * cap)) + align256(sizeof(uint32_t) * (size_t)(kStripes * cap)) +
+           align256(sizeof(uint32_t) * kStripes) +
            align256(sizeof(uint32_t) * (size_t)(n_cells > 0 ? n_cells : 1)) +
            align256(sizeof(CellPoint) * (size_t)(n > 0 ? n : 1)) + align256(sizeof(uint32_t));
 }
@@ -600,6 +651,8 @@ void learned_scratch_carve(void* base, int64_t n, int64_t n_cells, LearnedScratc
     sc.stripe_cap = stripe_cap_for(n);
     sc.staged = p;
     p += align256(sizeof(CellPoint) * (size_t)(kStripes * sc.stripe_cap));
+    sc.staged_rank = (uint32_t*)p;
+    p += align256(sizeof(uint32_t) * (size_t)(kStripes * sc.stripe_cap));
     sc.stripe_count = (uint32_t*)p;
     p += align256(sizeof(uint32_t) * kStripes);
     sc.cell_count = (uint32_t*)p;
@@ -611,10 +664,13 @@ void learned_scratch_carve(void* base, int64_t n, int64_t n_cells, LearnedScratc
 
 namespace {
 
+// The refine variant for the launch shape: 5 or more blocks per SM asked for
+// take the 48-register build, fewer (or the default) the 64-register one.
 template <bool kMulti, bool kBins>
-void* pick_refine(uint32_t flags) {
-    return (flags & kLearnedFp64Walk) ? (void*)learned_refine_kernel<kMulti, kBins, true>
-                                      : (void*)learned_refine_kernel<kMulti, kBins, false>;
+const void* pick_refine(uint32_t flags, int blocks_per_sm) {
+    if (flags & kLearnedFp64Walk) return (const void*)learned_refine_kernel<kMulti, kBins, true, 4>;
+    if (blocks_per_sm >= 5) return (const void*)learned_refine_kernel<kMulti, kBins, false, 5>;
+    return (const void*)learned_refine_kernel<kMulti, kBins, false, 4>;
 }
 
 // Grid of a persistent kernel: blocks_per_sm per SM when given (capped at the
@@ -636,8 +692,14 @@ int launch_passes(cudaStream_t s, vs_context* ctx, const LqArgs& a) {
     const int64_t n = a.q.n;
     const LearnedShape& sh = a.q.shape;
     const int map_grid = grid_for(n, kThreads, sh.map_blocks_per_sm > 0 ? sh.map_blocks_per_sm : 8);
-    if (sh.flags & kLearnedBsearch) learned_map_kernel<kMulti, true><<<map_grid, kThreads, 0, s>>>(a);
-    else learned_map_kernel<kMulti, false><<<map_grid, kThreads, 0, s>>>(a);
+    const bool two = sh.map_packets == 2;
+    if (sh.flags & kLearnedBsearch) {
+        if (two) learned_map_kernel<kMulti, true, 2><<<map_grid, kThreads, 0, s>>>(a);
+        else learned_map_kernel<kMulti, true, 1><<<map_grid, kThreads, 0, s>>>(a);
+    } else {
+        if (two) learned_map_kernel<kMulti, false, 2><<<map_grid, kThreads, 0, s>>>(a);
+        else learned_map_kernel<kMulti, false, 1><<<map_grid, kThreads, 0, s>>>(a);
+    }
     VS_LAUNCHED("learned_map", s);
     VS_TRY(exclusive_scan_u32(a.cell_count, a.cell_count, a.q.n_cells, (uint32_t*)a.n_grouped, s));
     if (ctx) phase_mark(ctx, 1);
@@ -645,7 +707,8 @@ int launch_passes(cudaStream_t s, vs_context* ctx, const LqArgs& a) {
     VS_LAUNCHED("learned_place", s);
     if (ctx) phase_mark(ctx, 2);
     if (a.q.accept_mask) {
-        const void* kernel = a.q.has_ring_bins ? pick_refine<kMulti, true>(sh.flags) : pick_refine<kMulti, false>(sh.flags);
+        const void* kernel = a.q.has_ring_bins ? pick_refine<kMulti, true>(sh.flags, sh.refine_blocks_per_sm)
+                                               : pick_refine<kMulti, false>(sh.flags, sh.refine_blocks_per_sm);
         const int grid = persistent_grid(kernel, n, sh.refine_blocks_per_sm);
         void* args[] = {(void*)&a};
         VS_CUDA_TRY(cudaLaunchKernel(kernel, dim3(grid), dim3(kThreads), args, 0, s));
@@ -669,6 +732,7 @@ int enqueue_learned(cudaStream_t s, vs_context* ctx, const LearnedQuery& q, cons
     a.q = q;
     if (single) a.single = *single;
     a.staged = (CellPoint*)sc.staged;
+    a.staged_rank = sc.staged_rank;
     a.stripe_count = sc.stripe_count;
     a.stripe_cap = sc.stripe_cap;
     a.cell_count = sc.cell_count;
