@@ -572,7 +572,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
             const int first = has ? __ffs(has) - 1 : 0, last = has ? 31 - __clz(has) : 0;
             const uint32_t run_lo = __shfl_sync(0xffffffffu, g.lo, first);
             const uint32_t run_hi = __shfl_sync(0xffffffffu, g.lo + g.len, last);
-            const bool one_job = !kMulti || __all_sync(0xffffffffu, g.len == 0 || g.job == __shfl_sync(0xffffffffu, g.job, first));
+            const int job0 = __shfl_sync(0xffffffffu, g.job, first);  // every lane takes part in the shuffle
+            const bool one_job = !kMulti || __all_sync(0xffffffffu, g.len == 0 || g.job == job0);
             const bool staged = has != 0 && one_job && run_hi - run_lo <= (uint32_t)kStageRecs;
             if (staged) {
                 __syncwarp();  // every lane is done with the buffer's previous run
@@ -590,7 +591,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                 bool inbox = false;
                 EntryRecord r;
                 if (k < g.len) {
-                    r = staged ? st[g.lo + k - run_lo] : recs[g.lo + k];
+                    const uint32_t si = g.lo + k - run_lo;  // unsigned: below the run wraps to a large index
+                    r = (staged && si < run_hi - run_lo) ? st[si] : recs[g.lo + k];
                     inbox = box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq);
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, inbox);
