@@ -22,6 +22,7 @@ JOIN_SORT = 1
 JOIN_BULK_LEAVES = 2
 JOIN_LEARNED_BSEARCH = 4
 JOIN_LEARNED_FP64_WALK = 8
+JOIN_LEARNED_NO_STAGE = 16
 
 # Every function the header declares; tests check the library exports them.
 EXPORTED = (

@@ -102,11 +102,12 @@ struct LearnedShape {
     int32_t map_blocks_per_sm;     // map pass blocks per SM (0 = 8)
     int32_t refine_blocks_per_sm;  // refine pass blocks per SM (0 = as many as fit)
     int32_t grab;                  // grouped points a refine warp takes per work grab (0 = 32; multiple of 32)
-    uint32_t flags;                // kLearnedBsearch | kLearnedFp64Walk
+    uint32_t flags;                // kLearnedBsearch | kLearnedFp64Walk | kLearnedNoStage
     int32_t map_packets;           // 32-point packets a map warp looks up together (1 or 2; 0 = 1)
 };
 constexpr uint32_t kLearnedBsearch = 1u;   // cell lookup by binary search over all cell keys (no RMI)
 constexpr uint32_t kLearnedFp64Walk = 2u;  // ring walks in FP64 (no FP32 edge stage)
+constexpr uint32_t kLearnedNoStage = 4u;   // entry records read from global memory (no bulk-copy staging)
 
 // Centre of level-L grid cell c on one axis: lo + (c + 0.5) * cell width,
 // one fused multiply-add, so the index build (from a cell's key) and the

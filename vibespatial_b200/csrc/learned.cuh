@@ -12,7 +12,6 @@ namespace vs {
 // Per-query scratch of the learned pipeline (points n, batch-wide cells).
 struct LearnedScratch {
     void* staged = nullptr;          // striped staging regions of matched points (CellPoint)
-    uint32_t* staged_rank = nullptr; // each staged point's rank in its cell (same layout)
     uint32_t* stripe_count = nullptr;
     int64_t stripe_cap = 0;
     uint32_t* cell_count = nullptr;  // counts, then start offsets after the scan

@@ -6,13 +6,12 @@
 //   map      input order: the point's job (batch) -> level-L cell key ->
 //            occupancy bit -> root table -> leaf model -> binary search inside
 //            the leaf's error window -> cell index (or none); the per-cell
-//            count increment returns the point's rank in its cell, and every
-//            matched point is appended to a striped staging region as one
-//            16-byte CellPoint (its FP32 offsets from the cell's anchor, its
-//            row and its cell) with its rank beside it
+//            counts are incremented, and every matched point is appended to
+//            a striped staging region as one 16-byte CellPoint: its FP32
+//            offsets from the cell's anchor, its row and its cell
 //   place    after an exclusive scan of the counts, every staged CellPoint is
-//            copied to its cell's start + its rank, so the points end up
-//            grouped by cell
+//            copied to its cell's next free position (per-cell cursors), so
+//            the points end up grouped by cell
 //   refine   a warp takes 32 consecutive grouped points, which share a
 //            candidate list except at cell boundaries, so the lanes read each
 //            entry record together (broadcast); each candidate is box-filtered
@@ -65,7 +64,6 @@ struct LqArgs {
     LearnedQuery q;
     LearnedJob single;  // the one job of a single join (kernel parameter space)
     CellPoint* staged;
-    uint32_t* staged_rank;  // each staged point's rank among its cell's points (same layout as staged)
     uint32_t* stripe_count;
     int64_t stripe_cap;
     uint32_t* cell_count;
@@ -76,6 +74,7 @@ struct LqArgs {
     unsigned long long* counters;
     unsigned long long* work;  // refine work queue (grouped points handed out)
     int64_t grab;              // grouped points a refine warp takes per grab (multiple of 32)
+    bool no_stage;             // entry records read from global memory (no bulk-copy staging)
 };
 
 // Job descriptor of a batch query (global memory) or of a single join (the
@@ -164,14 +163,22 @@ __device__ __forceinline__ int ring_location_split(float qx, float qy, float t, 
     bool inside = false;
     float2 a = xy32[end - 1];
     float2 b = xy32[start];
+    // an edge's start offset in y is the previous edge's end offset: carried
+    float dA = __fsub_rn(a.y, qy);
     int ia = end - 1;
     for (int i = start; i < end; ++i) {
         // the next vertex's load is in flight while this edge is decided
         const float2 nb = xy32[i + 1 < end ? i + 1 : i];
-        const int r = split_edge(qx, qy, t, a, b, xy, ia, i, P, inside, n32, n64);
-        if (r == 1) return LOC_BOUNDARY;
-        if (r == 2) return LOC_UNDECIDED;
+        const float dB = __fsub_rn(b.y, qy);
+        if (fabsf(dA) > t && fabsf(dB) > t && (dA > 0.f) == (dB > 0.f)) {
+            ++n32;  // both ends strictly on one side of the point's y: the edge changes nothing
+        } else {
+            const int r = split_edge(qx, qy, t, a, b, xy, ia, i, P, inside, n32, n64);
+            if (r == 1) return LOC_BOUNDARY;
+            if (r == 2) return LOC_UNDECIDED;
+        }
         a = b;
+        dA = dB;
         b = nb;
         ia = i;
     }
@@ -296,13 +303,10 @@ __device__ __forceinline__ int map_point(const LqArgs& a, int64_t i, int job, co
     return (int)(J.cell_base + (uint32_t)c);
 }
 
-// Count a packet's matched points (each point's count increment returns its
-// rank among its cell's points) and append them, with their ranks, to the
-// packet's stripe region.  The rank and stripe increments are independent,
-// so both round trips overlap.  Whole warp, converged.
+// Count a packet's matched points and append them to the packet's stripe
+// region.  Whole warp, converged.
 __device__ __forceinline__ void map_emit(const LqArgs& a, int64_t b0, int lane, int gc, float qx, float qy) {
-    uint32_t rank = 0;
-    if (gc >= 0) rank = atomicAdd(&a.cell_count[gc], 1u);
+    if (gc >= 0) atomicAdd(&a.cell_count[gc], 1u);
     const unsigned mm = __ballot_sync(0xffffffffu, gc >= 0);
     if (!mm) return;
     const int64_t stripe = (b0 >> 5) % kStripes;
@@ -315,9 +319,7 @@ __device__ __forceinline__ void map_emit(const LqArgs& a, int64_t b0, int lane, 
         p.qy = qy;
         p.row = (int32_t)(b0 + lane + a.q.row_base);
         p.gcell = (uint32_t)gc;
-        const int64_t slot = stripe * a.stripe_cap + sb + __popc(mm & ((1u << lane) - 1u));
-        a.staged[slot] = p;
-        a.staged_rank[slot] = rank;
+        a.staged[stripe * a.stripe_cap + sb + __popc(mm & ((1u << lane) - 1u))] = p;
     }
 }
 
@@ -355,39 +357,51 @@ __global__ void __launch_bounds__(kThreads, kPackets == 1 ? 8 : 6) learned_map_k
 
 // -------------------------------------------------------------- place ---
 // Pass 2 (place): after the exclusive scan of the counts (cell_count[c] is
-// then the first position of cell c), every staged point is copied to
-// cell_count[cell] + its rank: a permutation with no atomics.  A block walks
-// whole stripe regions; a warp keeps kPlaceUnroll groups of 32 records in
-// flight (record and rank loads, then cell starts, then stores).
+// then the first position of cell c), every staged point takes the next
+// position of its cell (warp-aggregated cursor increments) and is copied
+// there.  Records of one cell placed close together in time fill whole
+// 32-byte sectors in L2 before they are written back.  A block walks whole
+// stripe regions; a warp keeps kPlaceUnroll groups of 32 records in flight
+// (loads, then cursor increments, then stores).
 #ifndef VS_PLACE_UNROLL
-#define VS_PLACE_UNROLL 8
+#define VS_PLACE_UNROLL 4
 #endif
 constexpr int kPlaceUnroll = VS_PLACE_UNROLL;
 
 __global__ void __launch_bounds__(kThreads) learned_place_kernel(const LqArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     constexpr uint32_t kStep = 32u * kPlaceUnroll;
     for (int stripe = blockIdx.x; stripe < kStripes; stripe += gridDim.x) {
         const uint32_t cnt = a.stripe_count[stripe];
-        const int64_t off = (int64_t)stripe * a.stripe_cap;
-        for (uint32_t k0 = (uint32_t)warp * kStep + lane; k0 < cnt; k0 += (kThreads / 32) * kStep) {
+        const CellPoint* src = a.staged + (int64_t)stripe * a.stripe_cap;
+        // warp-uniform loop: every lane runs the same iterations
+        for (uint32_t k0 = (uint32_t)warp * kStep; k0 < cnt; k0 += (kThreads / 32) * kStep) {
             CellPoint p[kPlaceUnroll];
-            uint32_t rank[kPlaceUnroll];
+            int gc[kPlaceUnroll];
 #pragma unroll
             for (int u = 0; u < kPlaceUnroll; ++u) {
-                const uint32_t k = k0 + u * 32;
+                const uint32_t k = k0 + u * 32 + lane;
+                gc[u] = -1;
                 if (k < cnt) {
-                    p[u] = a.staged[off + k];
-                    rank[u] = a.staged_rank[off + k];
+                    p[u] = src[k];
+                    gc[u] = (int)p[u].gcell;
                 }
             }
-            uint32_t start[kPlaceUnroll];
+            unsigned peers[kPlaceUnroll];
+            uint32_t base[kPlaceUnroll];
 #pragma unroll
-            for (int u = 0; u < kPlaceUnroll; ++u)
-                if (k0 + u * 32 < cnt) start[u] = a.cell_count[p[u].gcell];
+            for (int u = 0; u < kPlaceUnroll; ++u) {
+                peers[u] = __match_any_sync(0xffffffffu, gc[u]);
+                base[u] = 0;
+                if (gc[u] >= 0 && lane == __ffs(peers[u]) - 1)
+                    base[u] = atomicAdd(&a.cell_count[gc[u]], (uint32_t)__popc(peers[u]));
+            }
 #pragma unroll
-            for (int u = 0; u < kPlaceUnroll; ++u)
-                if (k0 + u * 32 < cnt) a.grouped[start[u] + rank[u]] = p[u];
+            for (int u = 0; u < kPlaceUnroll; ++u) {
+                const uint32_t b = __shfl_sync(0xffffffffu, base[u], __ffs(peers[u]) - 1);
+                if (gc[u] >= 0) a.grouped[b + __popc(peers[u] & lt)] = p[u];
+            }
         }
     }
 }
@@ -574,7 +588,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
             const uint32_t run_hi = __shfl_sync(0xffffffffu, g.lo + g.len, last);
             const int job0 = __shfl_sync(0xffffffffu, g.job, first);  // every lane takes part in the shuffle
             const bool one_job = !kMulti || __all_sync(0xffffffffu, g.len == 0 || g.job == job0);
-            const bool staged = has != 0 && one_job && run_hi - run_lo <= (uint32_t)kStageRecs;
+            const bool staged = !a.no_stage && has != 0 && one_job && run_hi - run_lo <= (uint32_t)kStageRecs;
             if (staged) {
                 __syncwarp();  // every lane is done with the buffer's previous run
                 if (lane == 0) bulk_load(s_recs[warp], recs + run_lo, (run_hi - run_lo) * (uint32_t)sizeof(EntryRecord),
@@ -642,8 +656,7 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 size_t learned_scratch_bytes(int64_t n, int64_t n_cells) {
     const int64_t cap = stripe_cap_for(n);
-    return align256(sizeof(CellPoint) * (size_t)(kStripes * cap)) + align256(sizeof(uint32_t) * (size_t)(kStripes * cap)) +
-           align256(sizeof(uint32_t) * kStripes) +
+    return align256(sizeof(CellPoint) * (size_t)(kStripes * cap)) + align256(sizeof(uint32_t) * kStripes) +
            align256(sizeof(uint32_t) * (size_t)(n_cells > 0 ? n_cells : 1)) +
            align256(sizeof(CellPoint) * (size_t)(n > 0 ? n : 1)) + align256(sizeof(uint32_t));
 }
@@ -653,8 +666,6 @@ void learned_scratch_carve(void* base, int64_t n, int64_t n_cells, LearnedScratc
     sc.stripe_cap = stripe_cap_for(n);
     sc.staged = p;
     p += align256(sizeof(CellPoint) * (size_t)(kStripes * sc.stripe_cap));
-    sc.staged_rank = (uint32_t*)p;
-    p += align256(sizeof(uint32_t) * (size_t)(kStripes * sc.stripe_cap));
     sc.stripe_count = (uint32_t*)p;
     p += align256(sizeof(uint32_t) * kStripes);
     sc.cell_count = (uint32_t*)p;
@@ -734,7 +745,6 @@ int enqueue_learned(cudaStream_t s, vs_context* ctx, const LearnedQuery& q, cons
     a.q = q;
     if (single) a.single = *single;
     a.staged = (CellPoint*)sc.staged;
-    a.staged_rank = sc.staged_rank;
     a.stripe_count = sc.stripe_count;
     a.stripe_cap = sc.stripe_cap;
     a.cell_count = sc.cell_count;
@@ -745,6 +755,7 @@ int enqueue_learned(cudaStream_t s, vs_context* ctx, const LearnedQuery& q, cons
     a.counters = counters;
     a.work = work;
     a.grab = q.shape.grab > 0 ? (int64_t)((q.shape.grab + 31) / 32 * 32) : kJoinGrab;
+    a.no_stage = (q.shape.flags & kLearnedNoStage) != 0;
     VS_CUDA_TRY(cudaMemsetAsync(sc.cell_count, 0, (size_t)(q.n_cells > 0 ? q.n_cells : 1) * sizeof(uint32_t), s));
     VS_CUDA_TRY(cudaMemsetAsync(sc.stripe_count, 0, (size_t)kStripes * sizeof(uint32_t), s));
     if (q.n_jobs > 1) return launch_passes<true>(s, ctx, a);
