@@ -86,6 +86,7 @@ struct LearnedJob {
     const uint32_t* cell_start;
     const EntryRecord* recs;  // [n_entries] per-entry records, cell order
     const int2* c01;          // [n_geoms] coordinate range of a single-ring slot, (-1, -1) otherwise
+    const float4* ring_box32; // [n_rings] box of each ring's FP32 vertices (minx, miny, maxx, maxy)
     const float2* xy32;
     const double2* xy;
     const int32_t* item_geom;
@@ -140,6 +141,7 @@ struct LearnedIndex {
     int32_t n_leaves = 0;
     EntryRecord* recs = nullptr;     // [n_entries] record of each entry, cell order
     int2* c01 = nullptr;             // [n_geoms] single-ring coordinate range per slot
+    float4* ring_box32 = nullptr;    // [n_rings] box of each ring's FP32 vertices (everything if one is NaN)
     LearnedJob* desc = nullptr;      // device: this index as the query kernels see it
     LearnedJob h_desc{};             // host copy of *desc
     // FP32 tile-relative copies used by the split-precision filter

@@ -172,6 +172,38 @@ __global__ void split_copy_kernel(const vs_box* __restrict__ box, int64_t M, con
     }
 }
 
+// Box of every ring's FP32 (slot-relative) vertices, a warp per ring.  A
+// ring with a NaN vertex gets the whole plane, so no walk ever skips it.
+__global__ void ring_box_kernel(const int32_t* __restrict__ ring_off, int64_t n_rings,
+                                const float2* __restrict__ xy32, float4* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = warp; r < n_rings; r += nw) {
+        const int32_t c0 = ring_off[r], c1 = ring_off[r + 1];
+        float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
+        bool nan = false;
+        for (int32_t c = c0 + lane; c < c1; c += 32) {
+            const float2 v = xy32[c];
+            nan |= isnan(v.x) || isnan(v.y);
+            mnx = fminf(mnx, v.x);
+            mny = fminf(mny, v.y);
+            mxx = fmaxf(mxx, v.x);
+            mxy = fmaxf(mxy, v.y);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+            mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+        }
+        nan = __any_sync(0xffffffffu, nan);
+        if (lane == 0)
+            out[r] = nan ? make_float4(-INFINITY, -INFINITY, INFINITY, INFINITY) : make_float4(mnx, mny, mxx, mxy);
+    }
+}
+
 // Coordinate range of every single-ring slot: such polygons take the short
 // ring walk (c0 >= 0) unless the split walk would use the ring's y-bins.
 __global__ void slot_c01_kernel(int64_t M, const int32_t* __restrict__ geom_off, const int32_t* __restrict__ part_off,
@@ -592,6 +624,7 @@ void free_learned_index(vs_index* idx) {
     cudaFree(li.origin);
     cudaFree(li.err32);
     cudaFree(li.c01);
+    cudaFree(li.ring_box32);
     cudaFree(li.xy32);
     cudaFree(li.leaves);
     cudaFree(li.recs);
@@ -714,11 +747,13 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_TRY(dalloc(&li.origin, (size_t)M, bytes));
     VS_TRY(dalloc(&li.err32, (size_t)M, bytes));
     VS_TRY(dalloc(&li.c01, (size_t)M, bytes));
+    VS_TRY(dalloc(&li.ring_box32, (size_t)std::max<int32_t>(idx->n_rings, 1), bytes));
     VS_TRY(dalloc(&li.xy32, (size_t)std::max<int64_t>(idx->n_coords, 1), bytes));
     VS_TRY(dalloc(&li.recs, (size_t)E, bytes));
     VS_TRY(dalloc(&li.desc, 1, bytes));
     d.recs = li.recs;
     d.c01 = li.c01;
+    d.ring_box32 = li.ring_box32;
     d.xy32 = li.xy32;
     VS_CUDA_TRY(cudaMemcpyAsync(li.desc, &d, sizeof(d), cudaMemcpyHostToDevice, s));
     learned_desc_kernel<<<1, 1, 0, s>>>(idx->frame, li.desc);
@@ -729,6 +764,11 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     slot_c01_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, idx->geom_off, idx->part_off, idx->ring_off, idx->ring_bin,
                                                      li.c01);
     VS_CUDA_TRY(cudaGetLastError());
+    if (idx->n_rings > 0) {
+        ring_box_kernel<<<grid_for((int64_t)idx->n_rings * 32, 256), 256, 0, s>>>(idx->ring_off, idx->n_rings, li.xy32,
+                                                                                 li.ring_box32);
+        VS_CUDA_TRY(cudaGetLastError());
+    }
     Scratch<unsigned> bad;
     VS_TRY(bad.alloc(1, s));
     VS_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(unsigned), s));

@@ -222,6 +222,12 @@ __device__ __forceinline__ int geometry_location_split(float qx, float qy, float
         bool inside = false;
         const int r0 = J.part_off[part], r1 = J.part_off[part + 1];
         for (int ring = r0; ring < r1; ++ring) {
+            // A ring whose box lies strictly beyond the point (by more than t) neither holds it nor crosses its
+            // +x ray an odd number of times: the walk of it would change nothing.
+            const float4 box = J.ring_box32[ring];
+            if (__fadd_ru(qx, t) < box.x || __fsub_rd(qx, t) > box.z || __fadd_ru(qy, t) < box.y ||
+                __fsub_rd(qy, t) > box.w)
+                continue;
             const int c0 = J.ring_off[ring], c1 = J.ring_off[ring + 1];
             // the FP32 walk is cheap per edge, so bins pay off only on longer rings than for the FP64 walk
             const int rb = (kBins && J.rings.ring_bin && c1 - c0 >= kSplitBinMinVertices) ? J.rings.ring_bin[ring] : -1;
