@@ -254,10 +254,14 @@ __device__ __forceinline__ int learned_lookup(const LearnedJob& J, uint32_t gx, 
                                               unsigned long long& n_wide) {
     const uint32_t cell = hilbert_key_lut(gx, gy, J.L, lut);
     const uint32_t ob = cell >> J.occ_shift;
-    if (!((J.occ[ob >> 5] >> (ob & 31)) & 1u)) return -1;
+    // the occupancy word and the root-table entry depend only on the key:
+    // both loads are issued before either is tested
+    const uint32_t occ_word = J.occ[ob >> 5];
+    const uint32_t leaf_id = kBsearch ? 0u : (uint32_t)J.root_table[cell >> J.root_shift];
+    if (!((occ_word >> (ob & 31)) & 1u)) return -1;
     long long l0 = 0, h0 = J.n_cells;  // search [l0, h0)
     if constexpr (!kBsearch) {
-        const RmiLeaf lf = J.leaves[J.root_table[cell >> J.root_shift]];
+        const RmiLeaf lf = J.leaves[leaf_id];
         if (lf.lo > lf.hi) return -1;  // no stored key routes to this leaf
         const long long pred = rmi_predict(make_double2(lf.a, lf.b), cell);
         l0 = pred + lf.lo;
