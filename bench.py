@@ -165,12 +165,15 @@ def plan_median_ms(plan, pred, left, right, n_expect, use_graph=True, reps=5, wa
 
 def learned_ablations(_abi, ctx, indexes, pts, job_start, pred, left, right, n_pairs, base_opts, reps):
     """What each choice of the learned pipeline buys: the same batch plan with the RMI replaced by a binary
-    search over every cell key, with FP64 ring walks instead of the FP32 stage, and launched directly instead
-    of replayed from a CUDA graph (median device ms of each; same pairs)."""
+    search over every cell key, with FP64 ring walks instead of the FP32 stage, without the bulk-copy (TMA)
+    staging of candidate records, without the interior-box shortcut, and launched directly instead of replayed
+    from a CUDA graph (median device ms of each; same pairs)."""
     out = {}
     for name, extra, graph in (("graph_ms", {}, True), ("direct_launch_ms", {}, False),
                                ("rmi_replaced_by_bsearch_ms", {"learned_flags": _abi.JOIN_LEARNED_BSEARCH}, True),
-                               ("fp64_walk_ms", {"learned_flags": _abi.JOIN_LEARNED_FP64_WALK}, True)):
+                               ("fp64_walk_ms", {"learned_flags": _abi.JOIN_LEARNED_FP64_WALK}, True),
+                               ("no_record_staging_ms", {"learned_flags": _abi.JOIN_LEARNED_NO_STAGE}, True),
+                               ("no_interior_box_ms", {"learned_flags": _abi.JOIN_LEARNED_NO_INTERIOR}, True)):
         plan = _abi.BatchPlan(ctx, indexes, pts, job_start, options=dict(base_opts, **extra))
         out[name] = plan_median_ms(plan, pred, left, right, n_pairs, use_graph=graph, reps=reps)
         plan.close()

@@ -72,6 +72,7 @@ enum vs_method {
 #define VS_JOIN_LEARNED_FP64_WALK 8u /* ring walks in FP64 (the plain method's filter) instead of FP32 first */
 #define VS_JOIN_LEARNED_NO_STAGE 16u /* candidate records read by the lanes from global memory instead of one
                                         bulk copy (TMA) per 32-point packet into shared memory */
+#define VS_JOIN_LEARNED_NO_INTERIOR 32u /* every box candidate ring-walked: no interior-box shortcut */
 
 typedef struct vs_context vs_context;
 typedef struct vs_index vs_index;
@@ -313,7 +314,7 @@ typedef struct vs_batch_options {
     int32_t learned_map_blocks_per_sm;    /* learned: map pass blocks per SM (0 = 8) */
     int32_t learned_refine_blocks_per_sm; /* learned: refine pass blocks per SM (0 = as many as fit) */
     int32_t learned_grab;     /* learned: grouped points a refine warp takes per grab (0 = 32; rounded up to 32s) */
-    uint32_t learned_flags;   /* learned: VS_JOIN_LEARNED_BSEARCH | _FP64_WALK | _NO_STAGE (ablations) */
+    uint32_t learned_flags;   /* learned: VS_JOIN_LEARNED_BSEARCH | _FP64_WALK | _NO_STAGE | _NO_INTERIOR (ablations) */
     int32_t learned_map_packets; /* learned: 32-point packets a map warp looks up together, 1 or 2 (0 = 1) */
 } vs_batch_options;
 

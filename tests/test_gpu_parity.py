@@ -359,17 +359,19 @@ def test_join_host_grows_chunk_pair_buffer(vsabi, ctx, oracle):
         assert_same_pairs(hl, hr, el, er)
 
 
-@pytest.mark.parametrize("flags", ["bsearch", "fp64_walk", "both"])
+@pytest.mark.parametrize("flags", ["bsearch", "fp64_walk", "both", "no_stage", "no_interior"])
 @pytest.mark.parametrize("workload", ["zipf", "degenerate"])
 def test_learned_ablation_switches(vsabi, ctx, oracle, workload, flags):
-    """The learned method with its RMI replaced by a binary search over every cell key, or with FP64 ring walks
-    instead of the FP32 stage (the ablations the benchmark times), still gives the oracle's pairs."""
+    """The learned method with its RMI replaced by a binary search over every cell key, with FP64 ring walks
+    instead of the FP32 stage, without the bulk-copy staging of candidate records or without the interior-box
+    shortcut (the ablations the benchmark times) still gives the oracle's pairs."""
     from vibespatial_b200.testing import synthetic as syn
 
     w = (syn.zipf_join(seed=14, n_points=1_000_000, n_polys=50_000) if workload == "zipf"
          else syn.degenerate_join(seed=15, n_points=300_000, n_polys=3_000))
     f = {"bsearch": vsabi.JOIN_LEARNED_BSEARCH, "fp64_walk": vsabi.JOIN_LEARNED_FP64_WALK,
-         "both": vsabi.JOIN_LEARNED_BSEARCH | vsabi.JOIN_LEARNED_FP64_WALK}[flags]
+         "both": vsabi.JOIN_LEARNED_BSEARCH | vsabi.JOIN_LEARNED_FP64_WALK,
+         "no_stage": vsabi.JOIN_LEARNED_NO_STAGE, "no_interior": vsabi.JOIN_LEARNED_NO_INTERIOR}[flags]
     pts, _k1 = upload_points(vsabi, w.px, w.py)
     P, _k2 = upload_polys(vsabi, w.polys)
     index = vsabi.DeviceIndex(ctx, P, learned=True)

@@ -23,6 +23,7 @@ JOIN_BULK_LEAVES = 2
 JOIN_LEARNED_BSEARCH = 4
 JOIN_LEARNED_FP64_WALK = 8
 JOIN_LEARNED_NO_STAGE = 16
+JOIN_LEARNED_NO_INTERIOR = 32
 
 # Every function the header declares; tests check the library exports them.
 EXPORTED = (

@@ -286,7 +286,8 @@ int vs_join(vs_context* ctx, const vs_index* idx, const vs_points* pts, int32_t 
     LearnedShape shape{};
     shape.flags = ((flags & VS_JOIN_LEARNED_BSEARCH) ? kLearnedBsearch : 0u) |
                   ((flags & VS_JOIN_LEARNED_FP64_WALK) ? kLearnedFp64Walk : 0u) |
-                  ((flags & VS_JOIN_LEARNED_NO_STAGE) ? kLearnedNoStage : 0u);
+                  ((flags & VS_JOIN_LEARNED_NO_STAGE) ? kLearnedNoStage : 0u) |
+                  ((flags & VS_JOIN_LEARNED_NO_INTERIOR) ? kLearnedNoInterior : 0u);
     unsigned long long want = (unsigned long long)(pts->n / 64 + 65536);
     for (int attempt = 0; attempt < 2; ++attempt) {
         VS_TRY(ensure_defer_capacity(ctx, want));

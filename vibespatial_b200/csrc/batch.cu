@@ -407,7 +407,8 @@ int enqueue_batch(vs_batch_plan* p, cudaStream_t s, int mask, int32_t* left, int
         q.shape.map_packets = p->opts.learned_map_packets;
         q.shape.flags = ((p->opts.learned_flags & VS_JOIN_LEARNED_BSEARCH) ? kLearnedBsearch : 0u) |
                         ((p->opts.learned_flags & VS_JOIN_LEARNED_FP64_WALK) ? kLearnedFp64Walk : 0u) |
-                        ((p->opts.learned_flags & VS_JOIN_LEARNED_NO_STAGE) ? kLearnedNoStage : 0u);
+                        ((p->opts.learned_flags & VS_JOIN_LEARNED_NO_STAGE) ? kLearnedNoStage : 0u) |
+                        ((p->opts.learned_flags & VS_JOIN_LEARNED_NO_INTERIOR) ? kLearnedNoInterior : 0u);
         VS_TRY(enqueue_learned(s, nullptr, q, p->n_jobs == 1 ? &p->h_single : nullptr, p->lsc, a.sink, a.defer,
                                a.counters, &p->d_work[0]));
         if (mask) {
@@ -522,8 +523,9 @@ int vs_batch_plan_create(vs_context* ctx, const vs_index* const* indexes, int32_
         p->opts.learned_grab < 0 || p->opts.learned_grab > 4096 || p->opts.learned_map_packets < 0 ||
         p->opts.learned_map_packets > 2 ||
         (p->opts.learned_flags &
-         ~(VS_JOIN_LEARNED_BSEARCH | VS_JOIN_LEARNED_FP64_WALK | VS_JOIN_LEARNED_NO_STAGE)) != 0) {
-        set_error("learned launch shape out of range (blocks per SM 0..8, grab 0..4096, map packets 0..2, flags 4|8|16)");
+         ~(VS_JOIN_LEARNED_BSEARCH | VS_JOIN_LEARNED_FP64_WALK | VS_JOIN_LEARNED_NO_STAGE |
+           VS_JOIN_LEARNED_NO_INTERIOR)) != 0) {
+        set_error("learned launch shape out of range (blocks per SM 0..8, grab 0..4096, map packets 0..2, flags 4|8|16|32)");
         delete p;
         return VS_E_ARG;
     }

@@ -87,6 +87,7 @@ struct LearnedJob {
     const EntryRecord* recs;  // [n_entries] per-entry records, cell order
     const int2* c01;          // [n_geoms] coordinate range of a single-ring slot, (-1, -1) otherwise
     const float4* ring_box32; // [n_rings] box of each ring's FP32 vertices (minx, miny, maxx, maxy)
+    const float4* ib32;       // [n_geoms] interior box of each slot, relative to its origin (empty: none)
     const float2* xy32;
     const double2* xy;
     const int32_t* item_geom;
@@ -103,12 +104,13 @@ struct LearnedShape {
     int32_t map_blocks_per_sm;     // map pass blocks per SM (0 = 8)
     int32_t refine_blocks_per_sm;  // refine pass blocks per SM (0 = as many as fit)
     int32_t grab;                  // grouped points a refine warp takes per work grab (0 = 32; multiple of 32)
-    uint32_t flags;                // kLearnedBsearch | kLearnedFp64Walk | kLearnedNoStage
+    uint32_t flags;                // kLearnedBsearch | kLearnedFp64Walk | kLearnedNoStage | kLearnedNoInterior
     int32_t map_packets;           // 32-point packets a map warp looks up together (1 or 2; 0 = 1)
 };
 constexpr uint32_t kLearnedBsearch = 1u;   // cell lookup by binary search over all cell keys (no RMI)
 constexpr uint32_t kLearnedFp64Walk = 2u;  // ring walks in FP64 (no FP32 edge stage)
 constexpr uint32_t kLearnedNoStage = 4u;   // entry records read from global memory (no bulk-copy staging)
+constexpr uint32_t kLearnedNoInterior = 8u;  // every box candidate is ring-walked (no interior-box shortcut)
 
 // Centre of level-L grid cell c on one axis: lo + (c + 0.5) * cell width,
 // one fused multiply-add, so the index build (from a cell's key) and the
@@ -142,6 +144,7 @@ struct LearnedIndex {
     EntryRecord* recs = nullptr;     // [n_entries] record of each entry, cell order
     int2* c01 = nullptr;             // [n_geoms] single-ring coordinate range per slot
     float4* ring_box32 = nullptr;    // [n_rings] box of each ring's FP32 vertices (everything if one is NaN)
+    float4* ib32 = nullptr;          // [n_geoms] interior box per slot (csrc/learned.cu interior_box_kernel)
     LearnedJob* desc = nullptr;      // device: this index as the query kernels see it
     LearnedJob h_desc{};             // host copy of *desc
     // FP32 tile-relative copies used by the split-precision filter

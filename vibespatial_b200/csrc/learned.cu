@@ -204,6 +204,81 @@ __global__ void ring_box_kernel(const int32_t* __restrict__ ring_off, int64_t n_
     }
 }
 
+// Smallest s >= 0 for which the box [-s a, s a] x [-s b, s b] (a = 1 / ia,
+// b = 1 / ib) touches the segment (x0, y0) -> (x1, y1): the minimum over the
+// segment of max(|x| ia, |y| ib).  That function of the segment parameter is
+// convex and piecewise linear, so its minimum lies at an end or where |x| ia
+// and |y| ib are 0 or equal; all of these are evaluated.
+__device__ __forceinline__ double box_reach(double x0, double y0, double x1, double y1, double ia, double ib) {
+    const double dx = x1 - x0, dy = y1 - y0;
+    auto f = [&](double t) {
+        t = fmin(fmax(t, 0.0), 1.0);
+        return fmax(fabs(x0 + t * dx) * ia, fabs(y0 + t * dy) * ib);
+    };
+    double m = fmin(f(0.0), f(1.0));
+    if (dx != 0.0) m = fmin(m, f(-x0 / dx));
+    if (dy != 0.0) m = fmin(m, f(-y0 / dy));
+    const double p = dx * ia - dy * ib, q = dx * ia + dy * ib;
+    if (p != 0.0) m = fmin(m, f((y0 * ib - x0 * ia) / p));
+    if (q != 0.0) m = fmin(m, f(-(y0 * ib + x0 * ia) / q));
+    return m;
+}
+
+// Interior box of every slot, a warp per slot: an axis-aligned box around the
+// slot origin (its box centre) with the slot box's proportions that touches
+// no edge of any ring, kept only when the origin itself is strictly interior
+// (decided exactly).  Such a box lies in the face of the origin, so every
+// point strictly inside it is interior.  Its half sizes are 0.999 of the
+// largest such box (the margin dwarfs the FP64 rounding of the vertex
+// offsets, and boxes below 1e-9 of the coordinates' magnitude are dropped);
+// stored in FP32 relative to the origin, rounded inward.  Slots without one
+// get an empty box.
+__global__ void interior_box_kernel(const vs_box* __restrict__ boxes, int64_t M, const int32_t* __restrict__ geom_off,
+                                    const int32_t* __restrict__ part_off, const int32_t* __restrict__ ring_off,
+                                    const double2* __restrict__ xy, RingIndex ri, const double2* __restrict__ origin,
+                                    float4* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = warp; s < M; s += nw) {
+        const vs_box b = boxes[s];
+        const double2 o = origin[s];
+        const double ha = 0.5 * (b.maxx - b.minx), hb = 0.5 * (b.maxy - b.miny);
+        bool ok = b.minx <= b.maxx && b.miny <= b.maxy && ha > 0.0 && hb > 0.0;
+        int loc = LOC_OUTSIDE;
+        if (ok && lane == 0) {
+            unsigned n_exact = 0;
+            loc = geometry_location(o.x, o.y, xy, ring_off, part_off, geom_off, (int)s, ri, n_exact);
+        }
+        ok = ok && __shfl_sync(0xffffffffu, loc, 0) == LOC_INTERIOR;
+        double reach = INFINITY;
+        bool nan = false;
+        if (ok) {
+            const double ia = 1.0 / ha, ib = 1.0 / hb;
+            const int p0 = geom_off[s], p1 = geom_off[s + 1];
+            for (int ring = part_off[p0]; ring < part_off[p1]; ++ring) {  // warp-uniform
+                const int c0 = ring_off[ring], c1 = ring_off[ring + 1];
+                for (int i = c0 + lane; i < c1; i += 32) {
+                    const double2 v0 = xy[i == c0 ? c1 - 1 : i - 1], v1 = xy[i];
+                    nan |= isnan(v0.x) || isnan(v0.y) || isnan(v1.x) || isnan(v1.y);
+                    reach = fmin(reach, box_reach(v0.x - o.x, v0.y - o.y, v1.x - o.x, v1.y - o.y, ia, ib));
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1) reach = fmin(reach, __shfl_xor_sync(0xffffffffu, reach, k));
+        nan = __any_sync(0xffffffffu, nan);
+        if (lane == 0) {
+            const double hx = 0.999 * reach * ha, hy = 0.999 * reach * hb;
+            const double floor_abs = 1e-9 * fmax(fabs(o.x), fabs(o.y));
+            const bool keep = ok && !nan && reach > 0.0 && reach < INFINITY && hx > floor_abs && hy > floor_abs;
+            out[s] = keep ? make_float4(__double2float_ru(-hx), __double2float_ru(-hy), __double2float_rd(hx),
+                                        __double2float_rd(hy))
+                          : make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
+        }
+    }
+}
+
 // Coordinate range of every single-ring slot: such polygons take the short
 // ring walk (c0 >= 0) unless the split walk would use the ring's y-bins.
 __global__ void slot_c01_kernel(int64_t M, const int32_t* __restrict__ geom_off, const int32_t* __restrict__ part_off,
@@ -625,6 +700,7 @@ void free_learned_index(vs_index* idx) {
     cudaFree(li.err32);
     cudaFree(li.c01);
     cudaFree(li.ring_box32);
+    cudaFree(li.ib32);
     cudaFree(li.xy32);
     cudaFree(li.leaves);
     cudaFree(li.recs);
@@ -748,12 +824,14 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_TRY(dalloc(&li.err32, (size_t)M, bytes));
     VS_TRY(dalloc(&li.c01, (size_t)M, bytes));
     VS_TRY(dalloc(&li.ring_box32, (size_t)std::max<int32_t>(idx->n_rings, 1), bytes));
+    VS_TRY(dalloc(&li.ib32, (size_t)M, bytes));
     VS_TRY(dalloc(&li.xy32, (size_t)std::max<int64_t>(idx->n_coords, 1), bytes));
     VS_TRY(dalloc(&li.recs, (size_t)E, bytes));
     VS_TRY(dalloc(&li.desc, 1, bytes));
     d.recs = li.recs;
     d.c01 = li.c01;
     d.ring_box32 = li.ring_box32;
+    d.ib32 = li.ib32;
     d.xy32 = li.xy32;
     VS_CUDA_TRY(cudaMemcpyAsync(li.desc, &d, sizeof(d), cudaMemcpyHostToDevice, s));
     learned_desc_kernel<<<1, 1, 0, s>>>(idx->frame, li.desc);
@@ -763,6 +841,9 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_CUDA_TRY(cudaGetLastError());
     slot_c01_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, idx->geom_off, idx->part_off, idx->ring_off, idx->ring_bin,
                                                      li.c01);
+    VS_CUDA_TRY(cudaGetLastError());
+    interior_box_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
+                                                              idx->xy, idx->ring_index(), li.origin, li.ib32);
     VS_CUDA_TRY(cudaGetLastError());
     if (idx->n_rings > 0) {
         ring_box_kernel<<<grid_for((int64_t)idx->n_rings * 32, 256), 256, 0, s>>>(idx->ring_off, idx->n_rings, li.xy32,

@@ -75,6 +75,7 @@ struct LqArgs {
     unsigned long long* work;  // refine work queue (grouped points handed out)
     int64_t grab;              // grouped points a refine warp takes per grab (multiple of 32)
     bool no_stage;             // entry records read from global memory (no bulk-copy staging)
+    bool no_interior;          // every box candidate is ring-walked (no interior-box shortcut)
 };
 
 // Job descriptor of a batch query (global memory) or of a single join (the
@@ -611,6 +612,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                 }
                 phase ^= 1u;
             }
+            const float4* ib32 = job_desc<kMulti>(a, g.job).ib32;
             for (uint32_t k = 0; k < maxlen; ++k) {
                 bool inbox = false;
                 EntryRecord r;
@@ -619,21 +621,40 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                     r = (staged && si < run_hi - run_lo) ? st[si] : recs[g.lo + k];
                     inbox = box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq);
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, inbox);
+                // the point in the slot's frame; its error against the real p -
+                // origin is at most dq + |off error| (in r.err with the vertex
+                // error) + the rounding of this addition (es)
+                float sx = 0.f, sy = 0.f, t = 0.f;
+                bool walk = false, direct = false;
                 if (inbox) {
-                    QueuedPair& e = qp[nq + __popc(m & lt)];
-                    // the point in the slot's frame; its error against the real
-                    // p - origin is at most dq + |off error| (in r.err with the
-                    // vertex error) + the rounding of this addition (es)
-                    const float sx = __fadd_rn(g.p.qx, r.offx), sy = __fadd_rn(g.p.qy, r.offy);
+                    ++n_cand;
+                    sx = __fadd_rn(g.p.qx, r.offx);
+                    sy = __fadd_rn(g.p.qy, r.offy);
                     const float es = __fmaf_ru(fmaxf(fabsf(sx), fabsf(sy)), 6.1e-8f, 1e-37f);
+                    t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, g.dq), es), 1.0001f);
+                    walk = true;
+                    if (!a.no_interior) {
+                        // strictly inside the slot's interior box, whatever the
+                        // rounding: interior, no ring walk
+                        const float4 ib = ib32[r.slot];
+                        if (__fsub_rd(sx, t) > ib.x && __fadd_ru(sx, t) < ib.z && __fsub_rd(sy, t) > ib.y &&
+                            __fadd_ru(sy, t) < ib.w) {
+                            walk = false;
+                            direct = (a.q.accept_mask >> LOC_INTERIOR) & 1;
+                        }
+                    }
+                }
+                wemit_sync(out, a.sink, direct, g.p.row,
+                           direct ? job_desc<kMulti>(a, g.job).item_geom[r.slot] : 0);
+                const unsigned m = __ballot_sync(0xffffffffu, walk);
+                if (walk) {
+                    QueuedPair& e = qp[nq + __popc(m & lt)];
                     e.qx = sx;
                     e.qy = sy;
-                    e.t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, g.dq), es), 1.0001f);
+                    e.t = t;
                     e.row = g.p.row;
                     e.slot = r.slot;
                     e.job = g.job;
-                    ++n_cand;
                 }
                 nq += __popc(m);
                 __syncwarp();
@@ -766,6 +787,7 @@ int enqueue_learned(cudaStream_t s, vs_context* ctx, const LearnedQuery& q, cons
     a.work = work;
     a.grab = q.shape.grab > 0 ? (int64_t)((q.shape.grab + 31) / 32 * 32) : kJoinGrab;
     a.no_stage = (q.shape.flags & kLearnedNoStage) != 0;
+    a.no_interior = (q.shape.flags & kLearnedNoInterior) != 0;
     VS_CUDA_TRY(cudaMemsetAsync(sc.cell_count, 0, (size_t)(q.n_cells > 0 ? q.n_cells : 1) * sizeof(uint32_t), s));
     VS_CUDA_TRY(cudaMemsetAsync(sc.stripe_count, 0, (size_t)kStripes * sizeof(uint32_t), s));
     if (q.n_jobs > 1) return launch_passes<true>(s, ctx, a);
