@@ -28,7 +28,8 @@ constexpr int kRmiHidden = 32;
 //             the slot's FP32 vertices (xy32)
 //   err       bound on |FP32 vertex - (vertex - origin)| of the slot plus
 //             |off - (anchor - origin)|
-//   slot      the polygon's slot (its original row is item_geom[slot])
+//   slot      the polygon's slot (its original row is item_geom[slot]) in
+//             the low 31 bits; bit 31 set when the slot has an interior box
 // The learned index stores one record per entry, in cell order, so a
 // candidate is one 32-byte read.
 struct __align__(16) EntryRecord {
@@ -37,6 +38,13 @@ struct __align__(16) EntryRecord {
     float err;
     int32_t slot;
 };
+constexpr uint32_t kEntryInteriorBit = 0x80000000u;
+__host__ __device__ __forceinline__ int32_t entry_slot(const EntryRecord& r) {
+    return (int32_t)((uint32_t)r.slot & ~kEntryInteriorBit);
+}
+__host__ __device__ __forceinline__ bool entry_has_interior(const EntryRecord& r) {
+    return ((uint32_t)r.slot & kEntryInteriorBit) != 0;
+}
 
 // A query point matched to a cell: FP32 offsets from the cell's anchor, its
 // row, and its batch-wide cell number.  The map pass stages these, the place

@@ -302,7 +302,8 @@ __global__ void slot_c01_kernel(int64_t M, const int32_t* __restrict__ geom_off,
 __global__ void entry_recs_kernel(int64_t E, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ entries,
                                   const LearnedJob* __restrict__ d, const vs_box* __restrict__ boxes,
                                   const double2* __restrict__ origin, const float* __restrict__ err32,
-                                  EntryRecord* __restrict__ out, unsigned* __restrict__ bad) {
+                                  const float4* __restrict__ ib32, EntryRecord* __restrict__ out,
+                                  unsigned* __restrict__ bad) {
     const double u64 = 1.1102230246251565e-16;  // 2^-53
     const int L = d->L, sh = 32 - L;
     const double lox = d->lox, loy = d->loy, cwx = d->cwx, cwy = d->cwy;
@@ -330,7 +331,8 @@ __global__ void entry_recs_kernel(int64_t E, const uint32_t* __restrict__ keys, 
         const double ex = fabs((double)r.offx - dx) + fabs(dx) * u64;
         const double ey = fabs((double)r.offy - dy) + fabs(dy) * u64;
         r.err = __double2float_ru(((double)err32[slot] + fmax(ex, ey)) * (1.0 + 1e-6));
-        r.slot = slot;
+        const float4 ib = ib32[slot];
+        r.slot = (int32_t)((uint32_t)slot | (ib.x < ib.z ? kEntryInteriorBit : 0u));
         out[e] = r;
     }
 }
@@ -854,7 +856,7 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_TRY(bad.alloc(1, s));
     VS_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(unsigned), s));
     entry_recs_kernel<<<grid_for(E, 256), 256, 0, s>>>((int64_t)E, keys.p, li.entries, li.desc, boxes, li.origin,
-                                                       li.err32, li.recs, bad.p);
+                                                       li.err32, li.ib32, li.recs, bad.p);
     VS_CUDA_TRY(cudaGetLastError());
     unsigned h_bad = 0;
     VS_CUDA_TRY(cudaMemcpyAsync(&h_bad, bad.p, sizeof(h_bad), cudaMemcpyDeviceToHost, s));

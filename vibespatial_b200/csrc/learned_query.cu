@@ -495,12 +495,13 @@ __global__ void __launch_bounds__(kThreads, VS_JOIN_MIN_BLOCKS) learned_bbox_ker
                 if (k < g.len) {
                     const EntryRecord r = J.recs[g.lo + k];
                     if (box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq)) {
-                        const vs_box bb = J.boxes[r.slot];
+                        const int32_t slot = entry_slot(r);
+                        const vs_box bb = J.boxes[slot];
                         const double x = a.q.px[pi], y = a.q.py[pi];
                         if (x >= bb.minx && x <= bb.maxx && y >= bb.miny && y <= bb.maxy) {
                             ++n_cand;
                             want = true;
-                            right = J.item_geom[r.slot];
+                            right = J.item_geom[slot];
                         }
                     }
                 }
@@ -633,10 +634,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                     const float es = __fmaf_ru(fmaxf(fabsf(sx), fabsf(sy)), 6.1e-8f, 1e-37f);
                     t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, g.dq), es), 1.0001f);
                     walk = true;
-                    if (!a.no_interior) {
+                    if (!a.no_interior && entry_has_interior(r)) {
                         // strictly inside the slot's interior box, whatever the
                         // rounding: interior, no ring walk
-                        const float4 ib = ib32[r.slot];
+                        const float4 ib = ib32[entry_slot(r)];
                         if (__fsub_rd(sx, t) > ib.x && __fadd_ru(sx, t) < ib.z && __fsub_rd(sy, t) > ib.y &&
                             __fadd_ru(sy, t) < ib.w) {
                             walk = false;
@@ -645,7 +646,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                     }
                 }
                 wemit_sync(out, a.sink, direct, g.p.row,
-                           direct ? job_desc<kMulti>(a, g.job).item_geom[r.slot] : 0);
+                           direct ? job_desc<kMulti>(a, g.job).item_geom[entry_slot(r)] : 0);
                 const unsigned m = __ballot_sync(0xffffffffu, walk);
                 if (walk) {
                     QueuedPair& e = qp[nq + __popc(m & lt)];
@@ -653,7 +654,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                     e.qy = sy;
                     e.t = t;
                     e.row = g.p.row;
-                    e.slot = r.slot;
+                    e.slot = entry_slot(r);
                     e.job = g.job;
                 }
                 nq += __popc(m);
