@@ -580,6 +580,34 @@ int dalloc(T** p, size_t n, int64_t& bytes) {
     return VS_OK;
 }
 
+// Registrations (E) and distinct cells (n_cells) of the slot boxes at grid
+// level L, on scratch only: the count, emit, sort and unique-flag steps of
+// the build.
+int probe_level(cudaStream_t s, const vs_box* boxes, int64_t M, const double* frame, int L, uint32_t* cnt,
+                unsigned long long* tot, unsigned long long& E, uint32_t& n_cells) {
+    VS_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), s));
+    cell_count_kernel<<<grid_for(M, 256), 256, 0, s>>>(boxes, M, frame, L, cnt, tot);
+    VS_CUDA_TRY(cudaMemcpyAsync(&E, tot, sizeof(E), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    n_cells = 0;
+    if (E == 0 || E >= 0x7fffffffull) return VS_OK;
+    Scratch<uint32_t> off, keys, vals, flag, nc;
+    VS_TRY(off.alloc((size_t)M, s));
+    VS_TRY(keys.alloc((size_t)E, s));
+    VS_TRY(vals.alloc((size_t)E, s));
+    VS_TRY(flag.alloc((size_t)E, s));
+    VS_TRY(nc.alloc(1, s));
+    VS_TRY(exclusive_scan_u32(cnt, off.p, M, nullptr, s));
+    cell_emit_kernel<<<grid_for(M, 256), 256, 0, s>>>(boxes, M, frame, L, off.p, keys.p, vals.p);
+    VS_CUDA_TRY(cudaGetLastError());
+    VS_TRY(radix_sort_u32_u32(keys.p, vals.p, (int64_t)E, 2 * L, s));
+    cell_flag_kernel<<<grid_for((int64_t)E, 256), 256, 0, s>>>(keys.p, (int64_t)E, flag.p);
+    VS_TRY(exclusive_scan_u32(flag.p, flag.p, (int64_t)E, nc.p, s));
+    VS_CUDA_TRY(cudaMemcpyAsync(&n_cells, nc.p, sizeof(n_cells), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaStreamSynchronize(s));
+    return VS_OK;
+}
+
 int train_rmi(vs_context* ctx, vs_index* idx, int steps) {
     LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
@@ -719,6 +747,7 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     const vs_box* boxes = idx->nodes;  // level 0 = slot boxes
     // 1. grid level
     int L = opts ? opts->cell_level : 0;
+    const bool auto_level = L <= 0;
     if (L <= 0) {
         Scratch<double> acc;
         VS_TRY(acc.alloc(2, s));
@@ -745,6 +774,31 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
         VS_CUDA_TRY(cudaStreamSynchronize(s));
         if (L <= 1 || E <= (unsigned long long)(16 * M + (1 << 20))) break;
         --L;
+    }
+    // An automatic level is then refined (at most 3 levels) while a cell
+    // holds more than 2.5 entries on average and the finer level's
+    // registrations stay within the budget: the refine tests every entry of
+    // a point's cell, so long lists cost more than the extra registrations.
+    // (A box side mean is pulled up by a few wide boxes, such as multipolygons
+    // with spread parts, which leaves the cells too coarse for the rest.)
+    if (auto_level && E > 0) {
+        uint32_t nc = 0;
+        VS_TRY(probe_level(s, boxes, M, idx->frame, L, cnt.p, tot.p, E, nc));
+        const int l_max = std::min(15, L + 3);
+        while (L < l_max && nc > 0 && (double)E > 2.5 * (double)nc) {
+            unsigned long long e1 = 0;
+            uint32_t nc1 = 0;
+            VS_TRY(probe_level(s, boxes, M, idx->frame, L + 1, cnt.p, tot.p, e1, nc1));
+            if (e1 > (unsigned long long)(16 * M + (1 << 20)) || e1 >= 0x7fffffffull) break;
+            ++L;
+            E = e1;
+            nc = nc1;
+        }
+        // the counts of the chosen level, for the emit below
+        VS_CUDA_TRY(cudaMemsetAsync(tot.p, 0, sizeof(unsigned long long), s));
+        cell_count_kernel<<<grid_for(M, 256), 256, 0, s>>>(boxes, M, idx->frame, L, cnt.p, tot.p);
+        VS_CUDA_TRY(cudaMemcpyAsync(&E, tot.p, sizeof(E), cudaMemcpyDeviceToHost, s));
+        VS_CUDA_TRY(cudaStreamSynchronize(s));
     }
     if (E >= 0x7fffffffull) {
         set_error("learned index: too many cell registrations (%llu)", E);
