@@ -558,190 +558,120 @@ __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& ou
 // points: the lanes' cells ascend, so their candidate lists lie in one
 // contiguous run of the job's records, from the first lane's first record to
 // the last lane's last; a run of at most kStageRecs records arrives by one
-// bulk copy (TMA), and longer runs are read from global memory.  Two buffers
-// per warp: the next packet's run is copied while this packet is refined.
-constexpr int kStageRecs = 40;
+// bulk copy (TMA), and longer runs are read from global memory.
+constexpr int kStageRecs = 64;
 
-// A packet's grouped points: each lane's point and (once its range load has
-// returned) its job and candidate range.
-struct PacketLanes {
-    CellPoint p;
-    int job;
-    uint32_t lo, len;
-};
-
-// The staged run of one packet.
-struct PacketRun {
-    uint32_t lo, hi;
-    bool staged;
-};
-
-template <bool kMulti>
-__device__ __forceinline__ void fetch_range(const LqArgs& a, PacketLanes& k) {
-    k.job = 0;
-    k.lo = k.len = 0;
-    if (k.p.row >= 0) {
-        k.job = point_job<kMulti>(a.q, (int64_t)k.p.row - a.q.row_base);
-        const LearnedJob& J = job_desc<kMulti>(a, k.job);
-        const uint32_t c = k.p.gcell - J.cell_base;
-        k.lo = J.cell_start[c];
-        k.len = J.cell_start[c + 1] - k.lo;
-    }
-}
-
-__device__ __forceinline__ CellPoint fetch_point(const LqArgs& a, int64_t j, int64_t n) {
-    CellPoint p{0.f, 0.f, -1, 0u};
-    if (j < n) p = a.grouped[j];
-    return p;
-}
-
-// Warp-uniform: decide whether packet k's run is staged and, if so, start its
-// bulk copy into buf (lane 0).  The caller has synchronised the warp since the
-// buffer was last read.
-template <bool kMulti>
-__device__ __forceinline__ PacketRun stage_run(const LqArgs& a, const PacketLanes& k, EntryRecord* buf, uint64_t* bar,
-                                               int lane) {
-    PacketRun run{0u, 0u, false};
-    const unsigned has = __ballot_sync(0xffffffffu, k.len > 0);
-    const int first = has ? __ffs(has) - 1 : 0, last = has ? 31 - __clz(has) : 0;
-    run.lo = __shfl_sync(0xffffffffu, k.lo, first);
-    run.hi = __shfl_sync(0xffffffffu, k.lo + k.len, last);
-    const int job0 = __shfl_sync(0xffffffffu, k.job, first);  // every lane takes part in the shuffle
-    const bool one_job = !kMulti || __all_sync(0xffffffffu, k.len == 0 || k.job == job0);
-    run.staged = !a.no_stage && has != 0 && one_job && run.hi - run.lo <= (uint32_t)kStageRecs;
-    if (run.staged && lane == 0)
-        bulk_load(buf, job_desc<kMulti>(a, job0).recs + run.lo, (run.hi - run.lo) * (uint32_t)sizeof(EntryRecord),
-                  bar);
-    return run;
-}
-
-// Pass 3 with a location test.  Packets of 32 consecutive grouped points are
-// assigned to warps statically (units of a.grab points, warp w taking units
-// w, w + warps, ...), which lets a warp run a three-stage software pipeline:
-// while it refines packet k, the grouped points of packet k + 2 and the
-// candidate ranges of packet k + 1 are being loaded, and the run of packet
-// k + 1's entry records is bulk-copied into the other staging buffer.  For
-// packet k the warp walks its lanes' candidate lists; every (point,
-// candidate) pair that passes the FP32 box filter is either inside the
-// slot's interior box (emitted at once) or appended to a warp-local queue in
-// shared memory, converted to the slot's frame (q + off) with its error
-// tolerance.  Each time 32 pairs are queued, every lane refines one of them,
-// so the ring walks run with all lanes busy.  Neighbouring queue entries
-// mostly share a polygon, so vertex reads stay broadcasts.
+// kMinBlocks: resident blocks per SM the registers are capped for (4: 64
+// registers, no spills; 5: 48 registers, more warps, a few spills).
 template <bool kMulti, bool kBins, bool kF64, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(const LqArgs a) {
     __shared__ int2 s_buf[kThreads / 32][kWarpBuf];
     __shared__ unsigned s_cnt[kThreads / 32];
     __shared__ QueuedPair s_q[kThreads / 32][kQueue];
-    __shared__ __align__(128) EntryRecord s_recs[kThreads / 32][2][kStageRecs];
-    __shared__ uint64_t s_bar[kThreads / 32][2];
+    __shared__ __align__(128) EntryRecord s_recs[kThreads / 32][kStageRecs];
+    __shared__ uint64_t s_bar[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
         s_cnt[warp] = 0;
-        mbar_init(&s_bar[warp][0]);
-        mbar_init(&s_bar[warp][1]);
+        mbar_init(&s_bar[warp]);
     }
     __syncwarp();
-    uint32_t phase[2] = {0u, 0u};
+    uint32_t phase = 0;
     const WarpOut out{s_buf[warp], &s_cnt[warp]};
     QueuedPair* qp = s_q[warp];
+    const EntryRecord* st = s_recs[warp];
     const unsigned lt = (1u << lane) - 1u;
     const int64_t n = (int64_t)*a.n_grouped;
     unsigned long long n_cand = 0;
     unsigned n32 = 0, n64 = 0;
     int nq = 0;  // warp-uniform queue length
-    // packet number of the warp's k-th packet
-    const int64_t per_unit = a.grab / 32;
-    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    auto packet = [&](int64_t k) { return (gw + (k / per_unit) * nw) * per_unit + k % per_unit; };
-    // prologue: packet 0 complete and staged, packet 1's range in flight
-    PacketLanes cur, nxt;
-    cur.p = fetch_point(a, packet(0) * 32 + lane, n);
-    nxt.p = fetch_point(a, packet(1) * 32 + lane, n);
-    fetch_range<kMulti>(a, cur);
-    PacketRun run = stage_run<kMulti>(a, cur, s_recs[warp][0], &s_bar[warp][0], lane);
-    fetch_range<kMulti>(a, nxt);
-    for (int64_t k = 0; packet(k) * 32 < n; ++k) {  // warp-uniform
-        const int b = (int)(k & 1);
-        const CellPoint after = fetch_point(a, packet(k + 2) * 32 + lane, n);  // packet k + 2, in flight
-        if (run.staged && !__all_sync(0xffffffffu, mbar_wait_bounded(&s_bar[warp][b], phase[b]))) {
-            // record the timeout, give the copy one more bounded wait, stop this warp
-            if (lane == 0) atomicOr(&a.counters[4], 2ull);
-            mbar_wait_bounded(&s_bar[warp][b], phase[b]);
-            return;
-        }
-        if (run.staged) phase[b] ^= 1u;
-        const EntryRecord* st = s_recs[warp][b];
-        const uint32_t maxlen = warp_max_u32(cur.len);
-        const float dq = __fmaf_ru(fmaxf(fabsf(cur.p.qx), fabsf(cur.p.qy)), 6.1e-8f, 1e-37f);
-        const LearnedJob& J = job_desc<kMulti>(a, cur.job);
-        const EntryRecord* recs = J.recs;
-        for (uint32_t kk = 0; kk < maxlen; ++kk) {
-            bool inbox = false;
-            EntryRecord r;
-            if (kk < cur.len) {
-                const uint32_t si = cur.lo + kk - run.lo;  // unsigned: below the run wraps to a large index
-                r = (run.staged && si < run.hi - run.lo) ? st[si] : recs[cur.lo + kk];
-                inbox = box_filter_fp32(r.box, cur.p.qx, cur.p.qy, dq);
+    for (;;) {
+        const int64_t b0 = warp_grab(a.work, a.grab);
+        if (b0 >= n) break;
+        const int64_t e0 = b0 + a.grab < n ? b0 + a.grab : n;
+        for (int64_t base = b0; base < e0; base += 32) {
+            const GroupedLane g = load_grouped<kMulti>(a, base + lane, e0);
+            const uint32_t maxlen = warp_max_u32(g.len);
+            const EntryRecord* recs = job_desc<kMulti>(a, g.job).recs;
+            // stage the packet's run of records (warp-uniform decision)
+            const unsigned has = __ballot_sync(0xffffffffu, g.len > 0);
+            const int first = has ? __ffs(has) - 1 : 0, last = has ? 31 - __clz(has) : 0;
+            const uint32_t run_lo = __shfl_sync(0xffffffffu, g.lo, first);
+            const uint32_t run_hi = __shfl_sync(0xffffffffu, g.lo + g.len, last);
+            const int job0 = __shfl_sync(0xffffffffu, g.job, first);  // every lane takes part in the shuffle
+            const bool one_job = !kMulti || __all_sync(0xffffffffu, g.len == 0 || g.job == job0);
+            const bool staged = !a.no_stage && has != 0 && one_job && run_hi - run_lo <= (uint32_t)kStageRecs;
+            if (staged) {
+                __syncwarp();  // every lane is done with the buffer's previous run
+                if (lane == 0) bulk_load(s_recs[warp], recs + run_lo, (run_hi - run_lo) * (uint32_t)sizeof(EntryRecord),
+                                         &s_bar[warp]);
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&s_bar[warp], phase))) {
+                    // record the timeout, give the copy one more bounded wait, stop this warp
+                    if (lane == 0) atomicOr(&a.counters[4], 2ull);
+                    mbar_wait_bounded(&s_bar[warp], phase);
+                    return;
+                }
+                phase ^= 1u;
             }
-            // the point in the slot's frame; its error against the real p -
-            // origin is at most dq + |off error| (in r.err with the vertex
-            // error) + the rounding of this addition (es)
-            float sx = 0.f, sy = 0.f, t = 0.f;
-            bool walk = false, direct = false;
-            if (inbox) {
-                ++n_cand;
-                sx = __fadd_rn(cur.p.qx, r.offx);
-                sy = __fadd_rn(cur.p.qy, r.offy);
-                const float es = __fmaf_ru(fmaxf(fabsf(sx), fabsf(sy)), 6.1e-8f, 1e-37f);
-                t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, dq), es), 1.0001f);
-                walk = true;
-                if (!a.no_interior && entry_has_interior(r)) {
-                    // strictly inside the slot's interior box, whatever the
-                    // rounding: interior, no ring walk
-                    const float4 ib = J.ib32[entry_slot(r)];
-                    if (__fsub_rd(sx, t) > ib.x && __fadd_ru(sx, t) < ib.z && __fsub_rd(sy, t) > ib.y &&
-                        __fadd_ru(sy, t) < ib.w) {
-                        walk = false;
-                        direct = (a.q.accept_mask >> LOC_INTERIOR) & 1;
+            const float4* ib32 = job_desc<kMulti>(a, g.job).ib32;
+            for (uint32_t k = 0; k < maxlen; ++k) {
+                bool inbox = false;
+                EntryRecord r;
+                if (k < g.len) {
+                    const uint32_t si = g.lo + k - run_lo;  // unsigned: below the run wraps to a large index
+                    r = (staged && si < run_hi - run_lo) ? st[si] : recs[g.lo + k];
+                    inbox = box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq);
+                }
+                // the point in the slot's frame; its error against the real p -
+                // origin is at most dq + |off error| (in r.err with the vertex
+                // error) + the rounding of this addition (es)
+                float sx = 0.f, sy = 0.f, t = 0.f;
+                bool walk = false, direct = false;
+                if (inbox) {
+                    ++n_cand;
+                    sx = __fadd_rn(g.p.qx, r.offx);
+                    sy = __fadd_rn(g.p.qy, r.offy);
+                    const float es = __fmaf_ru(fmaxf(fabsf(sx), fabsf(sy)), 6.1e-8f, 1e-37f);
+                    t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, g.dq), es), 1.0001f);
+                    walk = true;
+                    if (!a.no_interior && entry_has_interior(r)) {
+                        // strictly inside the slot's interior box, whatever the
+                        // rounding: interior, no ring walk
+                        const float4 ib = ib32[entry_slot(r)];
+                        if (__fsub_rd(sx, t) > ib.x && __fadd_ru(sx, t) < ib.z && __fsub_rd(sy, t) > ib.y &&
+                            __fadd_ru(sy, t) < ib.w) {
+                            walk = false;
+                            direct = (a.q.accept_mask >> LOC_INTERIOR) & 1;
+                        }
                     }
                 }
-            }
-            wemit_sync(out, a.sink, direct, cur.p.row, direct ? J.item_geom[entry_slot(r)] : 0);
-            const unsigned m = __ballot_sync(0xffffffffu, walk);
-            if (walk) {
-                QueuedPair& e = qp[nq + __popc(m & lt)];
-                e.qx = sx;
-                e.qy = sy;
-                e.t = t;
-                e.row = cur.p.row;
-                e.slot = entry_slot(r);
-                e.job = cur.job;
-            }
-            nq += __popc(m);
-            __syncwarp();
-            if (nq >= 32) {
-                refine_queued<kMulti, kBins, kF64>(a, out, qp, 32, lane, n32, n64);
+                wemit_sync(out, a.sink, direct, g.p.row,
+                           direct ? job_desc<kMulti>(a, g.job).item_geom[entry_slot(r)] : 0);
+                const unsigned m = __ballot_sync(0xffffffffu, walk);
+                if (walk) {
+                    QueuedPair& e = qp[nq + __popc(m & lt)];
+                    e.qx = sx;
+                    e.qy = sy;
+                    e.t = t;
+                    e.row = g.p.row;
+                    e.slot = entry_slot(r);
+                    e.job = g.job;
+                }
+                nq += __popc(m);
                 __syncwarp();
-                if (lane < nq - 32) qp[lane] = qp[32 + lane];
-                nq -= 32;
-                __syncwarp();
+                if (nq >= 32) {
+                    refine_queued<kMulti, kBins, kF64>(a, out, qp, 32, lane, n32, n64);
+                    __syncwarp();
+                    if (lane < nq - 32) qp[lane] = qp[32 + lane];
+                    nq -= 32;
+                    __syncwarp();
+                }
             }
+            wflush(out, a.sink, false);
         }
-        wflush(out, a.sink, false);
-        // advance: packet k + 1 becomes current (its range has arrived: stage
-        // its run into the other buffer), packet k + 2's range is requested
-        cur = nxt;
-        __syncwarp();  // every lane is done with the other buffer's previous run
-        run = stage_run<kMulti>(a, cur, s_recs[warp][b ^ 1], &s_bar[warp][b ^ 1], lane);
-        nxt.p = after;
-        fetch_range<kMulti>(a, nxt);
     }
     if (nq > 0) refine_queued<kMulti, kBins, kF64>(a, out, qp, nq, lane, n32, n64);
     wflush(out, a.sink, true);
-    // a copy started for the packet after the last one (there is none) is
-    // never started: stage_run stages only runs with points (has != 0)
     add_counter(a.counters, 5, n_cand);
     add_counter(a.counters, 2, n32);
     add_counter(a.counters, 3, n64);
