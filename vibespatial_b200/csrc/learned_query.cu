@@ -260,24 +260,27 @@ __device__ __forceinline__ int learned_lookup(const LearnedJob& J, uint32_t gx, 
     const uint32_t occ_word = J.occ[ob >> 5];
     const uint32_t leaf_id = kBsearch ? 0u : (uint32_t)J.root_table[cell >> J.root_shift];
     if (!((occ_word >> (ob & 31)) & 1u)) return -1;
-    long long l0 = 0, h0 = J.n_cells;  // search [l0, h0)
+    // search [l0, h0) with 32-bit indices (a cell count fits in 31 bits)
+    int l0 = 0, h0 = (int)J.n_cells;
     if constexpr (!kBsearch) {
         const RmiLeaf lf = J.leaves[leaf_id];
         if (lf.lo > lf.hi) return -1;  // no stored key routes to this leaf
         const long long pred = rmi_predict(make_double2(lf.a, lf.b), cell);
-        l0 = pred + lf.lo;
-        h0 = pred + lf.hi + 1;
-        l0 = l0 < 0 ? 0 : l0;
-        h0 = h0 > J.n_cells ? J.n_cells : h0;
+        long long w0 = pred + lf.lo, w1 = pred + lf.hi + 1;
+        w0 = w0 < 0 ? 0 : w0;
+        w1 = w1 > J.n_cells ? J.n_cells : w1;
+        if (w1 <= w0) return -1;  // the window lies outside the stored keys
+        l0 = (int)w0;
+        h0 = (int)w1;
         if (h0 - l0 > 256) ++n_wide;
     }
-    const long long h1 = h0;
+    const int h1 = h0;
     while (l0 < h0) {
-        const long long mid = (l0 + h0) >> 1;
+        const int mid = (int)(((uint32_t)l0 + (uint32_t)h0) >> 1);
         if (J.cell_keys[mid] < cell) l0 = mid + 1;
         else h0 = mid;
     }
-    return (l0 < h1 && J.cell_keys[l0] == cell) ? (int)l0 : -1;
+    return (l0 < h1 && J.cell_keys[l0] == cell) ? l0 : -1;
 }
 
 // Job of every lane's point: lane 0 binary-searches the packet's first point,
