@@ -652,13 +652,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                            direct ? job_desc<kMulti>(a, g.job).item_geom[entry_slot(r)] : 0);
                 const unsigned m = __ballot_sync(0xffffffffu, walk);
                 if (walk) {
-                    QueuedPair& e = qp[nq + __popc(m & lt)];
-                    e.qx = sx;
-                    e.qy = sy;
-                    e.t = t;
-                    e.row = g.p.row;
-                    e.slot = entry_slot(r);
-                    e.job = g.job;
+                    // the queue entry as two 16-byte stores
+                    float4* e = reinterpret_cast<float4*>(&qp[nq + __popc(m & lt)]);
+                    e[0] = make_float4(sx, sy, t, __int_as_float(g.p.row));
+                    e[1] = make_float4(__int_as_float(entry_slot(r)), __int_as_float(g.job), 0.f, 0.f);
                 }
                 nq += __popc(m);
                 __syncwarp();
