@@ -312,7 +312,9 @@ typedef struct vs_batch_options {
     int32_t method;           /* VS_METHOD_RTREE (0) or VS_METHOD_LEARNED: every index with polygons
                                  must then have its learned part (VS_E_ARG otherwise) */
     int32_t learned_map_blocks_per_sm;    /* learned: map pass blocks per SM (0 = 8) */
-    int32_t learned_refine_blocks_per_sm; /* learned: refine pass blocks per SM (0 = as many as fit) */
+    int32_t learned_refine_blocks_per_sm; /* learned: refine pass blocks per SM: 1-3 run the 80-register build,
+                                             4 (and 0, the default: as many as fit) the 64-register one, 5-8 the
+                                             48-register one */
     int32_t learned_grab;     /* learned: grouped points a refine warp takes per grab (0 = 32; rounded up to 32s) */
     uint32_t learned_flags;   /* learned: VS_JOIN_LEARNED_BSEARCH | _FP64_WALK | _NO_STAGE | _NO_INTERIOR (ablations) */
     int32_t learned_map_packets; /* learned: 32-point packets a map warp looks up together, 1 or 2 (0 = 1) */
