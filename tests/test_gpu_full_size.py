@@ -48,6 +48,14 @@ def degenerate(vsabi, ctx, oracle):
     return SimpleNamespace(w=w, index=index, pts=pts, exp=exp, keep=(keep_p, keep_q))
 
 
+def test_degenerate_cell_level_is_refined(degenerate):
+    """The multipolygons' wide boxes pull the mean box side up (level 7 from it, 35 entries per cell); the automatic
+    level is refined while cells hold more than 2.5 entries on average, within the registration budget."""
+    info = degenerate.index.info()
+    assert info["cell_level"] >= 8
+    assert info["n_cell_entries"] / info["n_cells"] < 12.0
+
+
 @pytest.mark.parametrize("method", ["rtree", "learned"])
 @pytest.mark.parametrize("predicate", ["within", "intersects"])
 def test_degenerate_full_size(vsabi, degenerate, predicate, method):

@@ -616,69 +616,55 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) learned_refine_kernel(co
                 }
                 phase ^= 1u;
             }
-            const LearnedJob& J = job_desc<kMulti>(a, g.job);
-            // Candidates in chunks of 32: phase 1 box-tests each lane's
-            // candidates on its own (no warp synchronisation) into a bit mask
-            // of survivors; phase 2 steps the warp through the survivors only,
-            // converting, interior-testing and queueing them.
-            for (uint32_t k0 = 0; k0 < maxlen; k0 += 32) {
-                const uint32_t k1 = g.len < k0 ? 0u : (g.len - k0 < 32u ? g.len - k0 : 32u);
-                uint32_t bits = 0;
-                for (uint32_t k = 0; k < k1; ++k) {
-                    const uint32_t e = g.lo + k0 + k;
-                    const uint32_t si = e - run_lo;  // unsigned: below the run wraps to a large index
-                    const float4 box = (staged && si < run_hi - run_lo) ? st[si].box : recs[e].box;
-                    if (box_filter_fp32(box, g.p.qx, g.p.qy, g.dq)) bits |= 1u << k;
+            const float4* ib32 = job_desc<kMulti>(a, g.job).ib32;
+            for (uint32_t k = 0; k < maxlen; ++k) {
+                bool inbox = false;
+                EntryRecord r;
+                if (k < g.len) {
+                    const uint32_t si = g.lo + k - run_lo;  // unsigned: below the run wraps to a large index
+                    r = (staged && si < run_hi - run_lo) ? st[si] : recs[g.lo + k];
+                    inbox = box_filter_fp32(r.box, g.p.qx, g.p.qy, g.dq);
                 }
-                n_cand += (unsigned)__popc(bits);
-                while (__any_sync(0xffffffffu, bits != 0)) {  // warp-uniform
-                    bool walk = false, direct = false;
-                    float sx = 0.f, sy = 0.f, t = 0.f;
-                    int32_t slot = 0;
-                    if (bits) {
-                        const uint32_t k = (uint32_t)(__ffs(bits) - 1);
-                        bits &= bits - 1u;
-                        const uint32_t e = g.lo + k0 + k;
-                        const uint32_t si = e - run_lo;
-                        const EntryRecord r = (staged && si < run_hi - run_lo) ? st[si] : recs[e];
-                        slot = entry_slot(r);
-                        // the point in the slot's frame; its error against the
-                        // real p - origin is at most dq + |off error| (in r.err
-                        // with the vertex error) + the rounding of this
-                        // addition (es)
-                        sx = __fadd_rn(g.p.qx, r.offx);
-                        sy = __fadd_rn(g.p.qy, r.offy);
-                        const float es = __fmaf_ru(fmaxf(fabsf(sx), fabsf(sy)), 6.1e-8f, 1e-37f);
-                        t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, g.dq), es), 1.0001f);
-                        walk = true;
-                        if (!a.no_interior && entry_has_interior(r)) {
-                            // strictly inside the slot's interior box, whatever
-                            // the rounding: interior, no ring walk
-                            const float4 ib = J.ib32[slot];
-                            if (__fsub_rd(sx, t) > ib.x && __fadd_ru(sx, t) < ib.z && __fsub_rd(sy, t) > ib.y &&
-                                __fadd_ru(sy, t) < ib.w) {
-                                walk = false;
-                                direct = (a.q.accept_mask >> LOC_INTERIOR) & 1;
-                            }
+                // the point in the slot's frame; its error against the real p -
+                // origin is at most dq + |off error| (in r.err with the vertex
+                // error) + the rounding of this addition (es)
+                float sx = 0.f, sy = 0.f, t = 0.f;
+                bool walk = false, direct = false;
+                if (inbox) {
+                    ++n_cand;
+                    sx = __fadd_rn(g.p.qx, r.offx);
+                    sy = __fadd_rn(g.p.qy, r.offy);
+                    const float es = __fmaf_ru(fmaxf(fabsf(sx), fabsf(sy)), 6.1e-8f, 1e-37f);
+                    t = __fmul_ru(__fadd_ru(__fadd_ru(r.err, g.dq), es), 1.0001f);
+                    walk = true;
+                    if (!a.no_interior && entry_has_interior(r)) {
+                        // strictly inside the slot's interior box, whatever the
+                        // rounding: interior, no ring walk
+                        const float4 ib = ib32[entry_slot(r)];
+                        if (__fsub_rd(sx, t) > ib.x && __fadd_ru(sx, t) < ib.z && __fsub_rd(sy, t) > ib.y &&
+                            __fadd_ru(sy, t) < ib.w) {
+                            walk = false;
+                            direct = (a.q.accept_mask >> LOC_INTERIOR) & 1;
                         }
                     }
-                    wemit_sync(out, a.sink, direct, g.p.row, direct ? J.item_geom[slot] : 0);
-                    const unsigned m = __ballot_sync(0xffffffffu, walk);
-                    if (walk) {
-                        // the queue entry as two 16-byte stores
-                        float4* q = reinterpret_cast<float4*>(&qp[nq + __popc(m & lt)]);
-                        q[0] = make_float4(sx, sy, t, __int_as_float(g.p.row));
-                        q[1] = make_float4(__int_as_float(slot), __int_as_float(g.job), 0.f, 0.f);
-                    }
-                    nq += __popc(m);
+                }
+                wemit_sync(out, a.sink, direct, g.p.row,
+                           direct ? job_desc<kMulti>(a, g.job).item_geom[entry_slot(r)] : 0);
+                const unsigned m = __ballot_sync(0xffffffffu, walk);
+                if (walk) {
+                    // the queue entry as two 16-byte stores
+                    float4* e = reinterpret_cast<float4*>(&qp[nq + __popc(m & lt)]);
+                    e[0] = make_float4(sx, sy, t, __int_as_float(g.p.row));
+                    e[1] = make_float4(__int_as_float(entry_slot(r)), __int_as_float(g.job), 0.f, 0.f);
+                }
+                nq += __popc(m);
+                __syncwarp();
+                if (nq >= 32) {
+                    refine_queued<kMulti, kBins, kF64>(a, out, qp, 32, lane, n32, n64);
                     __syncwarp();
-                    if (nq >= 32) {
-                        refine_queued<kMulti, kBins, kF64>(a, out, qp, 32, lane, n32, n64);
-                        __syncwarp();
-                        if (lane < nq - 32) qp[lane] = qp[32 + lane];
-                        nq -= 32;
-                        __syncwarp();
-                    }
+                    if (lane < nq - 32) qp[lane] = qp[32 + lane];
+                    nq -= 32;
+                    __syncwarp();
                 }
             }
             wflush(out, a.sink, false);
