@@ -1034,24 +1034,28 @@ def run_ours(args, rank, world, local_rank):
     dx = torch.from_numpy(px).to(dev)
     dy = torch.from_numpy(py).to(dev)
     pts = _abi.make_points(dx, dy)
-    # learned + batched: the join as a one-job batch plan (the persistent
-    # learned pipeline replayed from a CUDA graph)
+    # size the pair buffers once (exact count from a first join)
+    cap = max(1024, N)
+    left = torch.empty(cap, dtype=torch.int32, device=dev)
+    right = torch.empty(cap, dtype=torch.int32, device=dev)
+    try:
+        n_pairs, _ = index.join_into(pts, pred, method, left, right)
+    except _abi.CapacityError as e:
+        cap = e.required
+        left = torch.empty(cap, dtype=torch.int32, device=dev)
+        right = torch.empty(cap, dtype=torch.int32, device=dev)
+        n_pairs, _ = index.join_into(pts, pred, method, left, right)
     plan = None
     plan_opts, plan_opts_src = None, None
     if batched:
+        # learned + batched: the join as a one-job batch plan (the persistent
+        # learned pipeline replayed from a CUDA graph), its launch shape from the
+        # autotuner (cached, else searched now, before any timing)
         from vibespatial_b200 import autotune
 
-        # launch shape from the autotuner (cached, else searched now, before any timing)
-        probe_cap = max(1024, N)
-        pl = torch.empty(probe_cap, dtype=torch.int32, device=dev)
-        pr = torch.empty(probe_cap, dtype=torch.int32, device=dev)
-        try:
-            plan_opts, plan_opts_src = autotune.tuned_options(
-                ctx, [index], pts, [0, N], pred, len(w.polys), left=pl, right=pr, use_cache=not args.autotune,
-                method=_abi.METHOD_LEARNED, with_source=True)
-        except _abi.CapacityError:  # more pairs than points: keep the defaults
-            plan_opts, plan_opts_src = dict(autotune.LEARNED_DEFAULTS), "defaults (pairs exceed the probe buffer)"
-        del pl, pr
+        plan_opts, plan_opts_src = autotune.tuned_options(
+            ctx, [index], pts, [0, N], pred, len(w.polys), left=left, right=right, use_cache=not args.autotune,
+            method=_abi.METHOD_LEARNED, with_source=True)
         plan = _abi.BatchPlan(ctx, [index], pts, [0, N], options=dict(plan_opts, method=_abi.METHOD_LEARNED))
 
     def join(lft, rgt):
@@ -1084,17 +1088,6 @@ def run_ours(args, rank, world, local_rank):
                 tdist.send(rgt[:n_local], dst=0)
         return counts
 
-    # size the pair buffers once (exact count from a first join)
-    cap = max(1024, N)
-    left = torch.empty(cap, dtype=torch.int32, device=dev)
-    right = torch.empty(cap, dtype=torch.int32, device=dev)
-    try:
-        n_pairs, _ = index.join_into(pts, pred, method, left, right)
-    except _abi.CapacityError as e:
-        cap = e.required
-        left = torch.empty(cap, dtype=torch.int32, device=dev)
-        right = torch.empty(cap, dtype=torch.int32, device=dev)
-        n_pairs, _ = index.join_into(pts, pred, method, left, right)
     assert join(left, right)[0] == n_pairs
     # plain R-tree on the same GPU, for the learned-vs-plain ratio
     plain = None
