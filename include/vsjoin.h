@@ -100,7 +100,8 @@ typedef struct vs_points {
 typedef struct vs_index_options {
     int32_t method_mask; /* bit 0: R-tree (always built), bit 1: learned cell index */
     int32_t cell_level;  /* learned index grid level (0 = choose automatically) */
-    int32_t rmi_leaves;  /* learned index leaf models (0 = 4096) */
+    int32_t rmi_leaves;  /* learned index leaf models (0 = 4096, or one per 64 cell keys above 256k keys;
+                            at most 65535) */
     int32_t rmi_train_steps; /* 0 = default */
     int32_t ring_bin_min_vertices; /* rings with at least this many vertices get 8 y-bins of edges, so a
                                       point's ring walk visits only the edges of its bin (0 = 16, < 0 = none) */

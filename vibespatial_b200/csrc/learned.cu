@@ -120,6 +120,21 @@ __global__ void cell_flag_kernel(const uint32_t* __restrict__ keys, int64_t E, u
         flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
 }
 
+// Sum over the distinct cells of (entries in the cell)^2, from the sorted
+// keys: each cell's first entry measures its run.  Divided by the entry
+// count it is the mean list length seen from an entry (its own cell's count).
+__global__ void cell_run_sq_kernel(const uint32_t* __restrict__ keys, int64_t E, unsigned long long* __restrict__ acc) {
+    unsigned long long t = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i > 0 && keys[i] == keys[i - 1]) continue;
+        int64_t j = i + 1;
+        while (j < E && keys[j] == keys[i]) ++j;
+        t += (unsigned long long)(j - i) * (unsigned long long)(j - i);
+    }
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0 && t) atomicAdd(acc, t);
+}
+
 __global__ void cell_compact_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ id, int64_t E,
                                     uint32_t* __restrict__ cell_keys, uint32_t* __restrict__ cell_start) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x) {
@@ -580,16 +595,17 @@ int dalloc(T** p, size_t n, int64_t& bytes) {
     return VS_OK;
 }
 
-// Registrations (E) and distinct cells (n_cells) of the slot boxes at grid
-// level L, on scratch only: the count, emit, sort and unique-flag steps of
-// the build.
+// Registrations (E), distinct cells (n_cells) and the sum over cells of
+// their squared entry counts (sum_sq) of the slot boxes at grid level L, on
+// scratch only: the count, emit, sort and unique-flag steps of the build.
 int probe_level(cudaStream_t s, const vs_box* boxes, int64_t M, const double* frame, int L, uint32_t* cnt,
-                unsigned long long* tot, unsigned long long& E, uint32_t& n_cells) {
+                unsigned long long* tot, unsigned long long& E, uint32_t& n_cells, unsigned long long& sum_sq) {
     VS_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), s));
     cell_count_kernel<<<grid_for(M, 256), 256, 0, s>>>(boxes, M, frame, L, cnt, tot);
     VS_CUDA_TRY(cudaMemcpyAsync(&E, tot, sizeof(E), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
     n_cells = 0;
+    sum_sq = 0;
     if (E == 0 || E >= 0x7fffffffull) return VS_OK;
     Scratch<uint32_t> off, keys, vals, flag, nc;
     VS_TRY(off.alloc((size_t)M, s));
@@ -603,7 +619,10 @@ int probe_level(cudaStream_t s, const vs_box* boxes, int64_t M, const double* fr
     VS_TRY(radix_sort_u32_u32(keys.p, vals.p, (int64_t)E, 2 * L, s));
     cell_flag_kernel<<<grid_for((int64_t)E, 256), 256, 0, s>>>(keys.p, (int64_t)E, flag.p);
     VS_TRY(exclusive_scan_u32(flag.p, flag.p, (int64_t)E, nc.p, s));
+    VS_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), s));
+    cell_run_sq_kernel<<<grid_for((int64_t)E, 256), 256, 0, s>>>(keys.p, (int64_t)E, tot);
     VS_CUDA_TRY(cudaMemcpyAsync(&n_cells, nc.p, sizeof(n_cells), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaMemcpyAsync(&sum_sq, tot, sizeof(sum_sq), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
     return VS_OK;
 }
@@ -738,6 +757,12 @@ void free_learned_index(vs_index* idx) {
     li = LearnedIndex{};
 }
 
+static int auto_leaves(int64_t n_keys) {
+    int64_t l = 4096;
+    while (l < 65536 && l * 64 < n_keys) l *= 2;
+    return (int)std::min<int64_t>(l, 65535);
+}
+
 int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* opts) {
     LearnedIndex& li = idx->learned;
     cudaStream_t s = ctx->stream;
@@ -775,24 +800,29 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
         if (L <= 1 || E <= (unsigned long long)(16 * M + (1 << 20))) break;
         --L;
     }
-    // An automatic level is then refined (at most 3 levels) while a cell
-    // holds more than 2.5 entries on average and the finer level's
-    // registrations stay within the budget: the refine tests every entry of
-    // a point's cell, so long lists cost more than the extra registrations.
-    // (A box side mean is pulled up by a few wide boxes, such as multipolygons
-    // with spread parts, which leaves the cells too coarse for the rest.)
+    // An automatic level is then refined (at most 3 levels) while the mean
+    // list length seen from an entry (sum over cells of count^2 / E) is above
+    // 2.5 and the finer level's registrations stay within the budget.  The
+    // refine tests every entry of a point's cell, and query points crowd
+    // where the boxes crowd, so the lists that matter are the long ones of
+    // the dense cells, which the plain mean E / n_cells hides under the many
+    // one-entry cells around them.  (A box side mean is also pulled up by a
+    // few wide boxes, such as multipolygons with spread parts, which leaves
+    // the cells too coarse for the rest.)
     if (auto_level && E > 0) {
         uint32_t nc = 0;
-        VS_TRY(probe_level(s, boxes, M, idx->frame, L, cnt.p, tot.p, E, nc));
+        unsigned long long sq = 0;
+        VS_TRY(probe_level(s, boxes, M, idx->frame, L, cnt.p, tot.p, E, nc, sq));
         const int l_max = std::min(15, L + 3);
-        while (L < l_max && nc > 0 && (double)E > 2.5 * (double)nc) {
-            unsigned long long e1 = 0;
+        while (L < l_max && nc > 0 && (double)sq > 2.5 * (double)E) {
+            unsigned long long e1 = 0, sq1 = 0;
             uint32_t nc1 = 0;
-            VS_TRY(probe_level(s, boxes, M, idx->frame, L + 1, cnt.p, tot.p, e1, nc1));
+            VS_TRY(probe_level(s, boxes, M, idx->frame, L + 1, cnt.p, tot.p, e1, nc1, sq1));
             if (e1 > (unsigned long long)(16 * M + (1 << 20)) || e1 >= 0x7fffffffull) break;
             ++L;
             E = e1;
             nc = nc1;
+            sq = sq1;
         }
         // the counts of the chosen level, for the emit below
         VS_CUDA_TRY(cudaMemsetAsync(tot.p, 0, sizeof(unsigned long long), s));
@@ -831,7 +861,7 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     VS_CUDA_TRY(cudaMemcpyAsync(li.cell_start + nc, &Eu, sizeof(Eu), cudaMemcpyHostToDevice, s));
     // 4. occupancy bitmap
 #ifndef VS_OCC_MAX_LEVEL
-#define VS_OCC_MAX_LEVEL 12
+#define VS_OCC_MAX_LEVEL 13  // 8 MB at level 13, L2-resident
 #endif
     li.occ_level = std::min(L, VS_OCC_MAX_LEVEL);
     const int64_t occ_bits = 1ll << (2 * li.occ_level);
@@ -840,7 +870,10 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     occ_kernel<<<grid_for(nc, 256), 256, 0, s>>>(li.cell_keys, nc, 2 * (L - li.occ_level), li.occ);
     VS_CUDA_TRY(cudaGetLastError());
     // 5. RMI (root tabulated over level-R ancestors)
-    li.n_leaves = (opts && opts->rmi_leaves > 0) ? std::min(opts->rmi_leaves, 65535) : 4096;
+    // leaves: 4096, or one per 64 stored keys (to the next power of two, at
+    // most 65535, the root table's 16-bit leaf ids) when there are more than
+    // 256k keys, so that a leaf's error window stays a few dozen keys wide
+    li.n_leaves = (opts && opts->rmi_leaves > 0) ? std::min(opts->rmi_leaves, 65535) : auto_leaves((int64_t)nc);
     li.root_level = std::min(L, 10);
     const int steps = (opts && opts->rmi_train_steps > 0) ? opts->rmi_train_steps : 300;
     cudaEvent_t e0, e1;
