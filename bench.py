@@ -1027,7 +1027,8 @@ def run_ours(args, rank, world, local_rank):
     batched = args.method == "learned-batched"
     pred = {"within": _abi.PRED_WITHIN, "intersects": _abi.PRED_INTERSECTS}[args.predicate]
     t0 = time.perf_counter()
-    index = _abi.DeviceIndex(ctx, P, learned=(method == _abi.METHOD_LEARNED), ring_bin_min_vertices=args.ring_bin_min)
+    index = _abi.DeviceIndex(ctx, P, learned=(method == _abi.METHOD_LEARNED), ring_bin_min_vertices=args.ring_bin_min,
+                             cell_level=args.cell_level)
     build_wall = time.perf_counter() - t0
     info = index.info()
     del d_poly
@@ -1459,6 +1460,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ring-bin-min", type=int, default=0,
                     help="rings with at least this many vertices get y-bins (0: library default, <0: none)")
+    ap.add_argument("--cell-level", type=int, default=0,
+                    help="learned index grid level of the join workloads (0: automatic); a scaled-down profiling "
+                         "run can keep the full-size workload's level")
     ap.add_argument("--autotune", action="store_true",
                     help="batched workload: search the launch shape now instead of using the cache/defaults")
     ap.add_argument("--profile", action="store_true",

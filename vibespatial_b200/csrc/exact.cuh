@@ -69,6 +69,24 @@ static __device__ __noinline__ int orient2d_exact(double ax, double ay, double b
     two_diff(bx, cx, bcx, bcxt);
     two_diff(ay, cy, acy, acyt);
     two_diff(by, cy, bcy, bcyt);
+    if (acxt == 0.0 && bcxt == 0.0 && acyt == 0.0 && bcyt == 0.0) {
+        // The differences are exact (lattice or nearby inputs), so the
+        // determinant is acx*bcy - acy*bcx = (p1 + q1) - (p2 + q2) with two
+        // exact products.  Its expansion x3 + x2 + x1 + x0 (Shewchuk's
+        // two-two-diff: nonoverlapping, x3 the largest, zeros possible)
+        // takes the sign of its largest nonzero component.  Same sign as the
+        // general sum below, in registers.
+        double p1, q1, p2, q2;
+        two_product(acx, bcy, p1, q1);
+        two_product(acy, bcx, p2, q2);
+        double i0, j0, z0, x0, x1, x2, x3;
+        two_diff(q1, q2, i0, x0);
+        two_sum(p1, i0, j0, z0);
+        two_diff(z0, p2, i0, x1);
+        two_sum(j0, i0, x3, x2);
+        const double top = x3 != 0.0 ? x3 : (x2 != 0.0 ? x2 : (x1 != 0.0 ? x1 : x0));
+        return (top > 0.0) - (top < 0.0);
+    }
     const double la[4] = {acx, acx, acxt, acxt};
     const double lb[4] = {bcy, bcyt, bcy, bcyt};
     const double ra[4] = {acy, acy, acyt, acyt};
@@ -204,11 +222,14 @@ __device__ __forceinline__ int ring_walk(double py, const double2* __restrict__ 
         return 0;
     }
     double2 a = xy[end - 1];
+    double2 b = xy[start];
     for (int i = start; i < end; ++i) {
-        const double2 b = xy[i];
+        // the next vertex's load is in flight while this edge is decided
+        const double2 nb = xy[i + 1 < end ? i + 1 : i];
         const int r = step(a, b, inside);
         if (r) return r;
         a = b;
+        b = nb;
     }
     return 0;
 }
