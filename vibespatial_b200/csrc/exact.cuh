@@ -222,14 +222,11 @@ __device__ __forceinline__ int ring_walk(double py, const double2* __restrict__ 
         return 0;
     }
     double2 a = xy[end - 1];
-    double2 b = xy[start];
     for (int i = start; i < end; ++i) {
-        // the next vertex's load is in flight while this edge is decided
-        const double2 nb = xy[i + 1 < end ? i + 1 : i];
+        const double2 b = xy[i];
         const int r = step(a, b, inside);
         if (r) return r;
         a = b;
-        b = nb;
     }
     return 0;
 }

@@ -18,10 +18,10 @@
 //            in FP32 against the entry's box relative to the same anchor
 //            (rounded outward); survivors are queued per warp and refined 32
 //            at a time with the FP32 crossing test on slot-relative
-//            coordinates; only edges whose FP32 decision lies within the
-//            rounding-error bound are re-decided in FP64 (the point's FP64
-//            coordinates are read back by row only then), and a pair the FP64
-//            filter cannot certify is deferred to the exact pass.
+//            coordinates; a pair with an edge whose FP32 decision lies within
+//            the rounding-error bound is deferred to the exact pass, which
+//            walks it on the FP64 coordinates (Shewchuk's stage-A filter, then
+//            the exact expansion).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -102,8 +102,8 @@ __device__ __forceinline__ int point_job(const LearnedQuery& q, int64_t pi) {
 // ------------------------------------------------------- split refine ---
 // One edge in FP32 on tile-relative coordinates.  Returns false when some
 // decision the exact walk needs lies within the rounding-error bound `t`
-// (the caller then re-decides the edge in FP64); otherwise applies the same
-// decision the exact walk would (the point cannot be on this edge).
+// (the caller then defers the pair to the exact pass); otherwise applies the
+// same decision the exact walk would (the point cannot be on this edge).
 __device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, float by, float px, float py, float t,
                                                bool& inside) {
     const float A2 = __fsub_rn(ay, py), B2 = __fsub_rn(by, py);
@@ -134,39 +134,40 @@ __device__ __forceinline__ bool edge_step_fp32(float ax, float ay, float bx, flo
     return false;
 }
 
-// One edge (vertex ia -> vertex ib) of the split ring walk: FP32 first, the
-// FP64 filter when the FP32 bound is inconclusive.  The FP64 point is read
-// from the query arrays (X, Y at pi) only then.  0: go on, 1: on the edge,
-// 2: undecided by the FP64 filter too.
+// The point's FP64 coordinates in the query arrays (X, Y at pi): read only to
+// pick a ring's y-bin.
 struct PointRef {
     const double* X;
     const double* Y;
     int64_t pi;
 };
 
-__device__ __forceinline__ int split_edge(float qx, float qy, float t, float2 a, float2 b,
-                                          const double2* __restrict__ xy, int ia, int ib, const PointRef& P,
-                                          bool& inside, unsigned& n32, unsigned& n64) {
+// One edge of the split ring walk in FP32.  0: decided, go on; 2: the FP32
+// bound is inconclusive, the pair goes to the exact pass (counted in n64).
+// Re-deciding such an edge in line in FP64 (the point's FP64 coordinates read
+// by row, the FP64 vertices, the stage-A filter) sent one lane on a long
+// detour while the others waited, and its registers made the 48-register
+// build spill; deferring the pair made the Zipf join 2% and the 256-job batch
+// 5% faster.
+__device__ __forceinline__ int split_edge(float qx, float qy, float t, float2 a, float2 b, bool& inside,
+                                          unsigned& n32, unsigned& n64) {
     if (edge_step_fp32(a.x, a.y, b.x, b.y, qx, qy, t, inside)) {
         ++n32;
         return 0;
     }
     ++n64;
-    const double2 A = xy[ia], B = xy[ib];
-    return edge_step_filtered(A.x, A.y, B.x, B.y, P.X[P.pi], P.Y[P.pi], inside);
+    return 2;
 }
 
 // Split-precision location of a point in one ring, every edge.
 __device__ __forceinline__ int ring_location_split(float qx, float qy, float t, const float2* __restrict__ xy32,
-                                                   const double2* __restrict__ xy, int start, int end,
-                                                   const PointRef& P, unsigned& n32, unsigned& n64) {
+                                                   int start, int end, unsigned& n32, unsigned& n64) {
     if (end - start < 2) return LOC_OUTSIDE;
     bool inside = false;
     float2 a = xy32[end - 1];
     float2 b = xy32[start];
     // an edge's start offset in y is the previous edge's end offset: carried
     float dA = __fsub_rn(a.y, qy);
-    int ia = end - 1;
     for (int i = start; i < end; ++i) {
         // the next vertex's load is in flight while this edge is decided
         const float2 nb = xy32[i + 1 < end ? i + 1 : i];
@@ -174,14 +175,11 @@ __device__ __forceinline__ int ring_location_split(float qx, float qy, float t, 
         if (fabsf(dA) > t && fabsf(dB) > t && (dA > 0.f) == (dB > 0.f)) {
             ++n32;  // both ends strictly on one side of the point's y: the edge changes nothing
         } else {
-            const int r = split_edge(qx, qy, t, a, b, xy, ia, i, P, inside, n32, n64);
-            if (r == 1) return LOC_BOUNDARY;
-            if (r == 2) return LOC_UNDECIDED;
+            if (split_edge(qx, qy, t, a, b, inside, n32, n64)) return LOC_UNDECIDED;
         }
         a = b;
         dA = dB;
         b = nb;
-        ia = i;
     }
     return inside ? LOC_INTERIOR : LOC_OUTSIDE;
 }
@@ -190,8 +188,7 @@ __device__ __forceinline__ int ring_location_split(float qx, float qy, float t, 
 // order; an edge that continues the previous one reuses its end vertex.  The
 // bin is chosen from the point's FP64 y (bins are defined on FP64 y).
 __device__ __forceinline__ int ring_location_split_binned(float qx, float qy, float t,
-                                                          const float2* __restrict__ xy32,
-                                                          const double2* __restrict__ xy, int start, int end,
+                                                          const float2* __restrict__ xy32, int start, int end,
                                                           const RingBins& bins, const uint16_t* __restrict__ edges,
                                                           const PointRef& P, unsigned& n32, unsigned& n64) {
     bool inside = false;
@@ -204,9 +201,7 @@ __device__ __forceinline__ int ring_location_split_binned(float qx, float qy, fl
         const int ia = i == start ? end - 1 : i - 1;
         const float2 a = ia == last ? lb : xy32[ia];
         const float2 b = xy32[i];
-        const int r = split_edge(qx, qy, t, a, b, xy, ia, i, P, inside, n32, n64);
-        if (r == 1) return LOC_BOUNDARY;
-        if (r == 2) return LOC_UNDECIDED;
+        if (split_edge(qx, qy, t, a, b, inside, n32, n64)) return LOC_UNDECIDED;
         last = i;
         lb = b;
     }
@@ -232,9 +227,9 @@ __device__ __forceinline__ int geometry_location_split(float qx, float qy, float
             const int c0 = J.ring_off[ring], c1 = J.ring_off[ring + 1];
             // the FP32 walk is cheap per edge, so bins pay off only on longer rings than for the FP64 walk
             const int rb = (kBins && J.rings.ring_bin && c1 - c0 >= kSplitBinMinVertices) ? J.rings.ring_bin[ring] : -1;
-            const int k = rb >= 0 ? ring_location_split_binned(qx, qy, t, J.xy32, J.xy, c0, c1, J.rings.bins[rb],
+            const int k = rb >= 0 ? ring_location_split_binned(qx, qy, t, J.xy32, c0, c1, J.rings.bins[rb],
                                                                J.rings.edges, P, n32, n64)
-                                  : ring_location_split(qx, qy, t, J.xy32, J.xy, c0, c1, P, n32, n64);
+                                  : ring_location_split(qx, qy, t, J.xy32, c0, c1, n32, n64);
             if (k == LOC_BOUNDARY || k == LOC_UNDECIDED) return k;
             if (k == LOC_INTERIOR) inside = !inside;
         }
@@ -536,7 +531,7 @@ __device__ __forceinline__ void refine_queued(const LqArgs& a, const WarpOut& ou
                                              J.rings);
         } else {
             const int2 cr = J.c01[jb.slot];
-            loc = cr.x >= 0 ? ring_location_split(jb.qx, jb.qy, jb.t, J.xy32, J.xy, cr.x, cr.y, P, n32, n64)
+            loc = cr.x >= 0 ? ring_location_split(jb.qx, jb.qy, jb.t, J.xy32, cr.x, cr.y, n32, n64)
                             : geometry_location_split<kBins>(jb.qx, jb.qy, jb.t, J, jb.slot, P, n32, n64);
         }
         if (loc == LOC_UNDECIDED) {
