@@ -78,6 +78,19 @@ struct LqArgs {
     bool no_interior;          // every box candidate is ring-walked (no interior-box shortcut)
 };
 
+// Streaming (evict-first) accesses for the read-once streams of the passes:
+// the query points, the staged cell points and the grouped cell points.  They
+// leave L2 to what is re-read: the index (cell keys, occupancy bitmap, leaves,
+// records, vertices) and the half-written sectors of the place pass.
+__device__ __forceinline__ CellPoint load_stream(const CellPoint* p) {
+    const float4 v = __ldcs(reinterpret_cast<const float4*>(p));
+    return CellPoint{v.x, v.y, __float_as_int(v.z), __float_as_uint(v.w)};
+}
+
+__device__ __forceinline__ void store_stream(CellPoint* p, const CellPoint& c) {
+    __stcs(reinterpret_cast<float4*>(p), make_float4(c.qx, c.qy, __int_as_float(c.row), __uint_as_float(c.gcell)));
+}
+
 // Job descriptor of a batch query (global memory) or of a single join (the
 // kernel parameters: uniform reads, no extra registers).
 template <bool kMulti>
@@ -299,7 +312,7 @@ __device__ __forceinline__ int map_point(const LqArgs& a, int64_t i, int job, co
     const LearnedQuery& q = a.q;
     if (i >= q.n) return -1;
     const LearnedJob& J = job_desc<kMulti>(a, job);
-    const double x = q.px[i], y = q.py[i];
+    const double x = __ldcs(q.px + i), y = __ldcs(q.py + i);
     if (!((q.pvalid == nullptr || q.pvalid[i]) && J.n_cells > 0 && x >= J.lox && x <= J.hix && y >= J.loy &&
           y <= J.hiy))
         return -1;
@@ -328,7 +341,7 @@ __device__ __forceinline__ void map_emit(const LqArgs& a, int64_t b0, int lane, 
         p.qy = qy;
         p.row = (int32_t)(b0 + lane + a.q.row_base);
         p.gcell = (uint32_t)gc;
-        a.staged[stripe * a.stripe_cap + sb + __popc(mm & ((1u << lane) - 1u))] = p;
+        store_stream(&a.staged[stripe * a.stripe_cap + sb + __popc(mm & ((1u << lane) - 1u))], p);
     }
 }
 
@@ -393,7 +406,7 @@ __global__ void __launch_bounds__(kThreads) learned_place_kernel(const LqArgs a)
                 const uint32_t k = k0 + u * 32 + lane;
                 gc[u] = -1;
                 if (k < cnt) {
-                    p[u] = src[k];
+                    p[u] = load_stream(src + k);
                     gc[u] = (int)p[u].gcell;
                 }
             }
@@ -438,7 +451,7 @@ __device__ __forceinline__ GroupedLane load_grouped(const LqArgs& a, int64_t j, 
     g.lo = g.len = 0;
     g.job = 0;
     if (j < e0) {
-        g.p = a.grouped[j];
+        g.p = load_stream(a.grouped + j);
         g.job = point_job<kMulti>(a.q, (int64_t)g.p.row - a.q.row_base);
         const LearnedJob& J = job_desc<kMulti>(a, g.job);
         const uint32_t c = g.p.gcell - J.cell_base;
