@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define VSJOIN_ABI_VERSION 1
+#define VSJOIN_ABI_VERSION 2
 
 enum vs_status {
     VS_OK = 0,
@@ -111,7 +111,8 @@ typedef struct vs_join_stats {
     int64_t candidates;       /* point/polygon pairs that passed the box filter */
     int64_t exact_fallbacks;  /* orientation signs that needed the exact expansion stage */
     int64_t fp32_edges;       /* edges decided by the FP32 tile-relative filter */
-    int64_t fp64_edges;       /* edges re-decided in FP64 because the FP32 bound was inconclusive */
+    int64_t fp64_edges;       /* edges the FP32 bound left inconclusive: their pairs go to the FP64 / exact
+                                 pass (the R-tree method: 0) */
     int64_t rmi_fallbacks;    /* learned-index lookups whose error window exceeded 256 cells (binary search) */
     float kernel_ms;          /* device time of the join kernels */
     float sort_ms;            /* device time of the optional pair sort */
@@ -135,6 +136,7 @@ typedef struct vs_index_info {
     int32_t rmi_max_window;
     int64_t n_binned_rings;   /* rings with y-bins */
     int64_t n_bin_edges;      /* (bin, edge) entries */
+    int32_t rmi_leaves;       /* learned-index leaf models (0 without the learned part) */
 } vs_index_info;
 
 /* ---------------------------------------------------------------------- */

@@ -29,7 +29,7 @@ def test_binding_covers_header():
 
     assert sorted(_abi.EXPORTED) == header_symbols()
     L = _abi.load()
-    assert L.vs_version() == 1
+    assert L.vs_version() == 2
     assert L.vs_last_error() is not None
 
 

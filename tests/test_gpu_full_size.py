@@ -50,10 +50,12 @@ def degenerate(vsabi, ctx, oracle):
 
 def test_degenerate_cell_level_is_refined(degenerate):
     """The multipolygons' wide boxes pull the mean box side up (level 7 from it, 35 entries per cell); the automatic
-    level is refined while cells hold more than 2.5 entries on average, within the registration budget."""
+    level is refined while an entry's cell holds more than 2.5 entries on average, within the registration budget
+    (level 10 would exceed it).  260k cell keys keep the default 4096 RMI leaves."""
     info = degenerate.index.info()
     assert info["cell_level"] >= 8
     assert info["n_cell_entries"] / info["n_cells"] < 12.0
+    assert info["rmi_leaves"] == 4096
 
 
 @pytest.mark.parametrize("method", ["rtree", "learned"])
@@ -162,6 +164,16 @@ def zipf(vsabi, ctx, oracle):
     index = vsabi.DeviceIndex(ctx, P, learned=True)
     exp = oracle.join(w.px, w.py, None, oracle_polys(oracle, w.polys), "within")
     return SimpleNamespace(w=w, index=index, pts=pts, exp=exp, keep=(keep_p, keep_q))
+
+
+def test_zipf_cell_level_follows_the_dense_cells(zipf):
+    """Zipf's clusters: the plain mean is 1.55 entries per cell at level 12, but an entry's cell holds 3.3 on
+    average, so the automatic level goes to 13 (2.4); its 5.5M cell keys get one RMI leaf per 64 keys, capped at
+    65535, which keeps the error windows a few dozen keys wide (432 with 4096 leaves)."""
+    info = zipf.index.info()
+    assert info["cell_level"] == 13
+    assert info["rmi_leaves"] == 65535
+    assert info["rmi_mean_window"] < 60
 
 
 @pytest.mark.parametrize("method", ["rtree", "learned"])

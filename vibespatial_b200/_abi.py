@@ -122,6 +122,7 @@ class IndexInfo(ctypes.Structure):
         ("build_ms", ctypes.c_float), ("rmi_train_ms", ctypes.c_float),
         ("rmi_mean_window", ctypes.c_float), ("rmi_max_window", ctypes.c_int32),
         ("n_binned_rings", ctypes.c_int64), ("n_bin_edges", ctypes.c_int64),
+        ("rmi_leaves", ctypes.c_int32),
     ]
 
     def as_dict(self):

@@ -236,6 +236,7 @@ int vs_index_info_get(const vs_index* idx, vs_index_info* info) {
     info->rmi_max_window = idx->learned.max_window;
     info->n_binned_rings = idx->n_binned_rings;
     info->n_bin_edges = idx->n_bin_edges;
+    info->rmi_leaves = idx->has_learned ? idx->learned.n_leaves : 0;
     return VS_OK;
 }
 
