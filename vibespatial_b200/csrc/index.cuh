@@ -187,7 +187,7 @@ struct vs_index {
     vs::RingBins* ring_bins = nullptr;  // [n_binned_rings]
     uint16_t* bin_edges = nullptr;      // [n_bin_edges]
     int64_t n_binned_rings = 0, n_bin_edges = 0;
-    int64_t n_split_binned_rings = 0;   // binned rings of >= kSplitBinMinVertices vertices
+    int64_t n_split_binned_rings = 0;   // binned rings the split walk takes binned (kSplitBinMin*)
     vs::RingIndex ring_index() const {
         vs::RingIndex ri;
         ri.ring_bin = ring_bin;

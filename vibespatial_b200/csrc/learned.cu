@@ -295,20 +295,26 @@ __global__ void interior_box_kernel(const vs_box* __restrict__ boxes, int64_t M,
 }
 
 // Coordinate range of every single-ring slot: such polygons take the short
-// ring walk (c0 >= 0) unless the split walk would use the ring's y-bins.
+// ring walk (c0 >= 0) unless the split walk uses the ring's y-bins (from
+// kSplitBinMinSingleRing vertices).  n_extra counts the rings this walks
+// binned below kSplitBinMinVertices, which the index's count of rings for
+// the binned walk does not hold yet.
 __global__ void slot_c01_kernel(int64_t M, const int32_t* __restrict__ geom_off, const int32_t* __restrict__ part_off,
                                 const int32_t* __restrict__ ring_off, const int32_t* __restrict__ ring_bin,
-                                int2* __restrict__ out) {
+                                int2* __restrict__ out, unsigned* __restrict__ n_extra) {
+    unsigned extra = 0;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M; s += (int64_t)gridDim.x * blockDim.x) {
         int2 r = make_int2(-1, -1);
         const int32_t p0 = geom_off[s], p1 = geom_off[s + 1];
         if (p1 - p0 == 1 && part_off[p0 + 1] - part_off[p0] == 1) {
             const int ring = part_off[p0];
             const int c0 = ring_off[ring], c1 = ring_off[ring + 1];
-            if (ring_bin == nullptr || ring_bin[ring] < 0 || c1 - c0 < kSplitBinMinVertices) r = make_int2(c0, c1);
+            if (ring_bin == nullptr || ring_bin[ring] < 0 || c1 - c0 < kSplitBinMinSingleRing) r = make_int2(c0, c1);
+            else if (c1 - c0 < kSplitBinMinVertices) ++extra;
         }
         out[s] = r;
     }
+    if (extra) atomicAdd(n_extra, extra);
 }
 
 // One record per (cell, polygon) entry, in cell order, relative to the cell's
@@ -928,8 +934,11 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     split_copy_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
                                                             idx->xy, li.origin, li.err32, li.xy32);
     VS_CUDA_TRY(cudaGetLastError());
+    Scratch<unsigned> n_extra;
+    VS_TRY(n_extra.alloc(1, s));
+    VS_CUDA_TRY(cudaMemsetAsync(n_extra.p, 0, sizeof(unsigned), s));
     slot_c01_kernel<<<grid_for(M, 256), 256, 0, s>>>(M, idx->geom_off, idx->part_off, idx->ring_off, idx->ring_bin,
-                                                     li.c01);
+                                                     li.c01, n_extra.p);
     VS_CUDA_TRY(cudaGetLastError());
     interior_box_kernel<<<grid_for(M * 32, 256), 256, 0, s>>>(boxes, M, idx->geom_off, idx->part_off, idx->ring_off,
                                                               idx->xy, idx->ring_index(), li.origin, li.ib32);
@@ -945,10 +954,12 @@ int build_learned_index(vs_context* ctx, vs_index* idx, const vs_index_options* 
     entry_recs_kernel<<<grid_for(E, 256), 256, 0, s>>>((int64_t)E, keys.p, li.entries, li.desc, boxes, li.origin,
                                                        li.err32, li.ib32, li.recs, bad.p);
     VS_CUDA_TRY(cudaGetLastError());
-    unsigned h_bad = 0;
+    unsigned h_bad = 0, h_extra = 0;
     VS_CUDA_TRY(cudaMemcpyAsync(&h_bad, bad.p, sizeof(h_bad), cudaMemcpyDeviceToHost, s));
+    VS_CUDA_TRY(cudaMemcpyAsync(&h_extra, n_extra.p, sizeof(h_extra), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaMemcpyAsync(&li.h_desc, li.desc, sizeof(LearnedJob), cudaMemcpyDeviceToHost, s));
     VS_CUDA_TRY(cudaStreamSynchronize(s));
+    idx->n_split_binned_rings += (int64_t)h_extra;  // single rings the split walk also takes binned
     if (h_bad) {
         set_error("learned index: a cell key did not decode to its cell");
         return VS_E_CUDA;

@@ -230,6 +230,8 @@ __device__ __forceinline__ int geometry_location_split(float qx, float qy, float
     for (int part = p0; part < p1; ++part) {
         bool inside = false;
         const int r0 = J.part_off[part], r1 = J.part_off[part + 1];
+        // the only ring of a polygon is walked binned from fewer vertices than a ring beside holes or parts
+        const int bin_min = (p1 - p0 == 1 && r1 - r0 == 1) ? kSplitBinMinSingleRing : kSplitBinMinVertices;
         for (int ring = r0; ring < r1; ++ring) {
             // A ring whose box lies strictly beyond the point (by more than t) neither holds it nor crosses its
             // +x ray an odd number of times: the walk of it would change nothing.
@@ -239,7 +241,7 @@ __device__ __forceinline__ int geometry_location_split(float qx, float qy, float
                 continue;
             const int c0 = J.ring_off[ring], c1 = J.ring_off[ring + 1];
             // the FP32 walk is cheap per edge, so bins pay off only on longer rings than for the FP64 walk
-            const int rb = (kBins && J.rings.ring_bin && c1 - c0 >= kSplitBinMinVertices) ? J.rings.ring_bin[ring] : -1;
+            const int rb = (kBins && J.rings.ring_bin && c1 - c0 >= bin_min) ? J.rings.ring_bin[ring] : -1;
             const int k = rb >= 0 ? ring_location_split_binned(qx, qy, t, J.xy32, c0, c1, J.rings.bins[rb],
                                                                J.rings.edges, P, n32, n64)
                                   : ring_location_split(qx, qy, t, J.xy32, c0, c1, n32, n64);

@@ -15,9 +15,12 @@ namespace vs {
 constexpr int kRingBins = 8;
 constexpr int kRingBinMinVertices = 16;  // default: rings with at least this many vertices are binned
 // The FP32 split walk is cheap per edge, so it uses a ring's bins only from
-// this length on (measured: 16-17-vertex rings with holes were slower
-// binned, 20-64-vertex stars faster).
-constexpr int kSplitBinMinVertices = 20;
+// these lengths on.  Measured: the only ring of a polygon (16-64-vertex
+// stars) was faster binned from 16 vertices (256-job batch 17.4 -> 16.8 ms);
+// a ring of a polygon with holes or several parts was slower binned at 16-17
+// vertices (degenerate refine 8.8 -> 9.2 ms) and faster from 20.
+constexpr int kSplitBinMinVertices = 20;    // a ring of a polygon with holes or several parts
+constexpr int kSplitBinMinSingleRing = 16;  // the only ring of a polygon
 
 struct __align__(16) RingBins {
     double y0;     // the ring's minimum y
