@@ -138,7 +138,7 @@ struct DistArgs {
     const double* dist_pt;    // dwithin: per point row (nullable)
     const double* dist_geom;  // dwithin: per polygon row (nullable)
     double dist_scalar;       // dwithin: the distance, or the largest per-polygon one
-    double radius;            // nearest, min pass: this round's radius
+    double radius;            // nearest, min pass: the search radius of this pass
     double* best;             // nearest: per point row minimum distance
     PairSink sink;
     unsigned long long* counters;
