@@ -180,16 +180,30 @@ def learned_ablations(_abi, ctx, indexes, pts, job_start, pred, left, right, n_p
     return out
 
 
+def workload_desc(args, name) -> str:
+    """The workload's description; a --scale other than 1 is named in it (the sizes then differ from the text)."""
+    scale = getattr(args, "scale", 1.0)
+    return WORKLOAD_DESC[name] + (f" (scaled by {scale:g})" if scale != 1.0 else "")
+
+
 def join_config(args, w) -> dict:
     """The workload's configuration, identical in both arms (arm-specific figures live outside it)."""
-    return {"workload": WORKLOAD_DESC[args.workload], "predicate": args.predicate, "n_points_per_gpu": w.n_points,
+    return {"workload": workload_desc(args, args.workload), "predicate": args.predicate, "n_points_per_gpu": w.n_points,
             "n_polygons": len(w.polys), "l2": "inputs larger than L2 (126 MB); no flush"}
 
 
 def batched_config(args, jobs) -> dict:
-    return {"workload": WORKLOAD_DESC["batched"], "predicate": args.predicate, "n_jobs": len(jobs),
+    return {"workload": workload_desc(args, "batched"), "predicate": args.predicate, "n_jobs": len(jobs),
             "n_points_per_gpu": int(sum(w.n_points for w in jobs)), "n_polygons": int(sum(len(w.polys) for w in jobs)),
             "l2": "inputs larger than L2 (126 MB); no flush"}
+
+
+def every(stride, what) -> str:
+    """'every point', 'every 2nd point', 'every 13th point'."""
+    if stride <= 1:
+        return f"every {what}"
+    suffix = "th" if 10 <= stride % 100 <= 20 else {1: "st", 2: "nd", 3: "rd"}.get(stride % 10, "th")
+    return f"every {stride}{suffix} {what}"
 
 
 def shapely_importable() -> bool:
@@ -291,7 +305,7 @@ def run_reference_batched(args, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": batched_config(args, jobs),
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
-                         "sample": f"every {stride}th job ({len(sample)} of {len(jobs)} jobs, {n} points), exact CPU "
+                         "sample": f"{every(stride, 'job')} ({len(sample)} of {len(jobs)} jobs, {n} points), exact CPU "
                                    "oracle (C + OpenMP): Shapely/GEOS is not installable here",
                          "shapely_importable": shapely_importable()},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -353,7 +367,7 @@ def run_reference_wkb(args, world):
         "impl": "reference", "metric": "WKB geometries decoded/sec", "value": value, "unit": "geometries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["wkb"], "rows": rows},
+        "config": {"workload": workload_desc(args, "wkb"), "rows": rows},
         "cpu_baseline": {"value": value, "unit": "geometries/s", "cores": threads, "kind": "port",
                          "sample": "both whole columns each step, CPU WKB decoder (oracle/wkb.c, C + OpenMP) "
                                    "restating the reference's staged host decode"},
@@ -465,7 +479,7 @@ def run_wkb(args, rank, world, local_rank):
         "metric": "WKB geometries decoded/sec", "value": value, "unit": "geometries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["wkb"], "rows": rows, "wkb_bytes": data_bytes,
+        "config": {"workload": workload_desc(args, "wkb"), "rows": rows, "wkb_bytes": data_bytes,
                    "sizes": sizes, "parallelism": f"columns per GPU ({world} GPU(s)), independent",
                    "l2": "inputs (1.5 GB of WKB + offsets) larger than L2; no flush",
                    "api": "_abi.wkb_decode per column (plan with one host sync for the sizes, output "
@@ -538,7 +552,7 @@ def run_reference_distance(args, world):
         "impl": "reference", "metric": "query points/sec", "value": value, "unit": "points/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "sample_points": n, "n_polygons": len(w.polys)},
+        "config": {"workload": workload_desc(args, args.workload), "sample_points": n, "n_polygons": len(w.polys)},
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
                          "sample": f"first {n} of {w.n_points} points vs all {len(w.polys)} polygons, CPU oracle "
                                    "(C + OpenMP, grid index, same distance arithmetic); Shapely/GEOS is not "
@@ -663,7 +677,7 @@ def run_distance(args, rank, world, local_rank):
         "metric": "query points/sec", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC[args.workload], "method": "rtree (distance walk)",
+        "config": {"workload": workload_desc(args, args.workload), "method": "rtree (distance walk)",
                    "n_points_per_gpu": N, "n_polygons": len(w.polys), "n_pairs": n_pairs,
                    "distance": None if nearest else DWITHIN_DISTANCE,
                    "parallelism": f"points sharded over {world} GPU(s), index replicated",
@@ -714,7 +728,7 @@ def run_reference_export(args, world):
         "impl": "reference", "metric": "join export rows/sec", "value": value, "unit": "rows/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["export"], "n_pairs": int(len(hl)), "n_rows": n_rows},
+        "config": {"workload": workload_desc(args, "export"), "n_pairs": int(len(hl)), "n_rows": n_rows},
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": 1, "kind": "port",
                          "sample": "the whole export each step: numpy restatement of the reference's host "
                                    "_adjust_join_indexers + attribute filter"},
@@ -814,7 +828,7 @@ def run_export(args, rank, world, local_rank):
         "metric": "join export rows/sec", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["export"], "n_pairs": n_pairs, "n_left": n_left, "n_right": n_right,
+        "config": {"workload": workload_desc(args, "export"), "n_pairs": n_pairs, "n_left": n_left, "n_right": n_right,
                    "n_rows": n_rows, "how": "left", "l2": "inputs (~0.6 GB) larger than L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind, "kernel_ms": kmed, "algorithmic_bytes_per_launch": B},
@@ -853,7 +867,7 @@ def run_reference_nearest_polygons(args, world):
         "impl": "reference", "metric": "query polygons/sec", "value": value, "unit": "polygons/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["nearest_polygons"], "sample_polygons": k, "n_points": w.n_points},
+        "config": {"workload": workload_desc(args, "nearest_polygons"), "sample_polygons": k, "n_points": w.n_points},
         "cpu_baseline": {"value": value, "unit": "polygons/s", "cores": threads, "kind": "port",
                          "sample": f"the first {k} polygons against all {w.n_points} points each step, CPU oracle "
                                    "(C + OpenMP); Shapely/GEOS is not installable here"},
@@ -926,7 +940,7 @@ def run_nearest_polygons(args, rank, world, local_rank):
         "metric": "query polygons/sec", "value": value, "unit": "polygons/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC["nearest_polygons"], "n_polygons": M, "n_points": w.n_points,
+        "config": {"workload": workload_desc(args, "nearest_polygons"), "n_polygons": M, "n_points": w.n_points,
                    "n_pairs": n_pairs, "point_index_build_wall_s": build_wall,
                    "l2": "inputs (800 MB of points, index 1.6 GB) larger than L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -985,7 +999,7 @@ def run_reference(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": join_config(args, w),
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
-                         "sample": f"every {stride}th point ({n} of {w.n_points}) vs all {len(w.polys)} polygons, "
+                         "sample": f"{every(stride, 'point')} ({n} of {w.n_points}) vs all {len(w.polys)} polygons, "
                                    "exact CPU oracle (C + OpenMP): Shapely/GEOS is not installable here",
                          "shapely_importable": shapely_importable()},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
